@@ -1,0 +1,333 @@
+"""Benchmark: incoherent closest-hit Mrays/s on the 21M-triangle OBVH workload.
+
+Workload (one "step" = one batch through the hot path): 1,024 level-5 icospheres
+plus a ground quad (20,971,522 triangles), built as SORT's OBVH (width 8,
+max depth 16, leaf 8); 4,194,304 cosine-weighted diffuse rays spawned from the
+hits of a 2048x2048 pinhole camera, traced closest-hit in one launch.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+ours: every rank holds a replica of the tree and traces its own 4M-ray batch
+(weak scaling, no collective on the data path). value = all ranks' rays / the
+slowest rank's device time. e2e = the same batch through the host-buffer C-ABI
+call (pinned host rays in, hits out, copies inside the timed region).
+reference: SORT's own OBVH code (compiled from its sources into oracle/_ref)
+on the host cores, on a bounded sample of the same rays each step; rank 0 only.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "Mrays/s incoherent closest-hit"
+UNIT = "Mrays/s"
+SPHERES, LEVEL, IMAGE = 1024, 5, 2048
+WIDTH, DEPTH, LEAF = 8, 16, 8
+NODE_BYTES = {4: 112, 8: 224}   # FP32 canonical wide node: W*24 B boxes + W*4 B refs
+TRI_BYTES = 36                  # 9 floats per triangle test
+RAY_IN, HIT_OUT = 32, 16
+CPU_SAMPLE = 262_144            # rays per CPU-baseline step
+
+
+def workload_config(extra=None):
+    cfg = {
+        "workload": "incoherent_21m: 1,024 level-5 icospheres + ground quad = 20,971,522 triangles, "
+                    "OBVH (width 8, depth 16, leaf 8), 4,194,304 cosine-diffuse closest-hit rays per GPU "
+                    "from 2048x2048 primary hits",
+        "scene_seed": 1,
+        "nodes": "fp32",
+        "l2": "inputs larger than L2: 1.25 GB tree + 128 MB rays per launch (no flush)",
+    }
+    if extra:
+        cfg.update(extra)
+    return cfg
+
+
+class ClockSampler:
+    """nvidia-smi clocks / throttle reasons sampled every 200 ms while running."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index: int):
+        self.index = index
+        self.rows = []
+        self.proc = None
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.index), f"--query-gpu={self.FIELDS}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            threading.Thread(target=self._read, daemon=True).start()
+        except OSError:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) >= 9:
+                self.rows.append(parts)
+
+    def __exit__(self, *exc):
+        if self.proc:
+            time.sleep(0.25)
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self):
+        if not self.rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        sm = [float(r[1]) for r in self.rows if r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in self.rows if r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[k] for r in self.rows for k in range(4) if r[5 + k].lower() == "active"})
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(self.rows)}
+
+
+def make_rays(acc, tri, rank: int, device):
+    """Primary camera rays traced on the GPU, then the diffuse + shadow batches."""
+    import torch
+
+    from sort_b200 import scenes
+    cam = scenes.camera_rays(IMAGE, IMAGE, seed=7)
+    h = acc.GetIntersect(torch.from_numpy(cam).to(device))
+    prim = h.prim.cpu().numpy()
+    t = h.t.cpu().numpy()
+    diffuse, shadow = scenes.bounce_rays(tri, cam, prim, t, IMAGE * IMAGE, seed=11 + rank)
+    return diffuse, shadow
+
+
+def reference_cpu(tri, rays, steps: int, warmup: int, threads: int, sample: int):
+    """SORT's OBVH on the host cores; returns (Mrays/s, description)."""
+    from oracle.oracle import Reference, reference_available
+    if not reference_available():
+        from oracle.oracle import Port
+        impl, kind = Port(), "port"
+    else:
+        impl, kind = Reference(), "reference"
+    tree = impl.build(tri, WIDTH, DEPTH, LEAF)
+    n = rays.shape[1]
+    times = []
+    for k in range(warmup + steps):
+        s = (k * sample) % max(1, n - sample)
+        block = np.ascontiguousarray(rays[:, s:s + sample])
+        t0 = time.perf_counter()
+        tree.closest(block, threads)
+        dt = time.perf_counter() - t0
+        if k >= warmup:
+            times.append(dt)
+    rate = sample * len(times) / sum(times) / 1e6
+    return rate, kind, f"{sample} of the {n} diffuse rays per step, {len(times)} timed steps"
+
+
+def run_reference(args):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    from sort_b200 import scenes
+    from oracle.oracle import Reference, reference_available
+    tri = scenes.sphere_field(SPHERES, LEVEL, seed=1)
+    if not reference_available():
+        print(json.dumps({"impl": "reference", "unavailable": "SORT reference library (oracle/_ref) not built"}))
+        return
+    ref = Reference()
+    threads = ref.hardware_threads()
+    tree = ref.build(tri, WIDTH, DEPTH, LEAF)
+    cam = scenes.camera_rays(IMAGE, IMAGE, seed=7)
+    prim, t, _, _ = tree.closest(cam, threads)
+    diffuse, _ = scenes.bounce_rays(tri, cam, prim, t, IMAGE * IMAGE, seed=11)
+    n = diffuse.shape[1]
+    sample = args.sample
+    times = []
+    for k in range(args.warmup + args.steps):
+        s = (k * sample) % max(1, n - sample)
+        block = np.ascontiguousarray(diffuse[:, s:s + sample])
+        t0 = time.perf_counter()
+        tree.closest(block, threads)
+        dt = time.perf_counter() - t0
+        if k >= args.warmup:
+            times.append(dt)
+    total = sum(times)
+    value = sample * len(times) / total / 1e6
+    out = {
+        "impl": "reference", "metric": METRIC, "value": round(value, 3), "unit": UNIT, "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(1e3 * total / len(times), 3),
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": workload_config({"sample_rays_per_step": sample}),
+        "cpu_baseline": {"value": round(value, 3), "unit": UNIT, "cores": threads, "kind": "reference",
+                         "sample": f"{sample} of the {n} diffuse rays per step (SORT Obvh::GetIntersect, AVX)"},
+        "e2e": {"value": round(value, 3), "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        "gpu_launches": 0,
+    }
+    print(json.dumps(out))
+
+
+def run_ours(args):
+    import torch
+    import torch.distributed as dist
+
+    from sort_b200 import Hits, Obvh, scenes
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    device = torch.device("cuda", local)
+    if world > 1:
+        import datetime
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600), device_id=device)
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+
+    tri = scenes.sphere_field(SPHERES, LEVEL, seed=1)
+    acc = Obvh(DEPTH, LEAF, device=local)
+    acc.Build(tri)
+    info = acc.info()
+    diffuse, shadow = make_rays(acc, tri, rank, device)
+    n = diffuse.shape[1]
+    d_diff = torch.from_numpy(diffuse).to(device)
+    d_shad = torch.from_numpy(shadow).to(device)
+
+    # SORT's traversal counters on these rays -> algorithmic bytes per ray.
+    node_tests, prim_tests = acc.TraceStats(d_diff, False)
+    a_nodes, a_prims = acc.TraceStats(d_shad, True)
+    bytes_closest = RAY_IN + HIT_OUT + (node_tests * NODE_BYTES[WIDTH] + prim_tests * TRI_BYTES) / n
+    bytes_any = RAY_IN + 4 + (a_nodes * NODE_BYTES[WIDTH] + a_prims * TRI_BYTES) / n
+
+    stream = torch.cuda.current_stream(device)
+    for _ in range(args.warmup):
+        acc.GetIntersect(d_diff)
+    torch.cuda.synchronize(device)
+    barrier()
+    torch.cuda.synchronize(device)
+    start, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with ClockSampler(local) as clocks:
+        start.record(stream)
+        for _ in range(args.steps):
+            acc.GetIntersect(d_diff)
+        end.record(stream)
+        torch.cuda.synchronize(device)
+    barrier()
+    torch.cuda.synchronize(device)
+    ms = start.elapsed_time(end)
+    t_max = torch.tensor([ms], device=device)
+    if world > 1:
+        dist.all_reduce(t_max, op=dist.ReduceOp.MAX)
+    ms_max = float(t_max.item())
+    value = world * n * args.steps / (ms_max / 1e3) / 1e6
+    launch_ms = ms / args.steps
+
+    # any-hit (shadow) launch, timed the same way
+    for _ in range(args.warmup):
+        acc.GetAttenuation(d_shad)
+    torch.cuda.synchronize(device)
+    s2, e2 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    s2.record(stream)
+    for _ in range(args.steps):
+        acc.GetAttenuation(d_shad)
+    e2.record(stream)
+    torch.cuda.synchronize(device)
+    any_ms = s2.elapsed_time(e2) / args.steps
+
+    # end to end through the host-buffer C-ABI call, pinned host memory
+    h_rays = torch.from_numpy(diffuse).pin_memory()
+    outs = Hits(torch.empty(n, dtype=torch.int32).pin_memory().numpy(),
+                torch.empty(n, dtype=torch.float32).pin_memory().numpy(),
+                torch.empty(n, dtype=torch.float32).pin_memory().numpy(),
+                torch.empty(n, dtype=torch.float32).pin_memory().numpy())
+    h_np = h_rays.numpy()
+    for _ in range(max(1, args.warmup)):
+        acc.GetIntersect(h_np, out=outs)
+    barrier()
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        acc.GetIntersect(h_np, out=outs)
+    e2e_s = time.perf_counter() - t0
+    t_e2e = torch.tensor([e2e_s], device=device)
+    if world > 1:
+        dist.all_reduce(t_e2e, op=dist.ReduceOp.MAX)
+    e2e_value = world * n * args.steps / float(t_e2e.item()) / 1e6
+
+    peaks_path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(peaks_path):
+        peak, peak_src = float(json.load(open(peaks_path))["hbm_gbs"]), "measured"
+    else:
+        peak, peak_src = 6650.0, "fallback"
+    achieved = bytes_closest * n / (launch_ms / 1e3) / 1e9
+    traffic = None
+    tpath = os.path.join(ROOT, "profiles", "traffic.json")
+    if os.path.exists(tpath):
+        tj = json.load(open(tpath))
+        if tj.get("workload") == "incoherent_21m" and tj.get("nodes") == "fp32":
+            traffic = tj.get("dram_bytes_per_launch")
+
+    if rank == 0:
+        out = {
+            "metric": METRIC, "value": round(value, 3), "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": round(ms_max / args.steps, 4), "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded procedural scene)",
+            "config": workload_config({"parallelism": f"replicas x{world}", "build_seconds": round(info["build_seconds"], 2),
+                                       "tree_device_bytes": info["device_bytes"]}),
+            "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
+                         "frac": round(achieved / peak, 4), "traffic": traffic,
+                         "peak_source": f"{peak_src} hbm_gbs (burst)",
+                         "algorithmic_bytes_per_ray": round(bytes_closest, 1),
+                         "node_tests_per_ray": round(node_tests / n, 3), "prim_tests_per_ray": round(prim_tests / n, 3),
+                         "kernel": "k_trace_fp32<8,false,128,false>", "launch_ms": round(launch_ms, 4)},
+            "anyhit": {"mrays_s": round(n / (any_ms / 1e3) / 1e6, 3), "launch_ms": round(any_ms, 4),
+                       "algorithmic_bytes_per_ray": round(bytes_any, 1),
+                       "achieved_gbs": round(bytes_any * n / (any_ms / 1e3) / 1e9, 1)},
+            "e2e": {"value": round(e2e_value, 3), "unit": UNIT, "h2d_bytes_per_step": int(n * 32),
+                    "d2h_bytes_per_step": int(n * 16)},
+            "clocks": clocks.summary(),
+            "gpu_launches": args.steps,
+        }
+        if world == 1 and not args.no_cpu_baseline:
+            threads = os.cpu_count() or 1
+            rate, kind, desc = reference_cpu(tri, diffuse, steps=3, warmup=1, threads=threads, sample=args.sample)
+            out["cpu_baseline"] = {"value": round(rate, 3), "unit": UNIT, "cores": threads, "kind": kind,
+                                   "sample": desc}
+        print(json.dumps(out))
+    acc.Release()
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+def main():
+    p = argparse.ArgumentParser()
+    p.add_argument("--gpus", type=int, default=1)
+    p.add_argument("--steps", type=int, default=10)
+    p.add_argument("--warmup", type=int, default=3)
+    p.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    p.add_argument("--sample", type=int, default=CPU_SAMPLE)
+    p.add_argument("--no-cpu-baseline", action="store_true")
+    args = p.parse_args()
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_ours(args)
+
+
+if __name__ == "__main__":
+    main()

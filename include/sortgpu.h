@@ -1,0 +1,152 @@
+/* sortgpu: B200-native ray-query engine behind SORT's Accelerator API.
+ *
+ * C ABI of libsortgpu.so. Plain pointers and sizes only; every entry point
+ * returns an sg_status (SG_OK == 0) and records a message for sg_last_error().
+ *
+ * What each entry point replaces in SORT (paths relative to SORT's src/):
+ *
+ *   sg_scene_create   Accelerator::Build (accel/accelerator.h:128) as
+ *                     Fbvh::Build (accel/fast_bvh.hpp:109-136), together with the
+ *                     scene box Scene::LoadScene computes first
+ *                     (core/scene.cpp:146-154) and Fbvh::Serialize's two
+ *                     parameters (accel/fast_bvh.h:159-162).
+ *   sg_trace_closest  Accelerator::GetIntersect(RenderContext&, const Ray&,
+ *                     SurfaceInteraction&) (accel/accelerator.h:74), as called by
+ *                     Scene::GetIntersect (core/scene.cpp:182-185), for a batch.
+ *   sg_trace_any      Accelerator::GetAttenuation (accel/accelerator.h:96,
+ *                     accel/accelerator.cpp:26-69) for opaque scenes, i.e. the
+ *                     any-hit query SORT builds from GetIntersect with
+ *                     query_shadow set (accel/fast_bvh.hpp:362-373); also stands in
+ *                     for IsOccluded (accel/accelerator.h:76-86), which SORT
+ *                     compiles out under ENABLE_TRANSPARENT_SHADOW.
+ *   sg_scene_destroy  the Accelerator's destructor (Scene owns it, core/scene.h).
+ *   sg_scene_info     Fbvh's build statistics (accel/fast_bvh.hpp:50-96 counters)
+ *                     and Accelerator::GetBBox / GetIsValid (accelerator.h:133-142).
+ *   sg_scene_topology no SORT counterpart as an API; exports the tree in the
+ *                     pre-order form the tests compare against SORT's own tree.
+ *   sg_build_topology_host
+ *                     Fbvh::Build alone, on the host, without a GPU: builds the
+ *                     tree and returns the same pre-order topology stream.
+ *   sg_trace_stats    SORT's traversal statistics for a batch (accel/fast_bvh.hpp:50-96
+ *                     and accel/accelerator.cpp:21-23: sRayCount, sIntersectionTest)
+ *                     plus the interior-node box tests; runs the same traversal.
+ *   sg_trace_closest_host / sg_trace_any_host
+ *                     the same queries on host buffers, with the host<->device
+ *                     copies done inside the call (what a caller that holds rays in
+ *                     host memory, like SORT's integrators, binds).
+ *
+ * Semantics carried over from SORT:
+ *   - hit identity is the primitive's index in input order (SORT returns a
+ *     Primitive*, whose index in ScenePrimitiveIterator order this is);
+ *   - a hit needs tmin < t <= tmax and is taken only if strictly nearer than
+ *     the current one; a miss returns prim = -1 and t = FLT_MAX;
+ *   - u, v are the barycentric weights of vertex 1 and vertex 2.
+ *
+ * Rays and hits are device pointers unless the function name ends in _host.
+ * Calls are ordered on the given CUDA stream (NULL = legacy default stream) and
+ * do not synchronise it; sg_*_host calls synchronise before returning.
+ */
+#ifndef SORTGPU_H
+#define SORTGPU_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef enum {
+    SG_OK = 0,
+    SG_ERR_INVALID_ARGUMENT = 1,
+    SG_ERR_CUDA = 2,
+    SG_ERR_OUT_OF_MEMORY = 3,
+    SG_ERR_UNSUPPORTED = 4,
+    SG_ERR_LIMIT = 5,
+    SG_ERR_INTERNAL = 6
+} sg_status;
+
+/* Child-box storage of the device tree. */
+typedef enum {
+    SG_NODES_FP32 = 0,   /* FP32 child boxes: hits and visit order bit-identical to SORT */
+    SG_NODES_QUANT8 = 1  /* 8-bit child boxes relative to the parent, rounded outward */
+} sg_node_format;
+
+typedef struct {
+    int32_t width;          /* 4 = SORT's Qbvh, 8 = SORT's Obvh */
+    int32_t max_depth;      /* Fbvh::m_maxNodeDepth (SORT default 16) */
+    int32_t max_leaf;       /* Fbvh::m_maxPriInLeaf (SORT default 8) */
+    int32_t node_format;    /* sg_node_format */
+    int32_t device;         /* CUDA device ordinal the tree lives on */
+    int32_t build_threads;  /* host threads for the build, 0 = all */
+} sg_build_opts;
+
+/* Structure-of-arrays ray batch: n entries in each array. */
+typedef struct {
+    const float* ox;
+    const float* oy;
+    const float* oz;
+    const float* dx;
+    const float* dy;
+    const float* dz;
+    const float* tmin;
+    const float* tmax;
+} sg_rays;
+
+typedef struct {
+    int32_t* prim;  /* primitive index, -1 on a miss */
+    float* t;       /* FLT_MAX on a miss */
+    float* u;       /* may be NULL */
+    float* v;       /* may be NULL */
+} sg_hits;
+
+typedef struct {
+    int64_t triangles;
+    int64_t interior_nodes;
+    int64_t leaves;
+    int32_t depth;           /* Fbvh::m_depth */
+    int32_t width;
+    int32_t node_format;
+    int32_t valid;           /* Accelerator::GetIsValid */
+    float bbox[6];           /* enlarged scene box: min xyz, max xyz */
+    int64_t device_bytes;    /* HBM held by the tree (nodes + triangles) */
+    double build_seconds;    /* host build time */
+} sg_scene_info;
+
+typedef struct sg_scene sg_scene;
+
+void sg_default_build_opts(sg_build_opts* opts);
+
+sg_status sg_scene_create(const float* triangles, int64_t ntri, const sg_build_opts* opts, sg_scene** out);
+sg_status sg_scene_destroy(sg_scene* scene);
+sg_status sg_scene_info_get(const sg_scene* scene, sg_scene_info* info);
+sg_status sg_scene_topology(const sg_scene* scene, int32_t* out, int64_t cap, int64_t* written);
+/* Topology stream: interior node [child_cnt, children...], leaf [0, count,
+ * primitive indices in leaf order]; pre-order from the root. Call with
+ * out = NULL / cap = 0 to learn the size (returns SG_ERR_LIMIT and sets written). */
+sg_status sg_build_topology_host(const float* triangles, int64_t ntri, const sg_build_opts* opts, int32_t* out,
+                                 int64_t cap, int64_t* written, int32_t* depth);
+
+sg_status sg_trace_closest(const sg_scene* scene, const sg_rays* rays, int64_t n, const sg_hits* hits, void* stream);
+sg_status sg_trace_any(const sg_scene* scene, const sg_rays* rays, int64_t n, uint8_t* occluded, void* stream);
+
+/* Counts over one batch (synchronises the stream): interior nodes box-tested and
+ * primitives tested, the latter counted per leaf entered as SORT's
+ * sIntersectionTest does. any = 0 closest-hit traversal, 1 any-hit traversal. */
+sg_status sg_trace_stats(const sg_scene* scene, const sg_rays* rays, int64_t n, int32_t any, int64_t* node_tests,
+                         int64_t* prim_tests, void* stream);
+
+/* Host-buffer forms. rays8 is one block of 8*n floats: ox[n], oy[n], oz[n],
+ * dx[n], dy[n], dz[n], tmin[n], tmax[n]. */
+sg_status sg_trace_closest_host(const sg_scene* scene, const float* rays8, int64_t n, int32_t* prim, float* t,
+                                float* u, float* v);
+sg_status sg_trace_any_host(const sg_scene* scene, const float* rays8, int64_t n, uint8_t* occluded);
+
+const char* sg_last_error(void);
+const char* sg_version(void);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* SORTGPU_H */

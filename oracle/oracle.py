@@ -1,0 +1,152 @@
+"""ctypes loaders for the two CPU oracles (TEST INFRASTRUCTURE ONLY).
+
+* ``Port``      -- the C restatement in oracle/port (built into oracle/_build).
+* ``Reference`` -- SORT's own sources compiled with the harness in oracle/ref
+                   (built into oracle/_ref; needs the reference tree to build).
+
+Only tests/, __graft_entry__.smoke() and bench.py's CPU-baseline leg use these.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+import subprocess
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+PORT_LIB = os.path.join(HERE, "_build", "liboracle.so")
+REF_LIB = os.path.join(HERE, "_ref", "libsortref.so")
+_vp = ctypes.c_void_p
+_i64 = ctypes.c_int64
+
+
+def build_port() -> str:
+    """Compile the restated oracle if needed (gcc only; no reference tree needed)."""
+    src = [os.path.join(HERE, "port", f) for f in ("oracle.c", "oracle.h")]
+    if not os.path.exists(PORT_LIB) or any(os.path.getmtime(s) > os.path.getmtime(PORT_LIB) for s in src):
+        subprocess.run(["make", "-C", HERE, "port"], check=True, capture_output=True)
+    return PORT_LIB
+
+
+def reference_available() -> bool:
+    return os.path.exists(REF_LIB)
+
+
+class _Tree:
+    def __init__(self, api, handle, width, ntri):
+        self.api, self.h, self.width, self.ntri = api, handle, width, ntri
+
+    def __del__(self):
+        try:
+            self.api._free(self.h)
+        except Exception:
+            pass
+
+    def topology(self) -> np.ndarray:
+        need = self.api._topo(self.h, None, 0)
+        need = -need if need < 0 else need
+        out = np.empty(max(need, 1), np.int32)
+        k = self.api._topo(self.h, out.ctypes.data, out.size)
+        return out[:k]
+
+    def depth(self) -> int:
+        return int(self.api._depth(self.h))
+
+    def bbox(self) -> np.ndarray:
+        b = np.empty(6, np.float32)
+        self.api._bbox(self.h, b.ctypes.data)
+        return b
+
+    def closest(self, rays: np.ndarray, threads: int = 0):
+        r = np.ascontiguousarray(rays, np.float32)
+        n = r.shape[1]
+        prim = np.empty(n, np.int32)
+        t = np.empty(n, np.float32)
+        u = np.empty(n, np.float32)
+        v = np.empty(n, np.float32)
+        self.api._closest(self.h, r.ctypes.data, n, prim.ctypes.data, t.ctypes.data, u.ctypes.data, v.ctypes.data,
+                          threads or os.cpu_count())
+        return prim, t, u, v
+
+    def any(self, rays: np.ndarray, threads: int = 0) -> np.ndarray:
+        r = np.ascontiguousarray(rays, np.float32)
+        n = r.shape[1]
+        occ = np.empty(n, np.uint8)
+        self.api._any(self.h, r.ctypes.data, n, occ.ctypes.data, threads or os.cpu_count())
+        return occ
+
+
+class Port:
+    """The C restatement (oracle/port/oracle.c)."""
+
+    def __init__(self):
+        L = ctypes.CDLL(build_port())
+        L.orc_build.restype = _vp
+        L.orc_build.argtypes = [ctypes.c_int, _vp, _i64, ctypes.c_int, ctypes.c_int]
+        L.orc_free.argtypes = [_vp]
+        L.orc_topology.restype = _i64
+        L.orc_topology.argtypes = [_vp, _vp, _i64]
+        L.orc_depth.argtypes = [_vp]
+        L.orc_scene_bbox.argtypes = [_vp, _vp]
+        L.orc_trace_closest.argtypes = [_vp, _vp, _i64, _vp, _vp, _vp, _vp, ctypes.c_int]
+        L.orc_trace_any.argtypes = [_vp, _vp, _i64, _vp, ctypes.c_int]
+        L.orc_count.argtypes = [_vp, _vp, _i64, ctypes.c_int, ctypes.POINTER(_i64), ctypes.POINTER(_i64),
+                                ctypes.c_int]
+        L.orc_ray_prepare.argtypes = [_vp, _vp, _vp]
+        L.orc_fp64_intersect.restype = ctypes.c_double
+        L.orc_fp64_intersect.argtypes = [_vp, _i64, _vp, _i64, _i64]
+        self.L = L
+        self._free, self._topo, self._depth, self._bbox = L.orc_free, L.orc_topology, L.orc_depth, L.orc_scene_bbox
+        self._closest, self._any = L.orc_trace_closest, L.orc_trace_any
+
+    def build(self, tri: np.ndarray, width: int, max_depth: int = 16, max_leaf: int = 8) -> _Tree:
+        tri = np.ascontiguousarray(tri, np.float32).reshape(-1, 9)
+        h = self.L.orc_build(width, tri.ctypes.data, tri.shape[0], max_depth, max_leaf)
+        if not h:
+            raise ValueError("oracle build failed")
+        return _Tree(self, h, width, tri.shape[0])
+
+    def count(self, tree: _Tree, rays: np.ndarray, any_hit: bool = False, threads: int = 0):
+        r = np.ascontiguousarray(rays, np.float32)
+        a, b = _i64(0), _i64(0)
+        self.L.orc_count(tree.h, r.ctypes.data, r.shape[1], 1 if any_hit else 0, ctypes.byref(a), ctypes.byref(b),
+                         threads or os.cpu_count())
+        return a.value, b.value
+
+    def fp64_t(self, tri: np.ndarray, prim: int, rays: np.ndarray, i: int) -> float:
+        tri = np.ascontiguousarray(tri, np.float32)
+        r = np.ascontiguousarray(rays, np.float32)
+        return float(self.L.orc_fp64_intersect(tri.ctypes.data, prim, r.ctypes.data, r.shape[1], i))
+
+
+class Reference:
+    """SORT's own QBVH/OBVH compiled from its sources (oracle/_ref/libsortref.so)."""
+
+    def __init__(self):
+        if not reference_available():
+            raise FileNotFoundError(REF_LIB)
+        L = ctypes.CDLL(REF_LIB)
+        L.sortref_scene_create.restype = _vp
+        L.sortref_scene_create.argtypes = [ctypes.c_int, _vp, ctypes.c_int, ctypes.c_int, ctypes.c_int]
+        L.sortref_scene_destroy.argtypes = [_vp]
+        L.sortref_topology.restype = _i64
+        L.sortref_topology.argtypes = [_vp, _vp, _i64]
+        L.sortref_depth.argtypes = [_vp]
+        L.sortref_scene_bbox.argtypes = [_vp, _vp]
+        L.sortref_trace_closest.argtypes = [_vp, _vp, _i64, _vp, _vp, _vp, _vp, ctypes.c_int]
+        L.sortref_trace_any.argtypes = [_vp, _vp, _i64, _vp, ctypes.c_int]
+        L.sortref_ray_prepare.argtypes = [_vp, _vp, _vp]
+        self.L = L
+        self._free, self._topo, self._depth = L.sortref_scene_destroy, L.sortref_topology, L.sortref_depth
+        self._bbox, self._closest, self._any = L.sortref_scene_bbox, L.sortref_trace_closest, L.sortref_trace_any
+
+    def build(self, tri: np.ndarray, width: int, max_depth: int = 16, max_leaf: int = 8) -> _Tree:
+        tri = np.ascontiguousarray(tri, np.float32).reshape(-1, 9)
+        h = self.L.sortref_scene_create(width, tri.ctypes.data, tri.shape[0], max_depth, max_leaf)
+        if not h:
+            raise ValueError("reference build failed")
+        return _Tree(self, h, width, tri.shape[0])
+
+    def hardware_threads(self) -> int:
+        return int(self.L.sortref_hardware_threads())

@@ -1,0 +1,336 @@
+// Oracle harness around SORT's own accelerator code.
+//
+// TEST INFRASTRUCTURE ONLY. This file is compiled together with SORT's
+// unmodified sources (accel/qbvh.cpp, accel/obvh.cpp, shape/triangle.cpp, ...)
+// by oracle/Makefile into oracle/_ref/libsortref.so. Only the test suite, the
+// smoke check and bench.py's CPU-baseline leg load that library; the product
+// (sort_b200) never links or calls it.
+//
+// What the harness supplies, because SORT's scene loader needs the absent TSL
+// library and a .sort stream:
+//   * the Scene / ScenePrimitiveIterator members the accelerator calls
+//     (core/scene.cpp:43-80, 112-185 restated over a harness-owned triangle list,
+//     including the 0.1% scene-box enlargement of core/scene.cpp:150-154);
+//   * an opaque MaterialBase (HasTransparency() == false) so any-hit queries take
+//     SORT's opaque early exit (accel/fast_bvh.hpp:362-373);
+//   * a thread pool that calls Accelerator::GetIntersect / GetAttenuation per ray,
+//     one RenderContext per worker, as SORT's tile workers do
+//     (work/image_evaluation/image_evaluation.cpp:184-264).
+//
+// Hit identity: SORT returns a const Primitive*; the harness maps it to the
+// primitive's index in ScenePrimitiveIterator order (= input triangle order).
+// Each triangle gets its own three vertices with texture coordinates
+// (0,0), (1,0), (0,1), so SORT's interpolated SurfaceInteraction::u/v
+// (simd/simd_triangle.h:327-337) equal the barycentric coordinates exactly.
+
+#include <algorithm>
+#include <atomic>
+#include <cfloat>
+#include <cmath>
+#include <cstdint>
+#include <cstring>
+#include <memory>
+#include <queue>
+#include <string>
+#include <thread>
+#include <unordered_map>
+#include <vector>
+
+// Scene's members are private and only core/scene.cpp (not linked) touches them;
+// the harness stands in for that file, so it opens them up here.
+#define private public
+#define protected public
+#include "core/scene.h"
+#include "entity/visual.h"
+#include "material/material.h"
+#include "core/render_context.h"
+#include "math/interaction.h"
+#undef private
+#undef protected
+
+#include "harness_width.h"
+
+// ---------------------------------------------------------------------------------
+// Harness-side entity / visual / material.
+
+namespace {
+
+class OpaqueMaterial : public MaterialBase {
+public:
+    void UpdateScatteringEvent(ScatteringEvent&, RenderContext&) const override {}
+    void UpdateMediumStack(const MediumInteraction&, const SE_Interaction, MediumStack&, RenderContext&) const override {}
+    void EvaluateMediumSample(const MediumInteraction&, MediumSample&) const override {}
+    Spectrum EvaluateTransparency(const SurfaceInteraction&) const override { return 0.0f; }
+    void BuildMaterial(Tsl_Namespace::ShadingContext*) override {}
+    StringID GetUniqueID() const override { return StringID(1u); }
+    bool HasTransparency() const override { return false; }
+    bool HasSSS() const override { return false; }
+    bool HasVolumeAttached() const override { return false; }
+    float GetVolumeStep() const override { return 0.0f; }
+    unsigned int GetVolumeStepCnt() const override { return 0; }
+    void Serialize(IStreamBase&) override {}
+};
+
+OpaqueMaterial g_opaque;
+
+// A MeshVisual filled directly from a flat triangle list (one triangle per three
+// vertices), mirroring what MeshVisual::Serialize does (entity/visual.cpp:26-33).
+class HarnessVisual : public MeshVisual {
+public:
+    void Fill(const float* tri, int ntri) {
+        m_memory = std::make_unique<Mesh>();
+        m_memory->m_vertices.resize((size_t)ntri * 3);
+        m_memory->m_indices.resize((size_t)ntri);
+        for (int i = 0; i < ntri; ++i) {
+            const float* p = tri + (size_t)i * 9;
+            Point a(p[0], p[1], p[2]), b(p[3], p[4], p[5]), c(p[6], p[7], p[8]);
+            Vector n = cross(c - a, b - a);
+            const float len = n.Length();
+            n = len > 0.0f ? n / len : Vector(0.0f, 1.0f, 0.0f);
+            const Point pts[3] = {a, b, c};
+            const float uv[3][2] = {{0.0f, 0.0f}, {1.0f, 0.0f}, {0.0f, 1.0f}};
+            for (int k = 0; k < 3; ++k) {
+                MeshVertex& mv = m_memory->m_vertices[(size_t)i * 3 + k];
+                mv.m_position = pts[k];
+                mv.m_normal = n;
+                mv.m_tangent = Vector(1.0f, 0.0f, 0.0f);
+                mv.m_texCoord = Vector2f(uv[k][0], uv[k][1]);
+            }
+            MeshFaceIndex& fi = m_memory->m_indices[(size_t)i];
+            fi.m_id[0] = i * 3;
+            fi.m_id[1] = i * 3 + 1;
+            fi.m_id[2] = i * 3 + 2;
+            fi.m_mat = &g_opaque;
+        }
+        m_memory->m_hasUV = true;
+        for (const auto& mi : m_memory->m_indices) {
+            m_triangles.push_back(std::make_unique<Triangle>(this, mi));
+            m_primitives.push_back(std::make_unique<Primitive>(m_memory.get(), mi.m_mat, m_triangles.back().get()));
+        }
+    }
+};
+
+class HarnessEntity : public Entity {
+public:
+    void Serialize(IStreamBase&) override {}
+    HarnessVisual* AddVisual() {
+        auto v = std::make_unique<HarnessVisual>();
+        HarnessVisual* raw = v.get();
+        m_visuals.push_back(std::move(v));
+        return raw;
+    }
+};
+
+struct RefScene {
+    Scene scene;
+    int width = 4;
+    std::unordered_map<const Primitive*, int32_t> index_of;
+    std::vector<const Primitive*> prims;
+};
+
+}  // namespace
+
+// ---------------------------------------------------------------------------------
+// Scene members SORT's accelerator calls (restated from core/scene.cpp:43-80).
+
+ScenePrimitiveIterator::ScenePrimitiveIterator(const Scene& scene) : m_scene(scene) { Reset(); }
+
+void ScenePrimitiveIterator::Reset() {
+    m_indices[0] = 0;
+    m_indices[1] = 0;
+    m_indices[2] = -1;
+}
+
+const Primitive* ScenePrimitiveIterator::Next() {
+    int eid = m_indices[0], vid = m_indices[1], pid = m_indices[2] + 1;
+    while (eid < (int)m_scene.m_entities.size()) {
+        m_indices[0] = eid;
+        const auto entity = m_scene.m_entities[eid].get();
+        while (vid < (int)entity->m_visuals.size()) {
+            m_indices[1] = vid;
+            const auto visual = entity->m_visuals[vid].get();
+            if (pid < (int)visual->m_primitives.size()) {
+                m_indices[2] = pid;
+                return visual->m_primitives[pid].get();
+            }
+            pid = 0;
+            ++vid;
+        }
+        vid = 0;
+        ++eid;
+    }
+    m_indices[0] = eid;
+    return nullptr;
+}
+
+unsigned Scene::GetPrimitiveCount() const {
+    unsigned cnt = 0;
+    for (const auto& e : m_entities) cnt += e->GetPrimitiveCount();
+    return cnt;
+}
+
+// Symbols referenced from linked SORT objects on paths the harness never reaches.
+Spectrum EvaluateTransparency(Tsl_Namespace::ShaderInstance*, const SurfaceInteraction&) { return 0.0f; }
+
+// ---------------------------------------------------------------------------------
+// Topology export: pre-order walk of SORT's tree.
+//   interior node: [child_cnt, child0 ..., child_{n-1} ...]
+//   leaf:          [0, pri_cnt, prim indices in SIMD-lane packing order]
+
+namespace {
+
+template <class Fn>
+void parallel_chunks(int64_t n, int nthreads, Fn&& fn) {
+    if (nthreads <= 0) nthreads = (int)std::max(1u, std::thread::hardware_concurrency());
+    std::atomic<int64_t> next{0};
+    const int64_t chunk = 4096;
+    auto worker = [&]() {
+        RenderContext rc;
+        rc.Init();
+        for (;;) {
+            const int64_t s = next.fetch_add(chunk);
+            if (s >= n) break;
+            const int64_t e = std::min(n, s + chunk);
+            for (int64_t i = s; i < e; ++i) fn(rc, i);
+        }
+    };
+    std::vector<std::thread> pool;
+    for (int t = 1; t < nthreads; ++t) pool.emplace_back(worker);
+    worker();
+    for (auto& th : pool) th.join();
+}
+
+}  // namespace
+
+extern "C" {
+
+// Build SORT's QBVH (width 4) or OBVH (width 8) over ntri triangles given as
+// 9 floats each (v0, v1, v2). max_depth / max_leaf are Fbvh's m_maxNodeDepth /
+// m_maxPriInLeaf (accel/fast_bvh.h:176-181, read from the scene stream in SORT).
+void* sortref_scene_create(int width, const float* tri, int ntri, int max_depth, int max_leaf) {
+    if ((width != 4 && width != 8) || ntri < 0) return nullptr;
+    auto* rs = new RefScene();
+    rs->width = width;
+    auto entity = std::make_unique<HarnessEntity>();
+    HarnessVisual* visual = entity->AddVisual();
+    visual->Fill(tri, ntri);
+    rs->scene.m_entities.push_back(std::move(entity));
+
+    ScenePrimitiveIterator iter(rs->scene);
+    int32_t idx = 0;
+    while (auto p = iter.Next()) {
+        rs->index_of[p] = idx++;
+        rs->prims.push_back(p);
+        rs->scene.m_bbox.Union(p->GetBBox());
+    }
+    // core/scene.cpp:150-154
+    static const auto threshold = 0.001f;
+    auto delta = (rs->scene.m_bbox.m_Max - rs->scene.m_bbox.m_Min) * threshold;
+    rs->scene.m_bbox.m_Min -= delta;
+    rs->scene.m_bbox.m_Max += delta;
+
+    if (width == 4)
+        rs->scene.m_accelerator.reset(harness_make_qbvh((unsigned)max_depth, (unsigned)max_leaf));
+    else
+        rs->scene.m_accelerator.reset(harness_make_obvh((unsigned)max_depth, (unsigned)max_leaf));
+    rs->scene.m_accelerator->Build(rs->scene);
+    return rs;
+}
+
+void sortref_scene_destroy(void* h) { delete (RefScene*)h; }
+
+int sortref_is_valid(void* h) { return ((RefScene*)h)->scene.m_accelerator->GetIsValid() ? 1 : 0; }
+
+// Scene box after the 0.1% enlargement: min xyz, max xyz.
+void sortref_scene_bbox(void* h, float* out6) {
+    const BBox& b = ((RefScene*)h)->scene.m_bbox;
+    for (int k = 0; k < 3; ++k) {
+        out6[k] = b.m_Min[k];
+        out6[3 + k] = b.m_Max[k];
+    }
+}
+
+// Tree depth SORT recorded (Fbvh::m_depth).
+int sortref_depth(void* h) {
+    RefScene* rs = (RefScene*)h;
+    if (rs->width == 4) return (int)harness_qbvh_depth(rs->scene.m_accelerator.get());
+    return (int)harness_obvh_depth(rs->scene.m_accelerator.get());
+}
+
+// Pre-order topology stream (format above). Returns the number of int32 written,
+// or the required size (negated) if cap is too small.
+int64_t sortref_topology(void* h, int32_t* out, int64_t cap) {
+    RefScene* rs = (RefScene*)h;
+    std::vector<int32_t> v;
+    if (!rs->scene.m_accelerator->GetIsValid()) return 0;
+    if (rs->width == 4)
+        harness_qbvh_topology(rs->scene.m_accelerator.get(), rs->index_of, v);
+    else
+        harness_obvh_topology(rs->scene.m_accelerator.get(), rs->index_of, v);
+    if ((int64_t)v.size() > cap) return -(int64_t)v.size();
+    std::memcpy(out, v.data(), v.size() * sizeof(int32_t));
+    return (int64_t)v.size();
+}
+
+// Closest hit for n rays given SoA (ox, oy, oz, dx, dy, dz, tmin, tmax; each n
+// floats, packed one after the other). Follows Scene::GetIntersect
+// (core/scene.cpp:182-185): t is reset to FLT_MAX, then the accelerator runs.
+// Miss: prim = -1, t = FLT_MAX, u = v = 0.
+void sortref_trace_closest(void* h, const float* rays, int64_t n, int32_t* prim, float* t, float* u, float* v,
+                           int nthreads) {
+    RefScene* rs = (RefScene*)h;
+    const Accelerator* acc = rs->scene.m_accelerator.get();
+    const bool valid = acc->GetIsValid();
+    parallel_chunks(n, nthreads, [&](RenderContext& rc, int64_t i) {
+        Ray r(Point(rays[i], rays[n + i], rays[2 * n + i]), Vector(rays[3 * n + i], rays[4 * n + i], rays[5 * n + i]), 0,
+              rays[6 * n + i], rays[7 * n + i]);
+        SurfaceInteraction inter;
+        inter.t = FLT_MAX;
+        const bool hit = valid && acc->GetIntersect(rc, r, inter);
+        if (hit && inter.primitive) {
+            prim[i] = rs->index_of.at(inter.primitive);
+            t[i] = inter.t;
+            u[i] = inter.u;
+            v[i] = inter.v;
+        } else {
+            prim[i] = -1;
+            t[i] = FLT_MAX;
+            u[i] = 0.0f;
+            v[i] = 0.0f;
+        }
+    });
+}
+
+// Any-hit (shadow) query through Accelerator::GetAttenuation
+// (accel/accelerator.cpp:26-69), as Scene::GetAttenuation calls it: occluded = 1 when
+// an opaque primitive lies in (tmin, tmax].
+void sortref_trace_any(void* h, const float* rays, int64_t n, uint8_t* occluded, int nthreads) {
+    RefScene* rs = (RefScene*)h;
+    const Accelerator* acc = rs->scene.m_accelerator.get();
+    const bool valid = acc->GetIsValid();
+    parallel_chunks(n, nthreads, [&](RenderContext& rc, int64_t i) {
+        Ray r(Point(rays[i], rays[n + i], rays[2 * n + i]), Vector(rays[3 * n + i], rays[4 * n + i], rays[5 * n + i]), 0,
+              rays[6 * n + i], rays[7 * n + i]);
+        Spectrum att(1.0f);
+        bool blocked = false;
+        if (valid) blocked = acc->GetAttenuation(r, att, rc, nullptr) && att.IsBlack();
+        occluded[i] = blocked ? 1 : 0;
+    });
+}
+
+// Ray::Prepare (math/ray.h:60-69) for one direction: the major axis it picks and
+// the shear constants. Exposed so the restated oracle can be pinned on it.
+void sortref_ray_prepare(const float* d, int* local_xyz, float* scale_xyz) {
+    Ray r(Point(0.0f), Vector(d[0], d[1], d[2]));
+    r.Prepare();
+    local_xyz[0] = r.m_local_x;
+    local_xyz[1] = r.m_local_y;
+    local_xyz[2] = r.m_local_z;
+    scale_xyz[0] = r.m_scale_x;
+    scale_xyz[1] = r.m_scale_y;
+    scale_xyz[2] = r.m_scale_z;
+}
+
+int sortref_hardware_threads(void) { return (int)std::max(1u, std::thread::hardware_concurrency()); }
+
+}  // extern "C"

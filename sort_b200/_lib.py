@@ -1,0 +1,97 @@
+"""ctypes binding of libsortgpu.so (the C ABI declared in include/sortgpu.h).
+
+The library is built in-tree by ``make -C sort_b200/csrc`` (``__graft_entry__.build``).
+Loading fails loudly when it is missing: there is no CPU fallback for any query.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "_lib", "libsortgpu.so")
+
+SG_OK = 0
+SG_NODES_FP32 = 0
+SG_NODES_QUANT8 = 1
+
+STATUS_NAMES = {0: "SG_OK", 1: "SG_ERR_INVALID_ARGUMENT", 2: "SG_ERR_CUDA", 3: "SG_ERR_OUT_OF_MEMORY",
+                4: "SG_ERR_UNSUPPORTED", 5: "SG_ERR_LIMIT", 6: "SG_ERR_INTERNAL"}
+
+
+class SortGpuError(RuntimeError):
+    """A libsortgpu call returned a status other than SG_OK."""
+
+    def __init__(self, status: int, message: str):
+        super().__init__(f"{STATUS_NAMES.get(status, status)}: {message}")
+        self.status = status
+
+
+class BuildOpts(ctypes.Structure):
+    _fields_ = [("width", ctypes.c_int32), ("max_depth", ctypes.c_int32), ("max_leaf", ctypes.c_int32),
+                ("node_format", ctypes.c_int32), ("device", ctypes.c_int32), ("build_threads", ctypes.c_int32)]
+
+
+class Rays(ctypes.Structure):
+    _fields_ = [(name, ctypes.c_void_p) for name in ("ox", "oy", "oz", "dx", "dy", "dz", "tmin", "tmax")]
+
+
+class Hits(ctypes.Structure):
+    _fields_ = [("prim", ctypes.c_void_p), ("t", ctypes.c_void_p), ("u", ctypes.c_void_p), ("v", ctypes.c_void_p)]
+
+
+class SceneInfo(ctypes.Structure):
+    _fields_ = [("triangles", ctypes.c_int64), ("interior_nodes", ctypes.c_int64), ("leaves", ctypes.c_int64),
+                ("depth", ctypes.c_int32), ("width", ctypes.c_int32), ("node_format", ctypes.c_int32),
+                ("valid", ctypes.c_int32), ("bbox", ctypes.c_float * 6), ("device_bytes", ctypes.c_int64),
+                ("build_seconds", ctypes.c_double)]
+
+
+_vp = ctypes.c_void_p
+_i64 = ctypes.c_int64
+_SIGNATURES = {
+    "sg_default_build_opts": (None, [ctypes.POINTER(BuildOpts)]),
+    "sg_scene_create": (ctypes.c_int, [_vp, _i64, ctypes.POINTER(BuildOpts), ctypes.POINTER(_vp)]),
+    "sg_scene_destroy": (ctypes.c_int, [_vp]),
+    "sg_scene_info_get": (ctypes.c_int, [_vp, ctypes.POINTER(SceneInfo)]),
+    "sg_scene_topology": (ctypes.c_int, [_vp, _vp, _i64, ctypes.POINTER(_i64)]),
+    "sg_build_topology_host": (ctypes.c_int, [_vp, _i64, ctypes.POINTER(BuildOpts), _vp, _i64,
+                                              ctypes.POINTER(_i64), ctypes.POINTER(ctypes.c_int32)]),
+    "sg_trace_closest": (ctypes.c_int, [_vp, ctypes.POINTER(Rays), _i64, ctypes.POINTER(Hits), _vp]),
+    "sg_trace_any": (ctypes.c_int, [_vp, ctypes.POINTER(Rays), _i64, _vp, _vp]),
+    "sg_trace_stats": (ctypes.c_int, [_vp, ctypes.POINTER(Rays), _i64, ctypes.c_int32, ctypes.POINTER(_i64),
+                                      ctypes.POINTER(_i64), _vp]),
+    "sg_trace_closest_host": (ctypes.c_int, [_vp, _vp, _i64, _vp, _vp, _vp, _vp]),
+    "sg_trace_any_host": (ctypes.c_int, [_vp, _vp, _i64, _vp]),
+    "sg_last_error": (ctypes.c_char_p, []),
+    "sg_version": (ctypes.c_char_p, []),
+}
+
+_lib = None
+
+
+def load() -> ctypes.CDLL:
+    """Load libsortgpu.so once; raises if it has not been built."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(LIB_PATH):
+        raise RuntimeError(f"{LIB_PATH} is missing: build it with `make -C sort_b200/csrc` "
+                           "(or __graft_entry__.build()); there is no CPU fallback")
+    lib = ctypes.CDLL(LIB_PATH)
+    for name, (res, args) in _SIGNATURES.items():
+        fn = getattr(lib, name)
+        fn.restype = res
+        fn.argtypes = args
+    _lib = lib
+    return lib
+
+
+def check(status: int) -> None:
+    if status != SG_OK:
+        msg = load().sg_last_error().decode("utf-8", "replace")
+        raise SortGpuError(status, msg)
+
+
+def exported_symbols() -> list[str]:
+    return sorted(_SIGNATURES)

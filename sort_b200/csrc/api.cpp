@@ -1,0 +1,424 @@
+// C ABI of libsortgpu (include/sortgpu.h): scene build + upload, batched
+// closest-hit / any-hit launches, host-buffer forms and error reporting.
+#include "sortgpu.h"
+
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cfloat>
+#include <chrono>
+#include <cstdio>
+#include <cstring>
+#include <mutex>
+#include <new>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+#include "builder.h"
+#include "trace_kernels.h"
+
+namespace {
+
+thread_local std::string g_last_error;
+
+sg_status fail(sg_status s, const std::string& msg) {
+    g_last_error = msg;
+    return s;
+}
+
+sg_status cuda_fail(cudaError_t e, const char* what) {
+    return fail(SG_ERR_CUDA, std::string(what) + ": " + cudaGetErrorString(e));
+}
+
+// Restores the caller's current device on scope exit.
+struct DeviceGuard {
+    int prev = -1;
+    bool ok = false;
+    explicit DeviceGuard(int dev) {
+        if (cudaGetDevice(&prev) != cudaSuccess) return;
+        ok = cudaSetDevice(dev) == cudaSuccess;
+    }
+    ~DeviceGuard() {
+        if (prev >= 0) cudaSetDevice(prev);
+    }
+};
+
+}  // namespace
+
+struct sg_scene {
+    int device = 0;
+    int width = 8;
+    int node_format = SG_NODES_FP32;
+    int stack_need = 1;
+    sg::BuiltTree tree;  // host copy of the topology (slot boxes released after upload)
+    float4* d_nodes = nullptr;
+    float4* d_tris = nullptr;
+    int* d_err = nullptr;
+    unsigned long long* d_stats = nullptr;
+    int64_t device_bytes = 0;
+    double build_seconds = 0.0;
+    // Scratch for the host-buffer entry points, grown on demand.
+    std::mutex scratch_lock;
+    void* d_scratch = nullptr;
+    size_t scratch_bytes = 0;
+    cudaStream_t stream = nullptr;
+};
+
+namespace {
+
+sg_status upload(sg_scene* s, const float* tri, int64_t ntri) {
+    const sg::BuiltTree& t = s->tree;
+    const int W = t.width;
+    const int f4 = W == 8 ? sg::NodeShape<8>::kF4 : sg::NodeShape<4>::kF4;
+    const int64_t nn = t.interior();
+    std::vector<float4> nodes(size_t(std::max<int64_t>(nn, 1)) * f4);
+    std::memset(nodes.data(), 0, nodes.size() * sizeof(float4));
+    const int Q = W / 4;
+    for (int64_t k = 0; k < nn; ++k) {
+        float* base = reinterpret_cast<float*>(&nodes[size_t(k) * f4]);
+        for (int a = 0; a < 3; ++a)
+            for (int j = 0; j < W; ++j) {
+                base[(2 * a) * Q * 4 + j] = t.lo[(size_t(k) * 3 + a) * W + j];
+                base[(2 * a + 1) * Q * 4 + j] = t.hi[(size_t(k) * 3 + a) * W + j];
+            }
+        int32_t* ch = reinterpret_cast<int32_t*>(base + 6 * Q * 4);
+        for (int j = 0; j < W; ++j) ch[j] = t.child[size_t(k) * W + j];
+    }
+    std::vector<float4> tris(size_t(std::max<int64_t>(ntri, 1)) * 3);
+    std::memset(tris.data(), 0, tris.size() * sizeof(float4));
+    for (int64_t i = 0; i < ntri; ++i) {
+        const int32_t p = t.order[size_t(i)];
+        const float* v = tri + int64_t(p) * 9;
+        float4* dst = &tris[size_t(i) * 3];
+        int32_t last = t.leaf_last[size_t(i)];
+        dst[0] = make_float4(v[0], v[1], v[2], 0.0f);
+        std::memcpy(&dst[0].w, &p, 4);
+        dst[1] = make_float4(v[3], v[4], v[5], 0.0f);
+        std::memcpy(&dst[1].w, &last, 4);
+        dst[2] = make_float4(v[6], v[7], v[8], 0.0f);
+    }
+    const size_t nb = nodes.size() * sizeof(float4), tb = tris.size() * sizeof(float4);
+    cudaError_t e = cudaMalloc(&s->d_nodes, nb);
+    if (e != cudaSuccess) return e == cudaErrorMemoryAllocation ? fail(SG_ERR_OUT_OF_MEMORY, "cudaMalloc(nodes) failed")
+                                                                 : cuda_fail(e, "cudaMalloc(nodes)");
+    e = cudaMalloc(&s->d_tris, tb);
+    if (e != cudaSuccess) return e == cudaErrorMemoryAllocation ? fail(SG_ERR_OUT_OF_MEMORY, "cudaMalloc(triangles) failed")
+                                                                 : cuda_fail(e, "cudaMalloc(triangles)");
+    if ((e = cudaMalloc(&s->d_err, sizeof(int))) != cudaSuccess) return cuda_fail(e, "cudaMalloc(status)");
+    if ((e = cudaMemcpy(s->d_nodes, nodes.data(), nb, cudaMemcpyHostToDevice)) != cudaSuccess)
+        return cuda_fail(e, "upload nodes");
+    if ((e = cudaMemcpy(s->d_tris, tris.data(), tb, cudaMemcpyHostToDevice)) != cudaSuccess)
+        return cuda_fail(e, "upload triangles");
+    if ((e = cudaMemset(s->d_err, 0, sizeof(int))) != cudaSuccess) return cuda_fail(e, "clear status");
+    s->device_bytes = int64_t(nb + tb);
+    return SG_OK;
+}
+
+void release(sg_scene* s) {
+    if (!s) return;
+    DeviceGuard g(s->device);
+    if (s->d_nodes) cudaFree(s->d_nodes);
+    if (s->d_tris) cudaFree(s->d_tris);
+    if (s->d_err) cudaFree(s->d_err);
+    if (s->d_stats) cudaFree(s->d_stats);
+    if (s->d_scratch) cudaFree(s->d_scratch);
+    if (s->stream) cudaStreamDestroy(s->stream);
+    delete s;
+}
+
+sg::DevTree dev_tree(const sg_scene* s) {
+    sg::DevTree d;
+    d.nodes = s->d_nodes;
+    d.tris = s->d_tris;
+    d.root = s->tree.root;
+    for (int k = 0; k < 3; ++k) {
+        d.box_lo[k] = s->tree.scene.mn[k];
+        d.box_hi[k] = s->tree.scene.mx[k];
+    }
+    return d;
+}
+
+sg_status check_status_word(const sg_scene* s, cudaStream_t st) {
+    int h = 0;
+    cudaError_t e = cudaMemcpyAsync(&h, s->d_err, sizeof(int), cudaMemcpyDeviceToHost, st);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+    if (e != cudaSuccess) return cuda_fail(e, "read traversal status");
+    if (h != 0) return fail(SG_ERR_INTERNAL, "traversal stack bound exceeded");
+    return SG_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+void sg_default_build_opts(sg_build_opts* o) {
+    if (!o) return;
+    o->width = 8;
+    o->max_depth = 16;
+    o->max_leaf = 8;
+    o->node_format = SG_NODES_FP32;
+    o->device = 0;
+    o->build_threads = 0;
+}
+
+sg_status sg_scene_create(const float* triangles, int64_t ntri, const sg_build_opts* opts, sg_scene** out) {
+    if (!out) return fail(SG_ERR_INVALID_ARGUMENT, "out is NULL");
+    *out = nullptr;
+    if (!opts) return fail(SG_ERR_INVALID_ARGUMENT, "opts is NULL");
+    if (ntri < 0 || (ntri > 0 && !triangles)) return fail(SG_ERR_INVALID_ARGUMENT, "bad triangle buffer");
+    if (opts->width != 4 && opts->width != 8) return fail(SG_ERR_INVALID_ARGUMENT, "width must be 4 or 8");
+    if (opts->max_leaf < 1 || opts->max_depth < 1) return fail(SG_ERR_INVALID_ARGUMENT, "max_leaf/max_depth < 1");
+    if (opts->node_format != SG_NODES_FP32) return fail(SG_ERR_UNSUPPORTED, "node format not available");
+    if (ntri >= int64_t(0x7fffffff)) return fail(SG_ERR_LIMIT, "more than 2^31-2 triangles");
+    int ndev = 0;
+    cudaError_t e = cudaGetDeviceCount(&ndev);
+    if (e != cudaSuccess) return cuda_fail(e, "cudaGetDeviceCount");
+    if (opts->device < 0 || opts->device >= ndev) return fail(SG_ERR_INVALID_ARGUMENT, "no such CUDA device");
+
+    sg_scene* s = new (std::nothrow) sg_scene();
+    if (!s) return fail(SG_ERR_OUT_OF_MEMORY, "host allocation failed");
+    s->device = opts->device;
+    s->width = opts->width;
+    s->node_format = opts->node_format;
+    sg::BuildParams bp;
+    bp.width = opts->width;
+    bp.max_depth = opts->max_depth;
+    bp.max_leaf = opts->max_leaf;
+    bp.threads = opts->build_threads;
+    const auto t0 = std::chrono::steady_clock::now();
+    try {
+        s->tree = sg::build_tree(triangles, ntri, bp);
+    } catch (const std::bad_alloc&) {
+        delete s;
+        return fail(SG_ERR_OUT_OF_MEMORY, "host memory exhausted during build");
+    } catch (const std::exception& ex) {
+        delete s;
+        return fail(SG_ERR_INVALID_ARGUMENT, ex.what());
+    }
+    s->build_seconds = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+    s->stack_need = std::max(1, s->tree.depth * (s->width - 1) + 1);
+    if (s->stack_need > 256) {
+        delete s;
+        return fail(SG_ERR_LIMIT, "tree too deep for the traversal stack (depth*(width-1)+1 > 256)");
+    }
+    DeviceGuard g(s->device);
+    if (!g.ok) {
+        delete s;
+        return fail(SG_ERR_CUDA, "cudaSetDevice failed");
+    }
+    sg_status st;
+    try {
+        st = upload(s, triangles, ntri);
+    } catch (const std::bad_alloc&) {
+        st = fail(SG_ERR_OUT_OF_MEMORY, "host memory exhausted during upload");
+    }
+    if (st != SG_OK) {
+        release(s);
+        return st;
+    }
+    std::vector<sg::Box>().swap(s->tree.slot_box);
+    std::vector<float>().swap(s->tree.lo);
+    std::vector<float>().swap(s->tree.hi);
+    *out = s;
+    return SG_OK;
+}
+
+sg_status sg_scene_destroy(sg_scene* s) {
+    release(s);
+    return SG_OK;
+}
+
+sg_status sg_scene_info_get(const sg_scene* s, sg_scene_info* info) {
+    if (!s || !info) return fail(SG_ERR_INVALID_ARGUMENT, "NULL argument");
+    std::memset(info, 0, sizeof(*info));
+    info->triangles = int64_t(s->tree.order.size());
+    info->interior_nodes = s->tree.interior();
+    info->leaves = s->tree.leaves;
+    info->depth = s->tree.depth;
+    info->width = s->width;
+    info->node_format = s->node_format;
+    info->valid = s->tree.root != sg::kEmptyRef ? 1 : 0;
+    for (int k = 0; k < 3; ++k) {
+        info->bbox[k] = s->tree.scene.mn[k];
+        info->bbox[3 + k] = s->tree.scene.mx[k];
+    }
+    info->device_bytes = s->device_bytes;
+    info->build_seconds = s->build_seconds;
+    return SG_OK;
+}
+
+sg_status sg_scene_topology(const sg_scene* s, int32_t* out, int64_t cap, int64_t* written) {
+    if (!s || !written) return fail(SG_ERR_INVALID_ARGUMENT, "NULL argument");
+    std::vector<int32_t> v;
+    sg::tree_topology(s->tree, v);
+    *written = int64_t(v.size());
+    if (int64_t(v.size()) > cap || (!out && !v.empty())) return fail(SG_ERR_LIMIT, "topology buffer too small");
+    if (!v.empty()) std::memcpy(out, v.data(), v.size() * sizeof(int32_t));
+    return SG_OK;
+}
+
+sg_status sg_build_topology_host(const float* triangles, int64_t ntri, const sg_build_opts* opts, int32_t* out,
+                                 int64_t cap, int64_t* written, int32_t* depth) {
+    if (!opts || !written) return fail(SG_ERR_INVALID_ARGUMENT, "NULL argument");
+    if (ntri < 0 || (ntri > 0 && !triangles)) return fail(SG_ERR_INVALID_ARGUMENT, "bad triangle buffer");
+    sg::BuildParams bp;
+    bp.width = opts->width;
+    bp.max_depth = opts->max_depth;
+    bp.max_leaf = opts->max_leaf;
+    bp.threads = opts->build_threads;
+    std::vector<int32_t> v;
+    try {
+        const sg::BuiltTree t = sg::build_tree(triangles, ntri, bp);
+        sg::tree_topology(t, v);
+        if (depth) *depth = t.depth;
+    } catch (const std::bad_alloc&) {
+        return fail(SG_ERR_OUT_OF_MEMORY, "host memory exhausted during build");
+    } catch (const std::exception& ex) {
+        return fail(SG_ERR_INVALID_ARGUMENT, ex.what());
+    }
+    *written = int64_t(v.size());
+    if (int64_t(v.size()) > cap || (!out && !v.empty())) return fail(SG_ERR_LIMIT, "topology buffer too small");
+    if (!v.empty()) std::memcpy(out, v.data(), v.size() * sizeof(int32_t));
+    return SG_OK;
+}
+
+static sg_status trace_common(const sg_scene* s, const sg_rays* rays, int64_t n, const sg_hits* hits, uint8_t* occ,
+                              bool any, cudaStream_t st) {
+    if (!s || !rays) return fail(SG_ERR_INVALID_ARGUMENT, "NULL scene or rays");
+    if (n < 0) return fail(SG_ERR_INVALID_ARGUMENT, "negative ray count");
+    if (n == 0) return SG_OK;
+    if (!rays->ox || !rays->oy || !rays->oz || !rays->dx || !rays->dy || !rays->dz || !rays->tmin || !rays->tmax)
+        return fail(SG_ERR_INVALID_ARGUMENT, "NULL ray array");
+    if (any ? !occ : (!hits || !hits->prim || !hits->t)) return fail(SG_ERR_INVALID_ARGUMENT, "NULL output array");
+    if (n > int64_t(0x7fffffff) * 128) return fail(SG_ERR_LIMIT, "batch too large");
+    DeviceGuard g(s->device);
+    if (!g.ok) return fail(SG_ERR_CUDA, "cudaSetDevice failed");
+    sg::DevRays r{rays->ox, rays->oy, rays->oz, rays->dx, rays->dy, rays->dz, rays->tmin, rays->tmax};
+    const cudaError_t e =
+        sg::launch_trace_fp32(s->width, any, dev_tree(s), r, n, s->stack_need, any ? nullptr : hits->prim,
+                              any ? nullptr : hits->t, any ? nullptr : hits->u, any ? nullptr : hits->v, occ,
+                              s->d_err, st);
+    if (e != cudaSuccess) return cuda_fail(e, "traversal launch");
+    return SG_OK;
+}
+
+sg_status sg_trace_closest(const sg_scene* s, const sg_rays* rays, int64_t n, const sg_hits* hits, void* stream) {
+    return trace_common(s, rays, n, hits, nullptr, false, (cudaStream_t)stream);
+}
+
+sg_status sg_trace_any(const sg_scene* s, const sg_rays* rays, int64_t n, uint8_t* occluded, void* stream) {
+    return trace_common(s, rays, n, nullptr, occluded, true, (cudaStream_t)stream);
+}
+
+static sg_status host_trace(const sg_scene* cs, const float* rays8, int64_t n, int32_t* prim, float* t, float* u,
+                            float* v, uint8_t* occ, bool any) {
+    if (!cs || !rays8) return fail(SG_ERR_INVALID_ARGUMENT, "NULL scene or rays");
+    if (n < 0) return fail(SG_ERR_INVALID_ARGUMENT, "negative ray count");
+    if (n == 0) return SG_OK;
+    if (any ? !occ : (!prim || !t)) return fail(SG_ERR_INVALID_ARGUMENT, "NULL output array");
+    sg_scene* s = const_cast<sg_scene*>(cs);
+    std::lock_guard<std::mutex> lock(s->scratch_lock);
+    DeviceGuard g(s->device);
+    if (!g.ok) return fail(SG_ERR_CUDA, "cudaSetDevice failed");
+    cudaError_t e;
+    if (!s->stream && (e = cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking)) != cudaSuccess)
+        return cuda_fail(e, "cudaStreamCreate");
+    const size_t in_bytes = size_t(n) * 8 * sizeof(float);
+    const size_t out_bytes = any ? size_t(n) : size_t(n) * 16;
+    const size_t need = in_bytes + out_bytes + 256;
+    if (s->scratch_bytes < need) {
+        if (s->d_scratch) cudaFree(s->d_scratch);
+        s->d_scratch = nullptr;
+        s->scratch_bytes = 0;
+        if ((e = cudaMalloc(&s->d_scratch, need)) != cudaSuccess)
+            return e == cudaErrorMemoryAllocation ? fail(SG_ERR_OUT_OF_MEMORY, "scratch allocation failed")
+                                                  : cuda_fail(e, "cudaMalloc(scratch)");
+        s->scratch_bytes = need;
+    }
+    float* d_rays = static_cast<float*>(s->d_scratch);
+    char* d_out = static_cast<char*>(s->d_scratch) + ((in_bytes + 255) & ~size_t(255));
+    cudaStream_t st = s->stream;
+    if ((e = cudaMemcpyAsync(d_rays, rays8, in_bytes, cudaMemcpyHostToDevice, st)) != cudaSuccess)
+        return cuda_fail(e, "copy rays to device");
+    sg_rays r{d_rays, d_rays + n, d_rays + 2 * n, d_rays + 3 * n, d_rays + 4 * n, d_rays + 5 * n, d_rays + 6 * n,
+              d_rays + 7 * n};
+    sg_status status;
+    if (any) {
+        status = trace_common(s, &r, n, nullptr, reinterpret_cast<uint8_t*>(d_out), true, st);
+        if (status != SG_OK) return status;
+        if ((e = cudaMemcpyAsync(occ, d_out, size_t(n), cudaMemcpyDeviceToHost, st)) != cudaSuccess)
+            return cuda_fail(e, "copy results to host");
+    } else {
+        int32_t* dp = reinterpret_cast<int32_t*>(d_out);
+        float* dt = reinterpret_cast<float*>(d_out + size_t(n) * 4);
+        float* du = reinterpret_cast<float*>(d_out + size_t(n) * 8);
+        float* dv = reinterpret_cast<float*>(d_out + size_t(n) * 12);
+        sg_hits h{dp, dt, u ? du : nullptr, v ? dv : nullptr};
+        status = trace_common(s, &r, n, &h, nullptr, false, st);
+        if (status != SG_OK) return status;
+        if ((e = cudaMemcpyAsync(prim, dp, size_t(n) * 4, cudaMemcpyDeviceToHost, st)) != cudaSuccess ||
+            (e = cudaMemcpyAsync(t, dt, size_t(n) * 4, cudaMemcpyDeviceToHost, st)) != cudaSuccess ||
+            (u && (e = cudaMemcpyAsync(u, du, size_t(n) * 4, cudaMemcpyDeviceToHost, st)) != cudaSuccess) ||
+            (v && (e = cudaMemcpyAsync(v, dv, size_t(n) * 4, cudaMemcpyDeviceToHost, st)) != cudaSuccess))
+            return cuda_fail(e, "copy results to host");
+    }
+    if ((e = cudaStreamSynchronize(st)) != cudaSuccess) return cuda_fail(e, "synchronize");
+    return check_status_word(s, st);
+}
+
+sg_status sg_trace_stats(const sg_scene* cs, const sg_rays* rays, int64_t n, int32_t any, int64_t* node_tests,
+                         int64_t* prim_tests, void* stream) {
+    if (!cs || !rays || !node_tests || !prim_tests) return fail(SG_ERR_INVALID_ARGUMENT, "NULL argument");
+    if (n < 0) return fail(SG_ERR_INVALID_ARGUMENT, "negative ray count");
+    if (!rays->ox || !rays->oy || !rays->oz || !rays->dx || !rays->dy || !rays->dz || !rays->tmin || !rays->tmax)
+        return fail(SG_ERR_INVALID_ARGUMENT, "NULL ray array");
+    *node_tests = *prim_tests = 0;
+    if (n == 0) return SG_OK;
+    sg_scene* s = const_cast<sg_scene*>(cs);
+    std::lock_guard<std::mutex> lock(s->scratch_lock);
+    DeviceGuard g(s->device);
+    if (!g.ok) return fail(SG_ERR_CUDA, "cudaSetDevice failed");
+    cudaError_t e;
+    cudaStream_t st = (cudaStream_t)stream;
+    if (!s->d_stats && (e = cudaMalloc(&s->d_stats, 2 * sizeof(unsigned long long))) != cudaSuccess)
+        return cuda_fail(e, "cudaMalloc(stats)");
+    const size_t need = size_t(n) * 16 + 256;
+    if (s->scratch_bytes < need) {
+        if (s->d_scratch) cudaFree(s->d_scratch);
+        s->d_scratch = nullptr;
+        s->scratch_bytes = 0;
+        if ((e = cudaMalloc(&s->d_scratch, need)) != cudaSuccess) return cuda_fail(e, "cudaMalloc(scratch)");
+        s->scratch_bytes = need;
+    }
+    char* out = static_cast<char*>(s->d_scratch);
+    if ((e = cudaMemsetAsync(s->d_stats, 0, 2 * sizeof(unsigned long long), st)) != cudaSuccess)
+        return cuda_fail(e, "clear stats");
+    sg::DevRays r{rays->ox, rays->oy, rays->oz, rays->dx, rays->dy, rays->dz, rays->tmin, rays->tmax};
+    e = sg::launch_trace_fp32_stats(s->width, any != 0, dev_tree(s), r, n, s->stack_need,
+                                    reinterpret_cast<int32_t*>(out), reinterpret_cast<float*>(out + size_t(n) * 4),
+                                    nullptr, nullptr, reinterpret_cast<uint8_t*>(out), s->d_err, s->d_stats, st);
+    if (e != cudaSuccess) return cuda_fail(e, "stats launch");
+    unsigned long long h[2] = {0, 0};
+    if ((e = cudaMemcpyAsync(h, s->d_stats, sizeof(h), cudaMemcpyDeviceToHost, st)) != cudaSuccess ||
+        (e = cudaStreamSynchronize(st)) != cudaSuccess)
+        return cuda_fail(e, "read stats");
+    *node_tests = int64_t(h[0]);
+    *prim_tests = int64_t(h[1]);
+    return check_status_word(s, st);
+}
+
+sg_status sg_trace_closest_host(const sg_scene* s, const float* rays8, int64_t n, int32_t* prim, float* t, float* u,
+                                float* v) {
+    return host_trace(s, rays8, n, prim, t, u, v, nullptr, false);
+}
+
+sg_status sg_trace_any_host(const sg_scene* s, const float* rays8, int64_t n, uint8_t* occluded) {
+    return host_trace(s, rays8, n, nullptr, nullptr, nullptr, nullptr, occluded, true);
+}
+
+const char* sg_last_error(void) { return g_last_error.c_str(); }
+
+const char* sg_version(void) { return "sortgpu 0.1 (sm_100a)"; }
+
+}  // extern "C"

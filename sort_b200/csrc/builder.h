@@ -1,0 +1,68 @@
+// Host-side wide-BVH builder producing the same tree as SORT's Fbvh::Build.
+//
+// The tree is split exactly as accel/fast_bvh.hpp:109-270 and
+// accel/bvh_utils.h:27-118 do (16-bin SAH on the centroid bounds' longest
+// axis, normalised by the parent box; breadth-first W-way split of each node;
+// std::partition of the primitive list; leaves of <= max_leaf primitives or at
+// max_depth), so leaf membership, leaf order and child order are identical to
+// SORT's. That identity is what makes closest-hit IDs match SORT even when two
+// triangles are hit at exactly the same distance.
+//
+// Differences from SORT, none of which change the tree:
+//   * subtrees are built concurrently (each only permutes its own range);
+//   * the result is a flat array form (BuiltTree) instead of unique_ptr nodes.
+#pragma once
+
+#include <cstdint>
+#include <vector>
+
+namespace sg {
+
+struct Box {
+    float mn[3], mx[3];
+};
+
+constexpr int32_t kLeafBit = int32_t(0x80000000u);
+constexpr int32_t kEmptyRef = -1;  // all bits set: never a valid node or leaf start
+
+inline bool ref_is_leaf(int32_t r) { return r < 0 && r != kEmptyRef; }
+inline int32_t leaf_ref(int64_t begin) { return int32_t(uint32_t(begin) | 0x80000000u); }
+inline int64_t leaf_begin(int32_t r) { return int64_t(uint32_t(r) & 0x7fffffffu); }
+
+struct BuildParams {
+    int width = 8;
+    int max_depth = 16;
+    int max_leaf = 8;
+    int threads = 0;  // 0 = hardware_concurrency
+};
+
+// Flat tree. Interior node k owns child[k*W + j] and, for child j on axis a,
+// lo[(k*3 + a)*W + j] / hi[(k*3 + a)*W + j]. Interior children of a node are
+// numbered consecutively (a node's first interior child is node
+// first_interior[k]). Empty child slots hold kEmptyRef and the empty box
+// (+FLT_MAX .. -FLT_MAX) SORT leaves in unused SIMD lanes.
+struct BuiltTree {
+    int width = 8;
+    int depth = 0;  // Fbvh::m_depth
+    Box scene{};    // enlarged scene box (core/scene.cpp:150-154)
+    int32_t root = kEmptyRef;
+    std::vector<int32_t> child;
+    std::vector<float> lo, hi;
+    std::vector<int32_t> first_interior;  // per node, -1 if none
+    std::vector<int32_t> order;           // primitive index of each leaf slot (leaf order)
+    std::vector<uint8_t> leaf_last;       // 1 on the last slot of every leaf
+    std::vector<Box> slot_box;            // per-slot primitive box (leaf order)
+    int64_t leaves = 0;
+    int64_t interior() const { return width ? int64_t(child.size()) / width : 0; }
+};
+
+// Builds over ntri triangles, 9 floats each (v0, v1, v2). Throws
+// std::invalid_argument / std::bad_alloc on bad input / memory exhaustion.
+BuiltTree build_tree(const float* tri, int64_t ntri, const BuildParams& p);
+
+// Pre-order topology in the oracle's comparison format:
+//   interior node: [child_cnt, child0 ..., child_{n-1} ...]
+//   leaf:          [0, pri_cnt, primitive indices in leaf order]
+void tree_topology(const BuiltTree& t, std::vector<int32_t>& out);
+
+}  // namespace sg
