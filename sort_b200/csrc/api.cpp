@@ -85,7 +85,8 @@ sg_status upload(sg_scene* s, const float* tri, int64_t ntri) {
         int32_t* ch = reinterpret_cast<int32_t*>(base + 6 * Q * 4);
         for (int j = 0; j < W; ++j) ch[j] = t.child[size_t(k) * W + j];
     }
-    std::vector<float4> tris(size_t(std::max<int64_t>(ntri, 1)) * 3);
+    // one zero padding slot at the end: the kernels fetch leaf triangles in pairs
+    std::vector<float4> tris(size_t(ntri + 1) * 3);
     std::memset(tris.data(), 0, tris.size() * sizeof(float4));
     for (int64_t i = 0; i < ntri; ++i) {
         const int32_t p = t.order[size_t(i)];

@@ -60,6 +60,13 @@ __device__ __forceinline__ void load_node(const float4* __restrict__ nodes, int3
 // STATS adds SORT's traversal counters (accel/fast_bvh.hpp:50-96): interior
 // nodes box-tested, and primitives tested counted per leaf entered
 // (sIntersectionTest += pri_cnt), accumulated into stats[0] / stats[1].
+//
+// Two GPU-side changes leave SORT's visit order intact:
+//   * the entry SORT would pop right after pushing an interior node's children
+//     (the nearest one) is kept in registers and descended into directly; only
+//     the others go to the stack, so a descent costs no stack round trip;
+//   * leaf triangles are fetched two at a time (the triangle array carries one
+//     padding slot), so the loads of the second overlap the test of the first.
 template <int W, bool ANY, int STACK, bool STATS>
 __global__ void __launch_bounds__(128) k_trace_fp32(DevTree tr, DevRays rays, int64_t n, int32_t* __restrict__ prim_out,
                                                     float* __restrict__ t_out, float* __restrict__ u_out,
@@ -87,105 +94,143 @@ __global__ void __launch_bounds__(128) k_trace_fp32(DevTree tr, DevRays rays, in
     if (f0 >= 0.0f && tr.root != kEmpty) {
         uint2 stk[STACK];
         int si = 0;
-        stk[si++] = make_uint2((uint32_t)tr.root, __float_as_uint(f0));
-        while (si > 0) {
-            const uint2 e = stk[--si];
-            const int32_t ref = (int32_t)e.x;
-            if (best_t < __uint_as_float(e.y)) continue;
-            if (ref < 0) {
-                int64_t s = (int64_t)((uint32_t)ref & 0x7fffffffu);
-                bool found = false;
-                unsigned tested = 0;
-                for (;;) {
-                    ++tested;
-                    const float4 a = __ldg(tr.tris + 3 * s);
-                    const float4 b = __ldg(tr.tris + 3 * s + 1);
-                    const float4 c = __ldg(tr.tris + 3 * s + 2);
-                    float t, u, v;
-                    if (tri_test(r, a, b, c, t, u, v) && t < best_t) {
-                        best_t = t;
-                        best_u = u;
-                        best_v = v;
-                        best_prim = __float_as_int(a.w);
-                        if (ANY) {
-                            found = true;
-                            break;
+        int32_t cur = tr.root;
+        float cur_d = f0;
+        bool done = false;
+        for (;;) {
+            bool descend = false;
+            if (!(best_t < cur_d)) {  // fast_bvh.hpp:343: skip when the hit is nearer than the entry
+                if (cur < 0) {
+                    int64_t s = (int64_t)((uint32_t)cur & 0x7fffffffu);
+                    unsigned tested = 0;
+                    for (;;) {
+                        const float4* q = tr.tris + 3 * s;
+                        const float4 a0 = __ldg(q), b0 = __ldg(q + 1), c0 = __ldg(q + 2);
+                        const float4 a1 = __ldg(q + 3), b1 = __ldg(q + 4), c1 = __ldg(q + 5);
+                        float t, u, v;
+                        ++tested;
+                        if (tri_test(r, a0, b0, c0, t, u, v) && t < best_t) {
+                            best_t = t;
+                            best_u = u;
+                            best_v = v;
+                            best_prim = __float_as_int(a0.w);
+                            if (ANY) {
+                                done = true;
+                                break;
+                            }
                         }
-                    }
-                    if (__float_as_int(b.w)) break;
-                    ++s;
-                }
-                if (STATS) {
-                    // whole leaf, as SORT counts it
-                    if (ANY && found)
-                        for (int64_t q = s; !__float_as_int(__ldg(tr.tris + 3 * q + 1).w); ++q) ++tested;
-                    prim_tests += tested;
-                }
-                if (ANY && found) break;
-                continue;
-            }
-            if (si + W > STACK) {  // cannot happen when STACK >= depth*(W-1)+1; reported, never overrun
-                atomicOr(err, 1);
-                break;
-            }
-            NodeData<W> nd;
-            load_node<W>(tr.nodes, ref, nd);
-            if (STATS) ++node_tests;
-            float d[W];
-            unsigned mask = 0;
-#pragma unroll
-            for (int j = 0; j < W; ++j) {
-                const bool hit = slab(r, nd.lo[0][j], nd.hi[0][j], nd.lo[1][j], nd.hi[1][j], nd.lo[2][j], nd.hi[2][j], d[j]);
-                if (hit && nd.ch[j] != kEmpty) mask |= 1u << j;
-            }
-            const int cnt = __popc(mask);
-            if (cnt == 0) continue;
-            if (cnt <= 2) {
-                // First two hit slots in index order.
-                int32_t c0 = 0, c1 = 0;
-                float t0 = 0.0f, t1 = 0.0f;
-                int seen = 0;
-#pragma unroll
-                for (int j = 0; j < W; ++j) {
-                    if (mask & (1u << j)) {
-                        if (seen == 0) {
-                            c0 = nd.ch[j];
-                            t0 = d[j];
-                        } else {
-                            c1 = nd.ch[j];
-                            t1 = d[j];
+                        if (__float_as_int(b0.w)) break;
+                        ++tested;
+                        if (tri_test(r, a1, b1, c1, t, u, v) && t < best_t) {
+                            best_t = t;
+                            best_u = u;
+                            best_v = v;
+                            best_prim = __float_as_int(a1.w);
+                            if (ANY) {
+                                ++s;
+                                done = true;
+                                break;
+                            }
                         }
-                        ++seen;
+                        if (__float_as_int(b1.w)) break;
+                        s += 2;
                     }
-                }
-                if (cnt == 1) {
-                    stk[si++] = make_uint2((uint32_t)c0, __float_as_uint(t0));
-                } else if (t0 < t1) {
-                    stk[si++] = make_uint2((uint32_t)c1, __float_as_uint(t1));
-                    stk[si++] = make_uint2((uint32_t)c0, __float_as_uint(t0));
+                    if (STATS) {
+                        if (ANY && done)  // whole leaf, as SORT counts it
+                            for (int64_t q = s; !__float_as_int(__ldg(tr.tris + 3 * q + 1).w); ++q) ++tested;
+                        prim_tests += tested;
+                    }
+                    if (ANY && done) break;
                 } else {
-                    stk[si++] = make_uint2((uint32_t)c0, __float_as_uint(t0));
-                    stk[si++] = make_uint2((uint32_t)c1, __float_as_uint(t1));
-                }
-            } else {
-                // Selection by decreasing distance, ties lowest slot first; only
-                // entries with distance > -1 take part (fast_bvh.hpp:438-453).
-                int pushed = 0;
-#pragma unroll
-                for (int j = 0; j < W; ++j) {
-                    const bool hj = (mask & (1u << j)) && d[j] > -1.0f;
-                    int rank = 0;
-#pragma unroll
-                    for (int k = 0; k < W; ++k) {
-                        const bool hk = (mask & (1u << k)) && d[k] > -1.0f;
-                        rank += (hk && (d[k] > d[j] || (d[k] == d[j] && k < j))) ? 1 : 0;
+                    if (si + W > STACK) {  // cannot happen when STACK >= depth*(W-1)+1; reported, never overrun
+                        atomicOr(err, 1);
+                        break;
                     }
-                    if (hj) {
-                        stk[si + rank] = make_uint2((uint32_t)nd.ch[j], __float_as_uint(d[j]));
-                        ++pushed;
+                    NodeData<W> nd;
+                    load_node<W>(tr.nodes, cur, nd);
+                    if (STATS) ++node_tests;
+                    float d[W];
+                    unsigned mask = 0;
+#pragma unroll
+                    for (int j = 0; j < W; ++j) {
+                        const bool hit =
+                            slab(r, nd.lo[0][j], nd.hi[0][j], nd.lo[1][j], nd.hi[1][j], nd.lo[2][j], nd.hi[2][j], d[j]);
+                        if (hit && nd.ch[j] != kEmpty) mask |= 1u << j;
+                    }
+                    const int cnt = __popc(mask);
+                    if (cnt == 1) {
+#pragma unroll
+                        for (int j = 0; j < W; ++j)
+                            if (mask & (1u << j)) {
+                                cur = nd.ch[j];
+                                cur_d = d[j];
+                            }
+                        descend = true;
+                    } else if (cnt == 2) {
+                        // SORT pushes the far one first (t0 < t1) or the second slot last
+                        // (otherwise); the one it would pop next is descended into.
+                        int32_t c0 = 0, c1 = 0;
+                        float t0 = 0.0f, t1 = 0.0f;
+                        bool first = true;
+#pragma unroll
+                        for (int j = 0; j < W; ++j) {
+                            if (mask & (1u << j)) {
+                                if (first) {
+                                    c0 = nd.ch[j];
+                                    t0 = d[j];
+                                    first = false;
+                                } else {
+                                    c1 = nd.ch[j];
+                                    t1 = d[j];
+                                }
+                            }
+                        }
+                        if (t0 < t1) {
+                            stk[si++] = make_uint2((uint32_t)c1, __float_as_uint(t1));
+                            cur = c0;
+                            cur_d = t0;
+                        } else {
+                            stk[si++] = make_uint2((uint32_t)c0, __float_as_uint(t0));
+                            cur = c1;
+                            cur_d = t1;
+                        }
+                        descend = true;
+                    } else if (cnt > 2) {
+                        // Selection by decreasing distance, ties lowest slot first; only
+                        // entries with distance > -1 take part (fast_bvh.hpp:438-453).
+                        int count = 0;
+#pragma unroll
+                        for (int j = 0; j < W; ++j) count += ((mask & (1u << j)) && d[j] > -1.0f) ? 1 : 0;
+#pragma unroll
+                        for (int j = 0; j < W; ++j) {
+                            const bool hj = (mask & (1u << j)) && d[j] > -1.0f;
+                            int rank = 0;
+#pragma unroll
+                            for (int k = 0; k < W; ++k) {
+                                const bool hk = (mask & (1u << k)) && d[k] > -1.0f;
+                                rank += (hk && (d[k] > d[j] || (d[k] == d[j] && k < j))) ? 1 : 0;
+                            }
+                            if (hj) {
+                                if (rank == count - 1) {
+                                    cur = nd.ch[j];
+                                    cur_d = d[j];
+                                } else {
+                                    stk[si + rank] = make_uint2((uint32_t)nd.ch[j], __float_as_uint(d[j]));
+                                }
+                            }
+                        }
+                        if (count > 0) {
+                            si += count - 1;
+                            descend = true;
+                        }
                     }
                 }
-                si += pushed;
+            }
+            if (!descend) {
+                if (si == 0) break;
+                const uint2 e = stk[--si];
+                cur = (int32_t)e.x;
+                cur_d = __uint_as_float(e.y);
             }
         }
     }
