@@ -30,6 +30,10 @@
  *   sg_trace_stats    SORT's traversal statistics for a batch (accel/fast_bvh.hpp:50-96
  *                     and accel/accelerator.cpp:21-23: sRayCount, sIntersectionTest)
  *                     plus the interior-node box tests; runs the same traversal.
+ *   sg_scene_set_tuning / sg_scene_get_tuning
+ *                     no SORT counterpart: launch schedule of the traversal
+ *                     kernels (SORT's scheduling knob is its thread count,
+ *                     work/image_evaluation/image_evaluation.cpp:70-75).
  *   sg_trace_closest_host / sg_trace_any_host
  *                     the same queries on host buffers, with the host<->device
  *                     copies done inside the call (what a caller that holds rays in
@@ -113,6 +117,17 @@ typedef struct {
     double build_seconds;    /* host build time */
 } sg_scene_info;
 
+/* Traversal launch schedule (results never depend on it). */
+typedef enum {
+    SG_SCHEDULE_THREAD_PER_RAY = 0, /* one ray per thread for the whole launch */
+    SG_SCHEDULE_PERSISTENT = 1      /* persistent warps; a finished lane takes its warp's next ray */
+} sg_schedule;
+
+typedef struct {
+    int32_t schedule;          /* sg_schedule */
+    int32_t refill_threshold;  /* idle lanes (1..32) that make a persistent warp fetch new rays */
+} sg_trace_tuning;
+
 typedef struct sg_scene sg_scene;
 
 void sg_default_build_opts(sg_build_opts* opts);
@@ -126,6 +141,9 @@ sg_status sg_scene_topology(const sg_scene* scene, int32_t* out, int64_t cap, in
  * out = NULL / cap = 0 to learn the size (returns SG_ERR_LIMIT and sets written). */
 sg_status sg_build_topology_host(const float* triangles, int64_t ntri, const sg_build_opts* opts, int32_t* out,
                                  int64_t cap, int64_t* written, int32_t* depth);
+
+sg_status sg_scene_set_tuning(sg_scene* scene, const sg_trace_tuning* tuning);
+sg_status sg_scene_get_tuning(const sg_scene* scene, sg_trace_tuning* tuning);
 
 sg_status sg_trace_closest(const sg_scene* scene, const sg_rays* rays, int64_t n, const sg_hits* hits, void* stream);
 sg_status sg_trace_any(const sg_scene* scene, const sg_rays* rays, int64_t n, uint8_t* occluded, void* stream);

@@ -40,6 +40,10 @@ class Hits(ctypes.Structure):
     _fields_ = [("prim", ctypes.c_void_p), ("t", ctypes.c_void_p), ("u", ctypes.c_void_p), ("v", ctypes.c_void_p)]
 
 
+class Tuning(ctypes.Structure):
+    _fields_ = [("schedule", ctypes.c_int32), ("refill_threshold", ctypes.c_int32)]
+
+
 class SceneInfo(ctypes.Structure):
     _fields_ = [("triangles", ctypes.c_int64), ("interior_nodes", ctypes.c_int64), ("leaves", ctypes.c_int64),
                 ("depth", ctypes.c_int32), ("width", ctypes.c_int32), ("node_format", ctypes.c_int32),
@@ -57,6 +61,8 @@ _SIGNATURES = {
     "sg_scene_topology": (ctypes.c_int, [_vp, _vp, _i64, ctypes.POINTER(_i64)]),
     "sg_build_topology_host": (ctypes.c_int, [_vp, _i64, ctypes.POINTER(BuildOpts), _vp, _i64,
                                               ctypes.POINTER(_i64), ctypes.POINTER(ctypes.c_int32)]),
+    "sg_scene_set_tuning": (ctypes.c_int, [_vp, ctypes.POINTER(Tuning)]),
+    "sg_scene_get_tuning": (ctypes.c_int, [_vp, ctypes.POINTER(Tuning)]),
     "sg_trace_closest": (ctypes.c_int, [_vp, ctypes.POINTER(Rays), _i64, ctypes.POINTER(Hits), _vp]),
     "sg_trace_any": (ctypes.c_int, [_vp, ctypes.POINTER(Rays), _i64, _vp, _vp]),
     "sg_trace_stats": (ctypes.c_int, [_vp, ctypes.POINTER(Rays), _i64, ctypes.c_int32, ctypes.POINTER(_i64),

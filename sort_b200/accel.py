@@ -200,6 +200,24 @@ class Accelerator:
                                               1 if any_hit else 0, ctypes.byref(a), ctypes.byref(b), s))
         return a.value, b.value
 
+    # -- launch schedule (results never depend on it) ------------------------------
+    def SetTuning(self, schedule: int | None = None, refill_threshold: int | None = None) -> None:
+        self._require()
+        lib = _lib.load()
+        t = _lib.Tuning()
+        _lib.check(lib.sg_scene_get_tuning(self._h, ctypes.byref(t)))
+        if schedule is not None:
+            t.schedule = int(schedule)
+        if refill_threshold is not None:
+            t.refill_threshold = int(refill_threshold)
+        _lib.check(lib.sg_scene_set_tuning(self._h, ctypes.byref(t)))
+
+    def GetTuning(self) -> dict:
+        self._require()
+        t = _lib.Tuning()
+        _lib.check(_lib.load().sg_scene_get_tuning(self._h, ctypes.byref(t)))
+        return {"schedule": t.schedule, "refill_threshold": t.refill_threshold}
+
     # -- introspection ------------------------------------------------------------
     def GetBBox(self):
         self._require()

@@ -51,6 +51,7 @@ struct sg_scene {
     int width = 8;
     int node_format = SG_NODES_FP32;
     int stack_need = 1;
+    sg::TraceTuning tuning;
     sg::BuiltTree tree;  // host copy of the topology (slot boxes released after upload)
     float4* d_nodes = nullptr;
     float4* d_tris = nullptr;
@@ -296,10 +297,21 @@ static sg_status trace_common(const sg_scene* s, const sg_rays* rays, int64_t n,
     DeviceGuard g(s->device);
     if (!g.ok) return fail(SG_ERR_CUDA, "cudaSetDevice failed");
     sg::DevRays r{rays->ox, rays->oy, rays->oz, rays->dx, rays->dy, rays->dz, rays->tmin, rays->tmax};
-    const cudaError_t e =
-        sg::launch_trace_fp32(s->width, any, dev_tree(s), r, n, s->stack_need, any ? nullptr : hits->prim,
-                              any ? nullptr : hits->t, any ? nullptr : hits->u, any ? nullptr : hits->v, occ,
-                              s->d_err, st);
+    sg::TraceLaunch L;
+    L.width = s->width;
+    L.any = any;
+    L.stack_need = s->stack_need;
+    L.tuning = s->tuning;
+    if (any) {
+        L.occ = occ;
+    } else {
+        L.prim = hits->prim;
+        L.t = hits->t;
+        L.u = hits->u;
+        L.v = hits->v;
+    }
+    L.err = s->d_err;
+    const cudaError_t e = sg::launch_trace_fp32(L, dev_tree(s), r, n, st);
     if (e != cudaSuccess) return cuda_fail(e, "traversal launch");
     return SG_OK;
 }
@@ -396,9 +408,17 @@ sg_status sg_trace_stats(const sg_scene* cs, const sg_rays* rays, int64_t n, int
     if ((e = cudaMemsetAsync(s->d_stats, 0, 2 * sizeof(unsigned long long), st)) != cudaSuccess)
         return cuda_fail(e, "clear stats");
     sg::DevRays r{rays->ox, rays->oy, rays->oz, rays->dx, rays->dy, rays->dz, rays->tmin, rays->tmax};
-    e = sg::launch_trace_fp32_stats(s->width, any != 0, dev_tree(s), r, n, s->stack_need,
-                                    reinterpret_cast<int32_t*>(out), reinterpret_cast<float*>(out + size_t(n) * 4),
-                                    nullptr, nullptr, reinterpret_cast<uint8_t*>(out), s->d_err, s->d_stats, st);
+    sg::TraceLaunch L;
+    L.width = s->width;
+    L.any = any != 0;
+    L.stack_need = s->stack_need;
+    L.tuning = s->tuning;
+    L.prim = reinterpret_cast<int32_t*>(out);
+    L.t = reinterpret_cast<float*>(out + size_t(n) * 4);
+    L.occ = reinterpret_cast<uint8_t*>(out);
+    L.err = s->d_err;
+    L.stats = s->d_stats;
+    e = sg::launch_trace_fp32(L, dev_tree(s), r, n, st);
     if (e != cudaSuccess) return cuda_fail(e, "stats launch");
     unsigned long long h[2] = {0, 0};
     if ((e = cudaMemcpyAsync(h, s->d_stats, sizeof(h), cudaMemcpyDeviceToHost, st)) != cudaSuccess ||
@@ -416,6 +436,24 @@ sg_status sg_trace_closest_host(const sg_scene* s, const float* rays8, int64_t n
 
 sg_status sg_trace_any_host(const sg_scene* s, const float* rays8, int64_t n, uint8_t* occluded) {
     return host_trace(s, rays8, n, nullptr, nullptr, nullptr, nullptr, occluded, true);
+}
+
+sg_status sg_scene_set_tuning(sg_scene* s, const sg_trace_tuning* t) {
+    if (!s || !t) return fail(SG_ERR_INVALID_ARGUMENT, "NULL argument");
+    if (t->schedule != SG_SCHEDULE_THREAD_PER_RAY && t->schedule != SG_SCHEDULE_PERSISTENT)
+        return fail(SG_ERR_INVALID_ARGUMENT, "unknown schedule");
+    if (t->refill_threshold < 1 || t->refill_threshold > 32)
+        return fail(SG_ERR_INVALID_ARGUMENT, "refill_threshold must be 1..32");
+    s->tuning.schedule = t->schedule;
+    s->tuning.refill_threshold = t->refill_threshold;
+    return SG_OK;
+}
+
+sg_status sg_scene_get_tuning(const sg_scene* s, sg_trace_tuning* t) {
+    if (!s || !t) return fail(SG_ERR_INVALID_ARGUMENT, "NULL argument");
+    t->schedule = s->tuning.schedule;
+    t->refill_threshold = s->tuning.refill_threshold;
+    return SG_OK;
 }
 
 const char* sg_last_error(void) { return g_last_error.c_str(); }

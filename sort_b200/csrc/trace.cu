@@ -1,6 +1,6 @@
 // Closest-hit and any-hit traversal of SORT-topology wide BVHs on sm_100a.
 //
-// One ray per thread. The traversal restates Fbvh::GetIntersect
+// The per-ray traversal restates Fbvh::GetIntersect
 // (accel/fast_bvh.hpp:305-504, SIMD branch):
 //   * root slab test against the enlarged scene box (scalar Intersect);
 //   * a stack of (node, entry distance) pairs; a popped entry is skipped when
@@ -8,12 +8,21 @@
 //   * a leaf tests its triangles in SIMD-lane packing order and keeps a hit only
 //     when strictly nearer (simd/simd_triangle.h:359-369), so the first of equal
 //     distances wins;
-//   * an interior node's hit children are pushed so the nearest pops first; equal
-//     distances pop the higher child slot first (the 1-, 2- and >=3-hit cases of
-//     lines 416-455 all reduce to that order);
+//   * an interior node's hit children are visited nearest first; equal distances
+//     visit the higher child slot first (the 1-, 2- and >=3-hit cases of lines
+//     416-455 all reduce to that order);
 //   * any-hit returns at the first triangle hit (opaque early exit, 362-373).
 // With FP32 child boxes and the same rounding, hits, distances and barycentrics
 // are bit-identical to SORT's.
+//
+// GPU-side choices that leave that order intact:
+//   * the entry SORT would pop right after pushing a node's children (the
+//     nearest) stays in registers and is descended into directly;
+//   * leaf triangles are fetched two at a time (the triangle array carries one
+//     padding slot), so the second's loads overlap the first's test;
+//   * two schedules: one ray per thread for the whole launch, or persistent
+//     warps in which a lane whose ray finished takes the next ray of its warp's
+//     range, so warps stay full instead of idling on their slowest ray.
 #include <cuda_runtime.h>
 
 #include "trace_common.cuh"
@@ -57,16 +66,214 @@ __device__ __forceinline__ void load_node(const float4* __restrict__ nodes, int3
     }
 }
 
-// STATS adds SORT's traversal counters (accel/fast_bvh.hpp:50-96): interior
-// nodes box-tested, and primitives tested counted per leaf entered
-// (sIntersectionTest += pri_cnt), accumulated into stats[0] / stats[1].
-//
-// Two GPU-side changes leave SORT's visit order intact:
-//   * the entry SORT would pop right after pushing an interior node's children
-//     (the nearest one) is kept in registers and descended into directly; only
-//     the others go to the stack, so a descent costs no stack round trip;
-//   * leaf triangles are fetched two at a time (the triangle array carries one
-//     padding slot), so the loads of the second overlap the test of the first.
+// One ray's traversal state. STATS adds SORT's traversal counters
+// (accel/fast_bvh.hpp:50-96): interior nodes box-tested, and primitives tested
+// counted per leaf entered (sIntersectionTest += pri_cnt).
+template <int W, bool ANY, int STACK, bool STATS>
+struct Traversal {
+    RayState r;
+    float best_t, best_u, best_v;
+    int32_t best_prim;
+    int32_t cur;
+    float cur_d;
+    int si;
+    unsigned node_tests, prim_tests;
+    uint2 stk[STACK];
+
+    // Loads ray i and runs the root test; returns false when the ray is already
+    // finished (root miss or empty tree).
+    __device__ __forceinline__ bool start(const DevTree& tr, const DevRays& rays, int64_t i) {
+        r.o[0] = rays.ox[i];
+        r.o[1] = rays.oy[i];
+        r.o[2] = rays.oz[i];
+        r.d[0] = rays.dx[i];
+        r.d[1] = rays.dy[i];
+        r.d[2] = rays.dz[i];
+        r.tmin = rays.tmin[i];
+        r.tmax = rays.tmax[i];
+        ray_setup(r);
+        best_t = FLT_MAX;
+        best_u = best_v = 0.0f;
+        best_prim = -1;
+        node_tests = prim_tests = 0;
+        si = 0;
+        const float f0 = root_intersect(r, tr.box_lo, tr.box_hi);
+        cur = tr.root;
+        cur_d = f0;
+        return f0 >= 0.0f && tr.root != kEmpty;
+    }
+
+    __device__ __forceinline__ void finish(int64_t i, int32_t* __restrict__ prim_out, float* __restrict__ t_out,
+                                           float* __restrict__ u_out, float* __restrict__ v_out,
+                                           uint8_t* __restrict__ occ_out, unsigned long long* __restrict__ stats) {
+        if (STATS) {
+            atomicAdd(stats, (unsigned long long)node_tests);
+            atomicAdd(stats + 1, (unsigned long long)prim_tests);
+        }
+        if (ANY) {
+            occ_out[i] = best_prim >= 0 ? 1 : 0;
+        } else {
+            prim_out[i] = best_prim;
+            t_out[i] = best_prim >= 0 ? best_t : FLT_MAX;
+            if (u_out) u_out[i] = best_prim >= 0 ? best_u : 0.0f;
+            if (v_out) v_out[i] = best_prim >= 0 ? best_v : 0.0f;
+        }
+    }
+
+    // Processes the entry `cur` (a leaf, an interior node, or a culled entry).
+    // Returns true when the ray is finished.
+    __device__ __forceinline__ bool step(const DevTree& tr, int* __restrict__ err) {
+        bool descend = false;
+        if (!(best_t < cur_d)) {  // fast_bvh.hpp:343: skip when the hit is nearer than the entry
+            if (cur < 0) {
+                if (leaf(tr)) return true;
+            } else {
+                if (si + W > STACK) {  // cannot happen when STACK >= depth*(W-1)+1; reported, never overrun
+                    atomicOr(err, 1);
+                    return true;
+                }
+                descend = interior(tr);
+            }
+        }
+        if (!descend) {
+            if (si == 0) return true;
+            const uint2 e = stk[--si];
+            cur = (int32_t)e.x;
+            cur_d = __uint_as_float(e.y);
+        }
+        return false;
+    }
+
+    // Leaf: triangles in leaf order; returns true on an any-hit early exit.
+    __device__ __forceinline__ bool leaf(const DevTree& tr) {
+        int64_t s = (int64_t)((uint32_t)cur & 0x7fffffffu);
+        unsigned tested = 0;
+        bool found = false;
+        for (;;) {
+            const float4* q = tr.tris + 3 * s;
+            const float4 a0 = __ldg(q), b0 = __ldg(q + 1), c0 = __ldg(q + 2);
+            const float4 a1 = __ldg(q + 3), b1 = __ldg(q + 4), c1 = __ldg(q + 5);
+            float t, u, v;
+            ++tested;
+            if (tri_test(r, a0, b0, c0, t, u, v) && t < best_t) {
+                best_t = t;
+                best_u = u;
+                best_v = v;
+                best_prim = __float_as_int(a0.w);
+                if (ANY) {
+                    found = true;
+                    break;
+                }
+            }
+            if (__float_as_int(b0.w)) break;
+            ++tested;
+            if (tri_test(r, a1, b1, c1, t, u, v) && t < best_t) {
+                best_t = t;
+                best_u = u;
+                best_v = v;
+                best_prim = __float_as_int(a1.w);
+                if (ANY) {
+                    ++s;
+                    found = true;
+                    break;
+                }
+            }
+            if (__float_as_int(b1.w)) break;
+            s += 2;
+        }
+        if (STATS) {
+            if (ANY && found)  // whole leaf, as SORT counts it
+                for (int64_t q = s; !__float_as_int(__ldg(tr.tris + 3 * q + 1).w); ++q) ++tested;
+            prim_tests += tested;
+        }
+        return ANY && found;
+    }
+
+    // Interior node: box-test the children, push all hits but the nearest and
+    // descend into that one. Returns false when no child is hit.
+    __device__ __forceinline__ bool interior(const DevTree& tr) {
+        NodeData<W> nd;
+        load_node<W>(tr.nodes, cur, nd);
+        if (STATS) ++node_tests;
+        float d[W];
+        unsigned mask = 0;
+#pragma unroll
+        for (int j = 0; j < W; ++j) {
+            const bool hit = slab(r, nd.lo[0][j], nd.hi[0][j], nd.lo[1][j], nd.hi[1][j], nd.lo[2][j], nd.hi[2][j], d[j]);
+            if (hit && nd.ch[j] != kEmpty) mask |= 1u << j;
+        }
+        const int cnt = __popc(mask);
+        if (cnt == 0) return false;
+        if (cnt == 1) {
+#pragma unroll
+            for (int j = 0; j < W; ++j)
+                if (mask & (1u << j)) {
+                    cur = nd.ch[j];
+                    cur_d = d[j];
+                }
+            return true;
+        }
+        if (cnt == 2) {
+            // SORT pushes the far one first when t0 < t1, else the second slot
+            // last; the one it would pop next is descended into.
+            int32_t c0 = 0, c1 = 0;
+            float t0 = 0.0f, t1 = 0.0f;
+            bool first = true;
+#pragma unroll
+            for (int j = 0; j < W; ++j) {
+                if (mask & (1u << j)) {
+                    if (first) {
+                        c0 = nd.ch[j];
+                        t0 = d[j];
+                        first = false;
+                    } else {
+                        c1 = nd.ch[j];
+                        t1 = d[j];
+                    }
+                }
+            }
+            if (t0 < t1) {
+                stk[si++] = make_uint2((uint32_t)c1, __float_as_uint(t1));
+                cur = c0;
+                cur_d = t0;
+            } else {
+                stk[si++] = make_uint2((uint32_t)c0, __float_as_uint(t0));
+                cur = c1;
+                cur_d = t1;
+            }
+            return true;
+        }
+        // >= 3 hits: SORT's selection loop (fast_bvh.hpp:438-453) pushes by
+        // decreasing distance, ties lowest slot first, only distances > -1; the
+        // last one it pushes is descended into instead.
+        unsigned left = 0;
+#pragma unroll
+        for (int j = 0; j < W; ++j) left |= (((mask >> j) & 1u) && d[j] > -1.0f) ? (1u << j) : 0u;
+        if (left == 0) return false;
+        for (;;) {
+            float best = -1.0f;
+            int32_t ref = 0;
+            unsigned pick = 0;
+#pragma unroll
+            for (int j = 0; j < W; ++j) {
+                if ((left & (1u << j)) && d[j] > best) {
+                    best = d[j];
+                    ref = nd.ch[j];
+                    pick = 1u << j;
+                }
+            }
+            left &= ~pick;
+            if (left == 0) {
+                cur = ref;
+                cur_d = best;
+                return true;
+            }
+            stk[si++] = make_uint2((uint32_t)ref, __float_as_uint(best));
+        }
+    }
+};
+
+// One ray per thread for the whole launch.
 template <int W, bool ANY, int STACK, bool STATS>
 __global__ void __launch_bounds__(128) k_trace_fp32(DevTree tr, DevRays rays, int64_t n, int32_t* __restrict__ prim_out,
                                                     float* __restrict__ t_out, float* __restrict__ u_out,
@@ -74,218 +281,108 @@ __global__ void __launch_bounds__(128) k_trace_fp32(DevTree tr, DevRays rays, in
                                                     int* __restrict__ err, unsigned long long* __restrict__ stats) {
     const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
+    Traversal<W, ANY, STACK, STATS> tv;
+    if (tv.start(tr, rays, i))
+        while (!tv.step(tr, err)) {
+        }
+    tv.finish(i, prim_out, t_out, u_out, v_out, occ_out, stats);
+}
 
-    RayState r;
-    r.o[0] = rays.ox[i];
-    r.o[1] = rays.oy[i];
-    r.o[2] = rays.oz[i];
-    r.d[0] = rays.dx[i];
-    r.d[1] = rays.dy[i];
-    r.d[2] = rays.dz[i];
-    r.tmin = rays.tmin[i];
-    r.tmax = rays.tmax[i];
-    ray_setup(r);
-
-    float best_t = FLT_MAX, best_u = 0.0f, best_v = 0.0f;
-    int32_t best_prim = -1;
-    unsigned node_tests = 0, prim_tests = 0;
-
-    const float f0 = root_intersect(r, tr.box_lo, tr.box_hi);
-    if (f0 >= 0.0f && tr.root != kEmpty) {
-        uint2 stk[STACK];
-        int si = 0;
-        int32_t cur = tr.root;
-        float cur_d = f0;
-        bool done = false;
+// Persistent warps: warp w owns rays [w*chunk, (w+1)*chunk). A lane whose ray
+// finished takes the next unassigned ray of that range once at least `refill`
+// lanes of the warp are idle, so the warp keeps issuing for full lanes.
+template <int W, bool ANY, int STACK, bool STATS>
+__global__ void __launch_bounds__(128) k_trace_fp32_persistent(DevTree tr, DevRays rays, int64_t n, int64_t chunk,
+                                                               int refill, int32_t* __restrict__ prim_out,
+                                                               float* __restrict__ t_out, float* __restrict__ u_out,
+                                                               float* __restrict__ v_out, uint8_t* __restrict__ occ_out,
+                                                               int* __restrict__ err,
+                                                               unsigned long long* __restrict__ stats) {
+    const unsigned lane = threadIdx.x & 31u;
+    const int64_t warp = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    int64_t next = warp * chunk;
+    const int64_t end = min(n, next + chunk);
+    const unsigned lt_mask = (1u << lane) - 1u;
+    Traversal<W, ANY, STACK, STATS> tv;
+    bool alive = false;
+    int64_t ray = -1;
+    for (;;) {
+        // Refill idle lanes from the warp's range (warp-uniform bookkeeping).
         for (;;) {
-            bool descend = false;
-            if (!(best_t < cur_d)) {  // fast_bvh.hpp:343: skip when the hit is nearer than the entry
-                if (cur < 0) {
-                    int64_t s = (int64_t)((uint32_t)cur & 0x7fffffffu);
-                    unsigned tested = 0;
-                    for (;;) {
-                        const float4* q = tr.tris + 3 * s;
-                        const float4 a0 = __ldg(q), b0 = __ldg(q + 1), c0 = __ldg(q + 2);
-                        const float4 a1 = __ldg(q + 3), b1 = __ldg(q + 4), c1 = __ldg(q + 5);
-                        float t, u, v;
-                        ++tested;
-                        if (tri_test(r, a0, b0, c0, t, u, v) && t < best_t) {
-                            best_t = t;
-                            best_u = u;
-                            best_v = v;
-                            best_prim = __float_as_int(a0.w);
-                            if (ANY) {
-                                done = true;
-                                break;
-                            }
-                        }
-                        if (__float_as_int(b0.w)) break;
-                        ++tested;
-                        if (tri_test(r, a1, b1, c1, t, u, v) && t < best_t) {
-                            best_t = t;
-                            best_u = u;
-                            best_v = v;
-                            best_prim = __float_as_int(a1.w);
-                            if (ANY) {
-                                ++s;
-                                done = true;
-                                break;
-                            }
-                        }
-                        if (__float_as_int(b1.w)) break;
-                        s += 2;
-                    }
-                    if (STATS) {
-                        if (ANY && done)  // whole leaf, as SORT counts it
-                            for (int64_t q = s; !__float_as_int(__ldg(tr.tris + 3 * q + 1).w); ++q) ++tested;
-                        prim_tests += tested;
-                    }
-                    if (ANY && done) break;
-                } else {
-                    if (si + W > STACK) {  // cannot happen when STACK >= depth*(W-1)+1; reported, never overrun
-                        atomicOr(err, 1);
-                        break;
-                    }
-                    NodeData<W> nd;
-                    load_node<W>(tr.nodes, cur, nd);
-                    if (STATS) ++node_tests;
-                    float d[W];
-                    unsigned mask = 0;
-#pragma unroll
-                    for (int j = 0; j < W; ++j) {
-                        const bool hit =
-                            slab(r, nd.lo[0][j], nd.hi[0][j], nd.lo[1][j], nd.hi[1][j], nd.lo[2][j], nd.hi[2][j], d[j]);
-                        if (hit && nd.ch[j] != kEmpty) mask |= 1u << j;
-                    }
-                    const int cnt = __popc(mask);
-                    if (cnt == 1) {
-#pragma unroll
-                        for (int j = 0; j < W; ++j)
-                            if (mask & (1u << j)) {
-                                cur = nd.ch[j];
-                                cur_d = d[j];
-                            }
-                        descend = true;
-                    } else if (cnt == 2) {
-                        // SORT pushes the far one first (t0 < t1) or the second slot last
-                        // (otherwise); the one it would pop next is descended into.
-                        int32_t c0 = 0, c1 = 0;
-                        float t0 = 0.0f, t1 = 0.0f;
-                        bool first = true;
-#pragma unroll
-                        for (int j = 0; j < W; ++j) {
-                            if (mask & (1u << j)) {
-                                if (first) {
-                                    c0 = nd.ch[j];
-                                    t0 = d[j];
-                                    first = false;
-                                } else {
-                                    c1 = nd.ch[j];
-                                    t1 = d[j];
-                                }
-                            }
-                        }
-                        if (t0 < t1) {
-                            stk[si++] = make_uint2((uint32_t)c1, __float_as_uint(t1));
-                            cur = c0;
-                            cur_d = t0;
-                        } else {
-                            stk[si++] = make_uint2((uint32_t)c0, __float_as_uint(t0));
-                            cur = c1;
-                            cur_d = t1;
-                        }
-                        descend = true;
-                    } else if (cnt > 2) {
-                        // Selection by decreasing distance, ties lowest slot first; only
-                        // entries with distance > -1 take part (fast_bvh.hpp:438-453).
-                        int count = 0;
-#pragma unroll
-                        for (int j = 0; j < W; ++j) count += ((mask & (1u << j)) && d[j] > -1.0f) ? 1 : 0;
-#pragma unroll
-                        for (int j = 0; j < W; ++j) {
-                            const bool hj = (mask & (1u << j)) && d[j] > -1.0f;
-                            int rank = 0;
-#pragma unroll
-                            for (int k = 0; k < W; ++k) {
-                                const bool hk = (mask & (1u << k)) && d[k] > -1.0f;
-                                rank += (hk && (d[k] > d[j] || (d[k] == d[j] && k < j))) ? 1 : 0;
-                            }
-                            if (hj) {
-                                if (rank == count - 1) {
-                                    cur = nd.ch[j];
-                                    cur_d = d[j];
-                                } else {
-                                    stk[si + rank] = make_uint2((uint32_t)nd.ch[j], __float_as_uint(d[j]));
-                                }
-                            }
-                        }
-                        if (count > 0) {
-                            si += count - 1;
-                            descend = true;
-                        }
-                    }
+            const unsigned idle = __ballot_sync(0xffffffffu, !alive);
+            if (idle == 0 || next >= end) break;
+            if (!alive) {
+                const int64_t idx = next + __popc(idle & lt_mask);
+                if (idx < end) {
+                    ray = idx;
+                    alive = tv.start(tr, rays, idx);
+                    if (!alive) tv.finish(idx, prim_out, t_out, u_out, v_out, occ_out, stats);
                 }
             }
-            if (!descend) {
-                if (si == 0) break;
-                const uint2 e = stk[--si];
-                cur = (int32_t)e.x;
-                cur_d = __uint_as_float(e.y);
-            }
+            next += __popc(idle);
         }
-    }
-
-    if (STATS) {
-        atomicAdd(stats, (unsigned long long)node_tests);
-        atomicAdd(stats + 1, (unsigned long long)prim_tests);
-    }
-    if (ANY) {
-        occ_out[i] = best_prim >= 0 ? 1 : 0;
-    } else {
-        prim_out[i] = best_prim;
-        t_out[i] = best_prim >= 0 ? best_t : FLT_MAX;
-        if (u_out) u_out[i] = best_prim >= 0 ? best_u : 0.0f;
-        if (v_out) v_out[i] = best_prim >= 0 ? best_v : 0.0f;
+        if (__ballot_sync(0xffffffffu, alive) == 0) break;  // range drained, all lanes done
+        // Traverse until enough lanes are idle to be worth refilling.
+        for (;;) {
+            if (alive && tv.step(tr, err)) {
+                tv.finish(ray, prim_out, t_out, u_out, v_out, occ_out, stats);
+                alive = false;
+            }
+            const unsigned busy = __ballot_sync(0xffffffffu, alive);
+            if (busy == 0) break;
+            if (next < end && 32 - __popc(busy) >= refill) break;
+        }
     }
 }
 
-template <int W, bool ANY, bool STATS>
-static cudaError_t launch_w(const DevTree& tr, const DevRays& rays, int64_t n, int stack_need, int32_t* prim, float* t,
-                            float* u, float* v, uint8_t* occ, int* err, unsigned long long* stats, cudaStream_t s) {
+template <int W, bool ANY, int STACK, bool STATS>
+static cudaError_t launch_stack(const TraceLaunch& L, const DevTree& tr, const DevRays& rays, int64_t n,
+                                cudaStream_t s) {
     const int threads = 128;
-    const int64_t blocks = (n + threads - 1) / threads;
-    if (stack_need <= 64)
-        k_trace_fp32<W, ANY, 64, STATS><<<(unsigned)blocks, threads, 0, s>>>(tr, rays, n, prim, t, u, v, occ, err, stats);
-    else if (stack_need <= 128)
-        k_trace_fp32<W, ANY, 128, STATS><<<(unsigned)blocks, threads, 0, s>>>(tr, rays, n, prim, t, u, v, occ, err, stats);
-    else if (stack_need <= 256)
-        k_trace_fp32<W, ANY, 256, STATS><<<(unsigned)blocks, threads, 0, s>>>(tr, rays, n, prim, t, u, v, occ, err, stats);
-    else
-        return cudaErrorInvalidValue;
+    if (L.tuning.schedule == kSchedulePersistent) {
+        int dev = 0, sms = 0, blocks_per_sm = 0;
+        cudaGetDevice(&dev);
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks_per_sm, k_trace_fp32_persistent<W, ANY, STACK, STATS>,
+                                                      threads, 0);
+        if (blocks_per_sm < 1) blocks_per_sm = 1;
+        if (sms < 1) sms = 1;
+        const int64_t warps_avail = (int64_t)sms * blocks_per_sm * (threads / 32);
+        int64_t chunk = (n + warps_avail - 1) / warps_avail;
+        if (chunk < 32) chunk = 32;
+        const int64_t warps = (n + chunk - 1) / chunk;
+        const int64_t blocks = (warps * 32 + threads - 1) / threads;
+        const int refill = L.tuning.refill_threshold < 1 ? 1 : (L.tuning.refill_threshold > 32 ? 32 : L.tuning.refill_threshold);
+        k_trace_fp32_persistent<W, ANY, STACK, STATS><<<(unsigned)blocks, threads, 0, s>>>(
+            tr, rays, n, chunk, refill, L.prim, L.t, L.u, L.v, L.occ, L.err, L.stats);
+    } else {
+        const int64_t blocks = (n + threads - 1) / threads;
+        k_trace_fp32<W, ANY, STACK, STATS><<<(unsigned)blocks, threads, 0, s>>>(tr, rays, n, L.prim, L.t, L.u, L.v,
+                                                                                L.occ, L.err, L.stats);
+    }
     return cudaGetLastError();
 }
 
+template <int W, bool ANY, bool STATS>
+static cudaError_t launch_w(const TraceLaunch& L, const DevTree& tr, const DevRays& rays, int64_t n, cudaStream_t s) {
+    if (L.stack_need <= 64) return launch_stack<W, ANY, 64, STATS>(L, tr, rays, n, s);
+    if (L.stack_need <= 128) return launch_stack<W, ANY, 128, STATS>(L, tr, rays, n, s);
+    if (L.stack_need <= 256) return launch_stack<W, ANY, 256, STATS>(L, tr, rays, n, s);
+    return cudaErrorInvalidValue;
+}
+
 template <bool STATS>
-static cudaError_t launch_any_width(int width, bool any, const DevTree& tr, const DevRays& rays, int64_t n,
-                                    int stack_need, int32_t* prim, float* t, float* u, float* v, uint8_t* occ, int* err,
-                                    unsigned long long* stats, cudaStream_t s) {
+static cudaError_t launch_any_width(const TraceLaunch& L, const DevTree& tr, const DevRays& rays, int64_t n,
+                                    cudaStream_t s) {
     if (n <= 0) return cudaSuccess;
-    if (width == 8)
-        return any ? launch_w<8, true, STATS>(tr, rays, n, stack_need, prim, t, u, v, occ, err, stats, s)
-                   : launch_w<8, false, STATS>(tr, rays, n, stack_need, prim, t, u, v, occ, err, stats, s);
-    return any ? launch_w<4, true, STATS>(tr, rays, n, stack_need, prim, t, u, v, occ, err, stats, s)
-               : launch_w<4, false, STATS>(tr, rays, n, stack_need, prim, t, u, v, occ, err, stats, s);
+    if (L.width == 8)
+        return L.any ? launch_w<8, true, STATS>(L, tr, rays, n, s) : launch_w<8, false, STATS>(L, tr, rays, n, s);
+    return L.any ? launch_w<4, true, STATS>(L, tr, rays, n, s) : launch_w<4, false, STATS>(L, tr, rays, n, s);
 }
 
-cudaError_t launch_trace_fp32(int width, bool any, const DevTree& tr, const DevRays& rays, int64_t n, int stack_need,
-                              int32_t* prim, float* t, float* u, float* v, uint8_t* occ, int* err, cudaStream_t s) {
-    return launch_any_width<false>(width, any, tr, rays, n, stack_need, prim, t, u, v, occ, err, nullptr, s);
-}
-
-cudaError_t launch_trace_fp32_stats(int width, bool any, const DevTree& tr, const DevRays& rays, int64_t n,
-                                    int stack_need, int32_t* prim, float* t, float* u, float* v, uint8_t* occ,
-                                    int* err, unsigned long long* stats, cudaStream_t s) {
-    return launch_any_width<true>(width, any, tr, rays, n, stack_need, prim, t, u, v, occ, err, stats, s);
+cudaError_t launch_trace_fp32(const TraceLaunch& L, const DevTree& tr, const DevRays& rays, int64_t n,
+                              cudaStream_t s) {
+    return L.stats ? launch_any_width<true>(L, tr, rays, n, s) : launch_any_width<false>(L, tr, rays, n, s);
 }
 
 }  // namespace sg

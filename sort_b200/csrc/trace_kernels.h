@@ -9,13 +9,29 @@
 
 namespace sg {
 
-// stack_need = depth * (width - 1) + 1, the deepest the traversal stack can grow.
-cudaError_t launch_trace_fp32(int width, bool any, const DevTree& tr, const DevRays& rays, int64_t n, int stack_need,
-                              int32_t* prim, float* t, float* u, float* v, uint8_t* occ, int* err, cudaStream_t s);
-// Same traversal, also accumulating SORT's counters into stats[0] (interior
-// nodes tested) and stats[1] (primitives tested).
-cudaError_t launch_trace_fp32_stats(int width, bool any, const DevTree& tr, const DevRays& rays, int64_t n,
-                                    int stack_need, int32_t* prim, float* t, float* u, float* v, uint8_t* occ,
-                                    int* err, unsigned long long* stats, cudaStream_t s);
+constexpr int kScheduleThreadPerRay = 0;  // one ray per thread for the whole launch
+constexpr int kSchedulePersistent = 1;    // persistent warps refilling idle lanes
+
+struct TraceTuning {
+    int schedule = kSchedulePersistent;
+    int refill_threshold = 8;  // idle lanes of a warp that trigger a refill (1..32)
+};
+
+struct TraceLaunch {
+    int width = 8;
+    bool any = false;
+    int stack_need = 1;  // depth * (width - 1) + 1, the deepest the stack can grow
+    TraceTuning tuning;
+    int32_t* prim = nullptr;
+    float* t = nullptr;
+    float* u = nullptr;
+    float* v = nullptr;
+    uint8_t* occ = nullptr;
+    int* err = nullptr;
+    unsigned long long* stats = nullptr;  // non-null: also accumulate SORT's traversal counters
+};
+
+cudaError_t launch_trace_fp32(const TraceLaunch& L, const DevTree& tr, const DevRays& rays, int64_t n,
+                              cudaStream_t s);
 
 }  // namespace sg

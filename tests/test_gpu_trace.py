@@ -166,3 +166,23 @@ def test_gpu_trace_stats_match_oracle_counters(port, width):
     ref = port.build(tri, width)
     for any_hit in (False, True):
         assert acc.TraceStats(d, any_hit) == port.count(ref, rays, any_hit)
+
+
+@pytest.mark.parametrize("width", [4, 8])
+def test_gpu_schedules_give_identical_results(port, width):
+    """The launch schedule (thread per ray, persistent warps with any refill
+    threshold) never changes a result."""
+    from sort_b200 import scenes
+    tri = scenes.sphere_field(32, 3, seed=15)
+    rays = np.concatenate([scenes.camera_rays(200, 200, seed=16), scenes.random_rays(60_000, seed=17)], axis=1)
+    acc = accel(width)
+    acc.Build(tri)
+    ref = port.build(tri, width)
+    rp, rt, ru, rv = ref.closest(rays)
+    ro = ref.any(rays)
+    for schedule, refill in ((0, 1), (1, 1), (1, 8), (1, 16), (1, 32)):
+        acc.SetTuning(schedule, refill)
+        assert acc.GetTuning() == {"schedule": schedule, "refill_threshold": refill}
+        prim, t, u, v, occ = run_device(acc, rays)
+        assert np.array_equal(prim, rp) and same_bits(t, rt) and same_bits(u, ru) and same_bits(v, rv)
+        assert np.array_equal(occ, ro)
