@@ -5,6 +5,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <atomic>
 #include <cfloat>
 #include <chrono>
 #include <cstdio>
@@ -57,6 +58,12 @@ struct sg_scene {
     float4* d_tris = nullptr;
     int* d_err = nullptr;
     unsigned long long* d_stats = nullptr;
+    // Ray counters of the persistent schedule: each launch zeroes and uses the
+    // next slot, so up to kCounterSlots launches on this scene may be in flight
+    // on different streams at once.
+    static constexpr int kCounterSlots = 64;
+    unsigned long long* d_counters = nullptr;
+    std::atomic<unsigned> next_counter{0};
     int64_t device_bytes = 0;
     double build_seconds = 0.0;
     // Scratch for the host-buffer entry points, grown on demand.
@@ -108,6 +115,8 @@ sg_status upload(sg_scene* s, const float* tri, int64_t ntri) {
     if (e != cudaSuccess) return e == cudaErrorMemoryAllocation ? fail(SG_ERR_OUT_OF_MEMORY, "cudaMalloc(triangles) failed")
                                                                  : cuda_fail(e, "cudaMalloc(triangles)");
     if ((e = cudaMalloc(&s->d_err, sizeof(int))) != cudaSuccess) return cuda_fail(e, "cudaMalloc(status)");
+    if ((e = cudaMalloc(&s->d_counters, sg_scene::kCounterSlots * sizeof(unsigned long long))) != cudaSuccess)
+        return cuda_fail(e, "cudaMalloc(counters)");
     if ((e = cudaMemcpy(s->d_nodes, nodes.data(), nb, cudaMemcpyHostToDevice)) != cudaSuccess)
         return cuda_fail(e, "upload nodes");
     if ((e = cudaMemcpy(s->d_tris, tris.data(), tb, cudaMemcpyHostToDevice)) != cudaSuccess)
@@ -124,6 +133,7 @@ void release(sg_scene* s) {
     if (s->d_tris) cudaFree(s->d_tris);
     if (s->d_err) cudaFree(s->d_err);
     if (s->d_stats) cudaFree(s->d_stats);
+    if (s->d_counters) cudaFree(s->d_counters);
     if (s->d_scratch) cudaFree(s->d_scratch);
     if (s->stream) cudaStreamDestroy(s->stream);
     delete s;
@@ -139,6 +149,12 @@ sg::DevTree dev_tree(const sg_scene* s) {
         d.box_hi[k] = s->tree.scene.mx[k];
     }
     return d;
+}
+
+unsigned long long* next_counter(const sg_scene* cs) {
+    sg_scene* s = const_cast<sg_scene*>(cs);
+    const unsigned k = s->next_counter.fetch_add(1, std::memory_order_relaxed) % sg_scene::kCounterSlots;
+    return s->d_counters + k;
 }
 
 sg_status check_status_word(const sg_scene* s, cudaStream_t st) {
@@ -311,6 +327,7 @@ static sg_status trace_common(const sg_scene* s, const sg_rays* rays, int64_t n,
         L.v = hits->v;
     }
     L.err = s->d_err;
+    L.counter = next_counter(s);
     const cudaError_t e = sg::launch_trace_fp32(L, dev_tree(s), r, n, st);
     if (e != cudaSuccess) return cuda_fail(e, "traversal launch");
     return SG_OK;
@@ -418,6 +435,7 @@ sg_status sg_trace_stats(const sg_scene* cs, const sg_rays* rays, int64_t n, int
     L.occ = reinterpret_cast<uint8_t*>(out);
     L.err = s->d_err;
     L.stats = s->d_stats;
+    L.counter = next_counter(s);
     e = sg::launch_trace_fp32(L, dev_tree(s), r, n, st);
     if (e != cudaSuccess) return cuda_fail(e, "stats launch");
     unsigned long long h[2] = {0, 0};

@@ -21,8 +21,8 @@
 //   * leaf triangles are fetched two at a time (the triangle array carries one
 //     padding slot), so the second's loads overlap the first's test;
 //   * two schedules: one ray per thread for the whole launch, or persistent
-//     warps in which a lane whose ray finished takes the next ray of its warp's
-//     range, so warps stay full instead of idling on their slowest ray.
+//     warps in which a lane whose ray finished takes the next ray of the batch,
+//     so warps stay full instead of idling on their slowest ray.
 #include <cuda_runtime.h>
 
 #include "trace_common.cuh"
@@ -288,40 +288,44 @@ __global__ void __launch_bounds__(128) k_trace_fp32(DevTree tr, DevRays rays, in
     tv.finish(i, prim_out, t_out, u_out, v_out, occ_out, stats);
 }
 
-// Persistent warps: warp w owns rays [w*chunk, (w+1)*chunk). A lane whose ray
-// finished takes the next unassigned ray of that range once at least `refill`
-// lanes of the warp are idle, so the warp keeps issuing for full lanes.
+// Persistent warps: a lane whose ray finished takes the next ray in batch order
+// once at least `refill` lanes of its warp are idle; the warp's leader claims
+// those rays from a launch-wide counter, so the whole GPU still advances
+// through the batch in order (neighbouring rays share tree nodes in L1/L2).
 template <int W, bool ANY, int STACK, bool STATS>
-__global__ void __launch_bounds__(128) k_trace_fp32_persistent(DevTree tr, DevRays rays, int64_t n, int64_t chunk,
-                                                               int refill, int32_t* __restrict__ prim_out,
-                                                               float* __restrict__ t_out, float* __restrict__ u_out,
-                                                               float* __restrict__ v_out, uint8_t* __restrict__ occ_out,
-                                                               int* __restrict__ err,
+__global__ void __launch_bounds__(128) k_trace_fp32_persistent(DevTree tr, DevRays rays, int64_t n,
+                                                               unsigned long long* __restrict__ counter, int refill,
+                                                               int32_t* __restrict__ prim_out, float* __restrict__ t_out,
+                                                               float* __restrict__ u_out, float* __restrict__ v_out,
+                                                               uint8_t* __restrict__ occ_out, int* __restrict__ err,
                                                                unsigned long long* __restrict__ stats) {
     const unsigned lane = threadIdx.x & 31u;
-    const int64_t warp = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-    int64_t next = warp * chunk;
-    const int64_t end = min(n, next + chunk);
     const unsigned lt_mask = (1u << lane) - 1u;
     Traversal<W, ANY, STACK, STATS> tv;
     bool alive = false;
+    bool drained = false;  // warp-uniform: the counter has passed n
     int64_t ray = -1;
     for (;;) {
-        // Refill idle lanes from the warp's range (warp-uniform bookkeeping).
-        for (;;) {
-            const unsigned idle = __ballot_sync(0xffffffffu, !alive);
-            if (idle == 0 || next >= end) break;
+        const unsigned idle = __ballot_sync(0xffffffffu, !alive);
+        if (idle != 0 && !drained) {
+            unsigned long long base = 0;
+            if (lane == 0) base = atomicAdd(counter, (unsigned long long)__popc(idle));
+            base = __shfl_sync(0xffffffffu, base, 0);
+            if ((int64_t)base >= n) drained = true;
             if (!alive) {
-                const int64_t idx = next + __popc(idle & lt_mask);
-                if (idx < end) {
+                const int64_t idx = (int64_t)base + __popc(idle & lt_mask);
+                if (idx < n) {
                     ray = idx;
                     alive = tv.start(tr, rays, idx);
                     if (!alive) tv.finish(idx, prim_out, t_out, u_out, v_out, occ_out, stats);
                 }
             }
-            next += __popc(idle);
         }
-        if (__ballot_sync(0xffffffffu, alive) == 0) break;  // range drained, all lanes done
+        const unsigned busy0 = __ballot_sync(0xffffffffu, alive);
+        if (busy0 == 0) {
+            if (drained) break;
+            continue;
+        }
         // Traverse until enough lanes are idle to be worth refilling.
         for (;;) {
             if (alive && tv.step(tr, err)) {
@@ -330,7 +334,7 @@ __global__ void __launch_bounds__(128) k_trace_fp32_persistent(DevTree tr, DevRa
             }
             const unsigned busy = __ballot_sync(0xffffffffu, alive);
             if (busy == 0) break;
-            if (next < end && 32 - __popc(busy) >= refill) break;
+            if (!drained && 32 - __popc(busy) >= refill) break;
         }
     }
 }
@@ -347,14 +351,14 @@ static cudaError_t launch_stack(const TraceLaunch& L, const DevTree& tr, const D
                                                       threads, 0);
         if (blocks_per_sm < 1) blocks_per_sm = 1;
         if (sms < 1) sms = 1;
-        const int64_t warps_avail = (int64_t)sms * blocks_per_sm * (threads / 32);
-        int64_t chunk = (n + warps_avail - 1) / warps_avail;
-        if (chunk < 32) chunk = 32;
-        const int64_t warps = (n + chunk - 1) / chunk;
-        const int64_t blocks = (warps * 32 + threads - 1) / threads;
+        int64_t blocks = (int64_t)sms * blocks_per_sm;
+        const int64_t needed = (n + threads - 1) / threads;
+        if (blocks > needed) blocks = needed;
         const int refill = L.tuning.refill_threshold < 1 ? 1 : (L.tuning.refill_threshold > 32 ? 32 : L.tuning.refill_threshold);
+        cudaError_t e = cudaMemsetAsync(L.counter, 0, sizeof(unsigned long long), s);
+        if (e != cudaSuccess) return e;
         k_trace_fp32_persistent<W, ANY, STACK, STATS><<<(unsigned)blocks, threads, 0, s>>>(
-            tr, rays, n, chunk, refill, L.prim, L.t, L.u, L.v, L.occ, L.err, L.stats);
+            tr, rays, n, L.counter, refill, L.prim, L.t, L.u, L.v, L.occ, L.err, L.stats);
     } else {
         const int64_t blocks = (n + threads - 1) / threads;
         k_trace_fp32<W, ANY, STACK, STATS><<<(unsigned)blocks, threads, 0, s>>>(tr, rays, n, L.prim, L.t, L.u, L.v,

@@ -29,6 +29,7 @@ struct TraceLaunch {
     uint8_t* occ = nullptr;
     int* err = nullptr;
     unsigned long long* stats = nullptr;  // non-null: also accumulate SORT's traversal counters
+    unsigned long long* counter = nullptr;  // persistent schedule: ray counter, zeroed on the stream first
 };
 
 cudaError_t launch_trace_fp32(const TraceLaunch& L, const DevTree& tr, const DevRays& rays, int64_t n,
