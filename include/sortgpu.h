@@ -120,7 +120,8 @@ typedef struct {
 /* Traversal launch schedule (results never depend on it). */
 typedef enum {
     SG_SCHEDULE_THREAD_PER_RAY = 0, /* one ray per thread for the whole launch */
-    SG_SCHEDULE_PERSISTENT = 1      /* persistent warps; a finished lane takes its warp's next ray */
+    SG_SCHEDULE_PERSISTENT = 1,     /* persistent warps; a finished lane takes the batch's next ray */
+    SG_SCHEDULE_COOPERATIVE = 2     /* W lanes per ray: one child box / one triangle per lane */
 } sg_schedule;
 
 typedef struct {
