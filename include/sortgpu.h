@@ -120,8 +120,7 @@ typedef struct {
 /* Traversal launch schedule (results never depend on it). */
 typedef enum {
     SG_SCHEDULE_THREAD_PER_RAY = 0, /* one ray per thread for the whole launch */
-    SG_SCHEDULE_PERSISTENT = 1,     /* persistent warps; a finished lane takes the batch's next ray */
-    SG_SCHEDULE_COOPERATIVE = 2     /* W lanes per ray: one child box / one triangle per lane */
+    SG_SCHEDULE_PERSISTENT = 1      /* persistent warps; a finished lane takes the batch's next ray */
 } sg_schedule;
 
 typedef struct {

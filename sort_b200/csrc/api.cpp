@@ -82,17 +82,16 @@ sg_status upload(sg_scene* s, const float* tri, int64_t ntri) {
     const int64_t nn = t.interior();
     std::vector<float4> nodes(size_t(std::max<int64_t>(nn, 1)) * f4);
     std::memset(nodes.data(), 0, nodes.size() * sizeof(float4));
+    const int Q = W / 4;  // float4 per plane
     for (int64_t k = 0; k < nn; ++k) {
-        for (int j = 0; j < W; ++j) {
-            float* lo = reinterpret_cast<float*>(&nodes[size_t(k) * f4 + 2 * j]);
-            float* hi = lo + 4;
-            for (int a = 0; a < 3; ++a) {
-                lo[a] = t.lo[(size_t(k) * 3 + a) * W + j];
-                hi[a] = t.hi[(size_t(k) * 3 + a) * W + j];
+        float* base = reinterpret_cast<float*>(&nodes[size_t(k) * f4]);
+        for (int a = 0; a < 3; ++a)
+            for (int j = 0; j < W; ++j) {
+                base[(2 * a) * Q * 4 + j] = t.lo[(size_t(k) * 3 + a) * W + j];
+                base[(2 * a + 1) * Q * 4 + j] = t.hi[(size_t(k) * 3 + a) * W + j];
             }
-            const int32_t ref = t.child[size_t(k) * W + j];
-            std::memcpy(&lo[3], &ref, 4);
-        }
+        int32_t* ch = reinterpret_cast<int32_t*>(base + 6 * Q * 4);
+        for (int j = 0; j < W; ++j) ch[j] = t.child[size_t(k) * W + j];
     }
     std::vector<float4> tris(size_t(ntri + sg::kPadSlots) * 3);
     std::memset(tris.data(), 0, tris.size() * sizeof(float4));
@@ -458,8 +457,7 @@ sg_status sg_trace_any_host(const sg_scene* s, const float* rays8, int64_t n, ui
 
 sg_status sg_scene_set_tuning(sg_scene* s, const sg_trace_tuning* t) {
     if (!s || !t) return fail(SG_ERR_INVALID_ARGUMENT, "NULL argument");
-    if (t->schedule != SG_SCHEDULE_THREAD_PER_RAY && t->schedule != SG_SCHEDULE_PERSISTENT &&
-        t->schedule != SG_SCHEDULE_COOPERATIVE)
+    if (t->schedule != SG_SCHEDULE_THREAD_PER_RAY && t->schedule != SG_SCHEDULE_PERSISTENT)
         return fail(SG_ERR_INVALID_ARGUMENT, "unknown schedule");
     if (t->refill_threshold < 1 || t->refill_threshold > 32)
         return fail(SG_ERR_INVALID_ARGUMENT, "refill_threshold must be 1..32");

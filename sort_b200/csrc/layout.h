@@ -7,11 +7,12 @@
 
 namespace sg {
 
-// Interior node, FP32 child boxes, child-major: child j of node k occupies
-// float4 [k*kF4 + 2j] = {lo_x, lo_y, lo_z, child reference bits} and
-// float4 [k*kF4 + 2j + 1] = {hi_x, hi_y, hi_z, 0}. A node is 2*W float4:
-// 256 B for W = 8, 128 B for W = 4. One lane can fetch one child with two
-// 128-bit loads; W lanes fetch a whole node in one coalesced sweep.
+// Interior node, FP32 child boxes, plane-major (structure of arrays):
+//   W = 8: 14 float4 = 224 B: lo_x[0:4], lo_x[4:8], hi_x[0:4], hi_x[4:8],
+//          lo_y.., hi_y.., lo_z.., hi_z.., child[0:4], child[4:8];
+//   W = 4:  8 float4 = 128 B: lo_x, hi_x, lo_y, hi_y, lo_z, hi_z, child[0:4],
+//          and 16 B of padding.
+// A thread reads a node with 14 (7) 128-bit loads covering 7 (4) sectors.
 //
 // Child reference: >= 0 interior node index; bit 31 set: leaf whose first
 // triangle slot is the low 31 bits; -1: empty slot (SORT's unused SIMD lane,
@@ -19,11 +20,17 @@ namespace sg {
 //
 // Triangles: 3 float4 per leaf slot, slots in leaf order:
 //   {v0.xyz, primitive index bits}, {v1.xyz, last-in-leaf flag bits}, {v2.xyz, 0}.
-// kPadSlots zero slots follow the last one so a kernel may fetch up to 8 slots
-// past any leaf start without leaving the allocation.
+// kPadSlots zero slots follow the last one so a kernel may fetch slots past a
+// leaf's last one without leaving the allocation.
 template <int W>
-struct NodeShape {
-    static constexpr int kF4 = 2 * W;
+struct NodeShape;
+template <>
+struct NodeShape<8> {
+    static constexpr int kF4 = 14;
+};
+template <>
+struct NodeShape<4> {
+    static constexpr int kF4 = 8;
 };
 
 constexpr int32_t kEmpty = -1;

@@ -39,17 +39,30 @@ struct NodeData {
 template <int W>
 __device__ __forceinline__ void load_node(const float4* __restrict__ nodes, int32_t ref, NodeData<W>& nd) {
     const float4* p = nodes + (size_t)ref * NodeShape<W>::kF4;
+    constexpr int Q = W / 4;  // float4 per plane
 #pragma unroll
-    for (int j = 0; j < W; ++j) {
-        const float4 l = __ldg(p + 2 * j);
-        const float4 h = __ldg(p + 2 * j + 1);
-        nd.lo[0][j] = l.x;
-        nd.lo[1][j] = l.y;
-        nd.lo[2][j] = l.z;
-        nd.ch[j] = __float_as_int(l.w);
-        nd.hi[0][j] = h.x;
-        nd.hi[1][j] = h.y;
-        nd.hi[2][j] = h.z;
+    for (int a = 0; a < 3; ++a) {
+#pragma unroll
+        for (int q = 0; q < Q; ++q) {
+            const float4 l = __ldg(p + (2 * a) * Q + q);
+            const float4 h = __ldg(p + (2 * a + 1) * Q + q);
+            nd.lo[a][4 * q + 0] = l.x;
+            nd.lo[a][4 * q + 1] = l.y;
+            nd.lo[a][4 * q + 2] = l.z;
+            nd.lo[a][4 * q + 3] = l.w;
+            nd.hi[a][4 * q + 0] = h.x;
+            nd.hi[a][4 * q + 1] = h.y;
+            nd.hi[a][4 * q + 2] = h.z;
+            nd.hi[a][4 * q + 3] = h.w;
+        }
+    }
+#pragma unroll
+    for (int q = 0; q < Q; ++q) {
+        const int4 c = __ldg(reinterpret_cast<const int4*>(p + 6 * Q + q));
+        nd.ch[4 * q + 0] = c.x;
+        nd.ch[4 * q + 1] = c.y;
+        nd.ch[4 * q + 2] = c.z;
+        nd.ch[4 * q + 3] = c.w;
     }
 }
 
@@ -373,7 +386,6 @@ static cudaError_t launch_any_width(const TraceLaunch& L, const DevTree& tr, con
 
 cudaError_t launch_trace_fp32(const TraceLaunch& L, const DevTree& tr, const DevRays& rays, int64_t n,
                               cudaStream_t s) {
-    if (L.tuning.schedule == kScheduleCooperative) return launch_trace_fp32_coop(L, tr, rays, n, s);
     return L.stats ? launch_any_width<true>(L, tr, rays, n, s) : launch_any_width<false>(L, tr, rays, n, s);
 }
 

@@ -86,26 +86,33 @@ __device__ __forceinline__ float root_intersect(const RayState& r, const float* 
 // One lane of IntersectBBox_SIMD (simd/simd_bbox.h:62-85). Returns whether the
 // slab interval is non-empty; d gets fmin on a hit and -1 on a miss, as SORT's
 // simd_pick_ps leaves it (validity of the slot is checked by the caller).
+//
+// SORT's lanes use _mm_min_ps / _mm_max_ps (a < b ? a : b); here fminf / fmaxf,
+// one instruction each. The two agree in value whenever neither input is NaN,
+// and no input is: 1/d and -o/d are finite after the |d| >= 1e-5 clamp, box
+// bounds are finite or +-FLT_MAX, so every t is finite or +-inf (rays must be
+// finite, as SORT assumes). Where they may differ — which of +0 and -0 an equal
+// pair returns — nothing downstream looks: entry distances are only compared.
 __device__ __forceinline__ bool slab(const RayState& r, float lx, float hx, float ly, float hy, float lz, float hz,
                                      float& d) {
     float f_min = r.tmin, f_max = r.tmax;
     {
         const float t1 = __fadd_rn(r.od[0], __fmul_rn(r.rcp[0], hx));
         const float t2 = __fadd_rn(r.od[0], __fmul_rn(r.rcp[0], lx));
-        f_min = sse_max(f_min, sse_min(t1, t2));
-        f_max = sse_min(f_max, sse_max(t1, t2));
+        f_min = fmaxf(f_min, fminf(t1, t2));
+        f_max = fminf(f_max, fmaxf(t1, t2));
     }
     {
         const float t1 = __fadd_rn(r.od[1], __fmul_rn(r.rcp[1], hy));
         const float t2 = __fadd_rn(r.od[1], __fmul_rn(r.rcp[1], ly));
-        f_min = sse_max(f_min, sse_min(t1, t2));
-        f_max = sse_min(f_max, sse_max(t1, t2));
+        f_min = fmaxf(f_min, fminf(t1, t2));
+        f_max = fminf(f_max, fmaxf(t1, t2));
     }
     {
         const float t1 = __fadd_rn(r.od[2], __fmul_rn(r.rcp[2], hz));
         const float t2 = __fadd_rn(r.od[2], __fmul_rn(r.rcp[2], lz));
-        f_min = sse_max(f_min, sse_min(t1, t2));
-        f_max = sse_min(f_max, sse_max(t1, t2));
+        f_min = fmaxf(f_min, fminf(t1, t2));
+        f_max = fminf(f_max, fmaxf(t1, t2));
     }
     const bool hit = f_min <= f_max;
     d = hit ? f_min : -1.0f;

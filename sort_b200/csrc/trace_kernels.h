@@ -11,10 +11,9 @@ namespace sg {
 
 constexpr int kScheduleThreadPerRay = 0;  // one ray per thread for the whole launch
 constexpr int kSchedulePersistent = 1;    // persistent warps refilling idle lanes
-constexpr int kScheduleCooperative = 2;   // W lanes per ray (one child / one triangle per lane)
 
 struct TraceTuning {
-    int schedule = kScheduleCooperative;
+    int schedule = kScheduleThreadPerRay;
     int refill_threshold = 8;  // idle lanes of a warp that trigger a refill (1..32)
 };
 
@@ -35,8 +34,4 @@ struct TraceLaunch {
 
 cudaError_t launch_trace_fp32(const TraceLaunch& L, const DevTree& tr, const DevRays& rays, int64_t n,
                               cudaStream_t s);
-// The cooperative schedule (trace_coop.cu); launch_trace_fp32 dispatches to it.
-cudaError_t launch_trace_fp32_coop(const TraceLaunch& L, const DevTree& tr, const DevRays& rays, int64_t n,
-                                   cudaStream_t s);
-
 }  // namespace sg
