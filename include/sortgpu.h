@@ -120,7 +120,9 @@ typedef struct {
 /* Traversal launch schedule (results never depend on it). */
 typedef enum {
     SG_SCHEDULE_THREAD_PER_RAY = 0, /* one ray per thread for the whole launch */
-    SG_SCHEDULE_PERSISTENT = 1      /* persistent warps; a finished lane takes the batch's next ray */
+    SG_SCHEDULE_PERSISTENT = 1,     /* persistent warps; a finished lane takes the batch's next ray */
+    SG_SCHEDULE_WHILE_WHILE = 2,    /* each warp alternates an interior phase and a leaf phase */
+    SG_SCHEDULE_SPECULATIVE = 3     /* while-while; lanes keep descending past their first leaf */
 } sg_schedule;
 
 typedef struct {

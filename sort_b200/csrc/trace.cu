@@ -126,7 +126,7 @@ struct Traversal {
         bool descend = false;
         if (!(best_t < cur_d)) {  // fast_bvh.hpp:343: skip when the hit is nearer than the entry
             if (cur < 0) {
-                if (leaf(tr)) return true;
+                if (leaf(tr, cur)) return true;
             } else {
                 if (si + W > STACK) {  // cannot happen when STACK >= depth*(W-1)+1; reported, never overrun
                     atomicOr(err, 1);
@@ -145,8 +145,8 @@ struct Traversal {
     }
 
     // Leaf: triangles in leaf order; returns true on an any-hit early exit.
-    __device__ __forceinline__ bool leaf(const DevTree& tr) {
-        int64_t s = (int64_t)((uint32_t)cur & 0x7fffffffu);
+    __device__ __forceinline__ bool leaf(const DevTree& tr, int32_t ref) {
+        int64_t s = (int64_t)((uint32_t)ref & 0x7fffffffu);
         unsigned tested = 0;
         bool found = false;
         for (;;) {
@@ -273,6 +273,82 @@ struct Traversal {
     }
 };
 
+// While-while traversal, one ray per thread: the warp alternates an interior
+// phase and a leaf phase, so lanes walking interior nodes and lanes testing
+// triangles do not split every iteration.
+//
+// Interior phase: a lane pops / descends until its entry is an un-culled leaf,
+// which it parks as its pending leaf. With SPEC, a lane that already holds a
+// pending leaf keeps descending (speculatively) while other lanes still lack
+// one, and stops at its next leaf. Leaf phase: every lane with a pending leaf
+// re-checks the cull against its current hit and tests the leaf.
+//
+// Leaves are tested in SORT's order and each is culled with the hit found so
+// far, so results are SORT's: a speculative visit only sees interior nodes
+// that SORT visits too, or that SORT culls — and then every leaf below is culled
+// here as well, because a child's entry distance is never below its parent's
+// (each slab bound of a child lies inside the parent's, and the rounded
+// t = -o/d + b/d is monotonic in b).
+template <int W, bool ANY, int STACK, bool SPEC>
+__global__ void __launch_bounds__(128) k_trace_fp32_ww(DevTree tr, DevRays rays, int64_t n,
+                                                       int32_t* __restrict__ prim_out, float* __restrict__ t_out,
+                                                       float* __restrict__ u_out, float* __restrict__ v_out,
+                                                       uint8_t* __restrict__ occ_out, int* __restrict__ err) {
+    const int64_t i0 = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    const bool valid = i0 < n;
+    const int64_t i = valid ? i0 : n - 1;  // lanes past the batch end idle through the loop
+    Traversal<W, ANY, STACK, false> tv;
+    const bool started = tv.start(tr, rays, i);
+    bool have = valid && started;  // `cur` holds an entry still to process
+    bool pend = false;             // a parked leaf is waiting for the leaf phase
+    int32_t lf = 0;
+    float lf_d = 0.0f;
+    while (__any_sync(0xffffffffu, have || pend)) {
+        // Interior phase (warp-uniform loop; each lane does at most one unit per pass).
+        for (;;) {
+            const bool needs = have && !pend;
+            const bool spec = SPEC && have && pend;
+            if (!__any_sync(0xffffffffu, needs)) break;
+            if (needs || spec) {
+                bool descend = false;
+                bool blocked = false;
+                if (!(tv.best_t < tv.cur_d)) {
+                    if (tv.cur < 0) {
+                        if (!pend) {
+                            lf = tv.cur;
+                            lf_d = tv.cur_d;
+                            pend = true;
+                        } else {
+                            blocked = true;  // second leaf: wait for the leaf phase
+                        }
+                    } else if (tv.si + W > STACK) {  // cannot happen when STACK >= depth*(W-1)+1
+                        atomicOr(err, 1);
+                        have = false;
+                        blocked = true;
+                    } else {
+                        descend = tv.interior(tr);
+                    }
+                }
+                if (!descend && !blocked) {
+                    if (tv.si == 0) {
+                        have = false;
+                    } else {
+                        const uint2 e = tv.stk[--tv.si];
+                        tv.cur = (int32_t)e.x;
+                        tv.cur_d = __uint_as_float(e.y);
+                    }
+                }
+            }
+        }
+        // Leaf phase.
+        if (pend) {
+            pend = false;
+            if (!(tv.best_t < lf_d) && tv.leaf(tr, lf)) have = false;  // any-hit: done
+        }
+    }
+    if (valid) tv.finish(i, prim_out, t_out, u_out, v_out, occ_out, nullptr);
+}
+
 // One ray per thread for the whole launch.
 template <int W, bool ANY, int STACK, bool STATS>
 __global__ void __launch_bounds__(128) k_trace_fp32(DevTree tr, DevRays rays, int64_t n, int32_t* __restrict__ prim_out,
@@ -343,6 +419,18 @@ template <int W, bool ANY, int STACK, bool STATS>
 static cudaError_t launch_stack(const TraceLaunch& L, const DevTree& tr, const DevRays& rays, int64_t n,
                                 cudaStream_t s) {
     const int threads = 128;
+    // Counting launches keep the one-entry-per-step loop, whose interior-node
+    // visits are exactly SORT's (speculation visits extra ones).
+    if (!STATS && (L.tuning.schedule == kScheduleWhileWhile || L.tuning.schedule == kScheduleSpeculative)) {
+        const int64_t blocks = (n + threads - 1) / threads;
+        if (L.tuning.schedule == kScheduleSpeculative)
+            k_trace_fp32_ww<W, ANY, STACK, true><<<(unsigned)blocks, threads, 0, s>>>(tr, rays, n, L.prim, L.t, L.u,
+                                                                                      L.v, L.occ, L.err);
+        else
+            k_trace_fp32_ww<W, ANY, STACK, false><<<(unsigned)blocks, threads, 0, s>>>(tr, rays, n, L.prim, L.t, L.u,
+                                                                                       L.v, L.occ, L.err);
+        return cudaGetLastError();
+    }
     if (L.tuning.schedule == kSchedulePersistent) {
         int dev = 0, sms = 0, blocks_per_sm = 0;
         cudaGetDevice(&dev);

@@ -11,6 +11,8 @@ namespace sg {
 
 constexpr int kScheduleThreadPerRay = 0;  // one ray per thread for the whole launch
 constexpr int kSchedulePersistent = 1;    // persistent warps refilling idle lanes
+constexpr int kScheduleWhileWhile = 2;    // warp alternates interior and leaf phases
+constexpr int kScheduleSpeculative = 3;   // while-while, lanes keep descending past their first leaf
 
 struct TraceTuning {
     int schedule = kScheduleThreadPerRay;

@@ -180,7 +180,7 @@ def test_gpu_schedules_give_identical_results(port, width):
     ref = port.build(tri, width)
     rp, rt, ru, rv = ref.closest(rays)
     ro = ref.any(rays)
-    for schedule, refill in ((0, 1), (1, 1), (1, 8), (1, 16), (1, 32)):
+    for schedule, refill in ((0, 1), (1, 1), (1, 8), (1, 16), (1, 32), (2, 8), (3, 8)):
         acc.SetTuning(schedule, refill)
         assert acc.GetTuning() == {"schedule": schedule, "refill_threshold": refill}
         prim, t, u, v, occ = run_device(acc, rays)
