@@ -69,6 +69,7 @@ _SIGNATURES = {
                                       ctypes.POINTER(_i64), _vp]),
     "sg_trace_closest_host": (ctypes.c_int, [_vp, _vp, _i64, _vp, _vp, _vp, _vp]),
     "sg_trace_any_host": (ctypes.c_int, [_vp, _vp, _i64, _vp]),
+    "sg_trace_closest_host_static": (ctypes.c_int, [_vp, _vp, _i64, _vp, _vp, _vp, _vp, _vp]),
     "sg_last_error": (ctypes.c_char_p, []),
     "sg_version": (ctypes.c_char_p, []),
 }

@@ -167,6 +167,27 @@ sg_status check_status_word(const sg_scene* s, cudaStream_t st) {
 
 }  // namespace
 
+namespace sg {
+
+sg_status set_error(sg_status s, const char* msg) { return fail(s, msg); }
+
+sg_status scene_launch(const sg_scene* s, bool any, TraceLaunch* L, DevTree* tree, int* device) {
+    if (!s || !L || !tree || !device) return fail(SG_ERR_INVALID_ARGUMENT, "NULL argument");
+    L->width = s->width;
+    L->any = any;
+    L->stack_need = s->stack_need;
+    L->tuning = s->tuning;
+    L->err = s->d_err;
+    L->counter = next_counter(s);
+    *tree = dev_tree(s);
+    *device = s->device;
+    return SG_OK;
+}
+
+sg_status scene_status(const sg_scene* s, cudaStream_t st) { return check_status_word(s, st); }
+
+}  // namespace sg
+
 extern "C" {
 
 void sg_default_build_opts(sg_build_opts* o) {

@@ -1,0 +1,22 @@
+// Internal (not exported) access to a scene's launch parameters, for entry
+// points implemented outside api.cpp.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include "sortgpu.h"
+#include "trace_kernels.h"
+
+namespace sg {
+
+// Records msg for sg_last_error() and returns s.
+sg_status set_error(sg_status s, const char* msg);
+
+// Fills the launch description (width, stack bound, tuning, status word,
+// persistent-schedule counter slot) and the device tree of scene s.
+sg_status scene_launch(const sg_scene* s, bool any, TraceLaunch* L, DevTree* tree, int* device);
+
+// Synchronises st and reports the traversal status word of scene s.
+sg_status scene_status(const sg_scene* s, cudaStream_t st);
+
+}  // namespace sg
