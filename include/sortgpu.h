@@ -174,6 +174,30 @@ sg_status sg_trace_any_host(const sg_scene* scene, const float* rays8, int64_t n
 sg_status sg_trace_closest_host_static(const sg_scene* scene, const float* rays8, int64_t n, int32_t* prim, float* t,
                                        float* u, float* v, void* stream);
 
+/* ---- Path tracing -------------------------------------------------------
+ * SORT's PathTracing integrator (integrator/pathtracing.cpp:37-258) with its
+ * next-event estimation (integrator/integratormethod.cpp:100-192), Lambert and
+ * GGX-conductor BxDFs and one rectangular AreaLight, run as a wavefront over a
+ * scene built by sg_scene_create; replaces ImageEvaluation's per-pixel loop
+ * (work/image_evaluation/image_evaluation.cpp:210-238) for those materials.
+ *
+ * sg_pt_create: triangles/ntri as given to sg_scene_create (same order);
+ *   mat_of_tri[i] indexes materials (10 floats each: type 0 Lambert with albedo
+ *   r g b; type 1 GGX conductor reflection with eta r g b, k r g b, roughness),
+ *   or is -1 for the light's own surface (the light quad's two triangles, which
+ *   must be in the scene as SORT puts the quad in its accelerator);
+ *   light = centre x y z, size x, size z, intensity r g b of a rectangle facing -y.
+ * sg_pt_render: camera = eye xyz, target xyz, up xyz, vertical fov (degrees);
+ *   writes the mean radiance of spp samples per pixel to `image` (device,
+ *   width*height*3 floats, row-major from the top); max_depth as SORT's
+ *   max_recursive_depth; ordered on `stream`. */
+typedef struct sg_pt_scene sg_pt_scene;
+sg_status sg_pt_create(const sg_scene* scene, const float* triangles, int64_t ntri, const int32_t* mat_of_tri,
+                       const float* materials, int32_t nmat, const float* light, sg_pt_scene** out);
+sg_status sg_pt_render(sg_pt_scene* pt, const float* camera, int32_t width, int32_t height, int32_t spp,
+                       int32_t max_depth, uint64_t seed, float* image, void* stream);
+sg_status sg_pt_destroy(sg_pt_scene* pt);
+
 const char* sg_last_error(void);
 const char* sg_version(void);
 

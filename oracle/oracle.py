@@ -150,3 +150,42 @@ class Reference:
 
     def hardware_threads(self) -> int:
         return int(self.L.sortref_hardware_threads())
+
+
+class RefPathTracer:
+    """SORT's PathTracing::Li over a harness-built scene (oracle/ref/harness_pt.cpp)."""
+
+    def __init__(self):
+        if not reference_available():
+            raise FileNotFoundError(REF_LIB)
+        L = ctypes.CDLL(REF_LIB)
+        L.sortref_pt_scene_create.restype = _vp
+        L.sortref_pt_scene_create.argtypes = [ctypes.c_int, _vp, ctypes.c_int, _vp, ctypes.c_int, _vp, _vp,
+                                              ctypes.c_int, ctypes.c_int]
+        L.sortref_pt_scene_destroy.argtypes = [_vp]
+        L.sortref_pt_render.argtypes = [_vp, ctypes.c_int, _vp, ctypes.c_int, ctypes.c_int, ctypes.c_int,
+                                        ctypes.c_uint32, _vp, ctypes.c_int]
+        self.L = L
+        self.h = None
+
+    def build(self, tri, mat_of_tri, materials, light, width=8, max_depth=16, max_leaf=8):
+        self._keep = [np.ascontiguousarray(tri, np.float32).reshape(-1, 9),
+                      np.ascontiguousarray(mat_of_tri, np.int32), np.ascontiguousarray(materials, np.float32),
+                      np.ascontiguousarray(light, np.float32)]
+        t, m, mats, lt = self._keep
+        self.h = self.L.sortref_pt_scene_create(width, t.ctypes.data, t.shape[0], m.ctypes.data, mats.shape[0],
+                                                mats.ctypes.data, lt.ctypes.data, max_depth, max_leaf)
+        if not self.h:
+            raise ValueError("reference path-tracing scene build failed")
+        return self
+
+    def render(self, camera, width, height, spp, max_depth=5, seed=1, threads=0) -> np.ndarray:
+        cam = np.ascontiguousarray(camera, np.float32)
+        out = np.zeros((height, width, 3), np.float32)
+        self.L.sortref_pt_render(self.h, max_depth, cam.ctypes.data, width, height, spp, seed, out.ctypes.data,
+                                 threads or os.cpu_count())
+        return out
+
+    def __del__(self):
+        if self.h:
+            self.L.sortref_pt_scene_destroy(self.h)

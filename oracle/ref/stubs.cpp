@@ -19,7 +19,6 @@ void Material::BuildMaterial(Tsl_Namespace::ShadingContext*) {}
 
 const MaterialBase* MatManager::CreateMaterialProxy(const MaterialBase& material) { return &material; }
 
-Spectrum MediumStack::Tr(const Ray&, const float, RenderContext&) const { return 1.0f; }
 
 float MediumDensity::Sample(const Point&) const { return 0.0f; }
 void MediumDensity::Serialize(IStreamBase&) {}

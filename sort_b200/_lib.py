@@ -70,6 +70,10 @@ _SIGNATURES = {
     "sg_trace_closest_host": (ctypes.c_int, [_vp, _vp, _i64, _vp, _vp, _vp, _vp]),
     "sg_trace_any_host": (ctypes.c_int, [_vp, _vp, _i64, _vp]),
     "sg_trace_closest_host_static": (ctypes.c_int, [_vp, _vp, _i64, _vp, _vp, _vp, _vp, _vp]),
+    "sg_pt_create": (ctypes.c_int, [_vp, _vp, _i64, _vp, _vp, ctypes.c_int32, _vp, ctypes.POINTER(_vp)]),
+    "sg_pt_render": (ctypes.c_int, [_vp, _vp, ctypes.c_int32, ctypes.c_int32, ctypes.c_int32, ctypes.c_int32,
+                                    ctypes.c_uint64, _vp, _vp]),
+    "sg_pt_destroy": (ctypes.c_int, [_vp]),
     "sg_last_error": (ctypes.c_char_p, []),
     "sg_version": (ctypes.c_char_p, []),
 }

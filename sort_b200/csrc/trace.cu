@@ -349,13 +349,16 @@ __global__ void __launch_bounds__(128) k_trace_fp32_ww(DevTree tr, DevRays rays,
     if (valid) tv.finish(i, prim_out, t_out, u_out, v_out, occ_out, nullptr);
 }
 
-// One ray per thread for the whole launch.
+// One ray per thread for the whole launch. With n_dev set, the batch size is
+// min(n, *n_dev), read on the device (queues whose length only the GPU knows).
 template <int W, bool ANY, int STACK, bool STATS>
 __global__ void __launch_bounds__(128) k_trace_fp32(DevTree tr, DevRays rays, int64_t n, int32_t* __restrict__ prim_out,
                                                     float* __restrict__ t_out, float* __restrict__ u_out,
                                                     float* __restrict__ v_out, uint8_t* __restrict__ occ_out,
-                                                    int* __restrict__ err, unsigned long long* __restrict__ stats) {
+                                                    int* __restrict__ err, unsigned long long* __restrict__ stats,
+                                                    const int* __restrict__ n_dev) {
     const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (n_dev && i >= (int64_t)*n_dev) return;
     if (i >= n) return;
     Traversal<W, ANY, STACK, STATS> tv;
     if (tv.start(tr, rays, i))
@@ -421,7 +424,9 @@ static cudaError_t launch_stack(const TraceLaunch& L, const DevTree& tr, const D
     const int threads = 128;
     // Counting launches keep the one-entry-per-step loop, whose interior-node
     // visits are exactly SORT's (speculation visits extra ones).
-    if (!STATS && (L.tuning.schedule == kScheduleWhileWhile || L.tuning.schedule == kScheduleSpeculative)) {
+    // A device-side batch size is only read by the one-ray-per-thread kernel.
+    if (!STATS && !L.n_dev &&
+        (L.tuning.schedule == kScheduleWhileWhile || L.tuning.schedule == kScheduleSpeculative)) {
         const int64_t blocks = (n + threads - 1) / threads;
         if (L.tuning.schedule == kScheduleSpeculative)
             k_trace_fp32_ww<W, ANY, STACK, true><<<(unsigned)blocks, threads, 0, s>>>(tr, rays, n, L.prim, L.t, L.u,
@@ -431,7 +436,7 @@ static cudaError_t launch_stack(const TraceLaunch& L, const DevTree& tr, const D
                                                                                        L.v, L.occ, L.err);
         return cudaGetLastError();
     }
-    if (L.tuning.schedule == kSchedulePersistent) {
+    if (L.tuning.schedule == kSchedulePersistent && !L.n_dev) {
         int dev = 0, sms = 0, blocks_per_sm = 0;
         cudaGetDevice(&dev);
         cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
@@ -450,7 +455,7 @@ static cudaError_t launch_stack(const TraceLaunch& L, const DevTree& tr, const D
     } else {
         const int64_t blocks = (n + threads - 1) / threads;
         k_trace_fp32<W, ANY, STACK, STATS><<<(unsigned)blocks, threads, 0, s>>>(tr, rays, n, L.prim, L.t, L.u, L.v,
-                                                                                L.occ, L.err, L.stats);
+                                                                                L.occ, L.err, L.stats, L.n_dev);
     }
     return cudaGetLastError();
 }

@@ -45,7 +45,8 @@ def icosphere(level: int) -> tuple[np.ndarray, np.ndarray]:
          (4, 9, 5), (2, 4, 11), (6, 2, 10), (8, 6, 7), (9, 8, 1)]
     verts = np.array(v, dtype=np.float64)
     verts /= np.linalg.norm(verts, axis=1, keepdims=True)
-    faces = np.array(f, dtype=np.int64)
+    # wound so that cross(v2 - v0, v1 - v0) (SORT's geometric normal) points outward
+    faces = np.array(f, dtype=np.int64)[:, [0, 2, 1]]
     for _ in range(level):
         a, b, c = faces[:, 0], faces[:, 1], faces[:, 2]
         edges = np.concatenate([np.stack([a, b], 1), np.stack([b, c], 1), np.stack([c, a], 1)])
@@ -89,8 +90,9 @@ def sphere_field(spheres: int, level: int, seed: int = 1, ground_y: float = -11.
         tri[s] += centres[s]
     tri = tri.reshape(-1, 9)
     g = ground_half
-    ground = np.array([[-g, ground_y, -g, -g, ground_y, g, g, ground_y, g],
-                       [-g, ground_y, -g, g, ground_y, g, g, ground_y, -g]], dtype=np.float64)
+    # wound so that cross(v2 - v0, v1 - v0) points up (+y)
+    ground = np.array([[-g, ground_y, -g, g, ground_y, g, -g, ground_y, g],
+                       [-g, ground_y, -g, g, ground_y, -g, g, ground_y, g]], dtype=np.float64)
     return np.ascontiguousarray(np.concatenate([tri, ground]).astype(np.float32))
 
 
@@ -196,3 +198,75 @@ def random_rays(n: int, seed: int = 3, box: float = 12.0, axis_fraction: float =
     rays[6] = 0.0
     rays[7] = np.where(rng.random(n) < 0.3, rng.uniform(0.5, 30.0, n), FLT_MAX)
     return rays
+
+
+# Conductor Fresnel parameters (eta, k) per RGB channel for the GGX instances.
+CONDUCTORS = {
+    "gold": ((0.143, 0.374, 1.442), (3.983, 2.385, 1.603)),
+    "copper": ((0.200, 0.924, 1.102), (3.912, 2.452, 2.142)),
+    "silver": ((0.155, 0.117, 0.138), (4.828, 3.122, 2.147)),
+    "aluminium": ((1.657, 0.880, 0.521), (9.224, 6.270, 4.837)),
+}
+
+# Material record: 10 floats — type (0 Lambert, 1 GGX conductor reflection),
+# Lambert: albedo r g b; GGX: eta r g b, k r g b, roughness.
+MAT_FLOATS = 10
+
+
+def instance_materials(spheres: int, level: int, seed: int = 5):
+    """Per-instance materials for a sphere_field scene (same sphere count/level):
+    50% Lambert with albedo U(0.2, 0.8) per channel, 50% GGX conductor reflection
+    with roughness U(0.05, 0.5) and (eta, k) from CONDUCTORS; the ground is Lambert
+    0.5. Returns (mat_of_tri int32 (ntri,), materials float32 (nmat, 10))."""
+    rng = np.random.default_rng(seed)
+    names = list(CONDUCTORS)
+    mats = np.zeros((spheres + 1, MAT_FLOATS), np.float32)
+    for s in range(spheres):
+        if rng.random() < 0.5:
+            mats[s, 0] = 0.0
+            mats[s, 1:4] = rng.uniform(0.2, 0.8, 3)
+        else:
+            eta, k = CONDUCTORS[names[rng.integers(len(names))]]
+            mats[s, 0] = 1.0
+            mats[s, 1:4] = eta
+            mats[s, 4:7] = k
+            mats[s, 7] = rng.uniform(0.05, 0.5)
+    mats[spheres, 0] = 0.0
+    mats[spheres, 1:4] = 0.5
+    per_sphere = 20 * 4 ** level
+    mat_of_tri = np.concatenate([np.repeat(np.arange(spheres, dtype=np.int32), per_sphere),
+                                 np.full(2, spheres, np.int32)])
+    return mat_of_tri, mats
+
+
+# The rectangular area light of the path-traced workloads: centre, size x,
+# size z, RGB intensity; it faces -y (SORT's Quad with its +y normal turned down).
+AREA_LIGHT = np.array([0.0, 18.0, 0.0, 8.0, 8.0, 40.0, 40.0, 40.0], np.float32)
+
+# Pinhole camera: eye, target, up, vertical field of view (degrees).
+CAMERA = np.array([0.0, 0.0, 30.0, 0.0, 0.0, 0.0, 0.0, 1.0, 0.0, 45.0], np.float32)
+
+
+def light_triangles(light: np.ndarray) -> np.ndarray:
+    """The area light's rectangle as two triangles whose geometric normal
+    cross(v2 - v0, v1 - v0) points down (-y), as its Quad's normal does."""
+    cx, cy, cz, sx, sz = (float(v) for v in light[:5])
+    hx, hz = sx * 0.5, sz * 0.5
+    a = (cx - hx, cy, cz - hz)
+    b = (cx + hx, cy, cz - hz)
+    c = (cx + hx, cy, cz + hz)
+    d = (cx - hx, cy, cz + hz)
+    return np.array([[*a, *c, *b], [*a, *d, *c]], np.float32)
+
+
+def pt_scene(spheres: int, level: int, seed: int = 1, mat_seed: int = 5, light: np.ndarray | None = None):
+    """Path-tracing workload: (triangles without the light, materials per triangle,
+    material table, light, triangles with the light quad appended, materials per
+    triangle with -1 on the light quad). SORT keeps the light's quad as its own
+    primitive; the GPU engine traces it as its two triangles."""
+    light = AREA_LIGHT if light is None else light
+    tri = sphere_field(spheres, level, seed=seed)
+    mat_of_tri, mats = instance_materials(spheres, level, seed=mat_seed)
+    tri_gpu = np.ascontiguousarray(np.concatenate([tri, light_triangles(light)]))
+    mat_gpu = np.concatenate([mat_of_tri, np.array([-1, -1], np.int32)])
+    return tri, mat_of_tri, mats, light, tri_gpu, mat_gpu

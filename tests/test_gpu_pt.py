@@ -1,0 +1,60 @@
+"""GPU path tracer vs SORT's PathTracing::Li (statistical parity).
+
+SORT seeds its Mersenne Twister from the wall clock, so renders agree in
+distribution only. The bar, at equal sample counts, against SORT's own renders
+of the same scene (tests/golden/pt_spheres.npz, made by make_golden_pt.py):
+  * 4096 spp: RMSE to SORT's converged image at most 1.3x the RMSE between two
+    independent SORT 4096-spp renders, and each channel's mean within 1%;
+  * 16 spp: mean RMSE over 8 seeds within 25% of SORT's own 16-spp RMSE.
+"""
+import numpy as np
+import pytest
+
+from conftest import golden
+
+pytestmark = pytest.mark.gpu
+torch = pytest.importorskip("torch")
+
+
+def rmse(a, b):
+    return float(np.sqrt(np.mean((np.asarray(a, np.float64) - np.asarray(b, np.float64)) ** 2)))
+
+
+@pytest.fixture(scope="module")
+def tracer():
+    assert torch.cuda.is_available(), "GPU test needs a CUDA device"
+    from sort_b200 import scenes
+    from sort_b200.pathtracer import PathTracer
+    z = golden("pt_spheres")
+    _, _, mats, light, tri_gpu, mat_gpu = scenes.pt_scene(int(z["spheres"]), int(z["level"]))
+    pt = PathTracer(tri_gpu, mat_gpu, mats, light)
+    yield pt, z
+    pt.Release()
+
+
+def test_pt_converged_matches_sort(tracer):
+    pt, z = tracer
+    img = pt.Render(z["camera"], int(z["width"]), int(z["height"]), 4096, int(z["depth"]), seed=7).cpu().numpy()
+    conv = z["converged"]
+    assert np.isfinite(img).all()
+    r = rmse(img, conv)
+    assert r <= 1.3 * float(z["rmse_converged_pair"]), (r, float(z["rmse_converged_pair"]))
+    m_gpu, m_ref = img.mean(axis=(0, 1)), conv.mean(axis=(0, 1))
+    assert np.all(np.abs(m_gpu - m_ref) / m_ref < 0.01), (m_gpu, m_ref)
+
+
+def test_pt_16spp_noise_matches_sort(tracer):
+    pt, z = tracer
+    conv = z["converged"]
+    r = [rmse(pt.Render(z["camera"], int(z["width"]), int(z["height"]), 16, int(z["depth"]), seed=50 + k).cpu().numpy(),
+              conv) for k in range(8)]
+    ref = float(np.mean(z["rmse16"]))
+    assert abs(np.mean(r) - ref) <= 0.25 * ref, (np.mean(r), ref)
+
+
+def test_pt_same_seed_same_image(tracer):
+    pt, z = tracer
+    a = pt.Render(z["camera"], 32, 24, 4, 5, seed=9).cpu().numpy()
+    b = pt.Render(z["camera"], 32, 24, 4, 5, seed=9).cpu().numpy()
+    c = pt.Render(z["camera"], 32, 24, 4, 5, seed=10).cpu().numpy()
+    assert np.array_equal(a, b) and not np.array_equal(a, c)
