@@ -314,16 +314,110 @@ def run_ours(args):
         dist.destroy_process_group()
 
 
+PT_W, PT_H, PT_DEPTH = 1920, 1080, 5
+
+
+def pt_config(extra=None):
+    cfg = {
+        "workload": "pathtrace_21m: the incoherent_21m scene with per-sphere materials (50% Lambert albedo "
+                    "U(0.2,0.8), 50% GGX conductor roughness U(0.05,0.5)), one 8x8 area light, 1920x1080, "
+                    "max depth 5, Russian roulette after depth 3, NEE with MIS; one step = one sample per pixel",
+        "nodes": "fp32",
+    }
+    if extra:
+        cfg.update(extra)
+    return cfg
+
+
+def run_pathtrace(args):
+    """Path-traced samples/s (one step = one sample for every pixel of 1920x1080)."""
+    import torch
+
+    from sort_b200 import scenes
+    from sort_b200.pathtracer import PathTracer
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    if args.impl == "reference":
+        if rank != 0:
+            return
+        from oracle.oracle import RefPathTracer, reference_available
+        if not reference_available():
+            print(json.dumps({"impl": "reference", "unavailable": "SORT reference library (oracle/_ref) not built"}))
+            return
+        tri, m, mats, light, _, _ = scenes.pt_scene(SPHERES, LEVEL)
+        ref = RefPathTracer().build(tri, m, mats, light)
+        w, h = 192, 108  # bounded pixel sample of the same camera
+        times = []
+        for k in range(args.warmup + args.steps):
+            t0 = time.perf_counter()
+            ref.render(scenes.CAMERA, w, h, 1, PT_DEPTH, seed=1000 + k)
+            if k >= args.warmup:
+                times.append(time.perf_counter() - t0)
+        value = w * h * len(times) / sum(times) / 1e6
+        out = {"impl": "reference", "metric": "path-traced Msamples/s", "value": round(value, 4),
+               "unit": "Msamples/s", "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+               "ms_per_step": round(1e3 * sum(times) / len(times), 3), "higher_is_better": True, "scaling": "weak",
+               "vs_baseline": None, "dtype": "f32", "data": "synthetic", "config": pt_config({"pixels": w * h}),
+               "cpu_baseline": {"value": round(value, 4), "unit": "Msamples/s", "cores": os.cpu_count(),
+                                "kind": "reference", "sample": f"{w}x{h} pixels, 1 sample each per step"},
+               "e2e": {"value": round(value, 4), "unit": "Msamples/s", "h2d_bytes_per_step": 0,
+                       "d2h_bytes_per_step": 0}, "gpu_launches": 0}
+        print(json.dumps(out))
+        return
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    device = torch.device("cuda", local)
+    _, _, mats, light, tri_gpu, mat_gpu = scenes.pt_scene(SPHERES, LEVEL)
+    pt = PathTracer(tri_gpu, mat_gpu, mats, light, device=local)
+    img = torch.empty((PT_H, PT_W, 3), dtype=torch.float32, device=device)
+    stream = torch.cuda.current_stream(device)
+    pt.Render(scenes.CAMERA, PT_W, PT_H, args.warmup, PT_DEPTH, seed=1, out=img)
+    torch.cuda.synchronize(device)
+    start, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with ClockSampler(local) as clocks:
+        start.record(stream)
+        pt.Render(scenes.CAMERA, PT_W, PT_H, args.steps, PT_DEPTH, seed=2, out=img)
+        end.record(stream)
+        torch.cuda.synchronize(device)
+    ms = start.elapsed_time(end)
+    ext, sh = pt.RayCounts()
+    t0 = time.perf_counter()
+    pt.Render(scenes.CAMERA, PT_W, PT_H, args.steps, PT_DEPTH, seed=3, out=img)
+    host_img = img.cpu()
+    e2e_s = time.perf_counter() - t0
+    samples = PT_W * PT_H * args.steps
+    out = {"metric": "path-traced Msamples/s", "value": round(samples / (ms / 1e3) / 1e6, 3), "unit": "Msamples/s",
+           "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms / args.steps, 3),
+           "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+           "data": "synthetic (seeded procedural scene)",
+           "config": pt_config({"frame_spp_per_s": round(args.steps / (ms / 1e3), 3),
+                                "rays_per_sample": round((ext + sh) / samples, 3),
+                                "extension_rays": ext, "shadow_rays": sh,
+                                "mrays_s": round((ext + sh) / (ms / 1e3) / 1e6, 2)}),
+           "e2e": {"value": round(samples / e2e_s / 1e6, 3), "unit": "Msamples/s", "h2d_bytes_per_step": 0,
+                   "d2h_bytes_per_step": int(host_img.numel() * 4 / args.steps)},
+           "clocks": clocks.summary(), "image_mean": [round(float(v), 5) for v in host_img.mean(dim=(0, 1))],
+           # per sample: generate + per bounce (extend, shade, shadow, resolve, count) + clear and scale
+           "gpu_launches": args.steps * (1 + 5 * PT_DEPTH) + 2}
+    if rank == 0:
+        print(json.dumps(out))
+    pt.Release()
+
+
 def main():
     p = argparse.ArgumentParser()
     p.add_argument("--gpus", type=int, default=1)
     p.add_argument("--steps", type=int, default=200)
     p.add_argument("--warmup", type=int, default=5)
     p.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    p.add_argument("--workload", choices=["closest", "pathtrace"], default="closest")
     p.add_argument("--sample", type=int, default=CPU_SAMPLE)
     p.add_argument("--no-cpu-baseline", action="store_true")
     args = p.parse_args()
-    if args.impl == "reference":
+    if args.workload == "pathtrace":
+        run_pathtrace(args)
+    elif args.impl == "reference":
         run_reference(args)
     else:
         run_ours(args)

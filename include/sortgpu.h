@@ -197,6 +197,10 @@ sg_status sg_pt_create(const sg_scene* scene, const float* triangles, int64_t nt
 sg_status sg_pt_render(sg_pt_scene* pt, const float* camera, int32_t width, int32_t height, int32_t spp,
                        int32_t max_depth, uint64_t seed, float* image, void* stream);
 sg_status sg_pt_destroy(sg_pt_scene* pt);
+/* Rays the last sg_pt_render traced: extension (closest-hit) and shadow
+ * (any-hit) rays; synchronises `stream`. The counterpart of SORT's sRayCount /
+ * sShadowRayCount (accel/accelerator.cpp:21-23). */
+sg_status sg_pt_ray_counts(const sg_pt_scene* pt, int64_t* extension, int64_t* shadow, void* stream);
 
 const char* sg_last_error(void);
 const char* sg_version(void);

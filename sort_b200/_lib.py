@@ -74,6 +74,7 @@ _SIGNATURES = {
     "sg_pt_render": (ctypes.c_int, [_vp, _vp, ctypes.c_int32, ctypes.c_int32, ctypes.c_int32, ctypes.c_int32,
                                     ctypes.c_uint64, _vp, _vp]),
     "sg_pt_destroy": (ctypes.c_int, [_vp]),
+    "sg_pt_ray_counts": (ctypes.c_int, [_vp, ctypes.POINTER(_i64), ctypes.POINTER(_i64), _vp]),
     "sg_last_error": (ctypes.c_char_p, []),
     "sg_version": (ctypes.c_char_p, []),
 }

@@ -429,6 +429,14 @@ __global__ void k_zero(float* __restrict__ image, int n) {
     if (i < n) image[i] = 0.0f;
 }
 
+// Adds this bounce's queue lengths (extension rays, shadow rays) to the totals.
+__global__ void k_count_rays(const int* __restrict__ counters, unsigned long long* __restrict__ totals) {
+    if (threadIdx.x == 0) {
+        totals[0] += (unsigned long long)counters[0];
+        totals[1] += (unsigned long long)counters[2];
+    }
+}
+
 }  // namespace
 }  // namespace sg
 
@@ -442,8 +450,21 @@ struct sg_pt_scene {
     int cap = 0;
     void* d_buf = nullptr;
     size_t buf_bytes = 0;
-    int64_t stats_rays = 0;  // rays traced by the last render (extension + shadow)
+    unsigned long long* d_totals = nullptr;  // rays traced by the last render: extension, shadow
 };
+
+extern "C" sg_status sg_pt_ray_counts(const sg_pt_scene* ps, int64_t* extension, int64_t* shadow, void* stream) {
+    if (!ps || !extension || !shadow) return sg::set_error(SG_ERR_INVALID_ARGUMENT, "NULL argument");
+    *extension = *shadow = 0;
+    if (!ps->d_totals) return SG_OK;
+    unsigned long long h[2] = {0, 0};
+    cudaError_t e = cudaMemcpyAsync(h, ps->d_totals, sizeof(h), cudaMemcpyDeviceToHost, (cudaStream_t)stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize((cudaStream_t)stream);
+    if (e != cudaSuccess) return sg::set_error(SG_ERR_CUDA, cudaGetErrorString(e));
+    *extension = (int64_t)h[0];
+    *shadow = (int64_t)h[1];
+    return SG_OK;
+}
 
 namespace {
 
@@ -590,6 +611,9 @@ extern "C" sg_status sg_pt_render(sg_pt_scene* ps, const float* camera, int32_t 
     uint8_t* occ = (uint8_t*)take(scap);
     float* thr = (float*)take(cap * 12);
     int* counters = (int*)take(16);  // [0] current queue, [1] next queue, [2] shadow queue
+    unsigned long long* totals = (unsigned long long*)take(16);  // rays traced: extension, shadow
+    ps->d_totals = totals;
+    if ((e = cudaMemsetAsync(totals, 0, 16, s)) != cudaSuccess) return pt_fail(e);
 
     // Camera (perspective pinhole, as the oracle harness builds it).
     sg::Cam cam;
@@ -643,6 +667,7 @@ extern "C" sg_status sg_pt_render(sg_pt_scene* ps, const float* camera, int32_t 
             if ((e = sg::launch_trace_fp32(La, tree, sr, (int64_t)scap, s)) != cudaSuccess) return pt_fail(e);
             sg::k_resolve<<<(int)((scap + threads - 1) / threads), threads, 0, s>>>(sq, (int)scap, &counters[2], occ,
                                                                                    image);
+            sg::k_count_rays<<<1, 32, 0, s>>>(counters, totals);
             // the next queue becomes the current one
             if ((e = cudaMemcpyAsync(&counters[0], &counters[1], sizeof(int), cudaMemcpyDeviceToDevice, s)) !=
                 cudaSuccess)

@@ -45,6 +45,14 @@ class PathTracer:
                                             seed, img.data_ptr(), s))
         return img
 
+    def RayCounts(self, stream=None):
+        """(extension rays, shadow rays) traced by the last Render (synchronises)."""
+        import torch
+        a, b = ctypes.c_int64(0), ctypes.c_int64(0)
+        s = stream if stream is not None else torch.cuda.current_stream(torch.device("cuda", self.device)).cuda_stream
+        _lib.check(_lib.load().sg_pt_ray_counts(self._h, ctypes.byref(a), ctypes.byref(b), s))
+        return a.value, b.value
+
     def Release(self):
         if getattr(self, "_h", None) is not None:
             _lib.load().sg_pt_destroy(self._h)
