@@ -589,7 +589,7 @@ extern "C" sg_status sg_pt_render(sg_pt_scene* ps, const float* camera, int32_t 
     auto align = [](size_t x) { return (x + 255) & ~size_t(255); };
     const size_t qbytes = align(cap * 8 * 4) + align(cap * 4);
     const size_t need = 2 * qbytes + align(cap * 4) * 2 + align(scap * 8 * 4) + align(scap * 4) +
-                        align(scap * 3 * 4) + align(scap) + align(cap * 3 * 4) + 256;
+                        align(scap * 3 * 4) + align(scap) + align(cap * 3 * 4) + align(16) + align(16);
     if (ps->buf_bytes < need) {
         if (ps->d_buf) cudaFree(ps->d_buf);
         ps->d_buf = nullptr;
@@ -612,6 +612,7 @@ extern "C" sg_status sg_pt_render(sg_pt_scene* ps, const float* camera, int32_t 
     float* thr = (float*)take(cap * 12);
     int* counters = (int*)take(16);  // [0] current queue, [1] next queue, [2] shadow queue
     unsigned long long* totals = (unsigned long long*)take(16);  // rays traced: extension, shadow
+    if ((size_t)(b - (char*)ps->d_buf) > need) return sg::set_error(SG_ERR_INTERNAL, "render buffer layout overflow");
     ps->d_totals = totals;
     if ((e = cudaMemsetAsync(totals, 0, 16, s)) != cudaSuccess) return pt_fail(e);
 
