@@ -398,8 +398,8 @@ def run_pathtrace(args):
            "e2e": {"value": round(samples / e2e_s / 1e6, 3), "unit": "Msamples/s", "h2d_bytes_per_step": 0,
                    "d2h_bytes_per_step": int(host_img.numel() * 4 / args.steps)},
            "clocks": clocks.summary(), "image_mean": [round(float(v), 5) for v in host_img.mean(dim=(0, 1))],
-           # per sample: generate + per bounce (extend, shade, shadow, resolve, count) + clear and scale
-           "gpu_launches": args.steps * (1 + 5 * PT_DEPTH) + 2}
+           # per sample: generate, flush + per bounce (extend, shade, shadow, resolve, accumulate, count)
+           "gpu_launches": args.steps * (2 + 6 * PT_DEPTH) + 2}
     if rank == 0:
         print(json.dumps(out))
     pt.Release()

@@ -10,7 +10,10 @@
 //            shadow rays and the next rays are appended to compacted queues with
 //            one atomic per warp;
 //   shadow   any-hit traversal of the shadow queue;
-//   resolve  unoccluded shadow contributions are added to the image.
+//   resolve  unoccluded shadow contributions go to their path's two slots, and
+//            are added to the path's radiance in a fixed order; at the end of
+//            the wave each path's radiance is added to its pixel. Every sum has
+//            one writer in a fixed order, so an image is bit-reproducible.
 // Shading follows SORT's ScatteringEvent frame (scatteringevent.cpp:42-59) and
 // BxDFs: Lambert (lambert.cpp:34-38), MicroFacetReflection with GGX and
 // conductor Fresnel (microfacet.cpp:229-356, fresnel.h:119-130); the area light
@@ -283,7 +286,8 @@ __global__ void k_generate(Cam cam, int width, int height, uint2 key, uint32_t s
     const float3 d = normalize3(cam.fwd + cam.right * sx + cam.up * sy);
     put_ray(q.ray, cap, p, cam.eye, d, 0.0f, FLT_MAX);
     q.slot[p] = p;
-    thr[p] = thr[cap + p] = thr[2 * cap + p] = 1.0f;
+    thr[p] = thr[cap + p] = thr[2 * cap + p] = 1.0f;          // throughput
+    thr[3 * cap + p] = thr[4 * cap + p] = thr[5 * cap + p] = 0.0f;  // radiance of this sample
     if (p == 0) *count = width * height;
 }
 
@@ -291,11 +295,13 @@ __global__ void k_shade(PtDev sc, uint2 key, uint32_t sample, int bounce, int ma
                         const int* __restrict__ in_count, const int32_t* __restrict__ hit_prim,
                         const float* __restrict__ hit_t, Queue next, int* __restrict__ next_count, Queue shadow,
                         int shadow_cap, int* __restrict__ shadow_count, float* __restrict__ thr,
-                        float* __restrict__ image) {
+                        float* __restrict__ vis) {
     const int q = blockIdx.x * blockDim.x + threadIdx.x;
     if (q >= *in_count) return;
     const int p = in.slot[q];
     const int prim = hit_prim[q];
+#pragma unroll
+    for (int k = 0; k < 6; ++k) vis[k * cap + p] = 0.0f;  // this bounce's two shadow results
     bool cont = false, s1 = false, s2 = false;
     float3 X = f3(0, 0, 0), wi_next = f3(0, 0, 0), wi1 = f3(0, 0, 0), wi2 = f3(0, 0, 0), c1 = f3(0, 0, 0),
            c2 = f3(0, 0, 0);
@@ -313,9 +319,9 @@ __global__ void k_shade(PtDev sc, uint2 key, uint32_t sample, int bounce, int ma
         const float3 wo_w = -d;
         // Emission only where the camera ray lands (pathtracing.cpp:114-115).
         if (bounce == 0 && mid < 0 && dot3(wo_w, light_normal()) > 0.0f) {
-            atomicAdd(&image[3 * p + 0], Li.x);
-            atomicAdd(&image[3 * p + 1], Li.y);
-            atomicAdd(&image[3 * p + 2], Li.z);
+            thr[3 * cap + p] += Li.x;
+            thr[4 * cap + p] += Li.y;
+            thr[5 * cap + p] += Li.z;
         }
         const Frame fr = make_frame(f3(info.x, info.y, info.z));
         const float3 wo = fr.local(wo_w);
@@ -389,7 +395,7 @@ __global__ void k_shade(PtDev sc, uint2 key, uint32_t sample, int bounce, int ma
     const int i1 = warp_append(shadow_count, s1);
     if (i1 >= 0) {
         put_ray(shadow.ray, shadow_cap, i1, X, wi1, 0.01f, len1 - 0.01f);
-        shadow.slot[i1] = p;
+        shadow.slot[i1] = 2 * p;  // light-sample result
         shadow.contrib[i1] = c1.x;
         shadow.contrib[shadow_cap + i1] = c1.y;
         shadow.contrib[2 * shadow_cap + i1] = c1.z;
@@ -397,7 +403,7 @@ __global__ void k_shade(PtDev sc, uint2 key, uint32_t sample, int bounce, int ma
     const int i2 = warp_append(shadow_count, s2);
     if (i2 >= 0) {
         put_ray(shadow.ray, shadow_cap, i2, X, wi2, 0.001f, t2 - 0.001f);
-        shadow.slot[i2] = p;
+        shadow.slot[i2] = 2 * p + 1;  // BSDF-sample result
         shadow.contrib[i2] = c2.x;
         shadow.contrib[shadow_cap + i2] = c2.y;
         shadow.contrib[2 * shadow_cap + i2] = c2.z;
@@ -409,14 +415,36 @@ __global__ void k_shade(PtDev sc, uint2 key, uint32_t sample, int bounce, int ma
     }
 }
 
+// Unoccluded shadow rays leave their contribution in their path's slot (one
+// writer per slot, so the sums below do not depend on scheduling).
 __global__ void k_resolve(Queue shadow, int shadow_cap, const int* __restrict__ count, const uint8_t* __restrict__ occ,
-                          float* __restrict__ image) {
+                          float* __restrict__ vis, int cap) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= *count || occ[i]) return;
-    const int p = shadow.slot[i];
-    atomicAdd(&image[3 * p + 0], shadow.contrib[i]);
-    atomicAdd(&image[3 * p + 1], shadow.contrib[shadow_cap + i]);
-    atomicAdd(&image[3 * p + 2], shadow.contrib[2 * shadow_cap + i]);
+    const int code = shadow.slot[i];
+    const int p = code >> 1, which = code & 1;
+    vis[(3 * which + 0) * cap + p] = shadow.contrib[i];
+    vis[(3 * which + 1) * cap + p] = shadow.contrib[shadow_cap + i];
+    vis[(3 * which + 2) * cap + p] = shadow.contrib[2 * shadow_cap + i];
+}
+
+// EvaluateDirect's two terms are added to the path's radiance in SORT's order
+// (light sample, then BSDF sample), for every path shaded this bounce.
+__global__ void k_accumulate(Queue in, const int* __restrict__ in_count, const float* __restrict__ vis,
+                             float* __restrict__ thr, int cap) {
+    const int q = blockIdx.x * blockDim.x + threadIdx.x;
+    if (q >= *in_count) return;
+    const int p = in.slot[q];
+#pragma unroll
+    for (int c = 0; c < 3; ++c) thr[(3 + c) * cap + p] += vis[c * cap + p] + vis[(3 + c) * cap + p];
+}
+
+// End of a wave: each pixel's sample radiance goes into the image (one writer).
+__global__ void k_flush(const float* __restrict__ thr, int cap, int n, float* __restrict__ image) {
+    const int p = blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= n) return;
+#pragma unroll
+    for (int c = 0; c < 3; ++c) image[3 * p + c] += thr[(3 + c) * cap + p];
 }
 
 __global__ void k_scale(float* __restrict__ image, int n, float s) {
@@ -589,7 +617,7 @@ extern "C" sg_status sg_pt_render(sg_pt_scene* ps, const float* camera, int32_t 
     auto align = [](size_t x) { return (x + 255) & ~size_t(255); };
     const size_t qbytes = align(cap * 8 * 4) + align(cap * 4);
     const size_t need = 2 * qbytes + align(cap * 4) * 2 + align(scap * 8 * 4) + align(scap * 4) +
-                        align(scap * 3 * 4) + align(scap) + align(cap * 3 * 4) + align(16) + align(16);
+                        align(scap * 3 * 4) + align(scap) + align(cap * 6 * 4) + align(cap * 6 * 4) + align(16) + align(16);
     if (ps->buf_bytes < need) {
         if (ps->d_buf) cudaFree(ps->d_buf);
         ps->d_buf = nullptr;
@@ -609,7 +637,8 @@ extern "C" sg_status sg_pt_render(sg_pt_scene* ps, const float* camera, int32_t 
     float* hit_t = (float*)take(cap * 4);
     sg::Queue sq{(float*)take(scap * 32), (int*)take(scap * 4), (float*)take(scap * 12)};
     uint8_t* occ = (uint8_t*)take(scap);
-    float* thr = (float*)take(cap * 12);
+    float* thr = (float*)take(cap * 24);  // throughput and radiance per path
+    float* vis = (float*)take(cap * 24);  // two shadow results per path
     int* counters = (int*)take(16);  // [0] current queue, [1] next queue, [2] shadow queue
     unsigned long long* totals = (unsigned long long*)take(16);  // rays traced: extension, shadow
     if ((size_t)(b - (char*)ps->d_buf) > need) return sg::set_error(SG_ERR_INTERNAL, "render buffer layout overflow");
@@ -658,7 +687,7 @@ extern "C" sg_status sg_pt_render(sg_pt_scene* ps, const float* camera, int32_t 
             if ((e = cudaMemsetAsync(&counters[1], 0, 2 * sizeof(int), s)) != cudaSuccess) return pt_fail(e);
             sg::k_shade<<<blocks, threads, 0, s>>>(dev, key, (uint32_t)sample, bounce, max_depth, *cur, (int)cap,
                                                    &counters[0], hit_prim, hit_t, *nxt, &counters[1], sq, (int)scap,
-                                                   &counters[2], thr, image);
+                                                   &counters[2], thr, vis);
             sg::DevRays sr{sq.ray,            sq.ray + scap,     sq.ray + 2 * scap, sq.ray + 3 * scap,
                            sq.ray + 4 * scap, sq.ray + 5 * scap, sq.ray + 6 * scap, sq.ray + 7 * scap};
             sg::TraceLaunch La = base;
@@ -667,7 +696,8 @@ extern "C" sg_status sg_pt_render(sg_pt_scene* ps, const float* camera, int32_t 
             La.n_dev = &counters[2];
             if ((e = sg::launch_trace_fp32(La, tree, sr, (int64_t)scap, s)) != cudaSuccess) return pt_fail(e);
             sg::k_resolve<<<(int)((scap + threads - 1) / threads), threads, 0, s>>>(sq, (int)scap, &counters[2], occ,
-                                                                                   image);
+                                                                                   vis, (int)cap);
+            sg::k_accumulate<<<blocks, threads, 0, s>>>(*cur, &counters[0], vis, thr, (int)cap);
             sg::k_count_rays<<<1, 32, 0, s>>>(counters, totals);
             // the next queue becomes the current one
             if ((e = cudaMemcpyAsync(&counters[0], &counters[1], sizeof(int), cudaMemcpyDeviceToDevice, s)) !=
@@ -677,6 +707,7 @@ extern "C" sg_status sg_pt_render(sg_pt_scene* ps, const float* camera, int32_t 
             cur = nxt;
             nxt = t;
         }
+        sg::k_flush<<<blocks, threads, 0, s>>>(thr, (int)cap, P, image);
     }
     sg::k_scale<<<(img_n + threads - 1) / threads, threads, 0, s>>>(image, img_n, 1.0f / (float)spp);
     if ((e = cudaGetLastError()) != cudaSuccess) return pt_fail(e);
