@@ -54,6 +54,19 @@ def workload_config(extra=None):
     return cfg
 
 
+def raycast_config(extra=None):
+    cfg = {
+        "workload": "raycast_82k: 64 level-3 icospheres + ground quad = 81,922 triangles, QBVH (width 4, depth 16, "
+                    "leaf 8), 1,048,576 jittered primary rays (1024x1024 pinhole at (0,0,30), 45 deg) per GPU",
+        "scene_seed": 1,
+        "nodes": "fp32",
+        "l2": "tree (5 MB) is L2-resident by design of this workload; rays 32 MB",
+    }
+    if extra:
+        cfg.update(extra)
+    return cfg
+
+
 class ClockSampler:
     """nvidia-smi clocks / throttle reasons sampled every 200 ms while running."""
 
@@ -115,7 +128,7 @@ def make_rays(acc, tri, rank: int, device):
     return diffuse, shadow
 
 
-def reference_cpu(tri, rays, steps: int, warmup: int, threads: int, sample: int):
+def reference_cpu(tri, rays, steps: int, warmup: int, threads: int, sample: int, width: int = WIDTH):
     """SORT's OBVH on the host cores; returns (Mrays/s, description)."""
     from oracle.oracle import Reference, reference_available
     if not reference_available():
@@ -123,7 +136,7 @@ def reference_cpu(tri, rays, steps: int, warmup: int, threads: int, sample: int)
         impl, kind = Port(), "port"
     else:
         impl, kind = Reference(), "reference"
-    tree = impl.build(tri, WIDTH, DEPTH, LEAF)
+    tree = impl.build(tri, width, DEPTH, LEAF)
     n = rays.shape[1]
     times = []
     for k in range(warmup + steps):
@@ -199,11 +212,25 @@ def run_ours(args):
         if world > 1:
             dist.barrier()
 
-    tri = scenes.sphere_field(SPHERES, LEVEL, seed=1)
-    acc = Obvh(DEPTH, LEAF, device=local)
-    acc.Build(tri)
+    if args.workload == "raycast":
+        # raycast_82k: 64 level-3 icospheres + ground (81,922 triangles) as a QBVH,
+        # 1024x1024 jittered primary rays (closest-hit); shadow rays from their hits.
+        from sort_b200 import Qbvh
+        width = 4
+        tri = scenes.sphere_field(64, 3, seed=1)
+        acc = Qbvh(DEPTH, LEAF, device=local)
+        acc.Build(tri)
+        diffuse = scenes.camera_rays(1024, 1024, seed=7 + rank)
+        h = acc.GetIntersect(torch.from_numpy(diffuse).to(device))
+        _, shadow = scenes.bounce_rays(tri, diffuse, h.prim.cpu().numpy(), h.t.cpu().numpy(), diffuse.shape[1],
+                                       seed=11 + rank)
+    else:
+        width = WIDTH
+        tri = scenes.sphere_field(SPHERES, LEVEL, seed=1)
+        acc = Obvh(DEPTH, LEAF, device=local)
+        acc.Build(tri)
+        diffuse, shadow = make_rays(acc, tri, rank, device)
     info = acc.info()
-    diffuse, shadow = make_rays(acc, tri, rank, device)
     n = diffuse.shape[1]
     d_diff = torch.from_numpy(diffuse).to(device)
     d_shad = torch.from_numpy(shadow).to(device)
@@ -211,8 +238,8 @@ def run_ours(args):
     # SORT's traversal counters on these rays -> algorithmic bytes per ray.
     node_tests, prim_tests = acc.TraceStats(d_diff, False)
     a_nodes, a_prims = acc.TraceStats(d_shad, True)
-    bytes_closest = RAY_IN + HIT_OUT + (node_tests * NODE_BYTES[WIDTH] + prim_tests * TRI_BYTES) / n
-    bytes_any = RAY_IN + 4 + (a_nodes * NODE_BYTES[WIDTH] + a_prims * TRI_BYTES) / n
+    bytes_closest = RAY_IN + HIT_OUT + (node_tests * NODE_BYTES[width] + prim_tests * TRI_BYTES) / n
+    bytes_any = RAY_IN + 4 + (a_nodes * NODE_BYTES[width] + a_prims * TRI_BYTES) / n
 
     stream = torch.cuda.current_stream(device)
     for _ in range(args.warmup):
@@ -278,22 +305,25 @@ def run_ours(args):
     tpath = os.path.join(ROOT, "profiles", "traffic.json")
     if os.path.exists(tpath):
         tj = json.load(open(tpath))
-        if tj.get("workload") == "incoherent_21m" and tj.get("nodes") == "fp32":
+        if tj.get("workload") == ("raycast_82k" if width == 4 else "incoherent_21m") and tj.get("nodes") == "fp32":
             traffic = tj.get("dram_bytes_per_launch")
 
     if rank == 0:
         out = {
-            "metric": METRIC, "value": round(value, 3), "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "metric": METRIC if width == 8 else "Mrays/s primary closest-hit", "value": round(value, 3),
+            "unit": UNIT, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": round(ms_max / args.steps, 4), "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded procedural scene)",
-            "config": workload_config({"parallelism": f"replicas x{world}", "build_seconds": round(info["build_seconds"], 2),
+            "config": (raycast_config if width == 4 else workload_config)(
+                {"parallelism": f"replicas x{world}", "build_seconds": round(info["build_seconds"], 2),
                                        "tree_device_bytes": info["device_bytes"]}),
             "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
                          "frac": round(achieved / peak, 4), "traffic": traffic,
                          "peak_source": f"{peak_src} hbm_gbs (burst)",
                          "algorithmic_bytes_per_ray": round(bytes_closest, 1),
                          "node_tests_per_ray": round(node_tests / n, 3), "prim_tests_per_ray": round(prim_tests / n, 3),
-                         "kernel": "k_trace_fp32<8,false,128,false>", "launch_ms": round(launch_ms, 4)},
+                         "kernel": f"k_trace_fp32<{width},false,{64 if width == 4 else 128},false>",
+                         "launch_ms": round(launch_ms, 4)},
             "anyhit": {"mrays_s": round(n / (any_ms / 1e3) / 1e6, 3), "launch_ms": round(any_ms, 4),
                        "algorithmic_bytes_per_ray": round(bytes_any, 1),
                        "achieved_gbs": round(bytes_any * n / (any_ms / 1e3) / 1e9, 1)},
@@ -304,7 +334,8 @@ def run_ours(args):
         }
         if world == 1 and not args.no_cpu_baseline:
             threads = os.cpu_count() or 1
-            rate, kind, desc = reference_cpu(tri, diffuse, steps=3, warmup=1, threads=threads, sample=args.sample)
+            rate, kind, desc = reference_cpu(tri, diffuse, steps=3, warmup=1, threads=threads, sample=args.sample,
+                                             width=width)
             out["cpu_baseline"] = {"value": round(rate, 3), "unit": UNIT, "cores": threads, "kind": kind,
                                    "sample": desc}
         print(json.dumps(out))
@@ -411,7 +442,7 @@ def main():
     p.add_argument("--steps", type=int, default=200)
     p.add_argument("--warmup", type=int, default=5)
     p.add_argument("--impl", choices=["ours", "reference"], default="ours")
-    p.add_argument("--workload", choices=["closest", "pathtrace"], default="closest")
+    p.add_argument("--workload", choices=["closest", "raycast", "pathtrace"], default="closest")
     p.add_argument("--sample", type=int, default=CPU_SAMPLE)
     p.add_argument("--no-cpu-baseline", action="store_true")
     args = p.parse_args()
