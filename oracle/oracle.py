@@ -94,6 +94,8 @@ class Port:
         L.orc_count.argtypes = [_vp, _vp, _i64, ctypes.c_int, ctypes.POINTER(_i64), ctypes.POINTER(_i64),
                                 ctypes.c_int]
         L.orc_ray_prepare.argtypes = [_vp, _vp, _vp]
+        L.orc_tri_test.restype = ctypes.c_int
+        L.orc_tri_test.argtypes = [_vp, _i64, _vp, _i64, _i64, ctypes.POINTER(ctypes.c_float)]
         L.orc_fp64_intersect.restype = ctypes.c_double
         L.orc_fp64_intersect.argtypes = [_vp, _i64, _vp, _i64, _i64]
         self.L = L
@@ -113,6 +115,14 @@ class Port:
         self.L.orc_count(tree.h, r.ctypes.data, r.shape[1], 1 if any_hit else 0, ctypes.byref(a), ctypes.byref(b),
                          threads or os.cpu_count())
         return a.value, b.value
+
+    def tri_t(self, tri: np.ndarray, prim: int, rays: np.ndarray, i: int):
+        """SORT's FP32 watertight test of ray i against one triangle: t or None."""
+        tri = np.ascontiguousarray(tri, np.float32)
+        r = np.ascontiguousarray(rays, np.float32)
+        t = ctypes.c_float(0.0)
+        ok = self.L.orc_tri_test(tri.ctypes.data, prim, r.ctypes.data, r.shape[1], i, ctypes.byref(t))
+        return t.value if ok else None
 
     def fp64_t(self, tri: np.ndarray, prim: int, rays: np.ndarray, i: int) -> float:
         tri = np.ascontiguousarray(tri, np.float32)

@@ -675,6 +675,13 @@ void orc_count(const orc_tree* t, const float* rays, int64_t n, int any, int64_t
     *prim_tests = j.prim_tests;
 }
 
+int orc_tri_test(const float* tri, int64_t prim, const float* rays, int64_t n, int64_t i, float* t_out) {
+    oray r;
+    float u, v;
+    load_ray(&r, rays, n, i);
+    return tri_test(&r, tri + prim * 9, t_out, &u, &v);
+}
+
 double orc_fp64_intersect(const float* tri, int64_t prim, const float* rays, int64_t n, int64_t i) {
     double o[3], d[3], p[3][3];
     for (int k = 0; k < 3; ++k) {

@@ -58,6 +58,10 @@ void orc_count(const orc_tree* t, const float* rays, int64_t n, int any, int64_t
 /* Ray::Prepare for one direction (math/ray.h:60-69). */
 void orc_ray_prepare(const float* d, int* local_xyz, float* scale_xyz);
 
+/* SORT's FP32 watertight test of ray i against triangle prim alone
+ * (tmin < t <= tmax); returns 1 and t on a hit. */
+int orc_tri_test(const float* tri, int64_t prim, const float* rays, int64_t n, int64_t i, float* t_out);
+
 /* FP64 re-intersection of ray i with triangle prim (same watertight
  * formulation in doubles); returns t, or -1 on a miss. */
 double orc_fp64_intersect(const float* tri, int64_t prim, const float* rays, int64_t n, int64_t i);

@@ -80,10 +80,14 @@ sg_status upload(sg_scene* s, const float* tri, int64_t ntri) {
     const int W = t.width;
     const int f4 = W == 8 ? sg::NodeShape<8>::kF4 : sg::NodeShape<4>::kF4;
     const int64_t nn = t.interior();
-    std::vector<float4> nodes(size_t(std::max<int64_t>(nn, 1)) * f4);
-    std::memset(nodes.data(), 0, nodes.size() * sizeof(float4));
+    std::vector<float4> nodes;
+    if (s->node_format == SG_NODES_QUANT8) {
+        sg::quantize_nodes(t, nodes);
+    } else {
+        nodes.assign(size_t(std::max<int64_t>(nn, 1)) * f4, make_float4(0.0f, 0.0f, 0.0f, 0.0f));
+    }
     const int Q = W / 4;  // float4 per plane
-    for (int64_t k = 0; k < nn; ++k) {
+    for (int64_t k = 0; s->node_format == SG_NODES_FP32 && k < nn; ++k) {
         float* base = reinterpret_cast<float*>(&nodes[size_t(k) * f4]);
         for (int a = 0; a < 3; ++a)
             for (int j = 0; j < W; ++j) {
@@ -177,6 +181,7 @@ sg_status scene_launch(const sg_scene* s, bool any, TraceLaunch* L, DevTree* tre
     L->any = any;
     L->stack_need = s->stack_need;
     L->tuning = s->tuning;
+    L->q8 = s->node_format == SG_NODES_QUANT8;
     L->err = s->d_err;
     L->counter = next_counter(s);
     *tree = dev_tree(s);
@@ -207,7 +212,8 @@ sg_status sg_scene_create(const float* triangles, int64_t ntri, const sg_build_o
     if (ntri < 0 || (ntri > 0 && !triangles)) return fail(SG_ERR_INVALID_ARGUMENT, "bad triangle buffer");
     if (opts->width != 4 && opts->width != 8) return fail(SG_ERR_INVALID_ARGUMENT, "width must be 4 or 8");
     if (opts->max_leaf < 1 || opts->max_depth < 1) return fail(SG_ERR_INVALID_ARGUMENT, "max_leaf/max_depth < 1");
-    if (opts->node_format != SG_NODES_FP32) return fail(SG_ERR_UNSUPPORTED, "node format not available");
+    if (opts->node_format != SG_NODES_FP32 && opts->node_format != SG_NODES_QUANT8)
+        return fail(SG_ERR_UNSUPPORTED, "unknown node format");
     if (ntri >= int64_t(0x7fffffff)) return fail(SG_ERR_LIMIT, "more than 2^31-2 triangles");
     int ndev = 0;
     cudaError_t e = cudaGetDeviceCount(&ndev);
@@ -338,6 +344,7 @@ static sg_status trace_common(const sg_scene* s, const sg_rays* rays, int64_t n,
     L.any = any;
     L.stack_need = s->stack_need;
     L.tuning = s->tuning;
+    L.q8 = s->node_format == SG_NODES_QUANT8;
     if (any) {
         L.occ = occ;
     } else {
@@ -450,6 +457,7 @@ sg_status sg_trace_stats(const sg_scene* cs, const sg_rays* rays, int64_t n, int
     L.any = any != 0;
     L.stack_need = s->stack_need;
     L.tuning = s->tuning;
+    L.q8 = s->node_format == SG_NODES_QUANT8;
     L.prim = reinterpret_cast<int32_t*>(out);
     L.t = reinterpret_cast<float*>(out + size_t(n) * 4);
     L.occ = reinterpret_cast<uint8_t*>(out);

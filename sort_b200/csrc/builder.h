@@ -13,6 +13,8 @@
 //   * the result is a flat array form (BuiltTree) instead of unique_ptr nodes.
 #pragma once
 
+#include <vector_types.h>
+
 #include <cstdint>
 #include <vector>
 
@@ -59,6 +61,10 @@ struct BuiltTree {
 // Builds over ntri triangles, 9 floats each (v0, v1, v2). Throws
 // std::invalid_argument / std::bad_alloc on bad input / memory exhaustion.
 BuiltTree build_tree(const float* tri, int64_t ntri, const BuildParams& p);
+
+// 8-bit node format (quantize.cpp): one record per interior node in the layout
+// layout.h describes; every decoded child box contains the FP32 box.
+void quantize_nodes(const BuiltTree& t, std::vector<float4>& out);
 
 // Pre-order topology in the oracle's comparison format:
 //   interior node: [child_cnt, child0 ..., child_{n-1} ...]

@@ -36,6 +36,17 @@ struct NodeShape<4> {
 constexpr int32_t kEmpty = -1;
 constexpr int kPadSlots = 8;
 
+// Interior node, 8-bit child boxes (SG_NODES_QUANT8; see quantize.cpp):
+//   float4 0: origin x, y, z; w = the three scale exponents e + 127, one byte
+//             per axis (x in the low byte), scale = 2^e;
+//   W = 8: float4 1..3: per axis 8 lower-bound bytes then 8 upper-bound bytes;
+//          float4 4..5: child[0:8].  96 B.
+//   W = 4: float4 1: lo_x[4] hi_x[4] lo_y[4] hi_y[4]; float4 2: lo_z[4] hi_z[4]
+//          and 8 B of padding; float4 3: child[0:4].  64 B.
+// A bound decodes to fl(origin + q * scale).
+constexpr int kQ8F4W8 = 6;
+constexpr int kQ8F4W4 = 4;
+
 struct DevTree {
     const float4* nodes;
     const float4* tris;

@@ -66,10 +66,69 @@ __device__ __forceinline__ void load_node(const float4* __restrict__ nodes, int3
     }
 }
 
+// 8-bit node (layout.h, quantize.cpp): decode every child bound to
+// fl(origin + q * 2^e) (one rounding: q * 2^e is exact), giving FP32 boxes that
+// contain SORT's, which the unchanged slab test then uses.
+__device__ __forceinline__ float q8_bound(uint32_t word, int byte, float s, float origin) {
+    const float q = __uint_as_float(__byte_perm(word, 0x4B000000u, 0x7540u | (unsigned)byte)) - 8388608.0f;
+    return fmaf(q, s, origin);
+}
+
+template <int W>
+__device__ __forceinline__ void load_node_q8(const float4* __restrict__ nodes, int32_t ref, NodeData<W>& nd) {
+    const float4* p = nodes + (size_t)ref * (W == 8 ? kQ8F4W8 : kQ8F4W4);
+    const float4 h = __ldg(p);
+    const uint32_t eb = __float_as_uint(h.w);
+    const float org[3] = {h.x, h.y, h.z};
+    float s[3];
+#pragma unroll
+    for (int a = 0; a < 3; ++a) s[a] = __uint_as_float(((eb >> (8 * a)) & 0xffu) << 23);
+    if (W == 8) {
+#pragma unroll
+        for (int a = 0; a < 3; ++a) {
+            const uint4 q = __ldg(reinterpret_cast<const uint4*>(p + 1 + a));
+#pragma unroll
+            for (int j = 0; j < 4; ++j) {
+                nd.lo[a][j] = q8_bound(q.x, j, s[a], org[a]);
+                nd.lo[a][4 + j] = q8_bound(q.y, j, s[a], org[a]);
+                nd.hi[a][j] = q8_bound(q.z, j, s[a], org[a]);
+                nd.hi[a][4 + j] = q8_bound(q.w, j, s[a], org[a]);
+            }
+        }
+        const int4 c0 = __ldg(reinterpret_cast<const int4*>(p + 4));
+        const int4 c1 = __ldg(reinterpret_cast<const int4*>(p + 5));
+        nd.ch[0] = c0.x;
+        nd.ch[1] = c0.y;
+        nd.ch[2] = c0.z;
+        nd.ch[3] = c0.w;
+        nd.ch[4 % W] = c1.x;
+        nd.ch[5 % W] = c1.y;
+        nd.ch[6 % W] = c1.z;
+        nd.ch[7 % W] = c1.w;
+    } else {
+        const uint4 q01 = __ldg(reinterpret_cast<const uint4*>(p + 1));
+        const uint4 q2 = __ldg(reinterpret_cast<const uint4*>(p + 2));
+        const int4 c = __ldg(reinterpret_cast<const int4*>(p + 3));
+#pragma unroll
+        for (int j = 0; j < 4; ++j) {
+            nd.lo[0][j] = q8_bound(q01.x, j, s[0], org[0]);
+            nd.hi[0][j] = q8_bound(q01.y, j, s[0], org[0]);
+            nd.lo[1][j] = q8_bound(q01.z, j, s[1], org[1]);
+            nd.hi[1][j] = q8_bound(q01.w, j, s[1], org[1]);
+            nd.lo[2][j] = q8_bound(q2.x, j, s[2], org[2]);
+            nd.hi[2][j] = q8_bound(q2.y, j, s[2], org[2]);
+        }
+        nd.ch[0] = c.x;
+        nd.ch[1 % W] = c.y;
+        nd.ch[2 % W] = c.z;
+        nd.ch[3 % W] = c.w;
+    }
+}
+
 // One ray's traversal state. STATS adds SORT's traversal counters
 // (accel/fast_bvh.hpp:50-96): interior nodes box-tested, and primitives tested
 // counted per leaf entered (sIntersectionTest += pri_cnt).
-template <int W, bool ANY, int STACK, bool STATS>
+template <int W, bool ANY, int STACK, bool STATS, bool Q8 = false>
 struct Traversal {
     RayState r;
     float best_t, best_u, best_v;
@@ -193,7 +252,10 @@ struct Traversal {
     // descend into that one. Returns false when no child is hit.
     __device__ __forceinline__ bool interior(const DevTree& tr) {
         NodeData<W> nd;
-        load_node<W>(tr.nodes, cur, nd);
+        if (Q8)
+            load_node_q8<W>(tr.nodes, cur, nd);
+        else
+            load_node<W>(tr.nodes, cur, nd);
         if (STATS) ++node_tests;
         float d[W];
         unsigned mask = 0;
@@ -351,7 +413,8 @@ __global__ void __launch_bounds__(128) k_trace_fp32_ww(DevTree tr, DevRays rays,
 
 // One ray per thread for the whole launch. With n_dev set, the batch size is
 // min(n, *n_dev), read on the device (queues whose length only the GPU knows).
-template <int W, bool ANY, int STACK, bool STATS>
+// Q8 reads 8-bit nodes.
+template <int W, bool ANY, int STACK, bool STATS, bool Q8 = false>
 __global__ void __launch_bounds__(128) k_trace_fp32(DevTree tr, DevRays rays, int64_t n, int32_t* __restrict__ prim_out,
                                                     float* __restrict__ t_out, float* __restrict__ u_out,
                                                     float* __restrict__ v_out, uint8_t* __restrict__ occ_out,
@@ -360,7 +423,7 @@ __global__ void __launch_bounds__(128) k_trace_fp32(DevTree tr, DevRays rays, in
     const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (n_dev && i >= (int64_t)*n_dev) return;
     if (i >= n) return;
-    Traversal<W, ANY, STACK, STATS> tv;
+    Traversal<W, ANY, STACK, STATS, Q8> tv;
     if (tv.start(tr, rays, i))
         while (!tv.step(tr, err)) {
         }
@@ -424,6 +487,13 @@ static cudaError_t launch_stack(const TraceLaunch& L, const DevTree& tr, const D
     const int threads = 128;
     // Counting launches keep the one-entry-per-step loop, whose interior-node
     // visits are exactly SORT's (speculation visits extra ones).
+    // 8-bit nodes are read by the one-ray-per-thread kernel.
+    if (L.q8) {
+        const int64_t blocks = (n + threads - 1) / threads;
+        k_trace_fp32<W, ANY, STACK, STATS, true><<<(unsigned)blocks, threads, 0, s>>>(
+            tr, rays, n, L.prim, L.t, L.u, L.v, L.occ, L.err, L.stats, L.n_dev);
+        return cudaGetLastError();
+    }
     // A device-side batch size is only read by the one-ray-per-thread kernel.
     if (!STATS && !L.n_dev &&
         (L.tuning.schedule == kScheduleWhileWhile || L.tuning.schedule == kScheduleSpeculative)) {

@@ -33,6 +33,7 @@ struct TraceLaunch {
     unsigned long long* stats = nullptr;  // non-null: also accumulate SORT's traversal counters
     unsigned long long* counter = nullptr;  // persistent schedule: ray counter, zeroed on the stream first
     const int* n_dev = nullptr;  // if set, the batch is min(n, *n_dev) (one-ray-per-thread kernel)
+    bool q8 = false;             // interior nodes in the 8-bit format
 };
 
 cudaError_t launch_trace_fp32(const TraceLaunch& L, const DevTree& tr, const DevRays& rays, int64_t n,
