@@ -38,6 +38,7 @@ NODE_BYTES = {4: 112, 8: 224}   # FP32 canonical wide node: W*24 B boxes + W*4 B
 TRI_BYTES = 36                  # 9 floats per triangle test
 RAY_IN, HIT_OUT = 32, 16
 CPU_SAMPLE = 262_144            # rays per CPU-baseline step
+NODE_FORMATS = {"fp32": 0, "q8": 1}
 
 
 def workload_config(extra=None):
@@ -218,7 +219,7 @@ def run_ours(args):
         from sort_b200 import Qbvh
         width = 4
         tri = scenes.sphere_field(64, 3, seed=1)
-        acc = Qbvh(DEPTH, LEAF, device=local)
+        acc = Qbvh(DEPTH, LEAF, node_format=NODE_FORMATS[args.nodes], device=local)
         acc.Build(tri)
         diffuse = scenes.camera_rays(1024, 1024, seed=7 + rank)
         h = acc.GetIntersect(torch.from_numpy(diffuse).to(device))
@@ -227,7 +228,7 @@ def run_ours(args):
     else:
         width = WIDTH
         tri = scenes.sphere_field(SPHERES, LEVEL, seed=1)
-        acc = Obvh(DEPTH, LEAF, device=local)
+        acc = Obvh(DEPTH, LEAF, node_format=NODE_FORMATS[args.nodes], device=local)
         acc.Build(tri)
         diffuse, shadow = make_rays(acc, tri, rank, device)
     info = acc.info()
@@ -235,9 +236,24 @@ def run_ours(args):
     d_diff = torch.from_numpy(diffuse).to(device)
     d_shad = torch.from_numpy(shadow).to(device)
 
-    # SORT's traversal counters on these rays -> algorithmic bytes per ray.
-    node_tests, prim_tests = acc.TraceStats(d_diff, False)
-    a_nodes, a_prims = acc.TraceStats(d_shad, True)
+    # SORT's traversal counters on these rays -> algorithmic bytes per ray. The
+    # counts are SORT's (FP32 boxes), whatever node format is timed.
+    parity = None
+    if args.nodes == "fp32":
+        node_tests, prim_tests = acc.TraceStats(d_diff, False)
+        a_nodes, a_prims = acc.TraceStats(d_shad, True)
+    else:
+        ref_acc = type(acc)(DEPTH, LEAF, device=local)
+        ref_acc.Build(tri)
+        node_tests, prim_tests = ref_acc.TraceStats(d_diff, False)
+        a_nodes, a_prims = ref_acc.TraceStats(d_shad, True)
+        hf, hq = ref_acc.GetIntersect(d_diff), acc.GetIntersect(d_diff)
+        diff = hf.prim != hq.prim
+        tie = diff & (hf.prim >= 0) & (hq.prim >= 0) & ((hq.t - hf.t).abs() <= 1e-6 * hf.t)
+        parity = {"rays": n, "prim_differs": int(diff.sum()), "near_ties": int(tie.sum()),
+                  "same_prim_t_bits_equal": bool(torch.equal(hf.t[~diff], hq.t[~diff]))}
+        ref_acc.Release()
+        torch.cuda.empty_cache()
     bytes_closest = RAY_IN + HIT_OUT + (node_tests * NODE_BYTES[width] + prim_tests * TRI_BYTES) / n
     bytes_any = RAY_IN + 4 + (a_nodes * NODE_BYTES[width] + a_prims * TRI_BYTES) / n
 
@@ -315,6 +331,7 @@ def run_ours(args):
             "warmup": args.warmup, "ms_per_step": round(ms_max / args.steps, 4), "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded procedural scene)",
             "config": (raycast_config if width == 4 else workload_config)(
+                {"nodes": args.nodes} if args.nodes != "fp32" else {}) | (
                 {"parallelism": f"replicas x{world}", "build_seconds": round(info["build_seconds"], 2),
                                        "tree_device_bytes": info["device_bytes"]}),
             "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
@@ -322,7 +339,8 @@ def run_ours(args):
                          "peak_source": f"{peak_src} hbm_gbs (burst)",
                          "algorithmic_bytes_per_ray": round(bytes_closest, 1),
                          "node_tests_per_ray": round(node_tests / n, 3), "prim_tests_per_ray": round(prim_tests / n, 3),
-                         "kernel": f"k_trace_fp32<{width},false,{64 if width == 4 else 128},false>",
+                         "kernel": f"k_trace_fp32<{width},false,{64 if width == 4 else 128},false"
+                                   + (",true>" if args.nodes == "q8" else ">"),
                          "launch_ms": round(launch_ms, 4)},
             "anyhit": {"mrays_s": round(n / (any_ms / 1e3) / 1e6, 3), "launch_ms": round(any_ms, 4),
                        "algorithmic_bytes_per_ray": round(bytes_any, 1),
@@ -331,6 +349,7 @@ def run_ours(args):
                     "d2h_bytes_per_step": int(n * 16)},
             "clocks": clocks.summary(),
             "gpu_launches": args.steps,
+            **({"parity_vs_fp32_nodes": parity} if parity else {}),
         }
         if world == 1 and not args.no_cpu_baseline:
             threads = os.cpu_count() or 1
@@ -445,6 +464,8 @@ def main():
     p.add_argument("--workload", choices=["closest", "raycast", "pathtrace"], default="closest")
     p.add_argument("--sample", type=int, default=CPU_SAMPLE)
     p.add_argument("--no-cpu-baseline", action="store_true")
+    p.add_argument("--nodes", choices=sorted(NODE_FORMATS), default="fp32",
+                   help="child-box format of the timed tree (q8: 8-bit, outward-rounded)")
     args = p.parse_args()
     if args.workload == "pathtrace":
         run_pathtrace(args)
