@@ -455,13 +455,180 @@ def run_pathtrace(args):
     pt.Release()
 
 
+# batched_31m: 8 resident scenes from the ray-cast recipe at ~10k ... 16M
+# triangles, as (icosphere count, subdivision level).
+BATCH_SCENES = [(8, 3), (40, 3), (40, 4), (50, 5), (100, 5), (200, 5), (400, 5), (800, 5)]
+BATCH_MIN, BATCH_MAX = 4096, 4_194_304
+
+
+def batched_config(extra=None):
+    cfg = {
+        "workload": "batched_31m: 8 resident scenes (icosphere fields of 10,242 / 51,202 / 204,802 / 1,024,002 / "
+                    "2,048,002 / 4,096,002 / 8,192,002 / 16,384,002 triangles); per step a fixed list of ray "
+                    "batches, sizes log-uniform in [4,096, 4,194,304], scene uniform, 50% jittered primary / 50% "
+                    "cosine-diffuse bounce rays, closest hit; persistent batch kernel under a captured CUDA graph "
+                    "(autotuned) vs one plain launch per batch, same trees, FIFO order",
+        "l2": "inputs larger than L2: 2.4 GB of trees, ~1.2 GB of rays per step (no flush)",
+    }
+    if extra:
+        cfg.update(extra)
+    return cfg
+
+
+def run_batched(args):
+    """Batched uneven launch: Mrays/s and per-batch latency, persistent graph vs plain launches."""
+    import ctypes
+
+    import torch
+
+    from sort_b200 import Batch, Batcher, Obvh, Qbvh, _lib, scenes
+
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    rank = int(os.environ.get("RANK", "0"))
+    torch.cuda.set_device(local)
+    device = torch.device("cuda", local)
+    stream = torch.cuda.current_stream(device)
+    rng = np.random.default_rng(args.batch_seed)
+    accs, alts, pools, tri_counts = [], [], [], []
+    for k, (count, level) in enumerate(BATCH_SCENES):
+        tri = scenes.sphere_field(count, level, seed=100 + k)
+        a8 = Obvh(DEPTH, LEAF, device=local)
+        a8.Build(tri)
+        a4 = Qbvh(DEPTH, LEAF, device=local)
+        a4.Build(tri)
+        cam = scenes.camera_rays(IMAGE, IMAGE, seed=200 + k)
+        h = a8.GetIntersect(torch.from_numpy(cam).to(device))
+        diffuse, _ = scenes.bounce_rays(tri, cam, h.prim.cpu().numpy(), h.t.cpu().numpy(), IMAGE * IMAGE,
+                                        seed=300 + k + rank)
+        pools.append((torch.from_numpy(cam).to(device), torch.from_numpy(diffuse).to(device)))
+        accs.append(a8)
+        alts.append(a4)
+        tri_counts.append(int(tri.shape[0]))
+    sizes = np.exp(rng.uniform(np.log(BATCH_MIN), np.log(BATCH_MAX), args.batches)).astype(np.int64)
+    which = rng.integers(0, len(BATCH_SCENES), args.batches)
+    kind = rng.integers(0, 2, args.batches)
+    rays = []
+    for m, s, kd in zip(sizes, which, kind):
+        pool = pools[s][kd]
+        a = int(rng.integers(0, pool.shape[1] - m + 1))
+        rays.append(pool[:, a:a + m].contiguous())
+    del pools
+    torch.cuda.empty_cache()
+    total = int(sizes.sum())
+
+    # Autotune (tree width per scene, block / stack / refill) on this batch list.
+    batcher = Batcher(device=local, max_batches=max(args.batches, 16))
+    batches = [Batch(accs[s], r) for s, r in zip(which, rays)]
+    tuning, use_alt = batcher.autotune(batches, [alts[s] for s in which], reps=2)
+    chosen = {}
+    for s, u in zip(which, use_alt):
+        chosen[int(s)] = alts[s] if u else accs[s]
+    batches = [Batch(chosen[int(s)], r, hits=b.hits) for s, r, b in zip(which, rays, batches)]
+
+    # SORT's traversal counts per batch on the chosen trees -> algorithmic bytes.
+    alg_bytes = 0.0
+    for b in batches:
+        nt, pt = b.accel.TraceStats(b.rays, False)
+        alg_bytes += b.rays.shape[1] * (RAY_IN + HIT_OUT) + nt * NODE_BYTES[b.accel.WIDTH] + pt * TRI_BYTES
+
+    # Plain arm: one sg_trace_closest per batch, preallocated outputs, FIFO.
+    lib = _lib.load()
+    plain_calls = []
+    for b in batches:
+        r = b.rays
+        n = r.shape[1]
+        rs = _lib.Rays(*[r.data_ptr() + 4 * k * n for k in range(8)])
+        hs = _lib.Hits(b.hits.prim.data_ptr(), b.hits.t.data_ptr(), b.hits.u.data_ptr(), b.hits.v.data_ptr())
+        plain_calls.append((b.accel._h, ctypes.byref(rs), n, ctypes.byref(hs), rs, hs))
+    sptr = stream.cuda_stream
+
+    def plain_step(events=None):
+        for k, (h, rs, n, hs, _, _) in enumerate(plain_calls):
+            _lib.check(lib.sg_trace_closest(h, rs, n, hs, sptr))
+            if events is not None:
+                events[k].record(stream)
+
+    def timed(fn, steps):
+        torch.cuda.synchronize(device)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(steps):
+            fn()
+        e1.record(stream)
+        torch.cuda.synchronize(device)
+        return e0.elapsed_time(e1)
+
+    for _ in range(args.warmup):
+        plain_step()
+        batcher.run(batches)
+    torch.cuda.synchronize(device)
+    with ClockSampler(local) as clocks:
+        ms_plain = timed(plain_step, args.steps)
+        ms_pers = timed(lambda: batcher.run(batches), args.steps)
+
+    # Per-batch latency (completion since the step's start), one step at a time.
+    lat_plain, lat_pers, lat_sjf = [], [], []
+    order_sjf = sorted(range(len(batches)), key=lambda k: int(batches[k].rays.shape[1]))
+    for _ in range(args.steps):
+        ev = [torch.cuda.Event(enable_timing=True) for _ in batches]
+        e0 = torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize(device)
+        e0.record(stream)
+        plain_step(ev)
+        torch.cuda.synchronize(device)
+        lat_plain += [e0.elapsed_time(e) for e in ev]
+        batcher.run(batches)
+        lat_pers += [d / 1e6 for d in batcher.wait()]
+        batcher.run([batches[k] for k in order_sjf])
+        lat_sjf += [d / 1e6 for d in batcher.wait()]
+
+    def pct(x, q):
+        return round(float(np.percentile(np.asarray(x), q)), 3)
+
+    peaks_path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    peak, peak_src = ((float(json.load(open(peaks_path))["hbm_gbs"]), "measured") if os.path.exists(peaks_path)
+                      else (6650.0, "fallback"))
+    achieved = alg_bytes / (ms_pers / args.steps / 1e3) / 1e9
+    value = total * args.steps / (ms_pers / 1e3) / 1e6
+    plain_value = total * args.steps / (ms_plain / 1e3) / 1e6
+    ngroups = len({(b.accel.WIDTH) for b in batches})
+    if rank == 0:
+        out = {
+            "metric": "Mrays/s batched uneven closest-hit", "value": round(value, 3), "unit": UNIT, "n_gpus": 1,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms_pers / args.steps, 4),
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+            "data": "synthetic (seeded procedural scenes and rays)",
+            "config": batched_config({"batches": args.batches, "batch_seed": args.batch_seed, "rays_per_step": total,
+                                      "scene_triangles": tri_counts, "tuning": tuning,
+                                      "scene_widths": {str(s): chosen[s].WIDTH for s in sorted(chosen)}}),
+            "plain": {"value": round(plain_value, 3), "unit": UNIT, "ms_per_step": round(ms_plain / args.steps, 4),
+                      "latency_ms": {"p50": pct(lat_plain, 50), "p99": pct(lat_plain, 99)}},
+            "persistent": {"latency_ms": {"p50": pct(lat_pers, 50), "p99": pct(lat_pers, 99)},
+                           "shortest_first_latency_ms": {"p50": pct(lat_sjf, 50), "p99": pct(lat_sjf, 99)}},
+            "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
+                         "frac": round(achieved / peak, 4), "traffic": None,
+                         "peak_source": f"{peak_src} hbm_gbs (burst)",
+                         "algorithmic_bytes_per_ray": round(alg_bytes / total, 1),
+                         "kernel": "k_trace_batches"},
+            "clocks": clocks.summary(),
+            # per step: the graph's begin kernel + one persistent kernel per width group
+            "gpu_launches": args.steps * (1 + ngroups),
+        }
+        print(json.dumps(out))
+    batcher.Release()
+    for a in accs + alts:
+        a.Release()
+
+
 def main():
     p = argparse.ArgumentParser()
     p.add_argument("--gpus", type=int, default=1)
     p.add_argument("--steps", type=int, default=200)
     p.add_argument("--warmup", type=int, default=5)
     p.add_argument("--impl", choices=["ours", "reference"], default="ours")
-    p.add_argument("--workload", choices=["closest", "raycast", "pathtrace"], default="closest")
+    p.add_argument("--workload", choices=["closest", "raycast", "pathtrace", "batched"], default="closest")
+    p.add_argument("--batches", type=int, default=64, help="batched workload: ray batches per step")
+    p.add_argument("--batch-seed", type=int, default=7, help="batched workload: seed of the batch list")
     p.add_argument("--sample", type=int, default=CPU_SAMPLE)
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--nodes", choices=sorted(NODE_FORMATS), default="fp32",
@@ -469,6 +636,12 @@ def main():
     args = p.parse_args()
     if args.workload == "pathtrace":
         run_pathtrace(args)
+    elif args.workload == "batched":
+        if args.impl == "reference":
+            print(json.dumps({"impl": "reference", "unavailable": "batched workload: SORT has no batch API; "
+                              "its per-ray CPU rate is the closest workload's reference arm"}))
+        else:
+            run_batched(args)
     elif args.impl == "reference":
         run_reference(args)
     else:

@@ -174,6 +174,62 @@ sg_status sg_trace_any_host(const sg_scene* scene, const float* rays8, int64_t n
 sg_status sg_trace_closest_host_static(const sg_scene* scene, const float* rays8, int64_t n, int32_t* prim, float* t,
                                        float* u, float* v, void* stream);
 
+/* ---- Batched multi-scene traversal --------------------------------------
+ * A batcher traces many ray batches, over many resident scenes and of uneven
+ * sizes, in one replay of a captured CUDA graph: per group of batches sharing
+ * a tree width, node format and query, one persistent kernel drains all of
+ * them as one ray sequence, instead of one launch per batch. No SORT
+ * counterpart as an API: it stands in for SORT's render workers, which each
+ * call Accelerator::GetIntersect / GetAttenuation for their own rays
+ * (work/image_evaluation/image_evaluation.cpp:70-75, 153-279). A batch's
+ * results are exactly those of sg_trace_closest / sg_trace_any on its scene
+ * alone, whatever shares the run.
+ *
+ * sg_batch: rays are device SoA planes ox, oy, oz, dx, dy, dz, tmin, tmax;
+ *   plane k of ray i is rays[k * stride + i] (stride 0 = n), so a batch may be
+ *   a slice of a larger ray array. any = 0 writes hits, 1 writes occluded.
+ * sg_batcher_run: enqueues the run on `stream` (no synchronisation). Runs of
+ *   one batcher share its device tables: order them on one stream. budget_ns
+ *   > 0 stops warps from claiming rays once that long has passed since the
+ *   run's start; the rays they hold still finish. Up to max_batches batches.
+ * sg_batcher_wait: synchronises `stream`; per batch of the LAST run (caller
+ *   order) the ns from the run's start to the completion of its last ray, or
+ *   -1 if the budget left it incomplete (then returns SG_ERR_LIMIT).
+ * sg_batcher_autotune: picks, by timing runs of `batches` on `stream`, the
+ *   tree width per scene (alternatives[i]: the same triangles built at the
+ *   other width, or NULL; use_alternative[i] = 1 where that one is faster) and
+ *   the kernel tuning (block threads, stack, refill threshold), which it
+ *   installs in the batcher and returns in `best`. reps: timed runs per
+ *   candidate (0 = 3). */
+typedef struct {
+    const sg_scene* scene;
+    const float* rays;
+    int64_t stride;
+    int64_t n;
+    int32_t any;
+    int32_t reserved;
+    sg_hits hits;
+    uint8_t* occluded;
+} sg_batch;
+
+typedef struct {
+    int32_t block_threads;    /* rays per block: 64, 128 or 256 */
+    int32_t stack;            /* stack entries 64, 128 or 256; 0 or less than a tree needs = the least that fits */
+    int32_t refill_threshold; /* idle lanes (1..32) at which a warp claims new rays */
+    int32_t blocks_per_sm;    /* resident blocks per SM, 0 = as many as fit */
+} sg_batch_tuning;
+
+typedef struct sg_batcher sg_batcher;
+sg_status sg_batcher_create(int32_t device, int32_t max_batches, sg_batcher** out);
+sg_status sg_batcher_destroy(sg_batcher* batcher);
+sg_status sg_batcher_set_tuning(sg_batcher* batcher, const sg_batch_tuning* tuning);
+sg_status sg_batcher_get_tuning(const sg_batcher* batcher, sg_batch_tuning* tuning);
+sg_status sg_batcher_run(sg_batcher* batcher, const sg_batch* batches, int32_t count, int64_t budget_ns, void* stream);
+sg_status sg_batcher_wait(sg_batcher* batcher, int64_t* done_ns, int32_t count, void* stream);
+sg_status sg_batcher_autotune(sg_batcher* batcher, const sg_batch* batches, const sg_scene* const* alternatives,
+                              int32_t count, int32_t reps, int32_t* use_alternative, sg_batch_tuning* best,
+                              void* stream);
+
 /* ---- Path tracing -------------------------------------------------------
  * SORT's PathTracing integrator (integrator/pathtracing.cpp:37-258) with its
  * next-event estimation (integrator/integratormethod.cpp:100-192), Lambert and

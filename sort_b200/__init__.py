@@ -7,5 +7,6 @@ interface over that library (accel.py), plus the seeded synthetic workloads
 """
 from .accel import Accelerator, Hits, Obvh, Qbvh, Scene, build_topology_host  # noqa: F401
 from ._lib import SortGpuError  # noqa: F401
+from .batcher import Batch, Batcher  # noqa: F401
 
-__all__ = ["Accelerator", "Qbvh", "Obvh", "Scene", "Hits", "SortGpuError", "build_topology_host"]
+__all__ = ["Accelerator", "Qbvh", "Obvh", "Scene", "Hits", "SortGpuError", "build_topology_host", "Batch", "Batcher"]

@@ -51,9 +51,28 @@ class SceneInfo(ctypes.Structure):
                 ("build_seconds", ctypes.c_double)]
 
 
+class Batch(ctypes.Structure):
+    _fields_ = [("scene", ctypes.c_void_p), ("rays", ctypes.c_void_p), ("stride", ctypes.c_int64),
+                ("n", ctypes.c_int64), ("any", ctypes.c_int32), ("reserved", ctypes.c_int32), ("hits", Hits),
+                ("occluded", ctypes.c_void_p)]
+
+
+class BatchTuning(ctypes.Structure):
+    _fields_ = [("block_threads", ctypes.c_int32), ("stack", ctypes.c_int32), ("refill_threshold", ctypes.c_int32),
+                ("blocks_per_sm", ctypes.c_int32)]
+
+
 _vp = ctypes.c_void_p
 _i64 = ctypes.c_int64
 _SIGNATURES = {
+    "sg_batcher_create": (ctypes.c_int, [ctypes.c_int32, ctypes.c_int32, ctypes.POINTER(_vp)]),
+    "sg_batcher_destroy": (ctypes.c_int, [_vp]),
+    "sg_batcher_set_tuning": (ctypes.c_int, [_vp, ctypes.POINTER(BatchTuning)]),
+    "sg_batcher_get_tuning": (ctypes.c_int, [_vp, ctypes.POINTER(BatchTuning)]),
+    "sg_batcher_run": (ctypes.c_int, [_vp, _vp, ctypes.c_int32, _i64, _vp]),
+    "sg_batcher_wait": (ctypes.c_int, [_vp, _vp, ctypes.c_int32, _vp]),
+    "sg_batcher_autotune": (ctypes.c_int, [_vp, _vp, _vp, ctypes.c_int32, ctypes.c_int32, _vp,
+                                           ctypes.POINTER(BatchTuning), _vp]),
     "sg_default_build_opts": (None, [ctypes.POINTER(BuildOpts)]),
     "sg_scene_create": (ctypes.c_int, [_vp, _i64, ctypes.POINTER(BuildOpts), ctypes.POINTER(_vp)]),
     "sg_scene_destroy": (ctypes.c_int, [_vp]),

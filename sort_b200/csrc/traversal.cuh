@@ -1,0 +1,323 @@
+// Per-ray wide-BVH traversal shared by the traversal kernels (trace.cu, batch.cu).
+//
+// Restates Fbvh::GetIntersect (accel/fast_bvh.hpp:305-504, SIMD branch); the
+// ordering rules are listed at the top of trace.cu.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include "trace_common.cuh"
+
+namespace sg {
+
+template <int W>
+struct NodeData {
+    float lo[3][W], hi[3][W];
+    int32_t ch[W];
+};
+
+template <int W>
+__device__ __forceinline__ void load_node(const float4* __restrict__ nodes, int32_t ref, NodeData<W>& nd) {
+    const float4* p = nodes + (size_t)ref * NodeShape<W>::kF4;
+    constexpr int Q = W / 4;  // float4 per plane
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+#pragma unroll
+        for (int q = 0; q < Q; ++q) {
+            const float4 l = __ldg(p + (2 * a) * Q + q);
+            const float4 h = __ldg(p + (2 * a + 1) * Q + q);
+            nd.lo[a][4 * q + 0] = l.x;
+            nd.lo[a][4 * q + 1] = l.y;
+            nd.lo[a][4 * q + 2] = l.z;
+            nd.lo[a][4 * q + 3] = l.w;
+            nd.hi[a][4 * q + 0] = h.x;
+            nd.hi[a][4 * q + 1] = h.y;
+            nd.hi[a][4 * q + 2] = h.z;
+            nd.hi[a][4 * q + 3] = h.w;
+        }
+    }
+#pragma unroll
+    for (int q = 0; q < Q; ++q) {
+        const int4 c = __ldg(reinterpret_cast<const int4*>(p + 6 * Q + q));
+        nd.ch[4 * q + 0] = c.x;
+        nd.ch[4 * q + 1] = c.y;
+        nd.ch[4 * q + 2] = c.z;
+        nd.ch[4 * q + 3] = c.w;
+    }
+}
+
+// 8-bit node (layout.h, quantize.cpp): decode every child bound to
+// fl(origin + q * 2^e) (one rounding: q * 2^e is exact), giving FP32 boxes that
+// contain SORT's, which the unchanged slab test then uses.
+__device__ __forceinline__ float q8_bound(uint32_t word, int byte, float s, float origin) {
+    const float q = __uint_as_float(__byte_perm(word, 0x4B000000u, 0x7540u | (unsigned)byte)) - 8388608.0f;
+    return fmaf(q, s, origin);
+}
+
+template <int W>
+__device__ __forceinline__ void load_node_q8(const float4* __restrict__ nodes, int32_t ref, NodeData<W>& nd) {
+    const float4* p = nodes + (size_t)ref * (W == 8 ? kQ8F4W8 : kQ8F4W4);
+    const float4 h = __ldg(p);
+    const uint32_t eb = __float_as_uint(h.w);
+    const float org[3] = {h.x, h.y, h.z};
+    float s[3];
+#pragma unroll
+    for (int a = 0; a < 3; ++a) s[a] = __uint_as_float(((eb >> (8 * a)) & 0xffu) << 23);
+    if (W == 8) {
+#pragma unroll
+        for (int a = 0; a < 3; ++a) {
+            const uint4 q = __ldg(reinterpret_cast<const uint4*>(p + 1 + a));
+#pragma unroll
+            for (int j = 0; j < 4; ++j) {
+                nd.lo[a][j] = q8_bound(q.x, j, s[a], org[a]);
+                nd.lo[a][4 + j] = q8_bound(q.y, j, s[a], org[a]);
+                nd.hi[a][j] = q8_bound(q.z, j, s[a], org[a]);
+                nd.hi[a][4 + j] = q8_bound(q.w, j, s[a], org[a]);
+            }
+        }
+        const int4 c0 = __ldg(reinterpret_cast<const int4*>(p + 4));
+        const int4 c1 = __ldg(reinterpret_cast<const int4*>(p + 5));
+        nd.ch[0] = c0.x;
+        nd.ch[1] = c0.y;
+        nd.ch[2] = c0.z;
+        nd.ch[3] = c0.w;
+        nd.ch[4 % W] = c1.x;
+        nd.ch[5 % W] = c1.y;
+        nd.ch[6 % W] = c1.z;
+        nd.ch[7 % W] = c1.w;
+    } else {
+        const uint4 q01 = __ldg(reinterpret_cast<const uint4*>(p + 1));
+        const uint4 q2 = __ldg(reinterpret_cast<const uint4*>(p + 2));
+        const int4 c = __ldg(reinterpret_cast<const int4*>(p + 3));
+#pragma unroll
+        for (int j = 0; j < 4; ++j) {
+            nd.lo[0][j] = q8_bound(q01.x, j, s[0], org[0]);
+            nd.hi[0][j] = q8_bound(q01.y, j, s[0], org[0]);
+            nd.lo[1][j] = q8_bound(q01.z, j, s[1], org[1]);
+            nd.hi[1][j] = q8_bound(q01.w, j, s[1], org[1]);
+            nd.lo[2][j] = q8_bound(q2.x, j, s[2], org[2]);
+            nd.hi[2][j] = q8_bound(q2.y, j, s[2], org[2]);
+        }
+        nd.ch[0] = c.x;
+        nd.ch[1 % W] = c.y;
+        nd.ch[2 % W] = c.z;
+        nd.ch[3 % W] = c.w;
+    }
+}
+
+// One ray's traversal state. STATS adds SORT's traversal counters
+// (accel/fast_bvh.hpp:50-96): interior nodes box-tested, and primitives tested
+// counted per leaf entered (sIntersectionTest += pri_cnt).
+template <int W, bool ANY, int STACK, bool STATS, bool Q8 = false>
+struct Traversal {
+    RayState r;
+    float best_t, best_u, best_v;
+    int32_t best_prim;
+    int32_t cur;
+    float cur_d;
+    int si;
+    unsigned node_tests, prim_tests;
+    uint2 stk[STACK];
+
+    // Loads ray i and runs the root test; returns false when the ray is already
+    // finished (root miss or empty tree).
+    __device__ __forceinline__ bool start(const DevTree& tr, const DevRays& rays, int64_t i) {
+        r.o[0] = rays.ox[i];
+        r.o[1] = rays.oy[i];
+        r.o[2] = rays.oz[i];
+        r.d[0] = rays.dx[i];
+        r.d[1] = rays.dy[i];
+        r.d[2] = rays.dz[i];
+        r.tmin = rays.tmin[i];
+        r.tmax = rays.tmax[i];
+        return begin(tr);
+    }
+
+    // Same as start, for a ray already stored in r.o, r.d, r.tmin, r.tmax.
+    __device__ __forceinline__ bool begin(const DevTree& tr) {
+        ray_setup(r);
+        best_t = FLT_MAX;
+        best_u = best_v = 0.0f;
+        best_prim = -1;
+        node_tests = prim_tests = 0;
+        si = 0;
+        const float f0 = root_intersect(r, tr.box_lo, tr.box_hi);
+        cur = tr.root;
+        cur_d = f0;
+        return f0 >= 0.0f && tr.root != kEmpty;
+    }
+
+    __device__ __forceinline__ void finish(int64_t i, int32_t* __restrict__ prim_out, float* __restrict__ t_out,
+                                           float* __restrict__ u_out, float* __restrict__ v_out,
+                                           uint8_t* __restrict__ occ_out, unsigned long long* __restrict__ stats) {
+        if (STATS) {
+            atomicAdd(stats, (unsigned long long)node_tests);
+            atomicAdd(stats + 1, (unsigned long long)prim_tests);
+        }
+        if (ANY) {
+            occ_out[i] = best_prim >= 0 ? 1 : 0;
+        } else {
+            prim_out[i] = best_prim;
+            t_out[i] = best_prim >= 0 ? best_t : FLT_MAX;
+            if (u_out) u_out[i] = best_prim >= 0 ? best_u : 0.0f;
+            if (v_out) v_out[i] = best_prim >= 0 ? best_v : 0.0f;
+        }
+    }
+
+    // Processes the entry `cur` (a leaf, an interior node, or a culled entry).
+    // Returns true when the ray is finished.
+    __device__ __forceinline__ bool step(const DevTree& tr, int* __restrict__ err) {
+        bool descend = false;
+        if (!(best_t < cur_d)) {  // fast_bvh.hpp:343: skip when the hit is nearer than the entry
+            if (cur < 0) {
+                if (leaf(tr, cur)) return true;
+            } else {
+                if (si + W > STACK) {  // cannot happen when STACK >= depth*(W-1)+1; reported, never overrun
+                    atomicOr(err, 1);
+                    return true;
+                }
+                descend = interior(tr);
+            }
+        }
+        if (!descend) {
+            if (si == 0) return true;
+            const uint2 e = stk[--si];
+            cur = (int32_t)e.x;
+            cur_d = __uint_as_float(e.y);
+        }
+        return false;
+    }
+
+    // Leaf: triangles in leaf order; returns true on an any-hit early exit.
+    __device__ __forceinline__ bool leaf(const DevTree& tr, int32_t ref) {
+        int64_t s = (int64_t)((uint32_t)ref & 0x7fffffffu);
+        unsigned tested = 0;
+        bool found = false;
+        for (;;) {
+            const float4* q = tr.tris + 3 * s;
+            const float4 a0 = __ldg(q), b0 = __ldg(q + 1), c0 = __ldg(q + 2);
+            const float4 a1 = __ldg(q + 3), b1 = __ldg(q + 4), c1 = __ldg(q + 5);
+            float t, u, v;
+            ++tested;
+            if (tri_test(r, a0, b0, c0, t, u, v) && t < best_t) {
+                best_t = t;
+                best_u = u;
+                best_v = v;
+                best_prim = __float_as_int(a0.w);
+                if (ANY) {
+                    found = true;
+                    break;
+                }
+            }
+            if (__float_as_int(b0.w)) break;
+            ++tested;
+            if (tri_test(r, a1, b1, c1, t, u, v) && t < best_t) {
+                best_t = t;
+                best_u = u;
+                best_v = v;
+                best_prim = __float_as_int(a1.w);
+                if (ANY) {
+                    ++s;
+                    found = true;
+                    break;
+                }
+            }
+            if (__float_as_int(b1.w)) break;
+            s += 2;
+        }
+        if (STATS) {
+            if (ANY && found)  // whole leaf, as SORT counts it
+                for (int64_t q = s; !__float_as_int(__ldg(tr.tris + 3 * q + 1).w); ++q) ++tested;
+            prim_tests += tested;
+        }
+        return ANY && found;
+    }
+
+    // Interior node: box-test the children, push all hits but the nearest and
+    // descend into that one. Returns false when no child is hit.
+    __device__ __forceinline__ bool interior(const DevTree& tr) {
+        NodeData<W> nd;
+        if (Q8)
+            load_node_q8<W>(tr.nodes, cur, nd);
+        else
+            load_node<W>(tr.nodes, cur, nd);
+        if (STATS) ++node_tests;
+        float d[W];
+        unsigned mask = 0;
+#pragma unroll
+        for (int j = 0; j < W; ++j) {
+            const bool hit = slab(r, nd.lo[0][j], nd.hi[0][j], nd.lo[1][j], nd.hi[1][j], nd.lo[2][j], nd.hi[2][j], d[j]);
+            if (hit && nd.ch[j] != kEmpty) mask |= 1u << j;
+        }
+        const int cnt = __popc(mask);
+        if (cnt == 0) return false;
+        if (cnt == 1) {
+#pragma unroll
+            for (int j = 0; j < W; ++j)
+                if (mask & (1u << j)) {
+                    cur = nd.ch[j];
+                    cur_d = d[j];
+                }
+            return true;
+        }
+        if (cnt == 2) {
+            // SORT pushes the far one first when t0 < t1, else the second slot
+            // last; the one it would pop next is descended into.
+            int32_t c0 = 0, c1 = 0;
+            float t0 = 0.0f, t1 = 0.0f;
+            bool first = true;
+#pragma unroll
+            for (int j = 0; j < W; ++j) {
+                if (mask & (1u << j)) {
+                    if (first) {
+                        c0 = nd.ch[j];
+                        t0 = d[j];
+                        first = false;
+                    } else {
+                        c1 = nd.ch[j];
+                        t1 = d[j];
+                    }
+                }
+            }
+            if (t0 < t1) {
+                stk[si++] = make_uint2((uint32_t)c1, __float_as_uint(t1));
+                cur = c0;
+                cur_d = t0;
+            } else {
+                stk[si++] = make_uint2((uint32_t)c0, __float_as_uint(t0));
+                cur = c1;
+                cur_d = t1;
+            }
+            return true;
+        }
+        // >= 3 hits: SORT's selection loop (fast_bvh.hpp:438-453) pushes by
+        // decreasing distance, ties lowest slot first, only distances > -1; the
+        // last one it pushes is descended into instead.
+        unsigned left = 0;
+#pragma unroll
+        for (int j = 0; j < W; ++j) left |= (((mask >> j) & 1u) && d[j] > -1.0f) ? (1u << j) : 0u;
+        if (left == 0) return false;
+        for (;;) {
+            float best = -1.0f;
+            int32_t ref = 0;
+            unsigned pick = 0;
+#pragma unroll
+            for (int j = 0; j < W; ++j) {
+                if ((left & (1u << j)) && d[j] > best) {
+                    best = d[j];
+                    ref = nd.ch[j];
+                    pick = 1u << j;
+                }
+            }
+            left &= ~pick;
+            if (left == 0) {
+                cur = ref;
+                cur_d = best;
+                return true;
+            }
+            stk[si++] = make_uint2((uint32_t)ref, __float_as_uint(best));
+        }
+    }
+};
+
+}  // namespace sg
