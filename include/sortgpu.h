@@ -67,7 +67,8 @@ typedef enum {
     SG_ERR_OUT_OF_MEMORY = 3,
     SG_ERR_UNSUPPORTED = 4,
     SG_ERR_LIMIT = 5,
-    SG_ERR_INTERNAL = 6
+    SG_ERR_INTERNAL = 6,
+    SG_ERR_CANCELLED = 7
 } sg_status;
 
 /* Child-box storage of the device tree. */
@@ -257,6 +258,85 @@ sg_status sg_pt_destroy(sg_pt_scene* pt);
  * (any-hit) rays; synchronises `stream`. The counterpart of SORT's sRayCount /
  * sShadowRayCount (accel/accelerator.cpp:21-23). */
 sg_status sg_pt_ray_counts(const sg_pt_scene* pt, int64_t* extension, int64_t* shadow, void* stream);
+
+/* ---- Render server ------------------------------------------------------
+ * A serving loop that keeps path-tracing scenes resident and renders requests
+ * of uneven sizes concurrently: every admitted request's pixels share one pool
+ * of in-flight paths and one set of wavefront queues (extension, shadow) over
+ * all scenes; a pool slot whose path ends takes the next pixel sample of any
+ * admitted request, and requests are admitted as soon as the pixel budget
+ * frees up (continuous batching). The bounce steps run as replays of a
+ * captured CUDA graph. Each pixel's samples are accumulated in sample order
+ * with the arithmetic of sg_pt_render, so a request's image is bit-identical to
+ * sg_pt_render of the same request, alone or in any mix.
+ * No SORT counterpart as an API: SORT renders one image per process
+ * (work/image_evaluation/image_evaluation.cpp:120-305).
+ *
+ * sg_server_opts: path_slots = paths in flight (each holds about 250 bytes of
+ *   path state in HBM); pixel_budget = pixels of admitted, unfinished requests
+ *   (20 bytes each: image + work queue entry); max_requests = requests admitted
+ *   at once; steps_per_poll = bounce steps per graph replay (even, >= 2).
+ * sg_server_add_scene: all scenes of a server share one tree width and node
+ *   format (SG_ERR_UNSUPPORTED otherwise); the sg_pt_scene and its sg_scene
+ *   must outlive the server.
+ * sg_server_submit: queues a request; image is a host buffer of
+ *   width*height*3 floats that holds the result when the request completes.
+ *   A request larger than pixel_budget fails with SG_ERR_LIMIT.
+ * sg_server_wait: blocks until the ticket completes or timeout_ns passes
+ *   (SG_ERR_LIMIT, the request keeps running); timeout_ns < 0 waits forever.
+ *   Each completed ticket can be waited for once.
+ * sg_server_cancel: a queued request is dropped; an admitted one stops taking
+ *   new pixel samples and completes once its paths in flight end; either way
+ *   its result reports SG_ERR_CANCELLED and its image is not written. */
+typedef struct {
+    int32_t device;
+    int32_t max_requests;
+    int64_t path_slots;
+    int64_t pixel_budget;
+    int32_t steps_per_poll;
+    int32_t reserved;
+} sg_server_opts;
+
+typedef struct {
+    int32_t scene;  /* from sg_server_add_scene */
+    int32_t width;
+    int32_t height;
+    int32_t spp;
+    int32_t max_depth;
+    int32_t reserved;
+    uint64_t seed;
+    float camera[10]; /* as sg_pt_render */
+    float* image;     /* host, width*height*3 floats */
+} sg_request;
+
+typedef struct {
+    int64_t ticket;
+    int32_t status;     /* SG_OK, SG_ERR_CANCELLED, or the error that ended it */
+    int32_t reserved;
+    int64_t submit_ns;  /* steady clock of the host */
+    int64_t admit_ns;
+    int64_t done_ns;    /* image in host memory */
+} sg_request_result;
+
+typedef struct {
+    int64_t requests_done;
+    int64_t samples_done;     /* pixel samples accumulated */
+    int64_t extension_rays;   /* closest-hit rays traced */
+    int64_t shadow_rays;      /* any-hit rays traced */
+    int64_t graph_replays;
+    int64_t queued;           /* submitted, not admitted */
+    int64_t admitted;         /* admitted, not complete */
+} sg_server_stats;
+
+typedef struct sg_server sg_server;
+void sg_default_server_opts(sg_server_opts* opts);
+sg_status sg_server_create(const sg_server_opts* opts, sg_server** out);
+sg_status sg_server_add_scene(sg_server* server, const sg_pt_scene* pt, int32_t* scene_id);
+sg_status sg_server_submit(sg_server* server, const sg_request* request, int64_t* ticket);
+sg_status sg_server_wait(sg_server* server, int64_t ticket, int64_t timeout_ns, sg_request_result* result);
+sg_status sg_server_cancel(sg_server* server, int64_t ticket);
+sg_status sg_server_stats_get(sg_server* server, sg_server_stats* stats);
+sg_status sg_server_destroy(sg_server* server);
 
 const char* sg_last_error(void);
 const char* sg_version(void);

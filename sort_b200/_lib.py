@@ -15,8 +15,10 @@ SG_OK = 0
 SG_NODES_FP32 = 0
 SG_NODES_QUANT8 = 1
 
+SG_ERR_LIMIT = 5
+SG_ERR_CANCELLED = 7
 STATUS_NAMES = {0: "SG_OK", 1: "SG_ERR_INVALID_ARGUMENT", 2: "SG_ERR_CUDA", 3: "SG_ERR_OUT_OF_MEMORY",
-                4: "SG_ERR_UNSUPPORTED", 5: "SG_ERR_LIMIT", 6: "SG_ERR_INTERNAL"}
+                4: "SG_ERR_UNSUPPORTED", 5: "SG_ERR_LIMIT", 6: "SG_ERR_INTERNAL", 7: "SG_ERR_CANCELLED"}
 
 
 class SortGpuError(RuntimeError):
@@ -62,9 +64,38 @@ class BatchTuning(ctypes.Structure):
                 ("blocks_per_sm", ctypes.c_int32)]
 
 
+class ServerOpts(ctypes.Structure):
+    _fields_ = [("device", ctypes.c_int32), ("max_requests", ctypes.c_int32), ("path_slots", ctypes.c_int64),
+                ("pixel_budget", ctypes.c_int64), ("steps_per_poll", ctypes.c_int32), ("reserved", ctypes.c_int32)]
+
+
+class Request(ctypes.Structure):
+    _fields_ = [("scene", ctypes.c_int32), ("width", ctypes.c_int32), ("height", ctypes.c_int32),
+                ("spp", ctypes.c_int32), ("max_depth", ctypes.c_int32), ("reserved", ctypes.c_int32),
+                ("seed", ctypes.c_uint64), ("camera", ctypes.c_float * 10), ("image", ctypes.c_void_p)]
+
+
+class RequestResult(ctypes.Structure):
+    _fields_ = [("ticket", ctypes.c_int64), ("status", ctypes.c_int32), ("reserved", ctypes.c_int32),
+                ("submit_ns", ctypes.c_int64), ("admit_ns", ctypes.c_int64), ("done_ns", ctypes.c_int64)]
+
+
+class ServerStats(ctypes.Structure):
+    _fields_ = [(name, ctypes.c_int64) for name in ("requests_done", "samples_done", "extension_rays", "shadow_rays",
+                                                    "graph_replays", "queued", "admitted")]
+
+
 _vp = ctypes.c_void_p
 _i64 = ctypes.c_int64
 _SIGNATURES = {
+    "sg_default_server_opts": (None, [ctypes.POINTER(ServerOpts)]),
+    "sg_server_create": (ctypes.c_int, [ctypes.POINTER(ServerOpts), ctypes.POINTER(_vp)]),
+    "sg_server_add_scene": (ctypes.c_int, [_vp, _vp, ctypes.POINTER(ctypes.c_int32)]),
+    "sg_server_submit": (ctypes.c_int, [_vp, ctypes.POINTER(Request), ctypes.POINTER(_i64)]),
+    "sg_server_wait": (ctypes.c_int, [_vp, _i64, _i64, ctypes.POINTER(RequestResult)]),
+    "sg_server_cancel": (ctypes.c_int, [_vp, _i64]),
+    "sg_server_stats_get": (ctypes.c_int, [_vp, ctypes.POINTER(ServerStats)]),
+    "sg_server_destroy": (ctypes.c_int, [_vp]),
     "sg_batcher_create": (ctypes.c_int, [ctypes.c_int32, ctypes.c_int32, ctypes.POINTER(_vp)]),
     "sg_batcher_destroy": (ctypes.c_int, [_vp]),
     "sg_batcher_set_tuning": (ctypes.c_int, [_vp, ctypes.POINTER(BatchTuning)]),

@@ -188,6 +188,39 @@ sg_status pt_fail(cudaError_t e) { return sg::set_error(SG_ERR_CUDA, cudaGetErro
 
 }  // namespace
 
+namespace sg {
+
+// Perspective pinhole, as the oracle harness builds SORT's PerspectiveCamera.
+Cam make_camera(const float* camera, int width, int height) {
+    Cam cam;
+    const float3 eye = make_float3(camera[0], camera[1], camera[2]);
+    float3 fwd = make_float3(camera[3] - eye.x, camera[4] - eye.y, camera[5] - eye.z);
+    const float fl = std::sqrt(fwd.x * fwd.x + fwd.y * fwd.y + fwd.z * fwd.z);
+    fwd = make_float3(fwd.x / fl, fwd.y / fl, fwd.z / fl);
+    const float3 up = make_float3(camera[6], camera[7], camera[8]);
+    float3 right = make_float3(fwd.y * up.z - fwd.z * up.y, fwd.z * up.x - fwd.x * up.z, fwd.x * up.y - fwd.y * up.x);
+    const float rl = std::sqrt(right.x * right.x + right.y * right.y + right.z * right.z);
+    right = make_float3(right.x / rl, right.y / rl, right.z / rl);
+    const float3 upv = make_float3(right.y * fwd.z - right.z * fwd.y, right.z * fwd.x - right.x * fwd.z,
+                                   right.x * fwd.y - right.y * fwd.x);
+    cam.eye = eye;
+    cam.fwd = fwd;
+    cam.right = right;
+    cam.up = upv;
+    cam.half_h = std::tan(camera[9] * 3.14159265358979f / 180.0f * 0.5f);
+    cam.half_w = cam.half_h * (float)width / (float)height;
+    return cam;
+}
+
+sg_status pt_scene_parts(const sg_pt_scene* ps, PtDev* dev, const sg_scene** scene) {
+    if (!ps || !dev || !scene) return set_error(SG_ERR_INVALID_ARGUMENT, "NULL path-tracing scene");
+    *dev = PtDev{ps->d_prim, ps->d_mats, ps->light};
+    *scene = ps->scene;
+    return SG_OK;
+}
+
+}  // namespace sg
+
 extern "C" sg_status sg_pt_create(const sg_scene* scene, const float* triangles, int64_t ntri, const int32_t* mat_of_tri,
                                   const float* materials, int32_t nmat, const float* light, sg_pt_scene** out) {
     if (!scene || !out || !light || (ntri > 0 && (!triangles || !mat_of_tri)) || nmat < 0 || (nmat > 0 && !materials))
@@ -333,25 +366,7 @@ extern "C" sg_status sg_pt_render(sg_pt_scene* ps, const float* camera, int32_t 
     ps->d_totals = totals;
     if ((e = cudaMemsetAsync(totals, 0, 16, s)) != cudaSuccess) return pt_fail(e);
 
-    // Camera (perspective pinhole, as the oracle harness builds it).
-    sg::Cam cam;
-    const float3 eye = make_float3(camera[0], camera[1], camera[2]);
-    float3 fwd = make_float3(camera[3] - eye.x, camera[4] - eye.y, camera[5] - eye.z);
-    const float fl = std::sqrt(fwd.x * fwd.x + fwd.y * fwd.y + fwd.z * fwd.z);
-    fwd = make_float3(fwd.x / fl, fwd.y / fl, fwd.z / fl);
-    const float3 up = make_float3(camera[6], camera[7], camera[8]);
-    float3 right = make_float3(fwd.y * up.z - fwd.z * up.y, fwd.z * up.x - fwd.x * up.z, fwd.x * up.y - fwd.y * up.x);
-    const float rl = std::sqrt(right.x * right.x + right.y * right.y + right.z * right.z);
-    right = make_float3(right.x / rl, right.y / rl, right.z / rl);
-    const float3 upv = make_float3(right.y * fwd.z - right.z * fwd.y, right.z * fwd.x - right.x * fwd.z,
-                                   right.x * fwd.y - right.y * fwd.x);
-    cam.eye = eye;
-    cam.fwd = fwd;
-    cam.right = right;
-    cam.up = upv;
-    cam.half_h = std::tan(camera[9] * 3.14159265358979f / 180.0f * 0.5f);
-    cam.half_w = cam.half_h * (float)width / (float)height;
-
+    const sg::Cam cam = sg::make_camera(camera, width, height);
     const uint2 key = make_uint2((uint32_t)seed, (uint32_t)(seed >> 32));
     sg::PtDev dev{ps->d_prim, ps->d_mats, ps->light};
     const int threads = 256;

@@ -9,6 +9,8 @@
 #include <cfloat>
 #include <cstdint>
 
+#include "pt_types.h"
+
 namespace sg {
 
 // SORT's constants (math/utils.h:28-32).
@@ -16,30 +18,10 @@ constexpr float kPi = 3.1415926f;
 constexpr float kTwoPi = 6.2831852f;
 constexpr float kInvPi = 0.3183099f;
 
-struct PtMaterial {
-    int type;  // 0 Lambert, 1 GGX conductor reflection, 2 the light's own surface (white Lambert)
-    float a[3];
-    float k[3];
-    float rough;
-};
-
-struct PtLight {
-    float c[3];
-    float hx, hz;
-    float I[3];
-    float area;
-};
-
 struct Queue {
     float* ray;     // 8 * cap floats, SoA
     int* slot;      // path (pixel) per entry
     float* contrib; // shadow queue only: 3 * cap
-};
-
-struct PtDev {
-    const float4* prim;  // per primitive: geometric normal, material id (bits of w)
-    const PtMaterial* mats;
-    PtLight light;
 };
 
 // ---------------------------------------------------------------------------
@@ -243,11 +225,6 @@ __device__ __forceinline__ void put_ray(float* q, int cap, int i, float3 o, floa
     q[6 * cap + i] = tmin;
     q[7 * cap + i] = tmax;
 }
-
-struct Cam {
-    float3 eye, fwd, right, up;
-    float half_w, half_h;
-};
 
 // Pinhole camera ray through pixel p (jittered by the sample's random numbers),
 // as the reference harness's PerspectiveCamera builds it.

@@ -19,4 +19,8 @@ sg_status scene_launch(const sg_scene* s, bool any, TraceLaunch* L, DevTree* tre
 // Synchronises st and reports the traversal status word of scene s.
 sg_status scene_status(const sg_scene* s, cudaStream_t st);
 
+struct PtDev;
+// The shading tables of a path-tracing scene and the traversal scene it uses.
+sg_status pt_scene_parts(const sg_pt_scene* ps, PtDev* dev, const sg_scene** scene);
+
 }  // namespace sg

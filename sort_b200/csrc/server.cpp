@@ -1,0 +1,604 @@
+// sg_server (include/sortgpu.h): the host side of the render server.
+//
+// One loop thread per server owns the GPU work: it admits queued requests
+// (FIFO) while a request-table slot and a contiguous image range of the pixel
+// budget are free, stages the admissions, replays the captured bounce-step
+// graph, and reads the per-request completion flags of the previous replay
+// while the next one runs (two replays in flight). A completed request's
+// image is copied to its host buffer on a second stream, then its slot and
+// image range are released and its waiters are woken.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <chrono>
+#include <condition_variable>
+#include <cstring>
+#include <deque>
+#include <map>
+#include <mutex>
+#include <new>
+#include <string>
+#include <thread>
+#include <unordered_map>
+#include <vector>
+
+#include "scene_access.h"
+#include "serve_kernels.h"
+#include "sortgpu.h"
+#include "trace_kernels.h"
+
+namespace {
+
+constexpr int kMaxScenes = 64;
+
+int64_t now_ns() {
+    return std::chrono::duration_cast<std::chrono::nanoseconds>(std::chrono::steady_clock::now().time_since_epoch())
+        .count();
+}
+
+size_t align_up(size_t x) { return (x + 255) & ~size_t(255); }
+
+sg_status fail(sg_status s, const std::string& msg) { return sg::set_error(s, msg.c_str()); }
+
+// First-fit allocator of pixel ranges of the image arena.
+class Arena {
+public:
+    explicit Arena(int64_t n) {
+        if (n > 0) free_[0] = n;
+    }
+    int64_t alloc(int64_t n) {
+        for (auto it = free_.begin(); it != free_.end(); ++it) {
+            if (it->second < n) continue;
+            const int64_t off = it->first, len = it->second;
+            free_.erase(it);
+            if (len > n) free_[off + n] = len - n;
+            return off;
+        }
+        return -1;
+    }
+    void release(int64_t off, int64_t n) {
+        auto it = free_.emplace(off, n).first;
+        auto next = std::next(it);
+        if (next != free_.end() && it->first + it->second == next->first) {
+            it->second += next->second;
+            free_.erase(next);
+        }
+        if (it != free_.begin()) {
+            auto prev = std::prev(it);
+            if (prev->first + prev->second == it->first) {
+                prev->second += it->second;
+                free_.erase(it);
+            }
+        }
+    }
+
+private:
+    std::map<int64_t, int64_t> free_;
+};
+
+struct Ticket {
+    sg_request req{};
+    int64_t submit_ns = 0, admit_ns = 0, done_ns = 0;
+    int status = SG_OK;
+    int slot = -1;         // request-table index while admitted
+    int64_t arena = -1;    // first pixel of its image range
+    int64_t replay = -1;   // first replay that sees it admitted
+    bool cancel = false;
+    bool complete = false;
+};
+
+}  // namespace
+
+struct sg_server {
+    sg_server_opts opts{};
+    int width = 0;
+    int node_format = -1;
+    int stack_need = 1;
+    std::mutex mu;
+    std::condition_variable cv_work, cv_done;
+    std::thread loop;
+    bool stop = false;
+    sg_status loop_status = SG_OK;
+    std::string loop_msg;
+    int64_t next_ticket = 1;
+    std::deque<int64_t> pending;
+    std::unordered_map<int64_t, Ticket> tickets;
+    std::vector<int64_t> slot_ticket;
+    std::vector<int> free_slots;
+    std::vector<int> to_cancel;
+    Arena arena{0};
+    int64_t admitted = 0;
+    std::vector<sg::SrvScene> scenes;
+    sg_server_stats stats{};
+    // device
+    char* d_mem = nullptr;
+    sg::SrvBuffers b{};
+    sg::SrvRequest* d_requests = nullptr;
+    sg::SrvScene* d_scenes = nullptr;
+    sg::SrvControl* d_control = nullptr;
+    sg::SrvCounters* d_counters = nullptr;
+    float* d_images = nullptr;
+    // host (pinned)
+    sg::SrvRequest* h_requests = nullptr;
+    unsigned* h_units = nullptr;
+    sg::SrvControl* h_control[2] = {};
+    int* h_done[2] = {};
+    sg::SrvCounters* h_counters[2] = {};
+    cudaStream_t stream = nullptr, copy_stream = nullptr;
+    cudaEvent_t replay_done[2] = {}, copy_done = nullptr;
+    cudaGraphExec_t graph = nullptr;
+    int graph_stack = 0;
+};
+
+namespace {
+
+void free_server(sg_server* S) {
+    cudaSetDevice(S->opts.device);
+    if (S->stream) cudaStreamSynchronize(S->stream);
+    if (S->copy_stream) cudaStreamSynchronize(S->copy_stream);
+    if (S->graph) cudaGraphExecDestroy(S->graph);
+    for (int k = 0; k < 2; ++k) {
+        if (S->h_control[k]) cudaFreeHost(S->h_control[k]);
+        if (S->h_done[k]) cudaFreeHost(S->h_done[k]);
+        if (S->h_counters[k]) cudaFreeHost(S->h_counters[k]);
+        if (S->replay_done[k]) cudaEventDestroy(S->replay_done[k]);
+    }
+    if (S->copy_done) cudaEventDestroy(S->copy_done);
+    if (S->h_requests) cudaFreeHost(S->h_requests);
+    if (S->h_units) cudaFreeHost(S->h_units);
+    if (S->stream) cudaStreamDestroy(S->stream);
+    if (S->copy_stream) cudaStreamDestroy(S->copy_stream);
+    if (S->d_mem) cudaFree(S->d_mem);
+    delete S;
+}
+
+// Called with S->mu held: ends a ticket and wakes its waiters.
+void complete(sg_server* S, Ticket& t, int status) {
+    t.status = status;
+    t.done_ns = now_ns();
+    t.complete = true;
+    S->cv_done.notify_all();
+}
+
+sg_status capture(sg_server* S) {
+    const int stack = S->stack_need <= 64 ? 64 : S->stack_need <= 128 ? 128 : 256;
+    if (S->graph && S->graph_stack == stack) return SG_OK;
+    if (S->graph) {
+        cudaGraphExecDestroy(S->graph);
+        S->graph = nullptr;
+    }
+    cudaError_t e = cudaStreamBeginCapture(S->stream, cudaStreamCaptureModeThreadLocal);
+    if (e != cudaSuccess) return fail(SG_ERR_CUDA, std::string("begin capture: ") + cudaGetErrorString(e));
+    cudaError_t le = sg::srv_enqueue_steps(S->b, S->opts.steps_per_poll, S->width, stack,
+                                           S->node_format == SG_NODES_QUANT8, S->stream);
+    cudaGraph_t g = nullptr;
+    e = cudaStreamEndCapture(S->stream, &g);
+    if (le != cudaSuccess || e != cudaSuccess) {
+        if (g) cudaGraphDestroy(g);
+        return fail(SG_ERR_CUDA, std::string("capture bounce steps: ") + cudaGetErrorString(le != cudaSuccess ? le : e));
+    }
+    e = cudaGraphInstantiate(&S->graph, g, 0);
+    cudaGraphDestroy(g);
+    if (e != cudaSuccess) return fail(SG_ERR_CUDA, std::string("instantiate: ") + cudaGetErrorString(e));
+    S->graph_stack = stack;
+    return SG_OK;
+}
+
+// Admits queued requests into the control block of the next replay (S->mu held).
+void admit(sg_server* S, sg::SrvControl& ctl, int64_t replay) {
+    ctl.nadmit = 0;
+    ctl.admit_total = 0;
+    while (!S->pending.empty() && ctl.nadmit < sg::kSrvMaxAdmit && !S->free_slots.empty()) {
+        const int64_t id = S->pending.front();
+        Ticket& t = S->tickets[id];
+        const int64_t P = int64_t(t.req.width) * t.req.height;
+        const int64_t off = S->arena.alloc(P);
+        if (off < 0) break;  // FIFO: wait for image memory
+        S->pending.pop_front();
+        const int r = S->free_slots.back();
+        S->free_slots.pop_back();
+        sg::SrvRequest& q = S->h_requests[r];
+        q = sg::SrvRequest{};
+        q.cam = sg::make_camera(t.req.camera, t.req.width, t.req.height);
+        q.key = make_uint2((uint32_t)t.req.seed, (uint32_t)(t.req.seed >> 32));
+        q.image = S->d_images + 3 * off;
+        q.scene = t.req.scene;
+        q.width = t.req.width;
+        q.height = t.req.height;
+        q.spp = t.req.spp;
+        q.max_depth = t.req.max_depth;
+        q.inv_spp = 1.0f / (float)t.req.spp;
+        q.cancelled = 0;
+        S->h_units[r] = (unsigned)P;
+        cudaMemcpyAsync(S->d_requests + r, &q, sizeof(q), cudaMemcpyHostToDevice, S->stream);
+        cudaMemsetAsync(q.image, 0, size_t(P) * 3 * sizeof(float), S->stream);
+        cudaMemcpyAsync(S->b.units_left + r, &S->h_units[r], sizeof(unsigned), cudaMemcpyHostToDevice, S->stream);
+        cudaMemsetAsync(S->b.done + r, 0, sizeof(int), S->stream);
+        ctl.admit[ctl.nadmit].request = r;
+        ctl.admit[ctl.nadmit].pixels = (int32_t)P;
+        ctl.admit[ctl.nadmit].first = ctl.admit_total;
+        ctl.nadmit++;
+        ctl.admit_total += P;
+        t.slot = r;
+        t.arena = off;
+        t.replay = replay;
+        t.admit_ns = now_ns();
+        S->slot_ticket[size_t(r)] = id;
+        S->admitted++;
+    }
+    for (int r : S->to_cancel) {
+        S->h_requests[r].cancelled = 1;
+        cudaMemcpyAsync(&S->d_requests[r].cancelled, &S->h_requests[r].cancelled, sizeof(int32_t),
+                        cudaMemcpyHostToDevice, S->stream);
+    }
+    S->to_cancel.clear();
+}
+
+// Reads the completion flags of replay k and hands out finished requests.
+sg_status collect(sg_server* S, int k, int64_t replay) {
+    cudaError_t e = cudaEventSynchronize(S->replay_done[k]);
+    if (e != cudaSuccess) return fail(SG_ERR_CUDA, std::string("bounce steps: ") + cudaGetErrorString(e));
+    std::vector<int64_t> done;
+    {
+        std::lock_guard<std::mutex> lk(S->mu);
+        for (size_t r = 0; r < S->slot_ticket.size(); ++r) {
+            const int64_t id = S->slot_ticket[r];
+            if (id < 0 || !S->h_done[k][r]) continue;
+            Ticket& t = S->tickets[id];
+            if (t.replay > replay) continue;  // admitted after this replay
+            done.push_back(id);
+        }
+        const sg::SrvCounters& c = *S->h_counters[k];
+        S->stats.samples_done = (int64_t)c.samples;
+        S->stats.extension_rays = (int64_t)c.ext_rays;
+        S->stats.shadow_rays = (int64_t)c.shadow_rays;
+    }
+    if (done.empty()) return SG_OK;
+    if ((e = cudaStreamWaitEvent(S->copy_stream, S->replay_done[k], 0)) != cudaSuccess)
+        return fail(SG_ERR_CUDA, cudaGetErrorString(e));
+    {
+        std::lock_guard<std::mutex> lk(S->mu);
+        for (int64_t id : done) {
+            Ticket& t = S->tickets[id];
+            if (t.cancel) continue;
+            const size_t bytes = size_t(t.req.width) * t.req.height * 3 * sizeof(float);
+            if ((e = cudaMemcpyAsync(t.req.image, S->d_images + 3 * t.arena, bytes, cudaMemcpyDeviceToHost,
+                                     S->copy_stream)) != cudaSuccess)
+                return fail(SG_ERR_CUDA, std::string("copy image: ") + cudaGetErrorString(e));
+        }
+    }
+    if ((e = cudaEventRecord(S->copy_done, S->copy_stream)) != cudaSuccess ||
+        (e = cudaEventSynchronize(S->copy_done)) != cudaSuccess)
+        return fail(SG_ERR_CUDA, std::string("copy image: ") + cudaGetErrorString(e));
+    std::lock_guard<std::mutex> lk(S->mu);
+    for (int64_t id : done) {
+        Ticket& t = S->tickets[id];
+        const int64_t P = int64_t(t.req.width) * t.req.height;
+        S->arena.release(t.arena, P);
+        S->slot_ticket[size_t(t.slot)] = -1;
+        S->free_slots.push_back(t.slot);
+        t.slot = -1;
+        S->admitted--;
+        S->stats.requests_done++;
+        complete(S, t, t.cancel ? SG_ERR_CANCELLED : SG_OK);
+    }
+    S->cv_work.notify_all();
+    return SG_OK;
+}
+
+void serve_loop(sg_server* S) {
+    cudaSetDevice(S->opts.device);
+    int64_t j = 0;
+    bool inflight = false;
+    sg_status st = SG_OK;
+    for (;;) {
+        bool launch = false;
+        {
+            std::unique_lock<std::mutex> lk(S->mu);
+            if (!inflight)
+                S->cv_work.wait(lk, [&] { return S->stop || !S->pending.empty() || S->admitted > 0; });
+            if (S->stop) break;
+            admit(S, *S->h_control[j % 2], j);
+            launch = S->admitted > 0;
+        }
+        if (launch) {
+            cudaError_t e = cudaSuccess;
+            if ((st = capture(S)) != SG_OK) break;
+            e = cudaMemcpyAsync(S->d_control, S->h_control[j % 2], sizeof(sg::SrvControl), cudaMemcpyHostToDevice,
+                                S->stream);
+            if (e == cudaSuccess) e = cudaGraphLaunch(S->graph, S->stream);
+            if (e == cudaSuccess)
+                e = cudaMemcpyAsync(S->h_done[j % 2], S->b.done, sizeof(int) * size_t(S->opts.max_requests),
+                                    cudaMemcpyDeviceToHost, S->stream);
+            if (e == cudaSuccess)
+                e = cudaMemcpyAsync(S->h_counters[j % 2], S->d_counters, sizeof(sg::SrvCounters),
+                                    cudaMemcpyDeviceToHost, S->stream);
+            if (e == cudaSuccess) e = cudaEventRecord(S->replay_done[j % 2], S->stream);
+            if (e != cudaSuccess) {
+                st = fail(SG_ERR_CUDA, std::string("replay: ") + cudaGetErrorString(e));
+                break;
+            }
+            std::lock_guard<std::mutex> lk(S->mu);
+            S->stats.graph_replays++;
+        }
+        if (inflight && (st = collect(S, int((j - 1) % 2), j - 1)) != SG_OK) break;
+        inflight = launch;
+        if (launch) ++j;
+    }
+    if (st == SG_OK && inflight) st = collect(S, int((j - 1) % 2), j - 1);
+    cudaStreamSynchronize(S->stream);
+    std::lock_guard<std::mutex> lk(S->mu);
+    if (st != SG_OK) {
+        S->loop_status = st;
+        S->loop_msg = sg_last_error();
+    }
+    for (auto& kv : S->tickets)
+        if (!kv.second.complete) complete(S, kv.second, st != SG_OK ? int(st) : int(SG_ERR_CANCELLED));
+    S->pending.clear();
+    S->stop = true;
+}
+
+}  // namespace
+
+extern "C" {
+
+void sg_default_server_opts(sg_server_opts* o) {
+    if (!o) return;
+    o->device = 0;
+    o->max_requests = 1024;
+    o->path_slots = int64_t(1) << 20;
+    o->pixel_budget = int64_t(1) << 24;
+    o->steps_per_poll = 4;
+    o->reserved = 0;
+}
+
+sg_status sg_server_create(const sg_server_opts* opts, sg_server** out) {
+    if (!opts || !out) return fail(SG_ERR_INVALID_ARGUMENT, "NULL argument");
+    *out = nullptr;
+    const sg_server_opts& o = *opts;
+    if (o.max_requests < 1 || o.max_requests > 65535) return fail(SG_ERR_INVALID_ARGUMENT, "max_requests out of range");
+    if (o.path_slots < 32 || o.path_slots > (int64_t(1) << 28))
+        return fail(SG_ERR_INVALID_ARGUMENT, "path_slots out of range");
+    if (o.pixel_budget < 1 || o.pixel_budget > (int64_t(1) << 31))
+        return fail(SG_ERR_INVALID_ARGUMENT, "pixel_budget out of range");
+    if (o.steps_per_poll < 2 || o.steps_per_poll % 2 != 0 || o.steps_per_poll > 64)
+        return fail(SG_ERR_INVALID_ARGUMENT, "steps_per_poll must be even, 2..64");
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || o.device < 0 || o.device >= ndev)
+        return fail(SG_ERR_INVALID_ARGUMENT, "no such CUDA device");
+    int prev = -1;
+    cudaGetDevice(&prev);
+    cudaSetDevice(o.device);
+    sg_server* S = new (std::nothrow) sg_server;
+    if (!S) return fail(SG_ERR_OUT_OF_MEMORY, "host allocation failed");
+    S->opts = o;
+    S->arena = Arena(o.pixel_budget);
+    S->slot_ticket.assign(size_t(o.max_requests), -1);
+    for (int r = o.max_requests - 1; r >= 0; --r) S->free_slots.push_back(r);
+    const size_t C = size_t(o.path_slots), R = size_t(o.max_requests), P = size_t(o.pixel_budget);
+    // Device layout.
+    sg::SrvBuffers& b = S->b;
+    int* st_arrays[5];
+    float* ray_q[3];
+    int* slot_q[3];
+    int* scene_q[3];
+    size_t total = 0;
+    std::vector<size_t> offs;
+    auto add = [&](size_t bytes) {
+        offs.push_back(total);
+        total += align_up(bytes);
+    };
+    add(R * sizeof(sg::SrvRequest));          // 0 requests
+    add(kMaxScenes * sizeof(sg::SrvScene));  // 1 scenes
+    add(sizeof(sg::SrvControl));             // 2 control
+    add(sizeof(sg::SrvCounters));            // 3 counters
+    add(R * sizeof(unsigned));               // 4 units_left
+    add(R * sizeof(int));                    // 5 done
+    add(P * sizeof(unsigned long long));     // 6 ring
+    add(P * 3 * sizeof(float));              // 7 images
+    for (int k = 0; k < 5; ++k) add(C * sizeof(int));  // 8..12 slot state
+    add(C * 6 * sizeof(float));              // 13 thr
+    add(C * 6 * sizeof(float));              // 14 vis
+    for (int k = 0; k < 2; ++k) {            // 15..20 extension queues
+        add(C * 8 * sizeof(float));
+        add(C * sizeof(int));
+        add(C * sizeof(int));
+    }
+    add(C * sizeof(int32_t));                // 21 hit prim
+    add(C * sizeof(float));                  // 22 hit t
+    add(2 * C * 8 * sizeof(float));          // 23 shadow rays
+    add(2 * C * sizeof(int));                // 24 shadow slots
+    add(2 * C * sizeof(int));                // 25 shadow scenes
+    add(2 * C * 3 * sizeof(float));          // 26 contributions
+    add(2 * C);                              // 27 occlusion
+    add(sizeof(int));                        // 28 status
+    cudaError_t e = cudaMalloc(&S->d_mem, total);
+    if (e != cudaSuccess) {
+        free_server(S);
+        if (prev >= 0) cudaSetDevice(prev);
+        return fail(e == cudaErrorMemoryAllocation ? SG_ERR_OUT_OF_MEMORY : SG_ERR_CUDA, "server buffers");
+    }
+    char* m = S->d_mem;
+    S->d_requests = reinterpret_cast<sg::SrvRequest*>(m + offs[0]);
+    S->d_scenes = reinterpret_cast<sg::SrvScene*>(m + offs[1]);
+    S->d_control = reinterpret_cast<sg::SrvControl*>(m + offs[2]);
+    S->d_counters = reinterpret_cast<sg::SrvCounters*>(m + offs[3]);
+    S->d_images = reinterpret_cast<float*>(m + offs[7]);
+    for (int k = 0; k < 5; ++k) st_arrays[k] = reinterpret_cast<int*>(m + offs[8 + k]);
+    for (int k = 0; k < 2; ++k) {
+        ray_q[k] = reinterpret_cast<float*>(m + offs[15 + 3 * k]);
+        slot_q[k] = reinterpret_cast<int*>(m + offs[16 + 3 * k]);
+        scene_q[k] = reinterpret_cast<int*>(m + offs[17 + 3 * k]);
+    }
+    b.requests = S->d_requests;
+    b.scenes = S->d_scenes;
+    b.control = S->d_control;
+    b.counters = S->d_counters;
+    b.units_left = reinterpret_cast<unsigned*>(m + offs[4]);
+    b.done = reinterpret_cast<int*>(m + offs[5]);
+    b.ring = reinterpret_cast<unsigned long long*>(m + offs[6]);
+    b.ring_cap = int64_t(P);
+    b.slots = int64_t(C);
+    b.st_req = st_arrays[0];
+    b.st_pix = st_arrays[1];
+    b.st_sample = st_arrays[2];
+    b.st_bounce = st_arrays[3];
+    b.st_state = st_arrays[4];
+    b.thr = reinterpret_cast<float*>(m + offs[13]);
+    b.vis = reinterpret_cast<float*>(m + offs[14]);
+    b.qa_ray = ray_q[0];
+    b.qa_slot = slot_q[0];
+    b.qa_scene = scene_q[0];
+    b.qb_ray = ray_q[1];
+    b.qb_slot = slot_q[1];
+    b.qb_scene = scene_q[1];
+    b.hit_prim = reinterpret_cast<int32_t*>(m + offs[21]);
+    b.hit_t = reinterpret_cast<float*>(m + offs[22]);
+    b.sq_ray = reinterpret_cast<float*>(m + offs[23]);
+    b.sq_slot = reinterpret_cast<int*>(m + offs[24]);
+    b.sq_scene = reinterpret_cast<int*>(m + offs[25]);
+    b.sq_contrib = reinterpret_cast<float*>(m + offs[26]);
+    b.occ = reinterpret_cast<uint8_t*>(m + offs[27]);
+    b.err = reinterpret_cast<int*>(m + offs[28]);
+    // Zeroed state: counters, idle slots (kSlotIdle == 0), flags, status.
+    e = cudaMemset(S->d_mem, 0, offs[6]);
+    if (e == cudaSuccess) e = cudaMemset(m + offs[8], 0, offs[13] - offs[8]);
+    if (e == cudaSuccess) e = cudaMemset(b.err, 0, sizeof(int));
+    if (e == cudaSuccess) e = cudaMallocHost(&S->h_requests, R * sizeof(sg::SrvRequest));
+    if (e == cudaSuccess) e = cudaMallocHost(&S->h_units, R * sizeof(unsigned));
+    for (int k = 0; k < 2 && e == cudaSuccess; ++k) {
+        e = cudaMallocHost(&S->h_control[k], sizeof(sg::SrvControl));
+        if (e == cudaSuccess) e = cudaMallocHost(&S->h_done[k], R * sizeof(int));
+        if (e == cudaSuccess) e = cudaMallocHost(&S->h_counters[k], sizeof(sg::SrvCounters));
+        if (e == cudaSuccess) e = cudaEventCreateWithFlags(&S->replay_done[k], cudaEventDisableTiming);
+    }
+    if (e == cudaSuccess) e = cudaEventCreateWithFlags(&S->copy_done, cudaEventDisableTiming);
+    if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&S->stream, cudaStreamNonBlocking);
+    if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&S->copy_stream, cudaStreamNonBlocking);
+    if (prev >= 0) cudaSetDevice(prev);
+    if (e != cudaSuccess) {
+        free_server(S);
+        return fail(SG_ERR_CUDA, std::string("server setup: ") + cudaGetErrorString(e));
+    }
+    S->loop = std::thread(serve_loop, S);
+    *out = S;
+    return SG_OK;
+}
+
+sg_status sg_server_add_scene(sg_server* S, const sg_pt_scene* pt, int32_t* scene_id) {
+    if (!S || !pt || !scene_id) return fail(SG_ERR_INVALID_ARGUMENT, "NULL argument");
+    sg::SrvScene sc{};
+    const sg_scene* scene = nullptr;
+    sg_status st = sg::pt_scene_parts(pt, &sc.pt, &scene);
+    if (st != SG_OK) return st;
+    sg::TraceLaunch L;
+    int device = 0;
+    if ((st = sg::scene_launch(scene, false, &L, &sc.tree, &device)) != SG_OK) return st;
+    if (device != S->opts.device) return fail(SG_ERR_INVALID_ARGUMENT, "scene lives on another device");
+    const int fmt = L.q8 ? SG_NODES_QUANT8 : SG_NODES_FP32;
+    std::lock_guard<std::mutex> lk(S->mu);
+    if (int(S->scenes.size()) >= kMaxScenes) return fail(SG_ERR_LIMIT, "too many scenes");
+    if (!S->scenes.empty() && (S->width != L.width || S->node_format != fmt))
+        return fail(SG_ERR_UNSUPPORTED, "all scenes of a server share one tree width and node format");
+    if (L.stack_need > 256) return fail(SG_ERR_LIMIT, "tree too deep for the traversal stack");
+    int prev = -1;
+    cudaGetDevice(&prev);
+    cudaSetDevice(S->opts.device);
+    const int id = int(S->scenes.size());
+    cudaError_t e = cudaMemcpy(S->d_scenes + id, &sc, sizeof(sc), cudaMemcpyHostToDevice);
+    if (prev >= 0) cudaSetDevice(prev);
+    if (e != cudaSuccess) return fail(SG_ERR_CUDA, std::string("scene table: ") + cudaGetErrorString(e));
+    S->scenes.push_back(sc);
+    S->width = L.width;
+    S->node_format = fmt;
+    S->stack_need = std::max(S->stack_need, L.stack_need);
+    *scene_id = id;
+    return SG_OK;
+}
+
+sg_status sg_server_submit(sg_server* S, const sg_request* q, int64_t* ticket) {
+    if (!S || !q || !ticket) return fail(SG_ERR_INVALID_ARGUMENT, "NULL argument");
+    if (q->width <= 0 || q->height <= 0 || q->spp <= 0 || q->spp > 65535 || q->max_depth <= 0 || !q->image)
+        return fail(SG_ERR_INVALID_ARGUMENT, "bad request");
+    const int64_t P = int64_t(q->width) * q->height;
+    std::lock_guard<std::mutex> lk(S->mu);
+    if (S->stop) return S->loop_status != SG_OK ? fail(S->loop_status, S->loop_msg) : fail(SG_ERR_INVALID_ARGUMENT, "server stopped");
+    if (q->scene < 0 || q->scene >= int(S->scenes.size())) return fail(SG_ERR_INVALID_ARGUMENT, "unknown scene");
+    if (P > S->opts.pixel_budget) return fail(SG_ERR_LIMIT, "request larger than the pixel budget");
+    const int64_t id = S->next_ticket++;
+    Ticket& t = S->tickets[id];
+    t.req = *q;
+    t.submit_ns = now_ns();
+    S->pending.push_back(id);
+    S->cv_work.notify_all();
+    *ticket = id;
+    return SG_OK;
+}
+
+sg_status sg_server_wait(sg_server* S, int64_t ticket, int64_t timeout_ns, sg_request_result* result) {
+    if (!S || !result) return fail(SG_ERR_INVALID_ARGUMENT, "NULL argument");
+    std::unique_lock<std::mutex> lk(S->mu);
+    auto it = S->tickets.find(ticket);
+    if (it == S->tickets.end()) return fail(SG_ERR_INVALID_ARGUMENT, "unknown ticket");
+    auto ready = [&] {
+        auto f = S->tickets.find(ticket);
+        return f == S->tickets.end() || f->second.complete;
+    };
+    if (timeout_ns < 0) {
+        S->cv_done.wait(lk, ready);
+    } else if (!S->cv_done.wait_for(lk, std::chrono::nanoseconds(timeout_ns), ready)) {
+        return fail(SG_ERR_LIMIT, "request still running");
+    }
+    it = S->tickets.find(ticket);
+    if (it == S->tickets.end()) return fail(SG_ERR_INVALID_ARGUMENT, "ticket already collected");
+    const Ticket& t = it->second;
+    result->ticket = ticket;
+    result->status = t.status;
+    result->reserved = 0;
+    result->submit_ns = t.submit_ns;
+    result->admit_ns = t.admit_ns;
+    result->done_ns = t.done_ns;
+    S->tickets.erase(it);
+    return SG_OK;
+}
+
+sg_status sg_server_cancel(sg_server* S, int64_t ticket) {
+    if (!S) return fail(SG_ERR_INVALID_ARGUMENT, "NULL server");
+    std::lock_guard<std::mutex> lk(S->mu);
+    auto it = S->tickets.find(ticket);
+    if (it == S->tickets.end()) return fail(SG_ERR_INVALID_ARGUMENT, "unknown ticket");
+    Ticket& t = it->second;
+    if (t.complete || t.cancel) return SG_OK;
+    t.cancel = true;
+    if (t.slot < 0) {  // still queued
+        S->pending.erase(std::remove(S->pending.begin(), S->pending.end(), ticket), S->pending.end());
+        complete(S, t, SG_ERR_CANCELLED);
+    } else {
+        S->to_cancel.push_back(t.slot);
+        S->cv_work.notify_all();
+    }
+    return SG_OK;
+}
+
+sg_status sg_server_stats_get(sg_server* S, sg_server_stats* out) {
+    if (!S || !out) return fail(SG_ERR_INVALID_ARGUMENT, "NULL argument");
+    std::lock_guard<std::mutex> lk(S->mu);
+    *out = S->stats;
+    out->queued = int64_t(S->pending.size());
+    out->admitted = S->admitted;
+    return SG_OK;
+}
+
+sg_status sg_server_destroy(sg_server* S) {
+    if (!S) return fail(SG_ERR_INVALID_ARGUMENT, "NULL server");
+    {
+        std::lock_guard<std::mutex> lk(S->mu);
+        S->stop = true;
+        S->cv_work.notify_all();
+    }
+    if (S->loop.joinable()) S->loop.join();
+    free_server(S);
+    return SG_OK;
+}
+
+}  // extern "C"

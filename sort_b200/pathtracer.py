@@ -16,14 +16,15 @@ from .accel import Obvh, Qbvh
 
 class PathTracer:
     def __init__(self, triangles, mat_of_tri, materials, light, width: int = 8, max_node_depth: int = 16,
-                 max_pri_in_leaf: int = 8, device: int = 0):
+                 max_pri_in_leaf: int = 8, device: int = 0, node_format: int = _lib.SG_NODES_FP32):
         self.tri = np.ascontiguousarray(np.asarray(triangles, np.float32).reshape(-1, 9))
         self.mat_of_tri = np.ascontiguousarray(np.asarray(mat_of_tri, np.int32))
         self.materials = np.ascontiguousarray(np.asarray(materials, np.float32).reshape(-1, 10))
         self.light = np.ascontiguousarray(np.asarray(light, np.float32))
         if self.mat_of_tri.shape[0] != self.tri.shape[0]:
             raise ValueError("one material index per triangle")
-        self.accel = (Qbvh if width == 4 else Obvh)(max_node_depth, max_pri_in_leaf, device=device)
+        self.accel = (Qbvh if width == 4 else Obvh)(max_node_depth, max_pri_in_leaf, node_format=node_format,
+                                                    device=device)
         self.accel.Build(self.tri)
         lib = _lib.load()
         h = ctypes.c_void_p()

@@ -1,0 +1,121 @@
+"""Render server (sg_server): every request's image is bit-identical to
+sg_pt_render of the same request, rendered alone or in a mix of requests that
+share the path pool and wavefront queues; admission, cancellation and limits.
+
+The pools here are small (a few thousand path slots, a pixel budget below the
+mix's total) so that slots are reused many times, requests wait for admission
+and several scenes share each queue.
+"""
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+torch = pytest.importorskip("torch")
+
+
+@pytest.fixture(scope="module")
+def tracers():
+    assert torch.cuda.is_available(), "GPU tests need a CUDA device"
+    from sort_b200 import scenes
+    from sort_b200.pathtracer import PathTracer
+    out = []
+    for spheres, level, seed in ((16, 2, 1), (32, 3, 2), (8, 3, 3)):
+        _, _, mats, light, tri, mat = scenes.pt_scene(spheres, level, seed=seed)
+        out.append(PathTracer(tri, mat, mats, light))
+    return out
+
+
+def requests():
+    from sort_b200 import scenes
+    cam2 = [4.0, 6.0, 28.0, 0.0, -2.0, 0.0, 0.0, 1.0, 0.0, 40.0]
+    return [  # scene, camera, width, height, spp, depth, seed
+        (0, scenes.CAMERA, 64, 48, 4, 5, 11), (1, scenes.CAMERA, 96, 64, 2, 5, 12), (2, cam2, 33, 17, 7, 4, 13),
+        (1, cam2, 128, 72, 1, 5, 14), (0, cam2, 16, 16, 16, 3, 15), (2, scenes.CAMERA, 80, 60, 3, 5, 16),
+        (0, scenes.CAMERA, 1, 1, 5, 5, 17), (1, scenes.CAMERA, 200, 10, 2, 6, 18)]
+
+
+def reference(tracers, req):
+    sc, cam, w, h, spp, depth, seed = req
+    img = tracers[sc].Render(cam, w, h, spp, depth, seed=seed)
+    torch.cuda.synchronize()
+    return img.cpu().numpy()
+
+
+def server(tracers, **kw):
+    from sort_b200.server import RenderServer
+    srv = RenderServer(**kw)
+    ids = [srv.add_scene(t) for t in tracers]
+    assert ids == list(range(len(tracers)))
+    return srv
+
+
+def test_each_request_matches_single_render_alone_and_mixed(tracers):
+    reqs = requests()
+    refs = [reference(tracers, r) for r in reqs]
+    srv = server(tracers, path_slots=3000, pixel_budget=20_000, max_requests=4)
+    for r, ref in zip(reqs, refs):  # alone
+        img, res = srv.wait(srv.submit(*r[:2], *r[2:6], seed=r[6]))
+        assert res["status"] == 0
+        assert np.array_equal(img.view(np.uint32), ref.view(np.uint32))
+    tickets = [srv.submit(*r[:2], *r[2:6], seed=r[6]) for r in reqs[::-1]]  # mixed, reverse order
+    for t, ref in zip(tickets, refs[::-1]):
+        img, res = srv.wait(t)
+        assert res["status"] == 0 and res["done_ns"] >= res["admit_ns"] >= res["submit_ns"]
+        assert np.array_equal(img.view(np.uint32), ref.view(np.uint32))
+    st = srv.stats()
+    assert st["requests_done"] == 2 * len(reqs)
+    assert st["samples_done"] == 2 * sum(w * h * spp for _, _, w, h, spp, _, _ in reqs)
+    assert st["queued"] == 0 and st["admitted"] == 0
+    srv.close()
+
+
+def test_cancel_leaves_others_unchanged(tracers):
+    from sort_b200 import _lib, scenes
+    reqs = requests()[:4]
+    refs = [reference(tracers, r) for r in reqs]
+    srv = server(tracers, path_slots=2048, pixel_budget=40_000, max_requests=8)
+    big = srv.submit(1, scenes.CAMERA, 160, 120, 64, 5, seed=99)
+    tickets = [srv.submit(*r[:2], *r[2:6], seed=r[6]) for r in reqs]
+    queued = srv.submit(2, scenes.CAMERA, 150, 150, 8, 5, seed=98)  # waits for the pixel budget
+    srv.cancel(big)
+    srv.cancel(queued)
+    for t, ref in zip(tickets, refs):
+        img, res = srv.wait(t)
+        assert res["status"] == 0 and np.array_equal(img.view(np.uint32), ref.view(np.uint32))
+    for t in (big, queued):
+        img, res = srv.wait(t)
+        assert img is None and res["status"] == _lib.SG_ERR_CANCELLED
+    srv.close()
+
+
+def test_limits_and_bad_requests(tracers):
+    from sort_b200 import SortGpuError, scenes
+    from sort_b200.pathtracer import PathTracer
+    srv = server(tracers[:1], path_slots=1024, pixel_budget=10_000, max_requests=2)
+    with pytest.raises(SortGpuError, match="LIMIT"):
+        srv.submit(0, scenes.CAMERA, 200, 100, 1)
+    with pytest.raises(SortGpuError, match="INVALID_ARGUMENT"):
+        srv.submit(3, scenes.CAMERA, 10, 10, 1)
+    with pytest.raises(SortGpuError, match="INVALID_ARGUMENT"):
+        srv.submit(0, scenes.CAMERA, 10, 10, 0)
+    _, _, mats, light, tri, mat = scenes.pt_scene(4, 1)
+    q4 = PathTracer(tri, mat, mats, light, width=4)
+    with pytest.raises(SortGpuError, match="UNSUPPORTED"):
+        srv.add_scene(q4)
+    # the server still serves after the refusals
+    img, res = srv.wait(srv.submit(0, scenes.CAMERA, 20, 10, 2, seed=4))
+    assert res["status"] == 0 and np.array_equal(img, reference(tracers, (0, scenes.CAMERA, 20, 10, 2, 5, 4)))
+    srv.close()
+
+
+def test_quantized_nodes_server(tracers):
+    from sort_b200 import _lib, scenes
+    from sort_b200.pathtracer import PathTracer
+    _, _, mats, light, tri, mat = scenes.pt_scene(16, 3, seed=7)
+    pt = PathTracer(tri, mat, mats, light, node_format=_lib.SG_NODES_QUANT8)
+    srv = server([pt], path_slots=4096, pixel_budget=50_000)
+    req = (0, scenes.CAMERA, 96, 54, 4, 5, 21)
+    img, res = srv.wait(srv.submit(*req[:2], *req[2:6], seed=req[6]))
+    assert res["status"] == 0
+    assert np.array_equal(img.view(np.uint32), reference([pt], req).view(np.uint32))
+    srv.close()
