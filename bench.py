@@ -620,13 +620,169 @@ def run_batched(args):
         a.Release()
 
 
+# serve_27m: 4 resident path-tracing scenes (~100k, 1M, 5M, 20M triangles) as
+# (icosphere count, subdivision level) with per-sphere materials.
+SERVE_SCENES = [(20, 4), (50, 5), (245, 5), (1000, 5)]
+
+
+def serve_config(extra=None):
+    cfg = {
+        "workload": "serve_27m: 4 resident path-tracing scenes (102,404 / 1,024,004 / 5,017,604 / 20,480,004 "
+                    "triangles, per-sphere Lambert / GGX-conductor materials, one area light); render requests "
+                    "arrive as a Poisson stream; each picks a scene uniformly, a tile from 64x64 to 1920x1080 "
+                    "(log-uniform scale), spp from {1, 4, 16, 64}, depth 5; latency = arrival to image in host "
+                    "memory; server (shared path pool + wavefront queues, continuous batching) vs FIFO "
+                    "per-request sg_pt_render launches",
+        "images": "bit-identical between the two arms (same per-pixel arithmetic and sample order), so equal RMSE",
+    }
+    if extra:
+        cfg.update(extra)
+    return cfg
+
+
+def run_serve(args):
+    """Serving: p50/p99 request latency and samples/s, server vs FIFO per-request launches."""
+    import queue as queue_mod
+
+    import torch
+
+    from sort_b200 import scenes
+    from sort_b200.pathtracer import PathTracer
+    from sort_b200.server import RenderServer
+
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    rank = int(os.environ.get("RANK", "0"))
+    torch.cuda.set_device(local)
+    device = torch.device("cuda", local)
+    tracers, tri_counts = [], []
+    for k, (count, level) in enumerate(SERVE_SCENES):
+        _, _, mats, light, tri, mat = scenes.pt_scene(count, level, seed=1 + k)
+        tracers.append(PathTracer(tri, mat, mats, light, device=local))
+        tri_counts.append(int(tri.shape[0]))
+    rng = np.random.default_rng(args.batch_seed)
+
+    def draw(n):
+        s = rng.uniform(0.0, 1.0, n)
+        w = np.round(64 * (1920 / 64) ** s).astype(int)
+        h = np.round(64 * (1080 / 64) ** s).astype(int)
+        spp = rng.choice([1, 4, 16, 64], n)
+        sc = rng.integers(0, len(tracers), n)
+        return [(int(a), int(b), int(c), int(d), 1000 + i) for i, (a, b, c, d) in enumerate(zip(sc, w, h, spp))]
+
+    reqs = draw(args.requests)
+    work = float(sum(w * h * spp for _, w, h, spp, _ in reqs))
+    out_imgs = [torch.empty((h, w, 3), dtype=torch.float32).pin_memory() for _, w, h, _, _ in reqs]
+
+    # Warm both arms (buffers at the largest size, graphs captured).
+    for t in tracers:
+        t.Render(scenes.CAMERA, 1920, 1080, 1, PT_DEPTH, seed=1)
+    torch.cuda.synchronize(device)
+    srv = RenderServer(device=local, path_slots=args.path_slots, pixel_budget=1 << 24, max_requests=1024,
+                       steps_per_poll=2)
+    for t in tracers:
+        srv.add_scene(t)
+    srv.wait(srv.submit(0, scenes.CAMERA, 64, 64, 1))
+
+    def fifo_run(arrivals):
+        """One worker renders requests in arrival order (sg_pt_render + copy out)."""
+        q = queue_mod.Queue()
+        lat = [0.0] * len(reqs)
+        t0 = time.perf_counter()
+
+        def worker():
+            stream = torch.cuda.current_stream(device)
+            for _ in range(len(reqs)):
+                i = q.get()
+                sc, w, h, spp, seed = reqs[i]
+                img = tracers[sc].Render(scenes.CAMERA, w, h, spp, PT_DEPTH, seed=seed)
+                out_imgs[i].copy_(img, non_blocking=True)
+                stream.synchronize()
+                lat[i] = time.perf_counter() - (t0 + arrivals[i])
+
+        th = threading.Thread(target=worker)
+        th.start()
+        for i, a in enumerate(arrivals):
+            d = t0 + a - time.perf_counter()
+            if d > 0:
+                time.sleep(d)
+            q.put(i)
+        th.join()
+        return lat, time.perf_counter() - t0
+
+    def server_run(arrivals):
+        tickets = [0] * len(reqs)
+        t0 = time.perf_counter()
+        for i, a in enumerate(arrivals):
+            d = t0 + a - time.perf_counter()
+            if d > 0:
+                time.sleep(d)
+            sc, w, h, spp, seed = reqs[i]
+            tickets[i] = srv.submit(sc, scenes.CAMERA, w, h, spp, PT_DEPTH, seed=seed, image=out_imgs[i].numpy())
+        lat = []
+        first_submit, last_done = None, 0
+        for t in tickets:
+            _, res = srv.wait(t)
+            lat.append(res["latency_s"])
+            first_submit = res["submit_ns"] if first_submit is None else min(first_submit, res["submit_ns"])
+            last_done = max(last_done, res["done_ns"])
+        return lat, (last_done - first_submit) / 1e9
+
+    def pct(x, q):
+        return round(1e3 * float(np.percentile(np.asarray(x), q)), 2)
+
+    # Closed loop (everything arrives at once): capacity of each arm.
+    zero = [0.0] * len(reqs)
+    with ClockSampler(local) as clocks:
+        fifo_lat0, fifo_span0 = fifo_run(zero)
+        srv_lat0, srv_span0 = server_run(zero)
+        fifo_rate = len(reqs) / fifo_span0
+        rows = []
+        for frac in args.loads:
+            lam = frac * fifo_rate
+            arr = np.cumsum(rng.exponential(1.0 / lam, len(reqs)))
+            arr = (arr - arr[0]).tolist()
+            fl, fs = fifo_run(arr)
+            sl, ss = server_run(arr)
+            rows.append({"load_vs_fifo_capacity": frac, "arrival_rate_req_s": round(lam, 3),
+                         "fifo": {"p50_ms": pct(fl, 50), "p99_ms": pct(fl, 99),
+                                  "msamples_s": round(work / fs / 1e6, 2)},
+                         "server": {"p50_ms": pct(sl, 50), "p99_ms": pct(sl, 99),
+                                    "msamples_s": round(work / ss / 1e6, 2)}})
+    st = srv.stats()
+    srv.close()
+    value = work / srv_span0 / 1e6
+    if rank == 0:
+        out = {
+            "metric": "served path-traced Msamples/s", "value": round(value, 3), "unit": "Msamples/s", "n_gpus": 1,
+            "steps": len(reqs), "warmup": 1, "ms_per_step": round(1e3 * srv_span0 / len(reqs), 3),
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+            "data": "synthetic (seeded procedural scenes and request stream)",
+            "config": serve_config({"requests": len(reqs), "seed": args.batch_seed, "scene_triangles": tri_counts,
+                                    "path_slots": args.path_slots, "samples_per_run": int(work)}),
+            "closed_loop": {"server": {"msamples_s": round(value, 2), "p50_ms": pct(srv_lat0, 50),
+                                       "p99_ms": pct(srv_lat0, 99)},
+                            "fifo": {"msamples_s": round(work / fifo_span0 / 1e6, 2), "p50_ms": pct(fifo_lat0, 50),
+                                     "p99_ms": pct(fifo_lat0, 99)}},
+            "poisson": rows,
+            "server_stats": st,
+            "clocks": clocks.summary(),
+        }
+        print(json.dumps(out))
+    for t in tracers:
+        t.Release()
+
+
 def main():
     p = argparse.ArgumentParser()
     p.add_argument("--gpus", type=int, default=1)
     p.add_argument("--steps", type=int, default=200)
     p.add_argument("--warmup", type=int, default=5)
     p.add_argument("--impl", choices=["ours", "reference"], default="ours")
-    p.add_argument("--workload", choices=["closest", "raycast", "pathtrace", "batched"], default="closest")
+    p.add_argument("--workload", choices=["closest", "raycast", "pathtrace", "batched", "serve"], default="closest")
+    p.add_argument("--requests", type=int, default=120, help="serve workload: requests per run")
+    p.add_argument("--path-slots", type=int, default=1 << 20, help="serve workload: server path pool")
+    p.add_argument("--loads", type=float, nargs="*", default=[0.5, 0.8, 1.0],
+                   help="serve workload: Poisson arrival rates as fractions of the FIFO arm's capacity")
     p.add_argument("--batches", type=int, default=64, help="batched workload: ray batches per step")
     p.add_argument("--batch-seed", type=int, default=7, help="batched workload: seed of the batch list")
     p.add_argument("--sample", type=int, default=CPU_SAMPLE)
@@ -636,6 +792,12 @@ def main():
     args = p.parse_args()
     if args.workload == "pathtrace":
         run_pathtrace(args)
+    elif args.workload == "serve":
+        if args.impl == "reference":
+            print(json.dumps({"impl": "reference", "unavailable": "serve workload: SORT renders one image per "
+                              "process; its per-sample CPU rate is the pathtrace workload's reference arm"}))
+        else:
+            run_serve(args)
     elif args.workload == "batched":
         if args.impl == "reference":
             print(json.dumps({"impl": "reference", "unavailable": "batched workload: SORT has no batch API; "
