@@ -13,6 +13,17 @@ slowest rank's device time. e2e = the same batch through the host-buffer C-ABI
 call (pinned host rays in, hits out, copies inside the timed region).
 reference: SORT's own OBVH code (compiled from its sources into oracle/_ref)
 on the host cores, on a bounded sample of the same rays each step; rank 0 only.
+
+Other workloads (--workload):
+  raycast    81,922-triangle QBVH, 1M jittered primary rays (L2-resident tree);
+  pathtrace  the 21M scene with per-sphere materials, 1920x1080, depth 5, one
+             sample per pixel per step (wavefront path tracer);
+  batched    8 resident scenes (10k..16M triangles), a list of uneven ray
+             batches per step: persistent multi-scene kernel under a captured
+             CUDA graph (autotuned) vs one plain launch per batch;
+  serve      4 resident path-tracing scenes, a Poisson stream of render
+             requests: the render server vs FIFO per-request renders.
+--nodes q8 times 8-bit child boxes (closest, raycast, pathtrace).
 """
 from __future__ import annotations
 
@@ -419,7 +430,7 @@ def run_pathtrace(args):
     torch.cuda.set_device(local)
     device = torch.device("cuda", local)
     _, _, mats, light, tri_gpu, mat_gpu = scenes.pt_scene(SPHERES, LEVEL)
-    pt = PathTracer(tri_gpu, mat_gpu, mats, light, device=local)
+    pt = PathTracer(tri_gpu, mat_gpu, mats, light, device=local, node_format=NODE_FORMATS[args.nodes])
     img = torch.empty((PT_H, PT_W, 3), dtype=torch.float32, device=device)
     stream = torch.cuda.current_stream(device)
     pt.Render(scenes.CAMERA, PT_W, PT_H, args.warmup, PT_DEPTH, seed=1, out=img)
@@ -441,7 +452,7 @@ def run_pathtrace(args):
            "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms / args.steps, 3),
            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
            "data": "synthetic (seeded procedural scene)",
-           "config": pt_config({"frame_spp_per_s": round(args.steps / (ms / 1e3), 3),
+           "config": pt_config({"nodes": args.nodes, "frame_spp_per_s": round(args.steps / (ms / 1e3), 3),
                                 "rays_per_sample": round((ext + sh) / samples, 3),
                                 "extension_rays": ext, "shadow_rays": sh,
                                 "mrays_s": round((ext + sh) / (ms / 1e3) / 1e6, 2)}),

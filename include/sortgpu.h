@@ -275,7 +275,10 @@ sg_status sg_pt_ray_counts(const sg_pt_scene* pt, int64_t* extension, int64_t* s
  * sg_server_opts: path_slots = paths in flight (each holds about 250 bytes of
  *   path state in HBM); pixel_budget = pixels of admitted, unfinished requests
  *   (20 bytes each: image + work queue entry); max_requests = requests admitted
- *   at once; steps_per_poll = bounce steps per graph replay (even, >= 2).
+ *   at once; steps_per_poll = bounce steps per graph replay (even, >= 2);
+ *   samples_per_claim = samples a pool slot renders of one pixel before the
+ *   pixel goes back to the shared work queue (1 = strict turn-taking between
+ *   requests; larger keeps neighbouring pixels together in the queues).
  * sg_server_add_scene: all scenes of a server share one tree width and node
  *   format (SG_ERR_UNSUPPORTED otherwise); the sg_pt_scene and its sg_scene
  *   must outlive the server.
@@ -294,7 +297,7 @@ typedef struct {
     int64_t path_slots;
     int64_t pixel_budget;
     int32_t steps_per_poll;
-    int32_t reserved;
+    int32_t samples_per_claim;
 } sg_server_opts;
 
 typedef struct {

@@ -66,7 +66,8 @@ class BatchTuning(ctypes.Structure):
 
 class ServerOpts(ctypes.Structure):
     _fields_ = [("device", ctypes.c_int32), ("max_requests", ctypes.c_int32), ("path_slots", ctypes.c_int64),
-                ("pixel_budget", ctypes.c_int64), ("steps_per_poll", ctypes.c_int32), ("reserved", ctypes.c_int32)]
+                ("pixel_budget", ctypes.c_int64), ("steps_per_poll", ctypes.c_int32),
+                ("samples_per_claim", ctypes.c_int32)]
 
 
 class Request(ctypes.Structure):

@@ -5,8 +5,9 @@
 // sg_pt_render's for the same request, pixel and sample.
 //
 // One step:
-//   regen       idle slots claim ring entries (one atomic per warp) and start
-//               the camera path of that pixel sample;
+//   regen       slots holding a pixel start its next sample; idle slots
+//               claim ring entries (one atomic per warp); each starts the
+//               camera path of that pixel sample;
 //   settle      the claim counter is pulled back to the ring's end if warps
 //               over-claimed;
 //   extend      closest-hit traversal of the extension queue, each ray in its
@@ -16,9 +17,10 @@
 //   shadow      any-hit traversal of the shadow queue;
 //   resolve     unoccluded shadow results to their slot;
 //   accumulate  both results added to the path's radiance (sg_pt_render's
-//               order); an ended path adds its radiance to its pixel, appends
-//               the pixel's next sample to the ring or, after the last, scales
-//               the pixel by 1/spp and counts it finished for its request;
+//               order); an ended path adds its radiance to its pixel; the slot
+//               keeps the pixel for its next sample, or at the end of a claim
+//               appends that sample to the ring, or after the last sample
+//               scales the pixel by 1/spp and counts it finished;
 //   advance     the next extension queue becomes the current one.
 // Every kernel's grid covers the pool (or the shadow queue) and reads its
 // length on the device, so a step is a fixed sequence of launches that a
@@ -78,14 +80,26 @@ __global__ void k_srv_regen(SrvBuffers b, float* __restrict__ qray, int* __restr
     const int64_t s = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     const bool in = s < b.slots;
     const unsigned long long tail = b.counters->tail;
-    const bool want = in && b.st_state[s] == kSlotIdle;
+    const int state = in ? b.st_state[s] : kSlotActive;
+    const bool want = state == kSlotIdle;
     const unsigned long long idx = warp_append64(&b.counters->head, want);
-    if (!want || idx >= tail) return;
-    const unsigned long long u = b.ring[idx % (unsigned long long)b.ring_cap];
-    const int r = (int)(u >> 48), sample = (int)((u >> 32) & 0xffffu), pix = (int)(u & 0xffffffffu);
+    int r, sample, pix;
+    if (state == kSlotNext) {  // the next sample of the pixel this slot holds
+        r = b.st_req[s];
+        pix = b.st_pix[s];
+        sample = b.st_sample[s];
+    } else if (want && idx < tail) {
+        const unsigned long long u = b.ring[idx % (unsigned long long)b.ring_cap];
+        r = (int)(u >> 48);
+        sample = (int)((u >> 32) & 0xffffu);
+        pix = (int)(u & 0xffffffffu);
+    } else {
+        return;
+    }
     const SrvRequest& q = b.requests[r];
     if (q.cancelled) {
         pixel_finished(b, r);
+        b.st_state[s] = kSlotIdle;
         return;
     }
     const int C = (int)b.slots;
@@ -213,21 +227,28 @@ __global__ void k_srv_accumulate(SrvBuffers b, const int* __restrict__ qslot) {
         pix = b.st_pix[s];
         sample = b.st_sample[s];
         const SrvRequest& rq = b.requests[r];
+        bool more = false;
         if (!rq.cancelled) {
             float* px = rq.image + 3 * (int64_t)pix;
 #pragma unroll
             for (int c = 0; c < 3; ++c) px[c] += thr[(3 + c) * C + s];
-            requeue = sample + 1 < rq.spp;
-            if (!requeue) {
+            more = sample + 1 < rq.spp;
+            if (!more) {
 #pragma unroll
                 for (int c = 0; c < 3; ++c) px[c] *= rq.inv_spp;
             }
         }
-        b.st_state[s] = kSlotIdle;
+        if (more && (sample + 1) % b.samples_per_claim != 0) {  // keep the pixel
+            b.st_sample[s] = sample + 1;
+            b.st_state[s] = kSlotNext;
+        } else {
+            requeue = more;
+            b.st_state[s] = kSlotIdle;
+            if (!more) pixel_finished(b, r);
+        }
     }
     const unsigned long long at = warp_append64(&b.counters->tail, requeue);
     if (requeue) b.ring[at % (unsigned long long)b.ring_cap] = srv_unit(r, sample + 1, pix);
-    if (ended && !requeue) pixel_finished(b, r);
     const unsigned m = __ballot_sync(__activemask(), ended);
     if (ended && (threadIdx.x & 31) == __ffs(m) - 1) atomicAdd(&b.counters->samples, (unsigned long long)__popc(m));
 }

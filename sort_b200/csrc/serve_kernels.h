@@ -2,11 +2,13 @@
 // bounce steps (serve.cu).
 //
 // Work is a ring of pixel samples: entry = (request, pixel, sample). Admission
-// appends sample 0 of every pixel of a request; a path that ends adds its
-// radiance to its pixel and appends the pixel's next sample at the ring's end,
-// so a pixel has at most one sample in flight (its samples accumulate in
-// order) and requests take turns pass by pass. Free path slots claim entries
-// from the ring's head.
+// appends sample 0 of every pixel of a request; free path slots claim entries
+// from the ring's head. A path that ends adds its radiance to its pixel; its
+// slot then renders the pixel's next sample itself, up to samples_per_claim
+// samples per claim, and after that appends the pixel's next sample at the
+// ring's end. So a pixel has at most one sample in flight (its samples
+// accumulate in order), requests take turns chunk by chunk, and slots keep
+// runs of neighbouring pixels (coherent camera and bounce rays).
 #pragma once
 
 #include <cuda_runtime.h>
@@ -66,9 +68,10 @@ __host__ __device__ inline unsigned long long srv_unit(int request, int sample, 
            (unsigned long long)(unsigned)pixel;
 }
 
-constexpr int kSlotIdle = 0;
-constexpr int kSlotActive = 1;
-constexpr int kSlotFinished = 2;
+constexpr int kSlotIdle = 0;      // claims a ring entry at the next regen
+constexpr int kSlotActive = 1;    // a path is in flight
+constexpr int kSlotFinished = 2;  // its path ended this step (accumulate settles it)
+constexpr int kSlotNext = 3;      // starts its pixel's next sample at the next regen
 
 struct SrvBuffers {
     const SrvRequest* requests;
@@ -79,7 +82,8 @@ struct SrvBuffers {
     int* done;                 // per request: 1 once every pixel is finished
     unsigned long long* ring;
     int64_t ring_cap;
-    int64_t slots;  // path pool size C
+    int64_t slots;          // path pool size C
+    int samples_per_claim;  // samples a slot renders of its pixel before returning it to the ring
     int* st_req;
     int* st_pix;
     int* st_sample;

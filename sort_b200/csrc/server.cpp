@@ -349,7 +349,7 @@ void sg_default_server_opts(sg_server_opts* o) {
     o->path_slots = int64_t(1) << 20;
     o->pixel_budget = int64_t(1) << 24;
     o->steps_per_poll = 4;
-    o->reserved = 0;
+    o->samples_per_claim = 8;
 }
 
 sg_status sg_server_create(const sg_server_opts* opts, sg_server** out) {
@@ -363,6 +363,8 @@ sg_status sg_server_create(const sg_server_opts* opts, sg_server** out) {
         return fail(SG_ERR_INVALID_ARGUMENT, "pixel_budget out of range");
     if (o.steps_per_poll < 2 || o.steps_per_poll % 2 != 0 || o.steps_per_poll > 64)
         return fail(SG_ERR_INVALID_ARGUMENT, "steps_per_poll must be even, 2..64");
+    if (o.samples_per_claim < 1 || o.samples_per_claim > 65535)
+        return fail(SG_ERR_INVALID_ARGUMENT, "samples_per_claim must be in 1..65535");
     int ndev = 0;
     if (cudaGetDeviceCount(&ndev) != cudaSuccess || o.device < 0 || o.device >= ndev)
         return fail(SG_ERR_INVALID_ARGUMENT, "no such CUDA device");
@@ -439,6 +441,7 @@ sg_status sg_server_create(const sg_server_opts* opts, sg_server** out) {
     b.ring = reinterpret_cast<unsigned long long*>(m + offs[6]);
     b.ring_cap = int64_t(P);
     b.slots = int64_t(C);
+    b.samples_per_claim = o.samples_per_claim;
     b.st_req = st_arrays[0];
     b.st_pix = st_arrays[1];
     b.st_sample = st_arrays[2];

@@ -58,3 +58,25 @@ def test_pt_same_seed_same_image(tracer):
     b = pt.Render(z["camera"], 32, 24, 4, 5, seed=9).cpu().numpy()
     c = pt.Render(z["camera"], 32, 24, 4, 5, seed=10).cpu().numpy()
     assert np.array_equal(a, b) and not np.array_equal(a, c)
+
+
+def test_pt_quantized_nodes_match_sort(tracer):
+    """8-bit child boxes: the same statistical bar against SORT's converged render;
+    hits can differ from the FP32-node render only at near-ties, so the two
+    renders of one seed agree to far below the 4096-spp noise."""
+    from sort_b200 import _lib, scenes
+    from sort_b200.pathtracer import PathTracer
+    pt32, z = tracer
+    _, _, mats, light, tri_gpu, mat_gpu = scenes.pt_scene(int(z["spheres"]), int(z["level"]))
+    pt8 = PathTracer(tri_gpu, mat_gpu, mats, light, node_format=_lib.SG_NODES_QUANT8)
+    assert pt8.accel.info()["node_format"] == _lib.SG_NODES_QUANT8
+    w, h, d = int(z["width"]), int(z["height"]), int(z["depth"])
+    img = pt8.Render(z["camera"], w, h, 4096, d, seed=7).cpu().numpy()
+    conv = z["converged"]
+    assert rmse(img, conv) <= 1.3 * float(z["rmse_converged_pair"])
+    m8, m_ref = img.mean(axis=(0, 1)), conv.mean(axis=(0, 1))
+    assert np.all(np.abs(m8 - m_ref) / m_ref < 0.01), (m8, m_ref)
+    a = pt32.Render(z["camera"], w, h, 64, d, seed=3).cpu().numpy()
+    b = pt8.Render(z["camera"], w, h, 64, d, seed=3).cpu().numpy()
+    assert rmse(a, b) <= 0.01 * float(z["rmse_converged_pair"]), rmse(a, b)
+    pt8.Release()

@@ -49,10 +49,11 @@ def server(tracers, **kw):
     return srv
 
 
-def test_each_request_matches_single_render_alone_and_mixed(tracers):
+@pytest.mark.parametrize("per_claim", [1, 3, 64])
+def test_each_request_matches_single_render_alone_and_mixed(tracers, per_claim):
     reqs = requests()
     refs = [reference(tracers, r) for r in reqs]
-    srv = server(tracers, path_slots=3000, pixel_budget=20_000, max_requests=4)
+    srv = server(tracers, path_slots=3000, pixel_budget=20_000, max_requests=4, samples_per_claim=per_claim)
     for r, ref in zip(reqs, refs):  # alone
         img, res = srv.wait(srv.submit(*r[:2], *r[2:6], seed=r[6]))
         assert res["status"] == 0
