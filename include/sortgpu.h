@@ -323,7 +323,7 @@ typedef struct {
 
 typedef struct {
     int64_t requests_done;
-    int64_t samples_done;     /* pixel samples accumulated */
+    int64_t samples_done;     /* pixel samples of the requests completed (not cancelled) */
     int64_t extension_rays;   /* closest-hit rays traced */
     int64_t shadow_rays;      /* any-hit rays traced */
     int64_t graph_replays;

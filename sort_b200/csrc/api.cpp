@@ -70,7 +70,15 @@ struct sg_scene {
     std::mutex scratch_lock;
     void* d_scratch = nullptr;
     size_t scratch_bytes = 0;
-    cudaStream_t stream = nullptr;
+    cudaStream_t stream = nullptr;  // host-buffer calls: copies in
+    // Host-buffer calls pipeline chunks: copies in on `stream`, kernels on two
+    // alternating streams (a chunk's tail overlaps the next chunk's start),
+    // copies out on a fourth; one event per chunk and stage.
+    static constexpr int kMaxChunks = 16;
+    cudaStream_t trace_stream[2] = {nullptr, nullptr};
+    cudaStream_t out_stream = nullptr;
+    cudaEvent_t in_done[kMaxChunks] = {};
+    cudaEvent_t trace_done[kMaxChunks] = {};
 };
 
 namespace {
@@ -139,6 +147,13 @@ void release(sg_scene* s) {
     if (s->d_counters) cudaFree(s->d_counters);
     if (s->d_scratch) cudaFree(s->d_scratch);
     if (s->stream) cudaStreamDestroy(s->stream);
+    for (cudaStream_t& x : s->trace_stream)
+        if (x) cudaStreamDestroy(x);
+    if (s->out_stream) cudaStreamDestroy(s->out_stream);
+    for (int k = 0; k < sg_scene::kMaxChunks; ++k) {
+        if (s->in_done[k]) cudaEventDestroy(s->in_done[k]);
+        if (s->trace_done[k]) cudaEventDestroy(s->trace_done[k]);
+    }
     delete s;
 }
 
@@ -379,8 +394,17 @@ static sg_status host_trace(const sg_scene* cs, const float* rays8, int64_t n, i
     DeviceGuard g(s->device);
     if (!g.ok) return fail(SG_ERR_CUDA, "cudaSetDevice failed");
     cudaError_t e;
-    if (!s->stream && (e = cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking)) != cudaSuccess)
-        return cuda_fail(e, "cudaStreamCreate");
+    if (!s->stream) {
+        if ((e = cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking)) != cudaSuccess ||
+            (e = cudaStreamCreateWithFlags(&s->trace_stream[0], cudaStreamNonBlocking)) != cudaSuccess ||
+            (e = cudaStreamCreateWithFlags(&s->trace_stream[1], cudaStreamNonBlocking)) != cudaSuccess ||
+            (e = cudaStreamCreateWithFlags(&s->out_stream, cudaStreamNonBlocking)) != cudaSuccess)
+            return cuda_fail(e, "cudaStreamCreate");
+        for (int k = 0; k < sg_scene::kMaxChunks; ++k)
+            if ((e = cudaEventCreateWithFlags(&s->in_done[k], cudaEventDisableTiming)) != cudaSuccess ||
+                (e = cudaEventCreateWithFlags(&s->trace_done[k], cudaEventDisableTiming)) != cudaSuccess)
+                return cuda_fail(e, "cudaEventCreate");
+    }
     const size_t in_bytes = size_t(n) * 8 * sizeof(float);
     const size_t out_bytes = any ? size_t(n) : size_t(n) * 16;
     const size_t need = in_bytes + out_bytes + 256;
@@ -395,33 +419,56 @@ static sg_status host_trace(const sg_scene* cs, const float* rays8, int64_t n, i
     }
     float* d_rays = static_cast<float*>(s->d_scratch);
     char* d_out = static_cast<char*>(s->d_scratch) + ((in_bytes + 255) & ~size_t(255));
-    cudaStream_t st = s->stream;
-    if ((e = cudaMemcpyAsync(d_rays, rays8, in_bytes, cudaMemcpyHostToDevice, st)) != cudaSuccess)
-        return cuda_fail(e, "copy rays to device");
-    sg_rays r{d_rays, d_rays + n, d_rays + 2 * n, d_rays + 3 * n, d_rays + 4 * n, d_rays + 5 * n, d_rays + 6 * n,
-              d_rays + 7 * n};
-    sg_status status;
-    if (any) {
-        status = trace_common(s, &r, n, nullptr, reinterpret_cast<uint8_t*>(d_out), true, st);
-        if (status != SG_OK) return status;
-        if ((e = cudaMemcpyAsync(occ, d_out, size_t(n), cudaMemcpyDeviceToHost, st)) != cudaSuccess)
-            return cuda_fail(e, "copy results to host");
-    } else {
-        int32_t* dp = reinterpret_cast<int32_t*>(d_out);
-        float* dt = reinterpret_cast<float*>(d_out + size_t(n) * 4);
-        float* du = reinterpret_cast<float*>(d_out + size_t(n) * 8);
-        float* dv = reinterpret_cast<float*>(d_out + size_t(n) * 12);
-        sg_hits h{dp, dt, u ? du : nullptr, v ? dv : nullptr};
-        status = trace_common(s, &r, n, &h, nullptr, false, st);
-        if (status != SG_OK) return status;
-        if ((e = cudaMemcpyAsync(prim, dp, size_t(n) * 4, cudaMemcpyDeviceToHost, st)) != cudaSuccess ||
-            (e = cudaMemcpyAsync(t, dt, size_t(n) * 4, cudaMemcpyDeviceToHost, st)) != cudaSuccess ||
-            (u && (e = cudaMemcpyAsync(u, du, size_t(n) * 4, cudaMemcpyDeviceToHost, st)) != cudaSuccess) ||
-            (v && (e = cudaMemcpyAsync(v, dv, size_t(n) * 4, cudaMemcpyDeviceToHost, st)) != cudaSuccess))
-            return cuda_fail(e, "copy results to host");
+    int32_t* dp = reinterpret_cast<int32_t*>(d_out);
+    float* dt = reinterpret_cast<float*>(d_out + size_t(n) * 4);
+    float* du = reinterpret_cast<float*>(d_out + size_t(n) * 8);
+    float* dv = reinterpret_cast<float*>(d_out + size_t(n) * 12);
+    uint8_t* docc = reinterpret_cast<uint8_t*>(d_out);
+    // Chunks of at least 512k rays (one chunk below 1M), at most kMaxChunks:
+    // chunk k's rays go in while chunk k-1 is traced and chunk k-2's hits come out.
+    const int64_t min_chunk = int64_t(1) << 19;
+    const int chunks = int(std::min<int64_t>(sg_scene::kMaxChunks, std::max<int64_t>(1, n / min_chunk / 2 * 2)));
+    const int64_t per = (n + chunks - 1) / chunks;
+    sg_status status = SG_OK;
+    for (int k = 0; k < chunks; ++k) {
+        const int64_t a = int64_t(k) * per;
+        const int64_t m = std::min(per, n - a);
+        if (m <= 0) break;
+        cudaStream_t tr = s->trace_stream[k & 1];
+        // Ray planes [a, a + m) of all eight arrays: one pitched copy.
+        if ((e = cudaMemcpy2DAsync(d_rays + a, size_t(n) * 4, rays8 + a, size_t(n) * 4, size_t(m) * 4, 8,
+                                   cudaMemcpyHostToDevice, s->stream)) != cudaSuccess ||
+            (e = cudaEventRecord(s->in_done[k], s->stream)) != cudaSuccess ||
+            (e = cudaStreamWaitEvent(tr, s->in_done[k], 0)) != cudaSuccess)
+            return cuda_fail(e, "copy rays to device");
+        const float* b = d_rays + a;
+        sg_rays r{b, b + n, b + 2 * n, b + 3 * n, b + 4 * n, b + 5 * n, b + 6 * n, b + 7 * n};
+        if (any) {
+            status = trace_common(s, &r, m, nullptr, docc + a, true, tr);
+        } else {
+            sg_hits h{dp + a, dt + a, u ? du + a : nullptr, v ? dv + a : nullptr};
+            status = trace_common(s, &r, m, &h, nullptr, false, tr);
+        }
+        if (status != SG_OK) break;
+        if ((e = cudaEventRecord(s->trace_done[k], tr)) != cudaSuccess ||
+            (e = cudaStreamWaitEvent(s->out_stream, s->trace_done[k], 0)) != cudaSuccess)
+            return cuda_fail(e, "order chunk copies");
+        cudaStream_t o = s->out_stream;
+        if (any) {
+            e = cudaMemcpyAsync(occ + a, docc + a, size_t(m), cudaMemcpyDeviceToHost, o);
+        } else {
+            e = cudaMemcpyAsync(prim + a, dp + a, size_t(m) * 4, cudaMemcpyDeviceToHost, o);
+            if (e == cudaSuccess) e = cudaMemcpyAsync(t + a, dt + a, size_t(m) * 4, cudaMemcpyDeviceToHost, o);
+            if (e == cudaSuccess && u) e = cudaMemcpyAsync(u + a, du + a, size_t(m) * 4, cudaMemcpyDeviceToHost, o);
+            if (e == cudaSuccess && v) e = cudaMemcpyAsync(v + a, dv + a, size_t(m) * 4, cudaMemcpyDeviceToHost, o);
+        }
+        if (e != cudaSuccess) return cuda_fail(e, "copy results to host");
     }
-    if ((e = cudaStreamSynchronize(st)) != cudaSuccess) return cuda_fail(e, "synchronize");
-    return check_status_word(s, st);
+    // Everything enqueued so far completes before returning, even after an error.
+    for (cudaStream_t x : {s->stream, s->trace_stream[0], s->trace_stream[1], s->out_stream})
+        if ((e = cudaStreamSynchronize(x)) != cudaSuccess) return cuda_fail(e, "synchronize");
+    if (status != SG_OK) return status;
+    return check_status_word(s, s->out_stream);
 }
 
 sg_status sg_trace_stats(const sg_scene* cs, const sg_rays* rays, int64_t n, int32_t any, int64_t* node_tests,

@@ -220,7 +220,7 @@ __global__ void k_srv_accumulate(SrvBuffers b, const int* __restrict__ qslot) {
 #pragma unroll
     for (int c = 0; c < 3; ++c) thr[(3 + c) * C + s] += b.vis[c * C + s] + b.vis[(3 + c) * C + s];
     const bool ended = b.st_state[s] == kSlotFinished;
-    bool requeue = false;
+    bool requeue = false, pixel_done = false;
     int r = 0, pix = 0, sample = 0;
     if (ended) {
         r = b.st_req[s];
@@ -243,14 +243,22 @@ __global__ void k_srv_accumulate(SrvBuffers b, const int* __restrict__ qslot) {
             b.st_state[s] = kSlotNext;
         } else {
             requeue = more;
+            pixel_done = !more;
             b.st_state[s] = kSlotIdle;
-            if (!more) pixel_finished(b, r);
         }
     }
     const unsigned long long at = warp_append64(&b.counters->tail, requeue);
     if (requeue) b.ring[at % (unsigned long long)b.ring_cap] = srv_unit(r, sample + 1, pix);
-    const unsigned m = __ballot_sync(__activemask(), ended);
-    if (ended && (threadIdx.x & 31) == __ffs(m) - 1) atomicAdd(&b.counters->samples, (unsigned long long)__popc(m));
+    // Finished pixels, one atomic per warp and request (a request's pixels
+    // finish together, so one counter per request would otherwise serialise).
+    const unsigned fm = __ballot_sync(__activemask(), pixel_done);
+    if (pixel_done) {
+        const unsigned peers = __match_any_sync(fm, r);
+        if ((int)(threadIdx.x & 31) == __ffs(peers) - 1) {
+            const unsigned c = (unsigned)__popc(peers);
+            if (atomicSub(&b.units_left[r], c) == c) b.done[r] = 1;
+        }
+    }
 }
 
 __global__ void k_srv_advance(SrvBuffers b) {

@@ -59,7 +59,7 @@ struct SrvCounters {
     int queue[4];               // [0] current extension queue, [1] next, [2] shadow queue
     unsigned long long head;    // ring entries claimed
     unsigned long long tail;    // ring entries appended
-    unsigned long long ext_rays, shadow_rays, samples;
+    unsigned long long ext_rays, shadow_rays;
 };
 
 // Ring entry: request (16 bits) | sample (16 bits) | pixel (32 bits).

@@ -249,7 +249,6 @@ sg_status collect(sg_server* S, int k, int64_t replay) {
             done.push_back(id);
         }
         const sg::SrvCounters& c = *S->h_counters[k];
-        S->stats.samples_done = (int64_t)c.samples;
         S->stats.extension_rays = (int64_t)c.ext_rays;
         S->stats.shadow_rays = (int64_t)c.shadow_rays;
     }
@@ -280,6 +279,7 @@ sg_status collect(sg_server* S, int k, int64_t replay) {
         t.slot = -1;
         S->admitted--;
         S->stats.requests_done++;
+        if (!t.cancel) S->stats.samples_done += P * t.req.spp;
         complete(S, t, t.cancel ? SG_ERR_CANCELLED : SG_OK);
     }
     S->cv_work.notify_all();

@@ -98,6 +98,27 @@ def test_gpu_host_entry_points_match_device(port):
     assert np.array_equal(occ_h, occ)
 
 
+@pytest.mark.parametrize("n", [1_048_576, 3_000_001])
+def test_gpu_host_entry_points_pipelined_chunks(n):
+    """Host-buffer calls large enough to be split into pipelined chunks (ragged
+    last chunk included) return exactly the device-buffer results; u/v may be
+    omitted."""
+    from sort_b200 import _lib, scenes
+    import ctypes
+    tri = scenes.sphere_field(32, 3, seed=15)
+    rays = np.ascontiguousarray(scenes.random_rays(n, seed=16))
+    acc = accel(8)
+    acc.Build(tri)
+    prim, t, u, v, occ = run_device(acc, rays)
+    h = acc.GetIntersect(rays)
+    assert np.array_equal(h.prim, prim) and same_bits(h.t, t) and same_bits(h.u, u) and same_bits(h.v, v)
+    assert np.array_equal(acc.GetAttenuation(rays), occ)
+    p2, t2 = np.empty(n, np.int32), np.empty(n, np.float32)
+    _lib.check(_lib.load().sg_trace_closest_host(acc._h, rays.ctypes.data, n, p2.ctypes.data, t2.ctypes.data,
+                                                 None, None))
+    assert np.array_equal(p2, prim) and same_bits(t2, t)
+
+
 @pytest.mark.parametrize("n", [1, 31, 127, 128, 129, 1000, 4097])
 def test_gpu_ragged_batches(n):
     from sort_b200 import scenes
