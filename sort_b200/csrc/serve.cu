@@ -146,27 +146,42 @@ __global__ void __launch_bounds__(kSrvBlock) k_srv_count(SrvBuffers b) {
 }
 
 // Exclusive scan of the bucket counts (one block); the total is the queue length.
+// Tiles of 1024 consecutive entries (coalesced), each scanned with warp
+// shuffles and one shared-memory pass over the 32 warp totals.
 __global__ void __launch_bounds__(1024) k_srv_scan(SrvBuffers b, int entries) {
-    __shared__ int part[1024];
-    const int per = (entries + 1023) / 1024;
-    const int a = threadIdx.x * per, e = min(entries, a + per);
-    int sum = 0;
-    for (int i = a; i < e; ++i) sum += b.bucket_counts[i];
-    part[threadIdx.x] = sum;
+    __shared__ int warp_total[32];
+    __shared__ int carry;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    if (threadIdx.x == 0) carry = 0;
     __syncthreads();
-    for (int off = 1; off < 1024; off <<= 1) {  // inclusive Hillis-Steele scan
-        const int v = threadIdx.x >= off ? part[threadIdx.x - off] : 0;
+    for (int base = 0; base < entries; base += 1024) {
+        const int i = base + threadIdx.x;
+        const int c = i < entries ? b.bucket_counts[i] : 0;
+        int x = c;  // inclusive scan within the warp
+#pragma unroll
+        for (int off = 1; off < 32; off <<= 1) {
+            const int y = __shfl_up_sync(0xffffffffu, x, off);
+            if (lane >= off) x += y;
+        }
+        if (lane == 31) warp_total[warp] = x;
         __syncthreads();
-        part[threadIdx.x] += v;
+        if (warp == 0) {
+            int w = warp_total[lane];
+#pragma unroll
+            for (int off = 1; off < 32; off <<= 1) {
+                const int y = __shfl_up_sync(0xffffffffu, w, off);
+                if (lane >= off) w += y;
+            }
+            warp_total[lane] = w;  // inclusive over warps
+        }
+        __syncthreads();
+        const int before = carry + (warp > 0 ? warp_total[warp - 1] : 0) + x - c;
+        if (i < entries) b.bucket_counts[i] = before;
+        __syncthreads();
+        if (threadIdx.x == 0) carry += warp_total[31];
         __syncthreads();
     }
-    int run = part[threadIdx.x] - sum;
-    for (int i = a; i < e; ++i) {
-        const int c = b.bucket_counts[i];
-        b.bucket_counts[i] = run;
-        run += c;
-    }
-    if (threadIdx.x == 1023) b.counters->queue[0] = part[1023];
+    if (threadIdx.x == 0) b.counters->queue[0] = carry;
 }
 
 // Each active slot to its place: bucket offset of its block + rank in the block.
