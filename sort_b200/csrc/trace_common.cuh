@@ -18,6 +18,7 @@ struct RayState {
     float o[3], d[3];
     float tmin, tmax;
     float rcp[3], od[3];  // resolveRayData: 1/d and -o/d with |d| clamped to >= 1e-5
+    int nhi[3];           // 1 where rcp < 0: the ray enters a box through its upper bound
     int ly;               // Ray::Prepare major axis; x = (ly + 2) % 3, z = (ly + 1) % 3
     float ox, oy, oz;     // origin in the permuted (local x, y, z) frame
     float sx, sy, sz;     // shear constants
@@ -39,6 +40,7 @@ __device__ __forceinline__ void ray_setup(RayState& r) {
         const float dk = fabsf(r.d[k]) < delta ? (r.d[k] < 0.0f ? -delta : delta) : r.d[k];
         r.rcp[k] = __frcp_rn(dk);
         r.od[k] = __fdiv_rn(-r.o[k], dk);
+        r.nhi[k] = r.rcp[k] < 0.0f ? 1 : 0;
     }
     const float ax = fabsf(r.d[0]), ay = fabsf(r.d[1]), az = fabsf(r.d[2]);
     int y;
@@ -114,6 +116,29 @@ __device__ __forceinline__ bool slab(const RayState& r, float lx, float hx, floa
         f_min = fmaxf(f_min, fminf(t1, t2));
         f_max = fminf(f_max, fmaxf(t1, t2));
     }
+    const bool hit = f_min <= f_max;
+    d = hit ? f_min : -1.0f;
+    return hit;
+}
+
+// slab() from each axis's entry plane n and exit plane f (n = lo, f = hi where
+// 1/d > 0, swapped where 1/d < 0). With 1/d finite and non-zero and lo <= hi,
+// t(b) = fl(-o/d + fl(b * 1/d)) is monotonic in b, so t(n) = min(t(lo), t(hi))
+// and t(f) = max(...) exactly, and the interval's bounds are the same maxima and
+// minima in another order: the result equals slab()'s for every box with
+// lo <= hi. Only empty slots (lo = +FLT_MAX > hi = -FLT_MAX) differ, and the
+// caller discards those by their -1 reference. Two flops and two comparisons
+// fewer per axis.
+__device__ __forceinline__ bool slab_near_far(const RayState& r, float nx, float fx, float ny, float fy, float nz,
+                                              float fz, float& d) {
+    const float tnx = __fadd_rn(r.od[0], __fmul_rn(r.rcp[0], nx));
+    const float tfx = __fadd_rn(r.od[0], __fmul_rn(r.rcp[0], fx));
+    const float tny = __fadd_rn(r.od[1], __fmul_rn(r.rcp[1], ny));
+    const float tfy = __fadd_rn(r.od[1], __fmul_rn(r.rcp[1], fy));
+    const float tnz = __fadd_rn(r.od[2], __fmul_rn(r.rcp[2], nz));
+    const float tfz = __fadd_rn(r.od[2], __fmul_rn(r.rcp[2], fz));
+    const float f_min = fmaxf(fmaxf(tnx, tny), fmaxf(tnz, r.tmin));
+    const float f_max = fminf(fminf(tfx, tfy), fminf(tfz, r.tmax));
     const bool hit = f_min <= f_max;
     d = hit ? f_min : -1.0f;
     return hit;

@@ -10,30 +10,36 @@
 
 namespace sg {
 
+// A node's child boxes as each ray sees them: per axis the plane it enters
+// through (nr, the lower bound when the direction is positive) and the plane
+// it leaves through (fr); see slab_near_far.
 template <int W>
 struct NodeData {
-    float lo[3][W], hi[3][W];
+    float nr[3][W], fr[3][W];
     int32_t ch[W];
 };
 
 template <int W>
-__device__ __forceinline__ void load_node(const float4* __restrict__ nodes, int32_t ref, NodeData<W>& nd) {
+__device__ __forceinline__ void load_node(const float4* __restrict__ nodes, int32_t ref, const RayState& r,
+                                          NodeData<W>& nd) {
     const float4* p = nodes + (size_t)ref * NodeShape<W>::kF4;
     constexpr int Q = W / 4;  // float4 per plane
 #pragma unroll
     for (int a = 0; a < 3; ++a) {
+        const float4* pn = p + (2 * a + r.nhi[a]) * Q;      // lo plane, or hi for a negative direction
+        const float4* pf = p + (2 * a + 1 - r.nhi[a]) * Q;  // the other one
 #pragma unroll
         for (int q = 0; q < Q; ++q) {
-            const float4 l = __ldg(p + (2 * a) * Q + q);
-            const float4 h = __ldg(p + (2 * a + 1) * Q + q);
-            nd.lo[a][4 * q + 0] = l.x;
-            nd.lo[a][4 * q + 1] = l.y;
-            nd.lo[a][4 * q + 2] = l.z;
-            nd.lo[a][4 * q + 3] = l.w;
-            nd.hi[a][4 * q + 0] = h.x;
-            nd.hi[a][4 * q + 1] = h.y;
-            nd.hi[a][4 * q + 2] = h.z;
-            nd.hi[a][4 * q + 3] = h.w;
+            const float4 l = __ldg(pn + q);
+            const float4 h = __ldg(pf + q);
+            nd.nr[a][4 * q + 0] = l.x;
+            nd.nr[a][4 * q + 1] = l.y;
+            nd.nr[a][4 * q + 2] = l.z;
+            nd.nr[a][4 * q + 3] = l.w;
+            nd.fr[a][4 * q + 0] = h.x;
+            nd.fr[a][4 * q + 1] = h.y;
+            nd.fr[a][4 * q + 2] = h.z;
+            nd.fr[a][4 * q + 3] = h.w;
         }
     }
 #pragma unroll
@@ -55,7 +61,8 @@ __device__ __forceinline__ float q8_bound(uint32_t word, int byte, float s, floa
 }
 
 template <int W>
-__device__ __forceinline__ void load_node_q8(const float4* __restrict__ nodes, int32_t ref, NodeData<W>& nd) {
+__device__ __forceinline__ void load_node_q8(const float4* __restrict__ nodes, int32_t ref, const RayState& r,
+                                             NodeData<W>& nd) {
     const float4* p = nodes + (size_t)ref * (W == 8 ? kQ8F4W8 : kQ8F4W4);
     const float4 h = __ldg(p);
     const uint32_t eb = __float_as_uint(h.w);
@@ -67,12 +74,15 @@ __device__ __forceinline__ void load_node_q8(const float4* __restrict__ nodes, i
 #pragma unroll
         for (int a = 0; a < 3; ++a) {
             const uint4 q = __ldg(reinterpret_cast<const uint4*>(p + 1 + a));
+            const bool flip = r.nhi[a] != 0;
+            const uint32_t n0 = flip ? q.z : q.x, n1 = flip ? q.w : q.y;
+            const uint32_t f0 = flip ? q.x : q.z, f1 = flip ? q.y : q.w;
 #pragma unroll
             for (int j = 0; j < 4; ++j) {
-                nd.lo[a][j] = q8_bound(q.x, j, s[a], org[a]);
-                nd.lo[a][4 + j] = q8_bound(q.y, j, s[a], org[a]);
-                nd.hi[a][j] = q8_bound(q.z, j, s[a], org[a]);
-                nd.hi[a][4 + j] = q8_bound(q.w, j, s[a], org[a]);
+                nd.nr[a][j] = q8_bound(n0, j, s[a], org[a]);
+                nd.nr[a][4 + j] = q8_bound(n1, j, s[a], org[a]);
+                nd.fr[a][j] = q8_bound(f0, j, s[a], org[a]);
+                nd.fr[a][4 + j] = q8_bound(f1, j, s[a], org[a]);
             }
         }
         const int4 c0 = __ldg(reinterpret_cast<const int4*>(p + 4));
@@ -89,14 +99,15 @@ __device__ __forceinline__ void load_node_q8(const float4* __restrict__ nodes, i
         const uint4 q01 = __ldg(reinterpret_cast<const uint4*>(p + 1));
         const uint4 q2 = __ldg(reinterpret_cast<const uint4*>(p + 2));
         const int4 c = __ldg(reinterpret_cast<const int4*>(p + 3));
+        const uint32_t lo[3] = {q01.x, q01.z, q2.x}, hi[3] = {q01.y, q01.w, q2.y};
 #pragma unroll
-        for (int j = 0; j < 4; ++j) {
-            nd.lo[0][j] = q8_bound(q01.x, j, s[0], org[0]);
-            nd.hi[0][j] = q8_bound(q01.y, j, s[0], org[0]);
-            nd.lo[1][j] = q8_bound(q01.z, j, s[1], org[1]);
-            nd.hi[1][j] = q8_bound(q01.w, j, s[1], org[1]);
-            nd.lo[2][j] = q8_bound(q2.x, j, s[2], org[2]);
-            nd.hi[2][j] = q8_bound(q2.y, j, s[2], org[2]);
+        for (int a = 0; a < 3; ++a) {
+            const uint32_t n = r.nhi[a] ? hi[a] : lo[a], f = r.nhi[a] ? lo[a] : hi[a];
+#pragma unroll
+            for (int j = 0; j < 4; ++j) {
+                nd.nr[a][j] = q8_bound(n, j, s[a], org[a]);
+                nd.fr[a][j] = q8_bound(f, j, s[a], org[a]);
+            }
         }
         nd.ch[0] = c.x;
         nd.ch[1 % W] = c.y;
@@ -238,15 +249,16 @@ struct Traversal {
     __device__ __forceinline__ bool interior(const DevTree& tr) {
         NodeData<W> nd;
         if (Q8)
-            load_node_q8<W>(tr.nodes, cur, nd);
+            load_node_q8<W>(tr.nodes, cur, r, nd);
         else
-            load_node<W>(tr.nodes, cur, nd);
+            load_node<W>(tr.nodes, cur, r, nd);
         if (STATS) ++node_tests;
         float d[W];
         unsigned mask = 0;
 #pragma unroll
         for (int j = 0; j < W; ++j) {
-            const bool hit = slab(r, nd.lo[0][j], nd.hi[0][j], nd.lo[1][j], nd.hi[1][j], nd.lo[2][j], nd.hi[2][j], d[j]);
+            const bool hit =
+                slab_near_far(r, nd.nr[0][j], nd.fr[0][j], nd.nr[1][j], nd.fr[1][j], nd.nr[2][j], nd.fr[2][j], d[j]);
             if (hit && nd.ch[j] != kEmpty) mask |= 1u << j;
         }
         const int cnt = __popc(mask);
