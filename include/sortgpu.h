@@ -341,6 +341,12 @@ sg_status sg_server_cancel(sg_server* server, int64_t ticket);
 sg_status sg_server_stats_get(sg_server* server, sg_server_stats* stats);
 sg_status sg_server_destroy(sg_server* server);
 
+/* Measurement aid, no SORT counterpart: the L2 read bandwidth (GB/s) a kernel
+ * reaches on `device`, reading a buffer of `bytes` (1..96 MiB, resident in L2)
+ * `reps` times with L1-bypassing 128-bit loads. The roofline of a workload
+ * whose tree fits in L2 is this figure, not HBM's. */
+sg_status sg_probe_l2_read_gbs(int32_t device, int64_t bytes, int32_t reps, double* gbs);
+
 const char* sg_last_error(void);
 const char* sg_version(void);
 

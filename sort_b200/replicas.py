@@ -1,0 +1,71 @@
+"""Multi-GPU work division for replicated scenes (one process per GPU).
+
+Rays, paths and render requests are independent, so every GPU holds a full
+replica of each scene's tree and takes a share of the work; no kernel reads
+another GPU's memory and nothing on the data path needs a collective. This
+module holds the host-side pieces: contiguous shares of a ray batch, tiles of
+an image dealt round-robin, a router that sends each render request to the
+replica with the least outstanding work, and the max-over-ranks reduction the
+timings use (torch.distributed, NCCL on GPUs, gloo on CPU).
+
+SORT's counterpart is its thread pool splitting one image into 64x64 tiles
+(work/image_evaluation/image_evaluation.cpp:153-279); here the split is across
+GPUs as well.
+"""
+from __future__ import annotations
+
+
+def shard_range(n: int, rank: int, world: int) -> tuple[int, int]:
+    """[start, stop) of rank's contiguous share of n items; shares differ by at most one."""
+    if world < 1 or not 0 <= rank < world or n < 0:
+        raise ValueError("need 0 <= rank < world and n >= 0")
+    base, extra = divmod(n, world)
+    start = rank * base + min(rank, extra)
+    return start, start + base + (1 if rank < extra else 0)
+
+
+def tiles(width: int, height: int, tile: int = 64) -> list[tuple[int, int, int, int]]:
+    """The image's tiles (x0, y0, x1, y1) in row-major order."""
+    if width <= 0 or height <= 0 or tile <= 0:
+        raise ValueError("positive sizes required")
+    return [(x, y, min(x + tile, width), min(y + tile, height))
+            for y in range(0, height, tile) for x in range(0, width, tile)]
+
+
+def rank_tiles(width: int, height: int, rank: int, world: int, tile: int = 64):
+    """Tiles dealt round-robin, so every rank gets a spread of the image."""
+    return tiles(width, height, tile)[rank::world]
+
+
+class ReplicaRouter:
+    """Sends each request to the replica with the least outstanding samples
+    (ties: lowest index), and releases that load when the request completes."""
+
+    def __init__(self, replicas: int):
+        if replicas < 1:
+            raise ValueError("at least one replica")
+        self.load = [0] * replicas
+        self.where = {}
+
+    def route(self, request_id, samples: int) -> int:
+        r = min(range(len(self.load)), key=lambda k: (self.load[k], k))
+        self.load[r] += int(samples)
+        self.where[request_id] = (r, int(samples))
+        return r
+
+    def done(self, request_id) -> int:
+        r, samples = self.where.pop(request_id)
+        self.load[r] -= samples
+        return r
+
+
+def max_over_ranks(value: float, device=None) -> float:
+    """The largest of every rank's value (the slowest rank's time); the value
+    itself without an initialised process group."""
+    import torch
+    import torch.distributed as dist
+    if not (dist.is_available() and dist.is_initialized()) or dist.get_world_size() == 1:
+        return float(value)
+    t = torch.tensor([float(value)], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())

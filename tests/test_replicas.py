@@ -1,0 +1,89 @@
+"""Multi-GPU work division, exercised as two gloo ranks on the CPU: shares of a
+ray batch and of an image's tiles cover the work exactly once, the timing
+reduction takes the slowest rank, and the request router balances load."""
+import os
+import socket
+
+import pytest
+
+torch = pytest.importorskip("torch")
+
+from sort_b200.replicas import ReplicaRouter, max_over_ranks, rank_tiles, shard_range, tiles  # noqa: E402
+
+
+def test_shard_range_partitions():
+    for n in (0, 1, 7, 4_194_304, 4_194_305):
+        for world in (1, 2, 3, 8):
+            spans = [shard_range(n, r, world) for r in range(world)]
+            assert spans[0][0] == 0 and spans[-1][1] == n
+            assert all(a[1] == b[0] for a, b in zip(spans, spans[1:]))
+            sizes = [b - a for a, b in spans]
+            assert max(sizes) - min(sizes) <= 1
+    with pytest.raises(ValueError):
+        shard_range(10, 2, 2)
+
+
+def test_tiles_cover_image_once():
+    w, h = 1920, 1080
+    seen = set()
+    for r in range(3):
+        for t in rank_tiles(w, h, r, 3):
+            assert t not in seen
+            seen.add(t)
+    assert seen == set(tiles(w, h))
+    assert sum((x1 - x0) * (y1 - y0) for x0, y0, x1, y1 in seen) == w * h
+
+
+def test_router_balances_and_releases():
+    rt = ReplicaRouter(2)
+    a = rt.route("a", 100)
+    b = rt.route("b", 10)
+    c = rt.route("c", 10)
+    assert (a, b, c) == (0, 1, 1)
+    assert rt.route("d", 5) == 1 and rt.load == [100, 25]
+    rt.done("a")
+    assert rt.route("e", 1) == 0
+
+
+def _free_port():
+    with socket.socket() as s:
+        s.bind(("127.0.0.1", 0))
+        return s.getsockname()[1]
+
+
+def _worker(rank, world, port, n, out):
+    import torch.distributed as dist
+    os.environ["MASTER_ADDR"] = "127.0.0.1"
+    os.environ["MASTER_PORT"] = str(port)
+    dist.init_process_group("gloo", rank=rank, world_size=world)
+    try:
+        start, stop = shard_range(n, rank, world)
+        spans = [None] * world
+        dist.all_gather_object(spans, (start, stop))
+        slowest = max_over_ranks(1.0 + rank)  # rank 1 is "slower"
+        mine = rank_tiles(640, 360, rank, world)
+        all_tiles = [None] * world
+        dist.all_gather_object(all_tiles, mine)
+        if rank == 0:
+            out.put((spans, slowest, all_tiles))
+    finally:
+        dist.destroy_process_group()
+
+
+def test_two_gloo_ranks():
+    import torch.multiprocessing as mp
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    port = _free_port()
+    n = 1_000_003
+    procs = [ctx.Process(target=_worker, args=(r, 2, port, n, q)) for r in range(2)]
+    for p in procs:
+        p.start()
+    spans, slowest, all_tiles = q.get(timeout=120)
+    for p in procs:
+        p.join(timeout=60)
+        assert p.exitcode == 0
+    assert spans[0] == (0, 500_002) and spans[1] == (500_002, n)
+    assert slowest == 2.0
+    flat = [t for ts in all_tiles for t in ts]
+    assert len(flat) == len(set(flat)) == len(tiles(640, 360))
