@@ -272,7 +272,7 @@ sg_status sg_pt_ray_counts(const sg_pt_scene* pt, int64_t* extension, int64_t* s
  * No SORT counterpart as an API: SORT renders one image per process
  * (work/image_evaluation/image_evaluation.cpp:120-305).
  *
- * sg_server_opts: path_slots = paths in flight, up to 2^24 (each holds about 230 bytes of
+ * sg_server_opts: path_slots = paths in flight (each holds about 250 bytes of
  *   path state in HBM); pixel_budget = pixels of admitted, unfinished requests
  *   (20 bytes each: image + work queue entry); max_requests = requests admitted
  *   at once; steps_per_poll = bounce steps per graph replay (even, >= 2);

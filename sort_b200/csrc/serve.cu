@@ -6,17 +6,14 @@
 //
 // One step:
 //   regen       slots holding a pixel start its next sample; idle slots
-//               claim ring entries (one atomic per warp); each writes the
-//               camera ray of that pixel sample into its slot;
+//               claim ring entries (one atomic per warp); each starts the
+//               camera path of that pixel sample;
 //   settle      the claim counter is pulled back to the ring's end if warps
 //               over-claimed;
-//   count/scan/scatter
-//               the extension queue: active slots sorted by bounce, slot order
-//               within a bounce (a stable counting sort over the pool);
-//   extend      closest-hit traversal of the queue, each ray in its own
-//               scene's tree;
-//   shade       shade_vertex per hit; shadow rays appended with their scene,
-//               the continuation written over the slot's ray;
+//   extend      closest-hit traversal of the extension queue, each ray in its
+//               own scene's tree;
+//   shade       shade_vertex per hit; shadow rays and continuations appended
+//               with their scene;
 //   shadow      any-hit traversal of the shadow queue;
 //   resolve     unoccluded shadow results to their slot;
 //   accumulate  both results added to the path's radiance (sg_pt_render's
@@ -24,7 +21,7 @@
 //               keeps the pixel for its next sample, or at the end of a claim
 //               appends that sample to the ring, or after the last sample
 //               scales the pixel by 1/spp and counts it finished;
-//   advance     the rays traced are counted and the shadow queue emptied.
+//   advance     the next extension queue becomes the current one.
 // Every kernel's grid covers the pool (or the shadow queue) and reads its
 // length on the device, so a step is a fixed sequence of launches that a
 // CUDA graph can replay.
@@ -36,6 +33,8 @@
 
 namespace sg {
 namespace {
+
+constexpr int kThreads = 256;
 
 __device__ __forceinline__ unsigned long long warp_append64(unsigned long long* counter, bool want) {
     const unsigned m = __ballot_sync(__activemask(), want);
@@ -76,7 +75,8 @@ __global__ void k_srv_admit_commit(SrvBuffers b) {
     if (threadIdx.x == 0 && blockIdx.x == 0) b.counters->tail += (unsigned long long)b.control->admit_total;
 }
 
-__global__ void k_srv_regen(SrvBuffers b) {
+__global__ void k_srv_regen(SrvBuffers b, float* __restrict__ qray, int* __restrict__ qslot,
+                            int* __restrict__ qscene) {
     const int64_t s = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     const bool in = s < b.slots;
     const unsigned long long tail = b.counters->tail;
@@ -103,13 +103,15 @@ __global__ void k_srv_regen(SrvBuffers b) {
         return;
     }
     const int C = (int)b.slots;
-    put_ray(b.ray, C, (int)s, q.cam.eye, camera_dir(q.cam, q.width, q.height, pix, q.key, (uint32_t)sample), 0.0f,
-            FLT_MAX);
+    const float3 d = camera_dir(q.cam, q.width, q.height, pix, q.key, (uint32_t)sample);
+    const int i = warp_append(&b.counters->queue[0], true);
+    put_ray(qray, C, i, q.cam.eye, d, 0.0f, FLT_MAX);
+    qslot[i] = (int)s;
+    qscene[i] = q.scene;
     b.st_req[s] = r;
     b.st_pix[s] = pix;
     b.st_sample[s] = sample;
     b.st_bounce[s] = 0;
-    b.st_scene[s] = q.scene;
     b.st_state[s] = kSlotActive;
     b.thr[s] = b.thr[C + s] = b.thr[2 * C + s] = 1.0f;
     b.thr[3 * C + s] = b.thr[4 * C + s] = b.thr[5 * C + s] = 0.0f;
@@ -120,129 +122,33 @@ __global__ void k_srv_settle(SrvBuffers b) {
         b.counters->head = b.counters->tail;
 }
 
-// Bucket of an active slot (its bounce), -1 for an inactive one.
-__device__ __forceinline__ int slot_bucket(const SrvBuffers& b, int64_t s) {
-    if (s >= b.slots || b.st_state[s] != kSlotActive) return -1;
-    return min(b.st_bounce[s], kSrvBuckets - 1);
-}
-
-// Per block of the pool: active slots per bucket (bucket-major layout).
-__global__ void __launch_bounds__(kSrvBlock) k_srv_count(SrvBuffers b) {
-    __shared__ int warp_count[kSrvBuckets][kSrvBlock / 32];
-    const int64_t s = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    const int bk = slot_bucket(b, s);
-    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-#pragma unroll
-    for (int k = 0; k < kSrvBuckets; ++k) {
-        const unsigned m = __ballot_sync(0xffffffffu, bk == k);
-        if (lane == 0) warp_count[k][warp] = __popc(m);
-    }
-    __syncthreads();
-    if (threadIdx.x < kSrvBuckets) {
-        int n = 0;
-        for (int w = 0; w < kSrvBlock / 32; ++w) n += warp_count[threadIdx.x][w];
-        b.bucket_counts[(int64_t)threadIdx.x * gridDim.x + blockIdx.x] = n;
-    }
-}
-
-// Exclusive scan of the bucket counts (one block); the total is the queue length.
-// Tiles of 1024 consecutive entries (coalesced), each scanned with warp
-// shuffles and one shared-memory pass over the 32 warp totals.
-__global__ void __launch_bounds__(1024) k_srv_scan(SrvBuffers b, int entries) {
-    __shared__ int warp_total[32];
-    __shared__ int carry;
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    if (threadIdx.x == 0) carry = 0;
-    __syncthreads();
-    for (int base = 0; base < entries; base += 1024) {
-        const int i = base + threadIdx.x;
-        const int c = i < entries ? b.bucket_counts[i] : 0;
-        int x = c;  // inclusive scan within the warp
-#pragma unroll
-        for (int off = 1; off < 32; off <<= 1) {
-            const int y = __shfl_up_sync(0xffffffffu, x, off);
-            if (lane >= off) x += y;
-        }
-        if (lane == 31) warp_total[warp] = x;
-        __syncthreads();
-        if (warp == 0) {
-            int w = warp_total[lane];
-#pragma unroll
-            for (int off = 1; off < 32; off <<= 1) {
-                const int y = __shfl_up_sync(0xffffffffu, w, off);
-                if (lane >= off) w += y;
-            }
-            warp_total[lane] = w;  // inclusive over warps
-        }
-        __syncthreads();
-        const int before = carry + (warp > 0 ? warp_total[warp - 1] : 0) + x - c;
-        if (i < entries) b.bucket_counts[i] = before;
-        __syncthreads();
-        if (threadIdx.x == 0) carry += warp_total[31];
-        __syncthreads();
-    }
-    if (threadIdx.x == 0) b.counters->queue[0] = carry;
-}
-
-// Each active slot to its place: bucket offset of its block + rank in the block.
-__global__ void __launch_bounds__(kSrvBlock) k_srv_scatter(SrvBuffers b) {
-    __shared__ int warp_count[kSrvBuckets][kSrvBlock / 32];
-    const int64_t s = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    const int bk = slot_bucket(b, s);
-    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    int rank = 0;
-#pragma unroll
-    for (int k = 0; k < kSrvBuckets; ++k) {
-        const unsigned m = __ballot_sync(0xffffffffu, bk == k);
-        if (bk == k) rank = __popc(m & ((1u << lane) - 1u));
-        if (lane == 0) warp_count[k][warp] = __popc(m);
-    }
-    __syncthreads();
-    if (bk < 0) return;
-    for (int w = 0; w < warp; ++w) rank += warp_count[bk][w];
-    b.queue[b.bucket_counts[(int64_t)bk * gridDim.x + blockIdx.x] + rank] = (int)s;
-}
-
-// Closest hit for every queued slot; each ray in its own scene's tree.
-template <int W, int STACK, bool Q8>
-__global__ void __launch_bounds__(128) k_srv_extend(SrvBuffers b) {
-    const int q = blockIdx.x * blockDim.x + threadIdx.x;
-    if (q >= b.counters->queue[0]) return;
-    const int s = b.queue[q];
-    const int C = (int)b.slots;
-    const DevTree tr = b.scenes[b.st_scene[s]].tree;
-    const DevRays rays{b.ray, b.ray + C, b.ray + 2 * C, b.ray + 3 * C, b.ray + 4 * C, b.ray + 5 * C, b.ray + 6 * C,
-                       b.ray + 7 * C};
-    Traversal<W, false, STACK, false, Q8> tv;
-    if (tv.start(tr, rays, s))
-        while (!tv.step(tr, b.err)) {
-        }
-    tv.finish(q, b.hit_prim, b.hit_t, nullptr, nullptr, nullptr, nullptr);
-}
-
-// Any hit over the shadow queue, rays of many scenes.
-template <int W, int STACK, bool Q8>
-__global__ void __launch_bounds__(128) k_srv_shadow(SrvBuffers b) {
+// One ray per thread over a queue of rays from many scenes.
+template <int W, bool ANY, int STACK, bool Q8>
+__global__ void __launch_bounds__(128) k_srv_trace(const SrvScene* __restrict__ scenes, const float* __restrict__ ray,
+                                                   const int* __restrict__ scene_of, int cap,
+                                                   const int* __restrict__ count, int32_t* __restrict__ prim,
+                                                   float* __restrict__ t, uint8_t* __restrict__ occ,
+                                                   int* __restrict__ err) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= b.counters->queue[2]) return;
-    const int SC = 2 * (int)b.slots;
-    const DevTree tr = b.scenes[b.sq_scene[i]].tree;
-    const float* ray = b.sq_ray;
-    const DevRays rays{ray, ray + SC, ray + 2 * SC, ray + 3 * SC, ray + 4 * SC, ray + 5 * SC, ray + 6 * SC,
-                       ray + 7 * SC};
-    Traversal<W, true, STACK, false, Q8> tv;
+    if (i >= *count) return;
+    const DevTree tr = scenes[scene_of[i]].tree;
+    const DevRays rays{ray, ray + cap, ray + 2 * cap, ray + 3 * cap, ray + 4 * cap, ray + 5 * cap, ray + 6 * cap,
+                       ray + 7 * cap};
+    Traversal<W, ANY, STACK, false, Q8> tv;
     if (tv.start(tr, rays, i))
-        while (!tv.step(tr, b.err)) {
+        while (!tv.step(tr, err)) {
         }
-    tv.finish(i, nullptr, nullptr, nullptr, nullptr, b.occ, nullptr);
+    tv.finish(i, prim, t, nullptr, nullptr, occ, nullptr);
 }
 
-__global__ void k_srv_shade(SrvBuffers b) {
+__global__ void k_srv_shade(SrvBuffers b, const float* __restrict__ qray, const int* __restrict__ qslot,
+                            const int* __restrict__ qscene, float* __restrict__ nray, int* __restrict__ nslot,
+                            int* __restrict__ nscene) {
     const int q = blockIdx.x * blockDim.x + threadIdx.x;
     if (q >= b.counters->queue[0]) return;
     const int C = (int)b.slots, SC = 2 * C;
-    const int s = b.queue[q];
-    const int sc = b.st_scene[s];
+    const int s = qslot[q];
+    const int sc = qscene[q];
     const int prim = b.hit_prim[q];
     float* thr = b.thr;
 #pragma unroll
@@ -250,9 +156,8 @@ __global__ void k_srv_shade(SrvBuffers b) {
     Vertex v;
     if (prim >= 0) {
         const SrvRequest& rq = b.requests[b.st_req[s]];
-        const float* ray = b.ray;
-        const float3 o = f3(ray[s], ray[C + s], ray[2 * C + s]);
-        const float3 d = f3(ray[3 * C + s], ray[4 * C + s], ray[5 * C + s]);
+        const float3 o = f3(qray[q], qray[C + q], qray[2 * C + q]);
+        const float3 d = f3(qray[3 * C + q], qray[4 * C + q], qray[5 * C + q]);
         v = shade_vertex(b.scenes[sc].pt, rq.key, (uint32_t)b.st_pix[s], (uint32_t)b.st_sample[s], b.st_bounce[s],
                          rq.max_depth, o, d, prim, b.hit_t[q], f3(thr[s], thr[C + s], thr[2 * C + s]));
         if (v.emit) {
@@ -284,8 +189,11 @@ __global__ void k_srv_shade(SrvBuffers b) {
         b.sq_contrib[SC + i2] = v.c2.y;
         b.sq_contrib[2 * SC + i2] = v.c2.z;
     }
-    if (v.cont) {  // the continuation replaces the slot's ray
-        put_ray(b.ray, C, s, v.X, v.wi_next, 0.0001f, FLT_MAX);
+    const int in = warp_append(&b.counters->queue[1], v.cont);
+    if (in >= 0) {
+        put_ray(nray, C, in, v.X, v.wi_next, 0.0001f, FLT_MAX);
+        nslot[in] = s;
+        nscene[in] = sc;
         b.st_bounce[s] += 1;
     } else {
         b.st_state[s] = kSlotFinished;
@@ -303,11 +211,11 @@ __global__ void k_srv_resolve(SrvBuffers b) {
     b.vis[(3 * which + 2) * C + s] = b.sq_contrib[2 * SC + i];
 }
 
-__global__ void k_srv_accumulate(SrvBuffers b) {
+__global__ void k_srv_accumulate(SrvBuffers b, const int* __restrict__ qslot) {
     const int q = blockIdx.x * blockDim.x + threadIdx.x;
     if (q >= b.counters->queue[0]) return;
     const int C = (int)b.slots;
-    const int s = b.queue[q];
+    const int s = qslot[q];
     float* thr = b.thr;
 #pragma unroll
     for (int c = 0; c < 3; ++c) thr[(3 + c) * C + s] += b.vis[c * C + s] + b.vis[(3 + c) * C + s];
@@ -358,30 +266,38 @@ __global__ void k_srv_advance(SrvBuffers b) {
     SrvCounters* c = b.counters;
     c->ext_rays += (unsigned long long)c->queue[0];
     c->shadow_rays += (unsigned long long)c->queue[2];
+    c->queue[0] = c->queue[1];
+    c->queue[1] = 0;
     c->queue[2] = 0;
 }
 
 template <int W, bool Q8, int STACK>
 cudaError_t enqueue_stack(const SrvBuffers& b, int iterations, cudaStream_t s) {
     const int C = (int)b.slots;
-    const int pool_blocks = (C + kSrvBlock - 1) / kSrvBlock;
+    const int pool_blocks = (C + kThreads - 1) / kThreads;
     const int trace_blocks = (C + 127) / 128;
     const int shadow_blocks = (2 * C + 127) / 128;
     for (int it = 0; it < iterations; ++it) {
+        const bool a_cur = (it % 2) == 0;  // even steps read queue A and write queue B
+        float* cray = a_cur ? b.qa_ray : b.qb_ray;
+        int* cslot = a_cur ? b.qa_slot : b.qb_slot;
+        int* cscene = a_cur ? b.qa_scene : b.qb_scene;
+        float* nray = a_cur ? b.qb_ray : b.qa_ray;
+        int* nslot = a_cur ? b.qb_slot : b.qa_slot;
+        int* nscene = a_cur ? b.qb_scene : b.qa_scene;
         if (it == 0) {
-            k_srv_admit<<<1184, kSrvBlock, 0, s>>>(b);
+            k_srv_admit<<<1184, kThreads, 0, s>>>(b);
             k_srv_admit_commit<<<1, 32, 0, s>>>(b);
         }
-        k_srv_regen<<<pool_blocks, kSrvBlock, 0, s>>>(b);
+        k_srv_regen<<<pool_blocks, kThreads, 0, s>>>(b, cray, cslot, cscene);
         k_srv_settle<<<1, 32, 0, s>>>(b);
-        k_srv_count<<<pool_blocks, kSrvBlock, 0, s>>>(b);
-        k_srv_scan<<<1, 1024, 0, s>>>(b, pool_blocks * kSrvBuckets);
-        k_srv_scatter<<<pool_blocks, kSrvBlock, 0, s>>>(b);
-        k_srv_extend<W, STACK, Q8><<<trace_blocks, 128, 0, s>>>(b);
-        k_srv_shade<<<pool_blocks, kSrvBlock, 0, s>>>(b);
-        k_srv_shadow<W, STACK, Q8><<<shadow_blocks, 128, 0, s>>>(b);
-        k_srv_resolve<<<(2 * C + kSrvBlock - 1) / kSrvBlock, kSrvBlock, 0, s>>>(b);
-        k_srv_accumulate<<<pool_blocks, kSrvBlock, 0, s>>>(b);
+        k_srv_trace<W, false, STACK, Q8><<<trace_blocks, 128, 0, s>>>(
+            b.scenes, cray, cscene, C, &b.counters->queue[0], b.hit_prim, b.hit_t, nullptr, b.err);
+        k_srv_shade<<<pool_blocks, kThreads, 0, s>>>(b, cray, cslot, cscene, nray, nslot, nscene);
+        k_srv_trace<W, true, STACK, Q8><<<shadow_blocks, 128, 0, s>>>(
+            b.scenes, b.sq_ray, b.sq_scene, 2 * C, &b.counters->queue[2], nullptr, nullptr, b.occ, b.err);
+        k_srv_resolve<<<(2 * C + kThreads - 1) / kThreads, kThreads, 0, s>>>(b);
+        k_srv_accumulate<<<pool_blocks, kThreads, 0, s>>>(b, cslot);
         k_srv_advance<<<1, 32, 0, s>>>(b);
     }
     return cudaGetLastError();

@@ -89,13 +89,15 @@ struct SrvBuffers {
     int* st_sample;
     int* st_bounce;
     int* st_state;
-    int* st_scene;
     float* thr;  // 6 * C: throughput, radiance of the current sample
     float* vis;  // 6 * C: this bounce's two shadow-ray results
-    float* ray;  // 8 * C: each slot's next extension ray (SoA by slot)
-    int* queue;  // extension queue: active slots ordered by (bounce, slot)
-    int* bucket_counts;  // kSrvBuckets * blocks of the pool: counts, then their exclusive scan
-    int32_t* hit_prim;   // per queue entry
+    float* qa_ray;
+    int* qa_slot;
+    int* qa_scene;
+    float* qb_ray;
+    int* qb_slot;
+    int* qb_scene;
+    int32_t* hit_prim;
     float* hit_t;
     float* sq_ray;  // shadow queue, 2 * C entries
     int* sq_slot;
@@ -105,15 +107,8 @@ struct SrvBuffers {
     int* err;
 };
 
-// The extension queue is sorted into buckets by bounce (deeper bounces share
-// the last bucket), slot order within a bucket, so a warp traces rays of one
-// bounce from neighbouring slots, which hold neighbouring pixels.
-constexpr int kSrvBuckets = 8;
-constexpr int kSrvBlock = 256;  // threads per block of the pool-wide kernels
-
 // Bytes of path state per pool slot (the buffers above, per slot).
-constexpr int64_t kSrvBytesPerSlot =
-    6 * 4 + 6 * 4 * 2 + 8 * 4 + 4 + 4 + 4 + 2 * (8 * 4 + 4 + 4 + 3 * 4 + 1);
+constexpr int64_t kSrvBytesPerSlot = 5 * 4 + 6 * 4 * 2 + 2 * (8 * 4 + 4 + 4) + 4 + 4 + 2 * (8 * 4 + 4 + 4 + 3 * 4 + 1);
 
 // Enqueues `iterations` bounce steps on s; the first takes this replay's
 // admissions. Tree width / stack / node format are those of every scene.

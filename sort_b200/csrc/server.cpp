@@ -349,7 +349,7 @@ void sg_default_server_opts(sg_server_opts* o) {
     o->path_slots = int64_t(1) << 20;
     o->pixel_budget = int64_t(1) << 24;
     o->steps_per_poll = 4;
-    o->samples_per_claim = 8;
+    o->samples_per_claim = 1;
 }
 
 sg_status sg_server_create(const sg_server_opts* opts, sg_server** out) {
@@ -357,7 +357,7 @@ sg_status sg_server_create(const sg_server_opts* opts, sg_server** out) {
     *out = nullptr;
     const sg_server_opts& o = *opts;
     if (o.max_requests < 1 || o.max_requests > 65535) return fail(SG_ERR_INVALID_ARGUMENT, "max_requests out of range");
-    if (o.path_slots < 32 || o.path_slots > (int64_t(1) << 24))
+    if (o.path_slots < 32 || o.path_slots > (int64_t(1) << 28))
         return fail(SG_ERR_INVALID_ARGUMENT, "path_slots out of range");
     if (o.pixel_budget < 1 || o.pixel_budget > (int64_t(1) << 31))
         return fail(SG_ERR_INVALID_ARGUMENT, "pixel_budget out of range");
@@ -380,14 +380,16 @@ sg_status sg_server_create(const sg_server_opts* opts, sg_server** out) {
     const size_t C = size_t(o.path_slots), R = size_t(o.max_requests), P = size_t(o.pixel_budget);
     // Device layout.
     sg::SrvBuffers& b = S->b;
-    int* st_arrays[6];
+    int* st_arrays[5];
+    float* ray_q[3];
+    int* slot_q[3];
+    int* scene_q[3];
     size_t total = 0;
     std::vector<size_t> offs;
     auto add = [&](size_t bytes) {
         offs.push_back(total);
         total += align_up(bytes);
     };
-    const size_t pool_blocks = (C + sg::kSrvBlock - 1) / sg::kSrvBlock;
     add(R * sizeof(sg::SrvRequest));          // 0 requests
     add(kMaxScenes * sizeof(sg::SrvScene));  // 1 scenes
     add(sizeof(sg::SrvControl));             // 2 control
@@ -396,20 +398,22 @@ sg_status sg_server_create(const sg_server_opts* opts, sg_server** out) {
     add(R * sizeof(int));                    // 5 done
     add(P * sizeof(unsigned long long));     // 6 ring
     add(P * 3 * sizeof(float));              // 7 images
-    for (int k = 0; k < 6; ++k) add(C * sizeof(int));  // 8..13 slot state
-    add(C * 6 * sizeof(float));              // 14 thr
-    add(C * 6 * sizeof(float));              // 15 vis
-    add(C * 8 * sizeof(float));              // 16 slot rays
-    add(C * sizeof(int));                    // 17 extension queue
-    add(pool_blocks * sg::kSrvBuckets * sizeof(int));  // 18 bucket counts
-    add(C * sizeof(int32_t));                // 19 hit prim
-    add(C * sizeof(float));                  // 20 hit t
-    add(2 * C * 8 * sizeof(float));          // 21 shadow rays
-    add(2 * C * sizeof(int));                // 22 shadow slots
-    add(2 * C * sizeof(int));                // 23 shadow scenes
-    add(2 * C * 3 * sizeof(float));          // 24 contributions
-    add(2 * C);                              // 25 occlusion
-    add(sizeof(int));                        // 26 status
+    for (int k = 0; k < 5; ++k) add(C * sizeof(int));  // 8..12 slot state
+    add(C * 6 * sizeof(float));              // 13 thr
+    add(C * 6 * sizeof(float));              // 14 vis
+    for (int k = 0; k < 2; ++k) {            // 15..20 extension queues
+        add(C * 8 * sizeof(float));
+        add(C * sizeof(int));
+        add(C * sizeof(int));
+    }
+    add(C * sizeof(int32_t));                // 21 hit prim
+    add(C * sizeof(float));                  // 22 hit t
+    add(2 * C * 8 * sizeof(float));          // 23 shadow rays
+    add(2 * C * sizeof(int));                // 24 shadow slots
+    add(2 * C * sizeof(int));                // 25 shadow scenes
+    add(2 * C * 3 * sizeof(float));          // 26 contributions
+    add(2 * C);                              // 27 occlusion
+    add(sizeof(int));                        // 28 status
     cudaError_t e = cudaMalloc(&S->d_mem, total);
     if (e != cudaSuccess) {
         free_server(S);
@@ -422,7 +426,12 @@ sg_status sg_server_create(const sg_server_opts* opts, sg_server** out) {
     S->d_control = reinterpret_cast<sg::SrvControl*>(m + offs[2]);
     S->d_counters = reinterpret_cast<sg::SrvCounters*>(m + offs[3]);
     S->d_images = reinterpret_cast<float*>(m + offs[7]);
-    for (int k = 0; k < 6; ++k) st_arrays[k] = reinterpret_cast<int*>(m + offs[8 + k]);
+    for (int k = 0; k < 5; ++k) st_arrays[k] = reinterpret_cast<int*>(m + offs[8 + k]);
+    for (int k = 0; k < 2; ++k) {
+        ray_q[k] = reinterpret_cast<float*>(m + offs[15 + 3 * k]);
+        slot_q[k] = reinterpret_cast<int*>(m + offs[16 + 3 * k]);
+        scene_q[k] = reinterpret_cast<int*>(m + offs[17 + 3 * k]);
+    }
     b.requests = S->d_requests;
     b.scenes = S->d_scenes;
     b.control = S->d_control;
@@ -438,23 +447,25 @@ sg_status sg_server_create(const sg_server_opts* opts, sg_server** out) {
     b.st_sample = st_arrays[2];
     b.st_bounce = st_arrays[3];
     b.st_state = st_arrays[4];
-    b.st_scene = st_arrays[5];
-    b.thr = reinterpret_cast<float*>(m + offs[14]);
-    b.vis = reinterpret_cast<float*>(m + offs[15]);
-    b.ray = reinterpret_cast<float*>(m + offs[16]);
-    b.queue = reinterpret_cast<int*>(m + offs[17]);
-    b.bucket_counts = reinterpret_cast<int*>(m + offs[18]);
-    b.hit_prim = reinterpret_cast<int32_t*>(m + offs[19]);
-    b.hit_t = reinterpret_cast<float*>(m + offs[20]);
-    b.sq_ray = reinterpret_cast<float*>(m + offs[21]);
-    b.sq_slot = reinterpret_cast<int*>(m + offs[22]);
-    b.sq_scene = reinterpret_cast<int*>(m + offs[23]);
-    b.sq_contrib = reinterpret_cast<float*>(m + offs[24]);
-    b.occ = reinterpret_cast<uint8_t*>(m + offs[25]);
-    b.err = reinterpret_cast<int*>(m + offs[26]);
+    b.thr = reinterpret_cast<float*>(m + offs[13]);
+    b.vis = reinterpret_cast<float*>(m + offs[14]);
+    b.qa_ray = ray_q[0];
+    b.qa_slot = slot_q[0];
+    b.qa_scene = scene_q[0];
+    b.qb_ray = ray_q[1];
+    b.qb_slot = slot_q[1];
+    b.qb_scene = scene_q[1];
+    b.hit_prim = reinterpret_cast<int32_t*>(m + offs[21]);
+    b.hit_t = reinterpret_cast<float*>(m + offs[22]);
+    b.sq_ray = reinterpret_cast<float*>(m + offs[23]);
+    b.sq_slot = reinterpret_cast<int*>(m + offs[24]);
+    b.sq_scene = reinterpret_cast<int*>(m + offs[25]);
+    b.sq_contrib = reinterpret_cast<float*>(m + offs[26]);
+    b.occ = reinterpret_cast<uint8_t*>(m + offs[27]);
+    b.err = reinterpret_cast<int*>(m + offs[28]);
     // Zeroed state: counters, idle slots (kSlotIdle == 0), flags, status.
     e = cudaMemset(S->d_mem, 0, offs[6]);
-    if (e == cudaSuccess) e = cudaMemset(m + offs[8], 0, offs[14] - offs[8]);
+    if (e == cudaSuccess) e = cudaMemset(m + offs[8], 0, offs[13] - offs[8]);
     if (e == cudaSuccess) e = cudaMemset(b.err, 0, sizeof(int));
     if (e == cudaSuccess) e = cudaMallocHost(&S->h_requests, R * sizeof(sg::SrvRequest));
     if (e == cudaSuccess) e = cudaMallocHost(&S->h_units, R * sizeof(unsigned));
