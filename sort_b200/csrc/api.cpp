@@ -424,9 +424,9 @@ static sg_status host_trace(const sg_scene* cs, const float* rays8, int64_t n, i
     float* du = reinterpret_cast<float*>(d_out + size_t(n) * 8);
     float* dv = reinterpret_cast<float*>(d_out + size_t(n) * 12);
     uint8_t* docc = reinterpret_cast<uint8_t*>(d_out);
-    // Chunks of at least 512k rays (one chunk below 1M), at most kMaxChunks:
+    // Chunks of at least 256k rays (one chunk below 512k), at most kMaxChunks:
     // chunk k's rays go in while chunk k-1 is traced and chunk k-2's hits come out.
-    const int64_t min_chunk = int64_t(1) << 19;
+    const int64_t min_chunk = int64_t(1) << 18;
     const int chunks = int(std::min<int64_t>(sg_scene::kMaxChunks, std::max<int64_t>(1, n / min_chunk / 2 * 2)));
     const int64_t per = (n + chunks - 1) / chunks;
     sg_status status = SG_OK;
