@@ -263,6 +263,26 @@ struct Traversal {
         }
         const int cnt = __popc(mask);
         if (cnt == 0) return false;
+        if (ANY && !STATS) {
+            // Any hit: before the first hit nothing is culled (the current hit
+            // distance stays FLT_MAX), so the answer is whether any triangle of
+            // the nodes the slab tests reach is hit, whatever the visit order.
+            // Descend into the lowest hit slot, push the others; SORT's
+            // near-first order is kept only where its counts are wanted.
+            const unsigned first = mask & (0u - mask);  // lowest set bit
+            int32_t fc = 0;
+#pragma unroll
+            for (int j = 0; j < W; ++j) {
+                if (!(mask & (1u << j))) continue;
+                if ((1u << j) == first)
+                    fc = nd.ch[j];
+                else
+                    stk[si++] = make_uint2((uint32_t)nd.ch[j], 0u);  // entry distance 0: never culled
+            }
+            cur = fc;
+            cur_d = 0.0f;
+            return true;
+        }
         if (cnt == 1) {
 #pragma unroll
             for (int j = 0; j < W; ++j)
