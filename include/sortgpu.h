@@ -151,6 +151,25 @@ sg_status sg_scene_get_tuning(const sg_scene* scene, sg_trace_tuning* tuning);
 sg_status sg_trace_closest(const sg_scene* scene, const sg_rays* rays, int64_t n, const sg_hits* hits, void* stream);
 sg_status sg_trace_any(const sg_scene* scene, const sg_rays* rays, int64_t n, uint8_t* occluded, void* stream);
 
+/* BSSRDF probe query: Accelerator::GetIntersect(const Ray&, BSSRDFIntersections&,
+ * RenderContext&, StringID) (accel/accelerator.h:122, accel/fast_bvh.hpp:656-819)
+ * for a batch. Per ray up to 4 (TOTAL_SSS_INTERSECTION_CNT) hits on primitives
+ * whose material equals ray_material[i], gathered and replaced exactly as SORT
+ * does (intersectTriangleMulti_SIMD, simd/simd_triangle.h:412-455), so the kept
+ * set and the slot of each hit are SORT's. prim_material: one material id per
+ * primitive (input order), device; ray_material: one per ray, device.
+ * hits: count[i] = hits kept; prim / t / u / v hold 4 entries per ray at
+ * [4*i + k] (prim -1, t FLT_MAX past count); u, v may be NULL. */
+typedef struct {
+    int32_t* count;
+    int32_t* prim;
+    float* t;
+    float* u;
+    float* v;
+} sg_multi_hits;
+sg_status sg_trace_multi(const sg_scene* scene, const sg_rays* rays, int64_t n, const int32_t* prim_material,
+                         const int32_t* ray_material, const sg_multi_hits* hits, void* stream);
+
 /* Counts over one batch (synchronises the stream): interior nodes box-tested and
  * primitives tested, the latter counted per leaf entered as SORT's
  * sIntersectionTest does. any = 0 closest-hit traversal, 1 any-hit traversal. */

@@ -76,6 +76,18 @@ class _Tree:
         self.api._any(self.h, r.ctypes.data, n, occ.ctypes.data, threads or os.cpu_count())
         return occ
 
+    def multi(self, rays: np.ndarray, ray_mat: np.ndarray, threads: int = 0):
+        """BSSRDF probe query: (count, prim, t, u, v), the last four (n, 4)."""
+        r = np.ascontiguousarray(rays, np.float32)
+        n = r.shape[1]
+        rm = np.ascontiguousarray(ray_mat, np.int32)
+        count = np.empty(n, np.int32)
+        prim = np.empty((n, 4), np.int32)
+        t, u, v = (np.empty((n, 4), np.float32) for _ in range(3))
+        self.api._multi(self.h, r.ctypes.data, n, rm.ctypes.data, count.ctypes.data, prim.ctypes.data, t.ctypes.data,
+                        u.ctypes.data, v.ctypes.data, threads or os.cpu_count())
+        return count, prim, t, u, v
+
 
 class Port:
     """The C restatement (oracle/port/oracle.c)."""
@@ -147,9 +159,25 @@ class Reference:
         L.sortref_trace_closest.argtypes = [_vp, _vp, _i64, _vp, _vp, _vp, _vp, ctypes.c_int]
         L.sortref_trace_any.argtypes = [_vp, _vp, _i64, _vp, ctypes.c_int]
         L.sortref_ray_prepare.argtypes = [_vp, _vp, _vp]
+        L.sortref_scene_create_mat.restype = _vp
+        L.sortref_scene_create_mat.argtypes = [ctypes.c_int, _vp, ctypes.c_int, _vp, ctypes.c_int, ctypes.c_int,
+                                               ctypes.c_int]
+        L.sortref_trace_multi.argtypes = [_vp, _vp, _i64, _vp, _vp, _vp, _vp, _vp, _vp, ctypes.c_int]
         self.L = L
         self._free, self._topo, self._depth = L.sortref_scene_destroy, L.sortref_topology, L.sortref_depth
         self._bbox, self._closest, self._any = L.sortref_scene_bbox, L.sortref_trace_closest, L.sortref_trace_any
+        self._multi = L.sortref_trace_multi
+
+    def build_materials(self, tri: np.ndarray, mat_of_tri: np.ndarray, nmat: int, width: int, max_depth: int = 16,
+                        max_leaf: int = 8) -> _Tree:
+        """A tree whose triangles carry materials 0..nmat-1 (for the multi-hit query)."""
+        tri = np.ascontiguousarray(tri, np.float32).reshape(-1, 9)
+        m = np.ascontiguousarray(mat_of_tri, np.int32)
+        h = self.L.sortref_scene_create_mat(width, tri.ctypes.data, tri.shape[0], m.ctypes.data, int(nmat),
+                                            max_depth, max_leaf)
+        if not h:
+            raise ValueError("reference build failed")
+        return _Tree(self, h, width, tri.shape[0])
 
     def build(self, tri: np.ndarray, width: int, max_depth: int = 16, max_leaf: int = 8) -> _Tree:
         tri = np.ascontiguousarray(tri, np.float32).reshape(-1, 9)

@@ -45,6 +45,7 @@
 #include "material/material.h"
 #include "core/render_context.h"
 #include "math/interaction.h"
+#include "scatteringevent/bssrdf/bssrdf.h"
 #undef private
 #undef protected
 
@@ -73,11 +74,25 @@ public:
 
 OpaqueMaterial g_opaque;
 
+// Opaque material with its own unique id, for the BSSRDF multi-hit query,
+// which keeps only hits on primitives of one material (by GetUniqueID).
+class TaggedMaterial : public OpaqueMaterial {
+public:
+    explicit TaggedMaterial(sid_t id) : m_id(id) {}
+    StringID GetUniqueID() const override { return StringID(m_id); }
+
+private:
+    sid_t m_id;
+};
+
+// Material index k of a harness scene maps to unique id kMaterialIdBase + k.
+constexpr sid_t kMaterialIdBase = 1000;
+
 // A MeshVisual filled directly from a flat triangle list (one triangle per three
 // vertices), mirroring what MeshVisual::Serialize does (entity/visual.cpp:26-33).
 class HarnessVisual : public MeshVisual {
 public:
-    void Fill(const float* tri, int ntri) {
+    void Fill(const float* tri, int ntri, MaterialBase* const* mats = nullptr) {
         m_memory = std::make_unique<Mesh>();
         m_memory->m_vertices.resize((size_t)ntri * 3);
         m_memory->m_indices.resize((size_t)ntri);
@@ -100,7 +115,7 @@ public:
             fi.m_id[0] = i * 3;
             fi.m_id[1] = i * 3 + 1;
             fi.m_id[2] = i * 3 + 2;
-            fi.m_mat = &g_opaque;
+            fi.m_mat = mats ? mats[i] : &g_opaque;
         }
         m_memory->m_hasUV = true;
         for (const auto& mi : m_memory->m_indices) {
@@ -126,6 +141,7 @@ struct RefScene {
     int width = 4;
     std::unordered_map<const Primitive*, int32_t> index_of;
     std::vector<const Primitive*> prims;
+    std::vector<std::unique_ptr<TaggedMaterial>> materials;
 };
 
 }  // namespace
@@ -207,13 +223,26 @@ extern "C" {
 // Build SORT's QBVH (width 4) or OBVH (width 8) over ntri triangles given as
 // 9 floats each (v0, v1, v2). max_depth / max_leaf are Fbvh's m_maxNodeDepth /
 // m_maxPriInLeaf (accel/fast_bvh.h:176-181, read from the scene stream in SORT).
-void* sortref_scene_create(int width, const float* tri, int ntri, int max_depth, int max_leaf) {
-    if ((width != 4 && width != 8) || ntri < 0) return nullptr;
+void* sortref_scene_create_mat(int width, const float* tri, int ntri, const int32_t* mat_of_tri, int nmat,
+                               int max_depth, int max_leaf) {
+    if ((width != 4 && width != 8) || ntri < 0 || nmat < 0) return nullptr;
     auto* rs = new RefScene();
     rs->width = width;
+    std::vector<MaterialBase*> mats;
+    if (mat_of_tri) {
+        for (int k = 0; k < nmat; ++k) rs->materials.push_back(std::make_unique<TaggedMaterial>(kMaterialIdBase + k));
+        mats.resize((size_t)ntri);
+        for (int i = 0; i < ntri; ++i) {
+            if (mat_of_tri[i] < 0 || mat_of_tri[i] >= nmat) {
+                delete rs;
+                return nullptr;
+            }
+            mats[(size_t)i] = rs->materials[(size_t)mat_of_tri[i]].get();
+        }
+    }
     auto entity = std::make_unique<HarnessEntity>();
     HarnessVisual* visual = entity->AddVisual();
-    visual->Fill(tri, ntri);
+    visual->Fill(tri, ntri, mat_of_tri ? mats.data() : nullptr);
     rs->scene.m_entities.push_back(std::move(entity));
 
     ScenePrimitiveIterator iter(rs->scene);
@@ -235,6 +264,44 @@ void* sortref_scene_create(int width, const float* tri, int ntri, int max_depth,
         rs->scene.m_accelerator.reset(harness_make_obvh((unsigned)max_depth, (unsigned)max_leaf));
     rs->scene.m_accelerator->Build(rs->scene);
     return rs;
+}
+
+void* sortref_scene_create(int width, const float* tri, int ntri, int max_depth, int max_leaf) {
+    return sortref_scene_create_mat(width, tri, ntri, nullptr, 0, max_depth, max_leaf);
+}
+
+// BSSRDF probe query through Scene::GetIntersect(const Ray&, BSSRDFIntersections&,
+// RenderContext&, StringID) (core/scene.cpp:221-225): up to
+// TOTAL_SSS_INTERSECTION_CNT (4) hits on primitives of material ray_mat[i], in
+// the slots SORT leaves them in. count[i] = hits kept; per ray 4 entries of
+// prim / t / u / v at [4 * i + k], entries past count are prim -1, t FLT_MAX.
+void sortref_trace_multi(void* h, const float* rays, int64_t n, const int32_t* ray_mat, int32_t* count,
+                         int32_t* prim, float* t, float* u, float* v, int nthreads) {
+    RefScene* rs = (RefScene*)h;
+    const bool valid = rs->scene.m_accelerator->GetIsValid();
+    parallel_chunks(n, nthreads, [&](RenderContext& rc, int64_t i) {
+        Ray r(Point(rays[i], rays[n + i], rays[2 * n + i]), Vector(rays[3 * n + i], rays[4 * n + i], rays[5 * n + i]), 0,
+              rays[6 * n + i], rays[7 * n + i]);
+        BSSRDFIntersections inter;  // what Scene::GetIntersect forwards to the accelerator
+        if (valid)
+            rs->scene.m_accelerator->GetIntersect(r, inter, rc, StringID(kMaterialIdBase + (sid_t)ray_mat[i]));
+        count[i] = (int32_t)inter.cnt;
+        for (unsigned k = 0; k < TOTAL_SSS_INTERSECTION_CNT; ++k) {
+            const int64_t o = 4 * i + k;
+            if (k < inter.cnt) {
+                const SurfaceInteraction& s = inter.intersections[k]->intersection;
+                prim[o] = rs->index_of.at(s.primitive);
+                t[o] = s.t;
+                u[o] = s.u;
+                v[o] = s.v;
+            } else {
+                prim[o] = -1;
+                t[o] = FLT_MAX;
+                u[o] = v[o] = 0.0f;
+            }
+        }
+        rc.m_memory_arena->Reset();
+    });
 }
 
 void sortref_scene_destroy(void* h) { delete (RefScene*)h; }

@@ -53,6 +53,11 @@ class SceneInfo(ctypes.Structure):
                 ("build_seconds", ctypes.c_double)]
 
 
+class MultiHits(ctypes.Structure):
+    _fields_ = [("count", ctypes.c_void_p), ("prim", ctypes.c_void_p), ("t", ctypes.c_void_p), ("u", ctypes.c_void_p),
+                ("v", ctypes.c_void_p)]
+
+
 class Batch(ctypes.Structure):
     _fields_ = [("scene", ctypes.c_void_p), ("rays", ctypes.c_void_p), ("stride", ctypes.c_int64),
                 ("n", ctypes.c_int64), ("any", ctypes.c_int32), ("reserved", ctypes.c_int32), ("hits", Hits),
@@ -126,6 +131,7 @@ _SIGNATURES = {
                                     ctypes.c_uint64, _vp, _vp]),
     "sg_pt_destroy": (ctypes.c_int, [_vp]),
     "sg_pt_ray_counts": (ctypes.c_int, [_vp, ctypes.POINTER(_i64), ctypes.POINTER(_i64), _vp]),
+    "sg_trace_multi": (ctypes.c_int, [_vp, ctypes.POINTER(Rays), _i64, _vp, _vp, ctypes.POINTER(MultiHits), _vp]),
     "sg_probe_l2_read_gbs": (ctypes.c_int, [ctypes.c_int32, _i64, ctypes.c_int32, ctypes.POINTER(ctypes.c_double)]),
     "sg_last_error": (ctypes.c_char_p, []),
     "sg_version": (ctypes.c_char_p, []),

@@ -188,6 +188,30 @@ class Accelerator:
 
     IsOccluded = GetAttenuation
 
+    def GetIntersectBSSRDF(self, rays, prim_material, ray_material, stream=None):
+        """SORT's BSSRDF probe query, GetIntersect(ray, BSSRDFIntersections&, rc,
+        matID) (accel/fast_bvh.hpp:656-819), for a CUDA ray batch: up to 4 hits
+        per ray on primitives whose material (prim_material, int32 per
+        primitive) equals the ray's (ray_material, int32 per ray). Returns
+        (count, prim, t, u, v); the last four have shape (n, 4), in SORT's slots."""
+        self._require()
+        torch = _torch()
+        rays = rays.contiguous()
+        n = rays.shape[1]
+        dev = rays.device
+        pm = torch.as_tensor(prim_material, dtype=torch.int32, device=dev).contiguous()
+        rm = torch.as_tensor(ray_material, dtype=torch.int32, device=dev).contiguous()
+        if pm.numel() != self._info.triangles or rm.numel() != n:
+            raise ValueError("one material per primitive and one per ray")
+        count = torch.empty(n, dtype=torch.int32, device=dev)
+        prim = torch.empty((n, 4), dtype=torch.int32, device=dev)
+        t, u, v = (torch.empty((n, 4), dtype=torch.float32, device=dev) for _ in range(3))
+        h = _lib.MultiHits(count.data_ptr(), prim.data_ptr(), t.data_ptr(), u.data_ptr(), v.data_ptr())
+        s = stream if stream is not None else torch.cuda.current_stream(dev).cuda_stream
+        _lib.check(_lib.load().sg_trace_multi(self._h, ctypes.byref(self._ray_struct(rays)), n, pm.data_ptr(),
+                                              rm.data_ptr(), ctypes.byref(h), s))
+        return count, prim, t, u, v
+
     def TraceStats(self, rays, any_hit: bool = False, stream=None):
         """(interior nodes tested, primitives tested) summed over a CUDA ray batch,
         counted as SORT's traversal statistics count them."""

@@ -64,3 +64,13 @@ def test_port_empty_scene(port):
     from sort_b200 import scenes
     prim, t, _, _ = tree.closest(scenes.random_rays(10))
     assert (prim == -1).all() and (t == np.float32(3.4028234663852886e38)).all()
+
+
+@pytest.mark.parametrize("width", [4, 8])
+def test_reference_multi_reproduces_golden(reference, width):
+    """The committed BSSRDF probe fixture is what SORT's code returns (pins it)."""
+    z = golden("multi")
+    tree = reference.build_materials(z["triangles"], z["mat_of_tri"], 3, width)
+    count, prim, t, u, v = tree.multi(z["rays"], z["ray_mat"])
+    assert np.array_equal(count, z[f"count{width}"]) and np.array_equal(prim, z[f"prim{width}"])
+    assert same_bits(t, z[f"t{width}"]) and same_bits(u, z[f"u{width}"]) and same_bits(v, z[f"v{width}"])
