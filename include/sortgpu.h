@@ -169,6 +169,14 @@ typedef struct {
 } sg_multi_hits;
 sg_status sg_trace_multi(const sg_scene* scene, const sg_rays* rays, int64_t n, const int32_t* prim_material,
                          const int32_t* ray_material, const sg_multi_hits* hits, void* stream);
+/* Host-buffer form for callers like SORT's per-ray integrators: the scene keeps
+ * one material id per primitive (sg_scene_set_materials, host array of the
+ * scene's triangle count, copied to the device); rays8 as sg_trace_closest_host;
+ * ray_material one per ray; outputs 1 (count) or 4 (prim, t, u, v) per ray.
+ * Synchronous. */
+sg_status sg_scene_set_materials(sg_scene* scene, const int32_t* material, int64_t n);
+sg_status sg_trace_multi_host(const sg_scene* scene, const float* rays8, int64_t n, const int32_t* ray_material,
+                              int32_t* count, int32_t* prim, float* t, float* u, float* v);
 
 /* Counts over one batch (synchronises the stream): interior nodes box-tested and
  * primitives tested, the latter counted per leaf entered as SORT's

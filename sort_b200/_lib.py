@@ -132,6 +132,8 @@ _SIGNATURES = {
     "sg_pt_destroy": (ctypes.c_int, [_vp]),
     "sg_pt_ray_counts": (ctypes.c_int, [_vp, ctypes.POINTER(_i64), ctypes.POINTER(_i64), _vp]),
     "sg_trace_multi": (ctypes.c_int, [_vp, ctypes.POINTER(Rays), _i64, _vp, _vp, ctypes.POINTER(MultiHits), _vp]),
+    "sg_scene_set_materials": (ctypes.c_int, [_vp, _vp, _i64]),
+    "sg_trace_multi_host": (ctypes.c_int, [_vp, _vp, _i64, _vp, _vp, _vp, _vp, _vp, _vp]),
     "sg_probe_l2_read_gbs": (ctypes.c_int, [ctypes.c_int32, _i64, ctypes.c_int32, ctypes.POINTER(ctypes.c_double)]),
     "sg_last_error": (ctypes.c_char_p, []),
     "sg_version": (ctypes.c_char_p, []),

@@ -79,6 +79,7 @@ struct sg_scene {
     cudaStream_t out_stream = nullptr;
     cudaEvent_t in_done[kMaxChunks] = {};
     cudaEvent_t trace_done[kMaxChunks] = {};
+    int32_t* d_material = nullptr;  // per primitive, for sg_trace_multi_host (sg_scene_set_materials)
 };
 
 namespace {
@@ -146,6 +147,7 @@ void release(sg_scene* s) {
     if (s->d_stats) cudaFree(s->d_stats);
     if (s->d_counters) cudaFree(s->d_counters);
     if (s->d_scratch) cudaFree(s->d_scratch);
+    if (s->d_material) cudaFree(s->d_material);
     if (s->stream) cudaStreamDestroy(s->stream);
     for (cudaStream_t& x : s->trace_stream)
         if (x) cudaStreamDestroy(x);
@@ -469,6 +471,77 @@ static sg_status host_trace(const sg_scene* cs, const float* rays8, int64_t n, i
         if ((e = cudaStreamSynchronize(x)) != cudaSuccess) return cuda_fail(e, "synchronize");
     if (status != SG_OK) return status;
     return check_status_word(s, s->out_stream);
+}
+
+sg_status sg_scene_set_materials(sg_scene* s, const int32_t* material, int64_t n) {
+    if (!s || (n > 0 && !material)) return fail(SG_ERR_INVALID_ARGUMENT, "NULL argument");
+    if (n != int64_t(s->tree.order.size())) return fail(SG_ERR_INVALID_ARGUMENT, "one material per primitive");
+    std::lock_guard<std::mutex> lock(s->scratch_lock);
+    DeviceGuard g(s->device);
+    if (!g.ok) return fail(SG_ERR_CUDA, "cudaSetDevice failed");
+    cudaError_t e;
+    if (!s->d_material && (e = cudaMalloc(&s->d_material, size_t(std::max<int64_t>(n, 1)) * 4)) != cudaSuccess)
+        return cuda_fail(e, "cudaMalloc(materials)");
+    if (n > 0 && (e = cudaMemcpy(s->d_material, material, size_t(n) * 4, cudaMemcpyHostToDevice)) != cudaSuccess)
+        return cuda_fail(e, "upload materials");
+    return SG_OK;
+}
+
+sg_status sg_trace_multi_host(const sg_scene* cs, const float* rays8, int64_t n, const int32_t* ray_material,
+                              int32_t* count, int32_t* prim, float* t, float* u, float* v) {
+    if (!cs || !rays8 || !ray_material || !count || !prim || !t) return fail(SG_ERR_INVALID_ARGUMENT, "NULL argument");
+    if (n < 0) return fail(SG_ERR_INVALID_ARGUMENT, "negative ray count");
+    if (n == 0) return SG_OK;
+    sg_scene* s = const_cast<sg_scene*>(cs);
+    if (!s->d_material) return fail(SG_ERR_INVALID_ARGUMENT, "no primitive materials (sg_scene_set_materials)");
+    std::lock_guard<std::mutex> lock(s->scratch_lock);
+    DeviceGuard g(s->device);
+    if (!g.ok) return fail(SG_ERR_CUDA, "cudaSetDevice failed");
+    cudaError_t e;
+    if (!s->stream && (e = cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking)) != cudaSuccess)
+        return cuda_fail(e, "cudaStreamCreate");
+    // rays 32 B, ray material 4, count 4, four (prim, t, u, v) 64 per ray
+    auto al = [](size_t x) { return (x + 255) & ~size_t(255); };
+    const size_t N = size_t(n);
+    const size_t need = al(N * 32) + al(N * 4) + al(N * 4) + 4 * al(N * 16);
+    if (s->scratch_bytes < need) {
+        if (s->d_scratch) cudaFree(s->d_scratch);
+        s->d_scratch = nullptr;
+        s->scratch_bytes = 0;
+        if ((e = cudaMalloc(&s->d_scratch, need)) != cudaSuccess) return cuda_fail(e, "cudaMalloc(scratch)");
+        s->scratch_bytes = need;
+    }
+    char* b = static_cast<char*>(s->d_scratch);
+    float* d_rays = reinterpret_cast<float*>(b);
+    b += al(N * 32);
+    int32_t* d_rm = reinterpret_cast<int32_t*>(b);
+    b += al(N * 4);
+    sg_multi_hits h;
+    h.count = reinterpret_cast<int32_t*>(b);
+    b += al(N * 4);
+    h.prim = reinterpret_cast<int32_t*>(b);
+    b += al(N * 16);
+    h.t = reinterpret_cast<float*>(b);
+    b += al(N * 16);
+    h.u = u ? reinterpret_cast<float*>(b) : nullptr;
+    b += al(N * 16);
+    h.v = v ? reinterpret_cast<float*>(b) : nullptr;
+    cudaStream_t st = s->stream;
+    if ((e = cudaMemcpyAsync(d_rays, rays8, N * 32, cudaMemcpyHostToDevice, st)) != cudaSuccess ||
+        (e = cudaMemcpyAsync(d_rm, ray_material, N * 4, cudaMemcpyHostToDevice, st)) != cudaSuccess)
+        return cuda_fail(e, "copy rays to device");
+    const sg_rays r{d_rays, d_rays + n, d_rays + 2 * n, d_rays + 3 * n, d_rays + 4 * n, d_rays + 5 * n, d_rays + 6 * n,
+                    d_rays + 7 * n};
+    sg_status status = sg_trace_multi(s, &r, n, s->d_material, d_rm, &h, st);
+    if (status != SG_OK) return status;
+    if ((e = cudaMemcpyAsync(count, h.count, N * 4, cudaMemcpyDeviceToHost, st)) != cudaSuccess ||
+        (e = cudaMemcpyAsync(prim, h.prim, N * 16, cudaMemcpyDeviceToHost, st)) != cudaSuccess ||
+        (e = cudaMemcpyAsync(t, h.t, N * 16, cudaMemcpyDeviceToHost, st)) != cudaSuccess ||
+        (u && (e = cudaMemcpyAsync(u, h.u, N * 16, cudaMemcpyDeviceToHost, st)) != cudaSuccess) ||
+        (v && (e = cudaMemcpyAsync(v, h.v, N * 16, cudaMemcpyDeviceToHost, st)) != cudaSuccess))
+        return cuda_fail(e, "copy results to host");
+    if ((e = cudaStreamSynchronize(st)) != cudaSuccess) return cuda_fail(e, "synchronize");
+    return check_status_word(s, st);
 }
 
 sg_status sg_trace_stats(const sg_scene* cs, const sg_rays* rays, int64_t n, int32_t any, int64_t* node_tests,

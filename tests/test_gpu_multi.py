@@ -54,3 +54,30 @@ def test_multi_kept_hits_are_hits_of_the_material():
             p = int(prim[i, k])
             assert z["mat_of_tri"][p] == z["ray_mat"][i]
             assert np.float32(port.tri_t(z["triangles"], p, rays, int(i))) == t[i, k]
+
+
+def test_multi_host_form_matches_device_form():
+    """sg_trace_multi_host (what the SORT adapter calls per ray) returns what the
+    device form returns, with the scene's resident material table."""
+    import ctypes
+    from sort_b200 import Obvh, _lib
+    z = golden("multi")
+    acc = Obvh()
+    acc.Build(z["triangles"])
+    rays = np.ascontiguousarray(z["rays"])
+    n = rays.shape[1]
+    count_d, prim_d, t_d, u_d, v_d = acc.GetIntersectBSSRDF(torch.from_numpy(rays).cuda(), z["mat_of_tri"],
+                                                            z["ray_mat"])
+    lib = _lib.load()
+    mats = np.ascontiguousarray(z["mat_of_tri"], np.int32)
+    _lib.check(lib.sg_scene_set_materials(acc._h, mats.ctypes.data, mats.size))
+    rm = np.ascontiguousarray(z["ray_mat"], np.int32)
+    count = np.empty(n, np.int32)
+    prim = np.empty((n, 4), np.int32)
+    t, u, v = (np.empty((n, 4), np.float32) for _ in range(3))
+    _lib.check(lib.sg_trace_multi_host(acc._h, rays.ctypes.data, n, rm.ctypes.data, count.ctypes.data,
+                                       prim.ctypes.data, t.ctypes.data, u.ctypes.data, v.ctypes.data))
+    assert np.array_equal(count, count_d.cpu().numpy()) and np.array_equal(prim, prim_d.cpu().numpy())
+    assert same_bits(t, t_d.cpu().numpy()) and same_bits(u, u_d.cpu().numpy()) and same_bits(v, v_d.cpu().numpy())
+    with pytest.raises(Exception):
+        _lib.check(lib.sg_scene_set_materials(acc._h, mats.ctypes.data, mats.size - 1))
