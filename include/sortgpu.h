@@ -84,7 +84,14 @@ typedef struct {
     int32_t node_format;    /* sg_node_format */
     int32_t device;         /* CUDA device ordinal the tree lives on */
     int32_t build_threads;  /* host threads for the build, 0 = all */
+    int32_t builder;        /* sg_builder: where the (same) tree is built */
 } sg_build_opts;
+
+/* Both builders produce SORT's Fbvh tree (same topology, leaf order, boxes). */
+typedef enum {
+    SG_BUILDER_HOST = 0, /* host threads, one subtree per thread below the top */
+    SG_BUILDER_GPU = 1   /* data-parallel passes on the scene's device */
+} sg_builder;
 
 /* Structure-of-arrays ray batch: n entries in each array. */
 typedef struct {

@@ -31,7 +31,12 @@ class SortGpuError(RuntimeError):
 
 class BuildOpts(ctypes.Structure):
     _fields_ = [("width", ctypes.c_int32), ("max_depth", ctypes.c_int32), ("max_leaf", ctypes.c_int32),
-                ("node_format", ctypes.c_int32), ("device", ctypes.c_int32), ("build_threads", ctypes.c_int32)]
+                ("node_format", ctypes.c_int32), ("device", ctypes.c_int32), ("build_threads", ctypes.c_int32),
+                ("builder", ctypes.c_int32)]
+
+
+SG_BUILDER_HOST = 0
+SG_BUILDER_GPU = 1
 
 
 class Rays(ctypes.Structure):

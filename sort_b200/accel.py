@@ -63,12 +63,13 @@ class Accelerator:
     WIDTH = 8
 
     def __init__(self, max_node_depth: int = 16, max_pri_in_leaf: int = 8, node_format: int = _lib.SG_NODES_FP32,
-                 device: int = 0, build_threads: int = 0):
+                 device: int = 0, build_threads: int = 0, builder: int = _lib.SG_BUILDER_HOST):
         self.max_node_depth = int(max_node_depth)
         self.max_pri_in_leaf = int(max_pri_in_leaf)
         self.node_format = int(node_format)
         self.device = int(device)
         self.build_threads = int(build_threads)
+        self.builder = int(builder)  # SG_BUILDER_HOST or SG_BUILDER_GPU: the same tree either way
         self._h = None
         self._info = None
 
@@ -90,6 +91,7 @@ class Accelerator:
         o.node_format = self.node_format
         o.device = self.device
         o.build_threads = self.build_threads
+        o.builder = self.builder
         return o
 
     # -- build ----------------------------------------------------------------------

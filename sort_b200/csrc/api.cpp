@@ -220,6 +220,7 @@ void sg_default_build_opts(sg_build_opts* o) {
     o->node_format = SG_NODES_FP32;
     o->device = 0;
     o->build_threads = 0;
+    o->builder = SG_BUILDER_HOST;
 }
 
 sg_status sg_scene_create(const float* triangles, int64_t ntri, const sg_build_opts* opts, sg_scene** out) {
@@ -247,12 +248,22 @@ sg_status sg_scene_create(const float* triangles, int64_t ntri, const sg_build_o
     bp.max_depth = opts->max_depth;
     bp.max_leaf = opts->max_leaf;
     bp.threads = opts->build_threads;
+    if (opts->builder != SG_BUILDER_HOST && opts->builder != SG_BUILDER_GPU) {
+        delete s;
+        return fail(SG_ERR_INVALID_ARGUMENT, "unknown builder");
+    }
     const auto t0 = std::chrono::steady_clock::now();
     try {
-        s->tree = sg::build_tree(triangles, ntri, bp);
+        if (opts->builder == SG_BUILDER_GPU)
+            s->tree = sg::build_tree_gpu(triangles, ntri, bp, opts->device);
+        else
+            s->tree = sg::build_tree(triangles, ntri, bp);
     } catch (const std::bad_alloc&) {
         delete s;
         return fail(SG_ERR_OUT_OF_MEMORY, "host memory exhausted during build");
+    } catch (const std::runtime_error& ex) {
+        delete s;
+        return fail(SG_ERR_CUDA, ex.what());
     } catch (const std::exception& ex) {
         delete s;
         return fail(SG_ERR_INVALID_ARGUMENT, ex.what());

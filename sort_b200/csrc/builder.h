@@ -62,6 +62,11 @@ struct BuiltTree {
 // std::invalid_argument / std::bad_alloc on bad input / memory exhaustion.
 BuiltTree build_tree(const float* tri, int64_t ntri, const BuildParams& p);
 
+// The same tree, built with data-parallel passes on CUDA device `device`
+// (builder_gpu.cu). Throws std::invalid_argument on bad input and
+// std::runtime_error on a CUDA error.
+BuiltTree build_tree_gpu(const float* tri, int64_t ntri, const BuildParams& p, int device);
+
 // 8-bit node format (quantize.cpp): one record per interior node in the layout
 // layout.h describes; every decoded child box contains the FP32 box.
 void quantize_nodes(const BuiltTree& t, std::vector<float4>& out);
