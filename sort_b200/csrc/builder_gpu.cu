@@ -153,7 +153,7 @@ __global__ void k_bin(int64_t n, const int* __restrict__ rid, const float* __res
     if (!bin_geometry(rt[r], axis, start, delta, inv)) return;
     const float c = axis == 0 ? cx[i] : (axis == 1 ? cy[i] : cz[i]);
     int b = __float2int_rz(__fmul_rn(__fsub_rn(c, start), inv));
-    b = min(b, kBins - 1);
+    b = max(0, min(b, kBins - 1));  // c >= start, so b >= 0 for finite input; the clamp guards the bins
     atomicAdd(&rt[r].bin_cnt[b], 1u);
     const int32_t p = idx[i];
     for (int a = 0; a < 6; ++a) {
@@ -324,27 +324,73 @@ struct DevBuf {
     }
 };
 
+// Compact per-range input (host -> device) and decision (device -> host).
+struct RangeIn {
+    int64_t s, e;
+    float area;
+    int pad;
+};
+struct RangeOut {
+    int split;
+    unsigned left;
+};
+
+__global__ void k_range_init(int nr, const RangeIn* __restrict__ in, RangeTask* __restrict__ rt) {
+    const int r = blockIdx.x * blockDim.x + threadIdx.x;
+    if (r >= nr) return;
+    RangeTask& t = rt[r];
+    t.s = in[r].s;
+    t.e = in[r].e;
+    t.node_area = in[r].area;
+    for (int a = 0; a < 3; ++a) {
+        t.inner[a] = f2o(FLT_MAX);
+        t.inner[3 + a] = f2o(-FLT_MAX);
+    }
+    for (int b = 0; b < kBins; ++b) {
+        t.bin_cnt[b] = 0;
+        for (int a = 0; a < 3; ++a) {
+            t.bin_box[b][a] = f2o(FLT_MAX);
+            t.bin_box[b][3 + a] = f2o(-FLT_MAX);
+        }
+    }
+    t.axis = 0;
+    t.split_pos = 0.0f;
+    t.split = 0;
+    t.left = 0;
+}
+
+__global__ void k_range_out(int nr, const RangeTask* __restrict__ rt, RangeOut* __restrict__ out) {
+    const int r = blockIdx.x * blockDim.x + threadIdx.x;
+    if (r >= nr) return;
+    out[r].split = rt[r].split;
+    out[r].left = rt[r].left;
+}
+
 struct Range {
     int64_t s, e;
 };
 
-struct NodeTask {  // a node under construction
-    int id;        // index into shape
+// A node under construction: SORT's to_split list (fifo) and done list.
+struct NodeTask {
+    int id;  // index into the shape array
     int depth;
     float area;
-    std::deque<Range> fifo;
-    std::vector<Range> done;
+    int head = 0, tail = 0, ndone = 0;
+    Range fifo[16];  // 1 + 2 * (W - 1) entries at most
+    Range done[8];
+    int total() const { return (tail - head) + ndone; }
 };
 
 struct ShapeNode {
     int64_t off = 0, cnt = 0;
-    std::vector<int> kids;  // indices into the shape array
-    std::vector<Box> kid_box;
+    int nkids = 0;
+    int kid[8];
+    Box kid_box[8];
 };
 
 unsigned grid(int64_t n, int t = 256) { return (unsigned)std::max<int64_t>(1, (n + t - 1) / t); }
 
-Box host_half_area_box(const int* o) {
+Box box_from_images(const int* o) {
     Box b;
     for (int a = 0; a < 3; ++a) {
         b.mn[a] = o2f(o[a]);
@@ -386,6 +432,8 @@ BuiltTree build_tree_gpu(const float* tri, int64_t ntri, const BuildParams& p, i
     DevBuf<int> d_rid, d_ml, d_mr, d_sl, d_sr, d_boxes;
     DevBuf<int64_t> d_pl, d_pr, d_starts, d_ends;
     DevBuf<RangeTask> d_rt;
+    DevBuf<RangeIn> d_in;
+    DevBuf<RangeOut> d_out;
     DevBuf<unsigned char> d_temp;
     const int64_t nn = std::max<int64_t>(n, 1);
     d_tri.alloc(size_t(nn) * 9);
@@ -431,7 +479,6 @@ BuiltTree build_tree_gpu(const float* tri, int64_t ntri, const BuildParams& p, i
     t.scene = scene;
     if (n == 0) return t;
 
-    // Scan scratch for n ints.
     size_t temp_bytes = 0;
     cub::DeviceScan::ExclusiveSum(nullptr, temp_bytes, d_ml.p, d_sl.p, (int)n);
     d_temp.alloc(temp_bytes);
@@ -440,8 +487,10 @@ BuiltTree build_tree_gpu(const float* tri, int64_t ntri, const BuildParams& p, i
     shape[0].off = 0;
     shape[0].cnt = n;
     int depth_max = 0;
-    std::vector<NodeTask> active;
-    auto start_node = [&](int id, int depth, const Box& box) {
+    // Nodes under construction, in order of their primitive ranges (disjoint), so
+    // the ranges split in a round come out sorted for the per-primitive lookup.
+    std::vector<NodeTask> active, next;
+    auto start_node = [&](std::vector<NodeTask>& into, int id, int depth, const Box& box) {
         const ShapeNode& sn = shape[size_t(id)];
         if (sn.cnt <= p.max_leaf || depth == p.max_depth) {  // splitNode's early return
             depth_max = std::max(depth_max, depth);
@@ -451,64 +500,43 @@ BuiltTree build_tree_gpu(const float* tri, int64_t ntri, const BuildParams& p, i
         nt.id = id;
         nt.depth = depth;
         nt.area = host_half_area(box);
-        nt.fifo.push_back({sn.off, sn.off + sn.cnt});
-        active.push_back(std::move(nt));
+        nt.fifo[nt.tail++] = {sn.off, sn.off + sn.cnt};
+        into.push_back(nt);
     };
-    start_node(0, 1, scene);
+    start_node(active, 0, 1, scene);
 
-    std::vector<RangeTask> rt;
-    std::vector<int64_t> starts, ends;
+    std::vector<RangeIn> rin;
+    std::vector<RangeOut> rout;
     std::vector<int> owner;
+    std::vector<int64_t> starts, ends;
     while (!active.empty()) {
         // One split per node: the front of its list, while SORT's loop would go on.
-        rt.clear();
-        starts.clear();
-        ends.clear();
+        rin.clear();
         owner.clear();
         for (size_t k = 0; k < active.size(); ++k) {
             NodeTask& nt = active[k];
-            if (nt.fifo.empty() || int(nt.fifo.size() + nt.done.size()) >= W) continue;
-            const Range r = nt.fifo.front();
-            nt.fifo.pop_front();
-            RangeTask x;
-            std::memset(&x, 0, sizeof(x));
-            x.s = r.s;
-            x.e = r.e;
-            x.node_area = nt.area;
-            for (int a = 0; a < 3; ++a) {
-                x.inner[a] = f2o(FLT_MAX);
-                x.inner[3 + a] = f2o(-FLT_MAX);
-            }
-            for (int b = 0; b < kBins; ++b)
-                for (int a = 0; a < 3; ++a) {
-                    x.bin_box[b][a] = f2o(FLT_MAX);
-                    x.bin_box[b][3 + a] = f2o(-FLT_MAX);
-                }
-            rt.push_back(x);
+            if (nt.head == nt.tail || nt.total() >= W) continue;
+            const Range r = nt.fifo[nt.head++];
+            rin.push_back({r.s, r.e, nt.area, 0});
             owner.push_back(int(k));
         }
-        if (!rt.empty()) {
-            // ranges sorted by start for the per-primitive lookup (they are disjoint)
-            std::vector<int> ord(rt.size());
-            for (size_t k = 0; k < ord.size(); ++k) ord[k] = int(k);
-            std::sort(ord.begin(), ord.end(), [&](int a, int b) { return rt[size_t(a)].s < rt[size_t(b)].s; });
-            std::vector<RangeTask> rs(rt.size());
-            std::vector<int> os(rt.size());
-            for (size_t k = 0; k < ord.size(); ++k) {
-                rs[k] = rt[size_t(ord[k])];
-                os[k] = owner[size_t(ord[k])];
-                starts.push_back(rs[k].s);
-                ends.push_back(rs[k].e);
+        const int nr = int(rin.size());
+        if (nr > 0) {
+            starts.resize(size_t(nr));
+            ends.resize(size_t(nr));
+            for (int k = 0; k < nr; ++k) {
+                starts[size_t(k)] = rin[size_t(k)].s;
+                ends[size_t(k)] = rin[size_t(k)].e;
             }
-            rt.swap(rs);
-            owner.swap(os);
-            const int nr = int(rt.size());
             d_rt.alloc(size_t(nr));
+            d_in.alloc(size_t(nr));
+            d_out.alloc(size_t(nr));
             d_starts.alloc(size_t(nr));
             d_ends.alloc(size_t(nr));
-            check(cudaMemcpy(d_rt.p, rt.data(), size_t(nr) * sizeof(RangeTask), cudaMemcpyHostToDevice), "ranges");
+            check(cudaMemcpy(d_in.p, rin.data(), size_t(nr) * sizeof(RangeIn), cudaMemcpyHostToDevice), "ranges");
             check(cudaMemcpy(d_starts.p, starts.data(), size_t(nr) * 8, cudaMemcpyHostToDevice), "ranges");
             check(cudaMemcpy(d_ends.p, ends.data(), size_t(nr) * 8, cudaMemcpyHostToDevice), "ranges");
+            k_range_init<<<grid(nr, 128), 128>>>(nr, d_in.p, d_rt.p);
             k_bounds<<<grid(n), 256>>>(n, d_starts.p, d_ends.p, nr, d_cx.p, d_cy.p, d_cz.p, d_rid.p, d_rt.p);
             k_bin<<<grid(n), 256>>>(n, d_rid.p, d_cx.p, d_cy.p, d_cz.p, d_idx.p, d_pb.p, n, d_rt.p);
             k_sweep<<<grid(nr, 128), 128>>>(nr, d_rt.p, p.max_leaf);
@@ -518,64 +546,73 @@ BuiltTree build_tree_gpu(const float* tri, int64_t ntri, const BuildParams& p, i
             check(cub::DeviceScan::ExclusiveSum(d_temp.p, temp_bytes, d_ml.p, d_sl.p, (int)n), "scan");
             check(cub::DeviceScan::ExclusiveSum(d_temp.p, temp_bytes, d_mr.p, d_sr.p, (int)n), "scan");
             k_pairs<<<grid(n), 256>>>(n, d_rid.p, d_rt.p, d_ml.p, d_mr.p, d_sl.p, d_sr.p, d_pl.p, d_pr.p);
+            k_range_out<<<grid(nr, 128), 128>>>(nr, d_rt.p, d_out.p);
             int last_sl = 0, last_ml = 0;
             check(cudaMemcpy(&last_sl, d_sl.p + (n - 1), 4, cudaMemcpyDeviceToHost), "pairs");
             check(cudaMemcpy(&last_ml, d_ml.p + (n - 1), 4, cudaMemcpyDeviceToHost), "pairs");
             const int64_t pairs = int64_t(last_sl) + last_ml;
             if (pairs > 0) k_swap<<<grid(pairs), 256>>>(pairs, d_pl.p, d_pr.p, d_cx.p, d_cy.p, d_cz.p, d_idx.p);
             check(cudaGetLastError(), "partition kernels");
-            check(cudaMemcpy(rt.data(), d_rt.p, size_t(nr) * sizeof(RangeTask), cudaMemcpyDeviceToHost), "results");
+            rout.resize(size_t(nr));
+            check(cudaMemcpy(rout.data(), d_out.p, size_t(nr) * sizeof(RangeOut), cudaMemcpyDeviceToHost), "results");
             for (int k = 0; k < nr; ++k) {
                 NodeTask& nt = active[size_t(owner[size_t(k)])];
-                const RangeTask& x = rt[size_t(k)];
-                const int64_t mid = x.s + x.left;
-                if (!x.split || mid == x.s || mid == x.e) {
-                    nt.done.push_back({x.s, x.e});
+                const RangeIn& x = rin[size_t(k)];
+                const int64_t mid = x.s + rout[size_t(k)].left;
+                if (!rout[size_t(k)].split || mid == x.s || mid == x.e) {
+                    nt.done[nt.ndone++] = {x.s, x.e};
                 } else {
-                    nt.fifo.push_back({x.s, mid});
-                    nt.fifo.push_back({mid, x.e});
+                    nt.fifo[nt.tail++] = {x.s, mid};
+                    nt.fifo[nt.tail++] = {mid, x.e};
                 }
             }
         }
-        // Nodes whose loop has ended: leaves, or children from their ranges.
-        std::vector<NodeTask> still;
-        std::vector<std::pair<int, int>> new_kids;  // (shape id, depth)
-        std::vector<int> new_parent;                // shape id of each new kid's parent
+        // Nodes whose loop has ended become leaves, or hand their ranges on as
+        // children (SORT's child order: the remaining list, then the done list).
+        struct Kid {
+            int id, depth, parent, j;  // j: position among the parent's children
+        };
+        std::vector<Kid> kids;
+        next.clear();
         for (NodeTask& nt : active) {
-            const int total = int(nt.fifo.size() + nt.done.size());
-            if (!nt.fifo.empty() && total < W) {
-                still.push_back(std::move(nt));
+            if (nt.head != nt.tail && nt.total() < W) {
+                next.push_back(nt);
                 continue;
             }
-            if (total == 1) {
+            if (nt.total() == 1) {
                 depth_max = std::max(depth_max, nt.depth);
                 continue;
             }
-            std::vector<Range> kids(nt.fifo.begin(), nt.fifo.end());
-            kids.insert(kids.end(), nt.done.begin(), nt.done.end());
-            for (const Range& r : kids) {
+            Range rs[8];
+            int m = 0;
+            for (int q = nt.head; q < nt.tail; ++q) rs[m++] = nt.fifo[q];
+            for (int q = 0; q < nt.ndone; ++q) rs[m++] = nt.done[q];
+            const int first_kid = int(shape.size());
+            for (int q = 0; q < m; ++q) {
                 ShapeNode sn;
-                sn.off = r.s;
-                sn.cnt = r.e - r.s;
-                shape.push_back(std::move(sn));
-                shape[size_t(nt.id)].kids.push_back(int(shape.size()) - 1);
-                new_kids.push_back({int(shape.size()) - 1, nt.depth + 1});
-                new_parent.push_back(nt.id);
+                sn.off = rs[q].s;
+                sn.cnt = rs[q].e - rs[q].s;
+                shape[size_t(nt.id)].kid[shape[size_t(nt.id)].nkids++] = int(shape.size());
+                shape.push_back(sn);
+            }
+            // in range order for the sorted active list
+            int ord[8];
+            for (int q = 0; q < m; ++q) ord[q] = q;
+            std::sort(ord, ord + m, [&](int a, int b) { return rs[a].s < rs[b].s; });
+            for (int q = 0; q < m; ++q) {
+                kids.push_back({first_kid + ord[q], nt.depth + 1, nt.id, ord[q]});
+                next.emplace_back();  // placeholder
+                next.back().id = -1;
             }
         }
-        active.swap(still);
-        if (!new_kids.empty()) {
-            // Boxes of the new children (their own SAH normaliser, and their parent's child boxes).
-            std::vector<int> ord(new_kids.size());
-            for (size_t k = 0; k < ord.size(); ++k) ord[k] = int(k);
-            std::sort(ord.begin(), ord.end(), [&](int a, int b) {
-                return shape[size_t(new_kids[size_t(a)].first)].off < shape[size_t(new_kids[size_t(b)].first)].off;
-            });
-            const int nk = int(ord.size());
-            starts.assign(size_t(nk), 0);
-            ends.assign(size_t(nk), 0);
+        if (!kids.empty()) {
+            // Boxes of the new children (kids are in range order): their own SAH
+            // normaliser, and their parent's child boxes.
+            const int nk = int(kids.size());
+            starts.resize(size_t(nk));
+            ends.resize(size_t(nk));
             for (int k = 0; k < nk; ++k) {
-                const ShapeNode& sn = shape[size_t(new_kids[size_t(ord[size_t(k)])].first)];
+                const ShapeNode& sn = shape[size_t(kids[size_t(k)].id)];
                 starts[size_t(k)] = sn.off;
                 ends[size_t(k)] = sn.off + sn.cnt;
             }
@@ -594,13 +631,23 @@ BuiltTree build_tree_gpu(const float* tri, int64_t ntri, const BuildParams& p, i
             k_range_boxes<<<grid(n), 256>>>(n, d_starts.p, d_ends.p, nk, d_idx.p, d_pb.p, n, d_boxes.p);
             check(cudaGetLastError(), "child boxes");
             check(cudaMemcpy(boxes.data(), d_boxes.p, boxes.size() * 4, cudaMemcpyDeviceToHost), "kids");
-            std::vector<Box> kb(static_cast<size_t>(nk));
-            for (int k = 0; k < nk; ++k) kb[size_t(ord[size_t(k)])] = host_half_area_box(&boxes[size_t(k) * 6]);
-            // parents' child boxes, in child order (a parent's kids are consecutive in new_kids)
-            for (size_t j = 0; j < new_kids.size(); ++j)
-                shape[size_t(new_parent[j])].kid_box.push_back(kb[j]);
-            for (size_t j = 0; j < new_kids.size(); ++j) start_node(new_kids[j].first, new_kids[j].second, kb[j]);
+            std::vector<NodeTask> filled;
+            filled.reserve(next.size());
+            size_t kk = 0;
+            for (size_t q = 0; q < next.size(); ++q) {
+                if (next[q].id >= 0) {
+                    filled.push_back(next[q]);
+                    continue;
+                }
+                const Kid& kd = kids[kk];
+                const Box b = box_from_images(&boxes[kk * 6]);
+                ++kk;
+                shape[size_t(kd.parent)].kid_box[kd.j] = b;
+                start_node(filled, kd.id, kd.depth, b);
+            }
+            next.swap(filled);
         }
+        active.swap(next);
     }
     t.depth = depth_max;
 
@@ -633,7 +680,7 @@ BuiltTree build_tree_gpu(const float* tri, int64_t ntri, const BuildParams& p, i
         t.leaf_last[size_t(sn.off + sn.cnt - 1)] = 1;
     };
     std::vector<std::pair<int, int32_t>> stack;  // (shape id, node index), filled depth-first in order
-    if (shape[0].kids.empty()) {
+    if (shape[0].nkids == 0) {
         t.root = leaf_ref(0);
         leaf(shape[0]);
     } else {
@@ -643,22 +690,23 @@ BuiltTree build_tree_gpu(const float* tri, int64_t ntri, const BuildParams& p, i
     while (!stack.empty()) {
         const auto [sid, idx] = stack.back();
         stack.pop_back();
-        const ShapeNode& sn = shape[size_t(sid)];
+        const ShapeNode sn = shape[size_t(sid)];
         int interior = 0;
-        for (int k : sn.kids) interior += shape[size_t(k)].kids.empty() ? 0 : 1;
+        for (int j = 0; j < sn.nkids; ++j) interior += shape[size_t(sn.kid[j])].nkids ? 1 : 0;
         const int32_t base = interior ? alloc(interior) : -1;
         t.first_interior[size_t(idx)] = base;
         int k = 0;
-        std::vector<std::pair<int, int32_t>> sub;
-        for (size_t j = 0; j < sn.kids.size(); ++j) {
-            const ShapeNode& kid = shape[size_t(sn.kids[j])];
+        std::pair<int, int32_t> sub[8];
+        int nsub = 0;
+        for (int j = 0; j < sn.nkids; ++j) {
+            const ShapeNode& kid = shape[size_t(sn.kid[j])];
             int32_t ref;
-            if (kid.kids.empty()) {
+            if (kid.nkids == 0) {
                 ref = leaf_ref(kid.off);
                 leaf(kid);
             } else {
                 ref = base + k++;
-                sub.push_back({sn.kids[j], ref});
+                sub[nsub++] = {sn.kid[j], ref};
             }
             t.child[size_t(idx) * W + j] = ref;
             for (int a = 0; a < 3; ++a) {
@@ -666,7 +714,7 @@ BuiltTree build_tree_gpu(const float* tri, int64_t ntri, const BuildParams& p, i
                 t.hi[(size_t(idx) * 3 + a) * W + j] = sn.kid_box[j].mx[a];
             }
         }
-        for (auto it = sub.rbegin(); it != sub.rend(); ++it) stack.push_back(*it);  // first child filled next
+        for (int q = nsub - 1; q >= 0; --q) stack.push_back(sub[q]);  // first child filled next
     }
     return t;
 }
