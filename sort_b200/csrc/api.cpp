@@ -289,7 +289,6 @@ sg_status sg_scene_create(const float* triangles, int64_t ntri, const sg_build_o
         release(s);
         return st;
     }
-    std::vector<sg::Box>().swap(s->tree.slot_box);
     std::vector<float>().swap(s->tree.lo);
     std::vector<float>().swap(s->tree.hi);
     *out = s;

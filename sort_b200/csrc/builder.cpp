@@ -314,11 +314,9 @@ BuiltTree build_tree(const float* tri, int64_t ntri, const BuildParams& p) {
     t.depth = c.depth.load();
 
     t.order.resize(size_t(ntri));
-    t.slot_box.resize(size_t(ntri));
     t.leaf_last.assign(size_t(ntri), 0);
     for (int64_t i = 0; i < ntri; ++i) {
         t.order[size_t(i)] = prims[size_t(i)].idx;
-        t.slot_box[size_t(i)] = pbox[size_t(prims[size_t(i)].idx)];
     }
     Flattener f{t, c, p.width};
     if (root.nkids == 0) {

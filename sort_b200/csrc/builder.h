@@ -53,7 +53,6 @@ struct BuiltTree {
     std::vector<int32_t> first_interior;  // per node, -1 if none
     std::vector<int32_t> order;           // primitive index of each leaf slot (leaf order)
     std::vector<uint8_t> leaf_last;       // 1 on the last slot of every leaf
-    std::vector<Box> slot_box;            // per-slot primitive box (leaf order)
     int64_t leaves = 0;
     int64_t interior() const { return width ? int64_t(child.size()) / width : 0; }
 };

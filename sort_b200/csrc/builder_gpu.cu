@@ -11,18 +11,27 @@
 // only on their order. Here every node under construction takes the split of
 // its front range in the same round, and a round is a few data-parallel passes
 // over the primitives of the ranges being split:
-//   * centroid bounds and bins (counts, primitive boxes) per range with
-//     atomics on order-preserving integer images of the floats;
+//   * centroid bounds and bins (counts, primitive boxes) per range: lanes of a
+//     warp with the same key combine their values (match + warp reductions),
+//     blocks inside one range combine in shared memory, and one lane per group
+//     applies atomics on order-preserving integer images of the floats;
 //   * the SAH sweep, one thread per range, in SORT's arithmetic order;
+//   * the boxes of both halves of every split range, reduced in the pass that
+//     counts the left half: they are the child boxes and the children's SAH
+//     normalisers, so no pass computes child boxes afterwards;
 //   * std::partition as libstdc++ performs it on random-access iterators: the
 //     k-th element of the left part that fails the predicate is swapped with
 //     the k-th element from the right end of the right part that passes it,
 //     so the result is found with two prefix sums and one swap per pair.
-// The host keeps each node's range list and finishes a node when SORT's loop
-// would; a finished node's ranges become its children, whose boxes (for their
-// own SAH normalisation and for the stored child boxes) are reduced on the
-// GPU. The tree, the leaf order and every box value are build_tree's; a box
-// bound that is zero may carry the other sign, which no comparison sees.
+// Centroids and primitive boxes travel with the primitives (slot order), so
+// every pass reads them coalesced. The nodes under construction live on the
+// GPU too, in primitive-range order: after the passes, one thread per node
+// applies its split to the node's range lists, a finished node writes its
+// children as shape nodes, and prefix sums place the continuing nodes and the
+// new ones in the next round's list. A round costs one 16-byte download (the
+// sizes of the next round). The host only flattens the finished shape tree.
+// The tree, the leaf order and every box value are build_tree's; a box bound
+// that is zero may carry the other sign, which no comparison sees.
 #include <cuda_runtime.h>
 
 #include <cub/device/device_scan.cuh>
@@ -30,7 +39,6 @@
 #include <algorithm>
 #include <cfloat>
 #include <cstring>
-#include <deque>
 #include <stdexcept>
 #include <string>
 #include <vector>
@@ -65,8 +73,9 @@ struct RangeTask {
     // decision
     int axis;
     float split_pos;
-    int split;       // 1 = partition this range
-    unsigned left;   // primitives passing the predicate
+    int split;           // 1 = partition this range
+    unsigned left;       // primitives passing the predicate
+    int half_box[2][6];  // primitive boxes of the left (passing) and right halves
 };
 
 __device__ __forceinline__ int find_range(const int64_t* __restrict__ starts, const int64_t* __restrict__ ends,
@@ -80,6 +89,43 @@ __device__ __forceinline__ int find_range(const int64_t* __restrict__ starts, co
             hi = mid - 1;
     }
     return (nr > 0 && starts[lo] <= i && i < ends[lo]) ? lo : -1;
+}
+
+__device__ __forceinline__ bool leads(unsigned peers) { return int(__ffs(peers)) - 1 == int(threadIdx.x & 31); }
+
+// Lanes with the same key combine: min over v[0..K), max over v[K..2K).
+// Every lane of the warp calls it; returns the lanes sharing the caller's key.
+template <int K>
+__device__ __forceinline__ unsigned group_minmax(long long key, int (&v)[2 * K]) {
+    const unsigned peers = __match_any_sync(0xffffffffu, key);
+    for (int a = 0; a < K; ++a) {
+        v[a] = __reduce_min_sync(peers, v[a]);
+        v[K + a] = __reduce_max_sync(peers, v[K + a]);
+    }
+    return peers;
+}
+
+__device__ __forceinline__ void atomic_box(int* dst, const int (&v)[6]) {
+    for (int a = 0; a < 3; ++a) {
+        atomicMin(&dst[a], v[a]);
+        atomicMax(&dst[3 + a], v[3 + a]);
+    }
+}
+
+__host__ __device__ __forceinline__ void empty_box(int* b) {
+    for (int a = 0; a < 3; ++a) {
+        b[a] = f2o(FLT_MAX);
+        b[3 + a] = f2o(-FLT_MAX);
+    }
+}
+
+// Blocks whose primitives all belong to one range (the common case while
+// ranges are large) reduce in shared memory first and touch the range's
+// global accumulators once; other blocks update them per warp group.
+__device__ __forceinline__ bool block_in_one_range(int r, int& shared_r) {
+    if (threadIdx.x == 0) shared_r = r;
+    __syncthreads();
+    return __syncthreads_and(r == shared_r && r >= 0) != 0;
 }
 
 __global__ void k_prim_setup(const float* __restrict__ tri, int64_t n, float* __restrict__ cx, float* __restrict__ cy,
@@ -103,20 +149,62 @@ __global__ void k_prim_setup(const float* __restrict__ tri, int64_t n, float* __
     idx[i] = (int32_t)i;
 }
 
-// Range id of every primitive (-1 outside the round's ranges) and centroid bounds.
-__global__ void k_bounds(int64_t n, const int64_t* __restrict__ starts, const int64_t* __restrict__ ends, int nr,
-                         const float* __restrict__ cx, const float* __restrict__ cy, const float* __restrict__ cz,
-                         int* __restrict__ rid, RangeTask* __restrict__ rt) {
-    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= n) return;
-    const int r = find_range(starts, ends, nr, i);
-    rid[i] = r;
-    if (r < 0) return;
-    const float c[3] = {cx[i], cy[i], cz[i]};
+// Union of all primitive boxes (the scene box before its enlargement).
+__global__ void __launch_bounds__(256) k_scene_box(int64_t n, const float* __restrict__ pb, int* __restrict__ out) {
+    __shared__ int sbox[6];
+    if (threadIdx.x == 0) empty_box(sbox);
+    __syncthreads();
+    int v[6];
+    empty_box(v);
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+        for (int a = 0; a < 3; ++a) {
+            v[a] = min(v[a], f2o(pb[a * n + i]));
+            v[3 + a] = max(v[3 + a], f2o(pb[(3 + a) * n + i]));
+        }
     for (int a = 0; a < 3; ++a) {
-        atomicMin(&rt[r].inner[a], f2o(c[a]));
-        atomicMax(&rt[r].inner[3 + a], f2o(c[a]));
+        v[a] = __reduce_min_sync(0xffffffffu, v[a]);
+        v[3 + a] = __reduce_max_sync(0xffffffffu, v[3 + a]);
     }
+    if ((threadIdx.x & 31) == 0) atomic_box(sbox, v);
+    __syncthreads();
+    if (threadIdx.x < 3) {
+        atomicMin(&out[threadIdx.x], sbox[threadIdx.x]);
+        atomicMax(&out[3 + threadIdx.x], sbox[3 + threadIdx.x]);
+    }
+}
+
+// Range id of every primitive (-1 outside the round's ranges) and centroid bounds.
+__global__ void __launch_bounds__(256) k_bounds(int64_t n, const int64_t* __restrict__ starts,
+                                                const int64_t* __restrict__ ends, int nr, const float* __restrict__ cx,
+                                                const float* __restrict__ cy, const float* __restrict__ cz,
+                                                int* __restrict__ rid, RangeTask* __restrict__ rt) {
+    __shared__ int sr, sbox[6];
+    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    const bool in = i < n;
+    const int r = in ? find_range(starts, ends, nr, i) : -1;
+    if (in) rid[i] = r;
+    if (threadIdx.x == 0) empty_box(sbox);
+    const bool one = block_in_one_range(r, sr);
+    int v[6];
+    if (r >= 0) {
+        v[0] = v[3] = f2o(cx[i]);
+        v[1] = v[4] = f2o(cy[i]);
+        v[2] = v[5] = f2o(cz[i]);
+    } else {
+        empty_box(v);
+    }
+    const unsigned peers = group_minmax<3>(r, v);
+    const bool lead = r >= 0 && leads(peers);
+    if (one) {
+        if (lead) atomic_box(sbox, v);
+        __syncthreads();
+        if (threadIdx.x < 3) {
+            atomicMin(&rt[r].inner[threadIdx.x], sbox[threadIdx.x]);
+            atomicMax(&rt[r].inner[3 + threadIdx.x], sbox[3 + threadIdx.x]);
+        }
+        return;
+    }
+    if (lead) atomic_box(rt[r].inner, v);
 }
 
 __device__ __forceinline__ float half_area(const float* mn, const float* mx) {
@@ -141,28 +229,54 @@ __device__ __forceinline__ bool bin_geometry(const RangeTask& t, int& axis, floa
     return true;
 }
 
-__global__ void k_bin(int64_t n, const int* __restrict__ rid, const float* __restrict__ cx, const float* __restrict__ cy,
-                      const float* __restrict__ cz, const int32_t* __restrict__ idx, const float* __restrict__ pb,
-                      int64_t np, RangeTask* __restrict__ rt) {
+// Bin counts and bin boxes (primitive boxes, slot order).
+__global__ void __launch_bounds__(256) k_bin(int64_t n, const int* __restrict__ rid, const float* __restrict__ cx,
+                                             const float* __restrict__ cy, const float* __restrict__ cz,
+                                             const float* __restrict__ pb, RangeTask* __restrict__ rt) {
+    __shared__ int sr;
+    __shared__ unsigned scnt[kBins];
+    __shared__ int sbox[kBins][6];
     const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= n) return;
-    const int r = rid[i];
-    if (r < 0) return;
-    int axis;
-    float start, delta, inv;
-    if (!bin_geometry(rt[r], axis, start, delta, inv)) return;
-    const float c = axis == 0 ? cx[i] : (axis == 1 ? cy[i] : cz[i]);
-    int b = __float2int_rz(__fmul_rn(__fsub_rn(c, start), inv));
-    b = max(0, min(b, kBins - 1));  // c >= start, so b >= 0 for finite input; the clamp guards the bins
-    atomicAdd(&rt[r].bin_cnt[b], 1u);
-    const int32_t p = idx[i];
-    for (int a = 0; a < 6; ++a) {
-        const int v = f2o(pb[a * np + p]);
-        if (a < 3)
-            atomicMin(&rt[r].bin_box[b][a], v);
-        else
-            atomicMax(&rt[r].bin_box[b][a], v);
+    const int r = i < n ? rid[i] : -1;
+    if (threadIdx.x < kBins) {
+        scnt[threadIdx.x] = 0;
+        empty_box(sbox[threadIdx.x]);
     }
+    const bool one = block_in_one_range(r, sr);
+    int axis = 0;
+    float start = 0.0f, delta = 0.0f, inv = 0.0f;
+    const bool binned = r >= 0 && bin_geometry(rt[r], axis, start, delta, inv);
+    int b = 0;
+    int v[6];
+    if (binned) {
+        const float c = axis == 0 ? cx[i] : (axis == 1 ? cy[i] : cz[i]);
+        b = __float2int_rz(__fmul_rn(__fsub_rn(c, start), inv));
+        b = max(0, min(b, kBins - 1));  // c >= start, so b >= 0 for finite input; the clamp guards the bins
+        for (int a = 0; a < 6; ++a) v[a] = f2o(pb[a * n + i]);
+    } else {
+        empty_box(v);
+    }
+    const unsigned peers = group_minmax<3>(binned ? ((long long)r << 4) | b : -1, v);
+    const bool lead = binned && leads(peers);
+    if (one) {  // every thread of the block is in range r (binned or not, uniformly)
+        if (lead) {
+            atomicAdd(&scnt[b], (unsigned)__popc(peers));
+            atomic_box(sbox[b], v);
+        }
+        __syncthreads();
+        if (binned && threadIdx.x < kBins && scnt[threadIdx.x]) {
+            const int k = threadIdx.x;
+            atomicAdd(&rt[r].bin_cnt[k], scnt[k]);
+            for (int a = 0; a < 3; ++a) {
+                atomicMin(&rt[r].bin_box[k][a], sbox[k][a]);
+                atomicMax(&rt[r].bin_box[k][3 + a], sbox[k][3 + a]);
+            }
+        }
+        return;
+    }
+    if (!lead) return;
+    atomicAdd(&rt[r].bin_cnt[b], (unsigned)__popc(peers));
+    atomic_box(rt[r].bin_box[b], v);
 }
 
 // The SAH sweep of pick_best_split and splitNode's decision, one thread per range.
@@ -223,13 +337,53 @@ __device__ __forceinline__ bool passes(const RangeTask& t, float x, float y, flo
     return c < t.split_pos;
 }
 
-__global__ void k_count_left(int64_t n, const int* __restrict__ rid, const float* __restrict__ cx,
-                             const float* __restrict__ cy, const float* __restrict__ cz, RangeTask* __restrict__ rt) {
+// Size and box of both halves of every range being split.
+__global__ void __launch_bounds__(256) k_count_left(int64_t n, const int* __restrict__ rid,
+                                                    const float* __restrict__ cx, const float* __restrict__ cy,
+                                                    const float* __restrict__ cz, const float* __restrict__ pb,
+                                                    RangeTask* __restrict__ rt) {
+    __shared__ int sr;
+    __shared__ unsigned sleft;
+    __shared__ int sbox[2][6];
     const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= n) return;
-    const int r = rid[i];
-    if (r < 0 || !rt[r].split) return;
-    if (passes(rt[r], cx[i], cy[i], cz[i])) atomicAdd(&rt[r].left, 1u);
+    const int r = i < n ? rid[i] : -1;
+    if (threadIdx.x == 0) {
+        sleft = 0;
+        empty_box(sbox[0]);
+        empty_box(sbox[1]);
+    }
+    const bool one = block_in_one_range(r, sr);
+    const bool act = r >= 0 && rt[r].split;
+    bool pass = false;
+    int v[6];
+    if (act) {
+        pass = passes(rt[r], cx[i], cy[i], cz[i]);
+        for (int a = 0; a < 6; ++a) v[a] = f2o(pb[a * n + i]);
+    } else {
+        empty_box(v);
+    }
+    const unsigned peers = group_minmax<3>(act ? ((long long)r << 1) | (pass ? 0 : 1) : -1, v);
+    const bool lead = act && leads(peers);
+    const int side = pass ? 0 : 1;
+    if (one) {  // `act` is uniform here
+        if (lead) {
+            if (pass) atomicAdd(&sleft, (unsigned)__popc(peers));
+            atomic_box(sbox[side], v);
+        }
+        __syncthreads();
+        if (act && threadIdx.x < 12) {
+            const int h = threadIdx.x / 6, a = threadIdx.x % 6;
+            if (a < 3)
+                atomicMin(&rt[r].half_box[h][a], sbox[h][a]);
+            else
+                atomicMax(&rt[r].half_box[h][a], sbox[h][a]);
+        }
+        if (act && threadIdx.x == 0 && sleft) atomicAdd(&rt[r].left, sleft);
+        return;
+    }
+    if (!lead) return;
+    if (pass) atomicAdd(&rt[r].left, (unsigned)__popc(peers));
+    atomic_box(rt[r].half_box[side], v);
 }
 
 // Misplaced elements: failing the predicate left of the cut (ml), passing it right of it (mr).
@@ -268,39 +422,27 @@ __global__ void k_pairs(int64_t n, const int* __restrict__ rid, const RangeTask*
     }
 }
 
-__global__ void k_swap(int64_t pairs, const int64_t* __restrict__ pl, const int64_t* __restrict__ pr,
-                       float* __restrict__ cx, float* __restrict__ cy, float* __restrict__ cz,
-                       int32_t* __restrict__ idx) {
-    const int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (k >= pairs) return;
-    const int64_t a = pl[k], b = pr[k];
-    float t = cx[a];
-    cx[a] = cx[b];
-    cx[b] = t;
-    t = cy[a];
-    cy[a] = cy[b];
-    cy[b] = t;
-    t = cz[a];
-    cz[a] = cz[b];
-    cz[b] = t;
-    const int32_t q = idx[a];
-    idx[a] = idx[b];
-    idx[b] = q;
+template <class T>
+__device__ __forceinline__ void swap_at(T* __restrict__ p, int64_t a, int64_t b) {
+    const T t = p[a];
+    p[a] = p[b];
+    p[b] = t;
 }
 
-// Boxes of ranges (children of finished nodes): union of primitive boxes.
-__global__ void k_range_boxes(int64_t n, const int64_t* __restrict__ starts, const int64_t* __restrict__ ends, int nr,
-                              const int32_t* __restrict__ idx, const float* __restrict__ pb, int64_t np,
-                              int* __restrict__ boxes) {
-    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= n) return;
-    const int r = find_range(starts, ends, nr, i);
-    if (r < 0) return;
-    const int32_t p = idx[i];
-    for (int a = 0; a < 3; ++a) {
-        atomicMin(&boxes[6 * r + a], f2o(pb[a * np + p]));
-        atomicMax(&boxes[6 * r + 3 + a], f2o(pb[(3 + a) * np + p]));
-    }
+// One thread per pair; the pair count is the total of the left misplaced flags.
+__global__ void k_swap(int64_t n, const int* __restrict__ sl, const int* __restrict__ ml,
+                       const int64_t* __restrict__ pl, const int64_t* __restrict__ pr, float* __restrict__ cx,
+                       float* __restrict__ cy, float* __restrict__ cz, float* __restrict__ pb,
+                       int32_t* __restrict__ idx) {
+    const int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    const int64_t pairs = int64_t(sl[n - 1]) + ml[n - 1];
+    if (k >= pairs) return;
+    const int64_t a = pl[k], b = pr[k];
+    swap_at(cx, a, b);
+    swap_at(cy, a, b);
+    swap_at(cz, a, b);
+    swap_at(idx, a, b);
+    for (int q = 0; q < 6; ++q) swap_at(pb + q * n, a, b);
 }
 
 void check(cudaError_t e, const char* what) {
@@ -324,69 +466,204 @@ struct DevBuf {
     }
 };
 
-// Compact per-range input (host -> device) and decision (device -> host).
-struct RangeIn {
-    int64_t s, e;
-    float area;
-    int pad;
-};
-struct RangeOut {
-    int split;
-    unsigned left;
+template <class T>
+struct PinnedBuf {
+    T* p = nullptr;
+    size_t n = 0;
+    void alloc(size_t count) {
+        if (count <= n) return;
+        count = std::max<size_t>(count, 2 * n);
+        if (p) cudaFreeHost(p);
+        p = nullptr;
+        n = 0;
+        check(cudaMallocHost(&p, std::max<size_t>(count, 1) * sizeof(T)), "cudaMallocHost");
+        n = count;
+    }
+    ~PinnedBuf() {
+        if (p) cudaFreeHost(p);
+    }
 };
 
-__global__ void k_range_init(int nr, const RangeIn* __restrict__ in, RangeTask* __restrict__ rt) {
-    const int r = blockIdx.x * blockDim.x + threadIdx.x;
-    if (r >= nr) return;
-    RangeTask& t = rt[r];
-    t.s = in[r].s;
-    t.e = in[r].e;
-    t.node_area = in[r].area;
+// A primitive range of a node under construction and the union of its primitive boxes.
+struct DRange {
+    int32_t s, e;
+    float mn[3], mx[3];
+};
+
+// A node under construction: SORT's to_split list (fifo) and done list.
+struct DNode {
+    int32_t id;  // shape index
+    int32_t depth;
+    float area;  // half_area of the node's box (SAH normaliser)
+    int32_t head, tail, ndone;
+    DRange fifo[15];  // 1 + 2 * (W - 1) entries at most
+    DRange done[8];
+};
+
+// The tree before flattening: a node's children are consecutive shape ids.
+struct DShape {
+    int32_t off, cnt, first_kid, nkids;
+    float mn[3], mx[3];  // box of the primitive range (the parent's child box)
+};
+
+struct RoundSummary {
+    int next;    // nodes under construction in the next round
+    int shapes;  // shape nodes this round adds
+    int depth_max;
+    int pad;
+};
+
+__device__ __forceinline__ bool starts_node(const DRange& x, int depth, int max_leaf, int max_depth) {
+    return (x.e - x.s) > max_leaf && depth != max_depth;  // else splitNode returns at once
+}
+
+__device__ __forceinline__ DRange make_range(int32_t s, int32_t e, const int (&img)[6]) {
+    DRange x;
+    x.s = s;
+    x.e = e;
     for (int a = 0; a < 3; ++a) {
-        t.inner[a] = f2o(FLT_MAX);
-        t.inner[3 + a] = f2o(-FLT_MAX);
+        x.mn[a] = o2f(img[a]);
+        x.mx[a] = o2f(img[3 + a]);
     }
+    return x;
+}
+
+// The front range of every node is split this round (range r belongs to node r).
+__global__ void k_node_ranges(int na, const DNode* __restrict__ nodes, RangeTask* __restrict__ rt,
+                              int64_t* __restrict__ starts, int64_t* __restrict__ ends) {
+    const int r = blockIdx.x * blockDim.x + threadIdx.x;
+    if (r >= na) return;
+    const DNode& nd = nodes[r];
+    const DRange& x = nd.fifo[nd.head];
+    RangeTask& t = rt[r];
+    t.s = starts[r] = x.s;
+    t.e = ends[r] = x.e;
+    t.node_area = nd.area;
+    empty_box(t.inner);
     for (int b = 0; b < kBins; ++b) {
         t.bin_cnt[b] = 0;
-        for (int a = 0; a < 3; ++a) {
-            t.bin_box[b][a] = f2o(FLT_MAX);
-            t.bin_box[b][3 + a] = f2o(-FLT_MAX);
-        }
+        empty_box(t.bin_box[b]);
     }
     t.axis = 0;
     t.split_pos = 0.0f;
     t.split = 0;
     t.left = 0;
+    empty_box(t.half_box[0]);
+    empty_box(t.half_box[1]);
 }
 
-__global__ void k_range_out(int nr, const RangeTask* __restrict__ rt, RangeOut* __restrict__ out) {
+// Applies the round's split to every node (SORT's loop body) and counts what
+// the node hands to the next round: itself, or its children that are nodes.
+__global__ void k_node_apply(int na, DNode* __restrict__ nodes, const RangeTask* __restrict__ rt, int W,
+                             int max_leaf, int max_depth, int* __restrict__ cnt_next, int* __restrict__ cnt_shape,
+                             RoundSummary* __restrict__ sum) {
     const int r = blockIdx.x * blockDim.x + threadIdx.x;
-    if (r >= nr) return;
-    out[r].split = rt[r].split;
-    out[r].left = rt[r].left;
+    if (r >= na) return;
+    DNode& nd = nodes[r];
+    const RangeTask& t = rt[r];
+    const DRange x = nd.fifo[nd.head];
+    const int32_t mid = x.s + int32_t(t.left);
+    int head = nd.head + 1, tail = nd.tail, ndone = nd.ndone;
+    if (!t.split || mid == x.s || mid == x.e) {
+        nd.done[ndone++] = x;
+    } else {
+        nd.fifo[tail++] = make_range(x.s, mid, t.half_box[0]);
+        nd.fifo[tail++] = make_range(mid, x.e, t.half_box[1]);
+    }
+    nd.head = head;
+    nd.tail = tail;
+    nd.ndone = ndone;
+    const int total = (tail - head) + ndone;
+    int next = 0, shapes = 0;
+    if (head != tail && total < W) {
+        next = 1;
+    } else if (total == 1) {
+        atomicMax(&sum->depth_max, nd.depth);
+    } else {
+        shapes = total;
+        int kid_max = 0;
+        for (int q = head; q < tail; ++q) {
+            if (starts_node(nd.fifo[q], nd.depth + 1, max_leaf, max_depth))
+                ++next;
+            else
+                kid_max = nd.depth + 1;
+        }
+        for (int q = 0; q < ndone; ++q) {
+            if (starts_node(nd.done[q], nd.depth + 1, max_leaf, max_depth))
+                ++next;
+            else
+                kid_max = nd.depth + 1;
+        }
+        if (kid_max) atomicMax(&sum->depth_max, kid_max);
+    }
+    cnt_next[r] = next;
+    cnt_shape[r] = shapes;
 }
 
-struct Range {
-    int64_t s, e;
-};
+__global__ void k_summary(int na, const int* __restrict__ cnt_next, const int* __restrict__ off_next,
+                          const int* __restrict__ cnt_shape, const int* __restrict__ off_shape,
+                          RoundSummary* __restrict__ sum) {
+    sum->next = off_next[na - 1] + cnt_next[na - 1];
+    sum->shapes = off_shape[na - 1] + cnt_shape[na - 1];
+}
 
-// A node under construction: SORT's to_split list (fifo) and done list.
-struct NodeTask {
-    int id;  // index into the shape array
-    int depth;
-    float area;
-    int head = 0, tail = 0, ndone = 0;
-    Range fifo[16];  // 1 + 2 * (W - 1) entries at most
-    Range done[8];
-    int total() const { return (tail - head) + ndone; }
-};
-
-struct ShapeNode {
-    int64_t off = 0, cnt = 0;
-    int nkids = 0;
-    int kid[8];
-    Box kid_box[8];
-};
+// Finished nodes write their children (SORT's child order: the remaining list,
+// then the done list) as shape nodes; the next round's nodes are the
+// continuing ones and the new children, in primitive-range order.
+__global__ void k_node_commit(int na, const DNode* __restrict__ cur, const int* __restrict__ off_next,
+                              const int* __restrict__ off_shape, const int* __restrict__ cnt_shape, int shape_base,
+                              int W, int max_leaf, int max_depth, DShape* __restrict__ shapes,
+                              DNode* __restrict__ next) {
+    const int r = blockIdx.x * blockDim.x + threadIdx.x;
+    if (r >= na) return;
+    const DNode& nd = cur[r];
+    const int total = (nd.tail - nd.head) + nd.ndone;
+    int o = off_next[r];
+    if (nd.head != nd.tail && total < W) {
+        next[o] = nd;
+        return;
+    }
+    const int m = cnt_shape[r];
+    if (m == 0) return;  // a single range: the node is a leaf
+    const int first = shape_base + off_shape[r];
+    shapes[nd.id].first_kid = first;
+    shapes[nd.id].nkids = m;
+    DRange ks[8];
+    int k = 0;
+    for (int q = nd.head; q < nd.tail; ++q) ks[k++] = nd.fifo[q];
+    for (int q = 0; q < nd.ndone; ++q) ks[k++] = nd.done[q];
+    int ord[8];
+    for (int q = 0; q < m; ++q) {
+        DShape& sh = shapes[first + q];
+        sh.off = ks[q].s;
+        sh.cnt = ks[q].e - ks[q].s;
+        sh.first_kid = -1;
+        sh.nkids = 0;
+        for (int a = 0; a < 3; ++a) {
+            sh.mn[a] = ks[q].mn[a];
+            sh.mx[a] = ks[q].mx[a];
+        }
+        int j = q;  // insertion by range start
+        while (j > 0 && ks[ord[j - 1]].s > ks[q].s) {
+            ord[j] = ord[j - 1];
+            --j;
+        }
+        ord[j] = q;
+    }
+    const int depth = nd.depth + 1;
+    for (int j = 0; j < m; ++j) {
+        const DRange& x = ks[ord[j]];
+        if (!starts_node(x, depth, max_leaf, max_depth)) continue;
+        DNode& c = next[o++];
+        c.id = first + ord[j];
+        c.depth = depth;
+        c.area = half_area(x.mn, x.mx);
+        c.head = 0;
+        c.tail = 1;
+        c.ndone = 0;
+        c.fifo[0] = x;
+    }
+}
 
 unsigned grid(int64_t n, int t = 256) { return (unsigned)std::max<int64_t>(1, (n + t - 1) / t); }
 
@@ -405,6 +682,20 @@ float host_half_area(const Box& b) {
     const float c = oy * oz;
     const float e = oz * ox;
     return (a + c) + e;
+}
+
+struct Stream {
+    cudaStream_t s = nullptr;
+    Stream() { check(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking), "cudaStreamCreate"); }
+    ~Stream() {
+        if (s) cudaStreamDestroy(s);
+    }
+};
+
+template <class T>
+void swap_bufs(DevBuf<T>& a, DevBuf<T>& b) {
+    std::swap(a.p, b.p);
+    std::swap(a.n, b.n);
 }
 
 }  // namespace
@@ -426,15 +717,21 @@ BuiltTree build_tree_gpu(const float* tri, int64_t ntri, const BuildParams& p, i
             if (d >= 0) cudaSetDevice(d);
         }
     } restore{prev};
+    Stream stream;
+    const cudaStream_t st = stream.s;
 
     DevBuf<float> d_tri, d_cx, d_cy, d_cz, d_pb;
     DevBuf<int32_t> d_idx;
-    DevBuf<int> d_rid, d_ml, d_mr, d_sl, d_sr, d_boxes;
+    DevBuf<int> d_rid, d_ml, d_mr, d_sl, d_sr, d_scene;
     DevBuf<int64_t> d_pl, d_pr, d_starts, d_ends;
     DevBuf<RangeTask> d_rt;
-    DevBuf<RangeIn> d_in;
-    DevBuf<RangeOut> d_out;
+    DevBuf<DNode> d_cur, d_next;
+    DevBuf<DShape> d_shapes;
+    DevBuf<int> d_cnt_next, d_off_next, d_cnt_shape, d_off_shape;
+    DevBuf<RoundSummary> d_sum;
     DevBuf<unsigned char> d_temp;
+    PinnedBuf<int> h_scene;
+    PinnedBuf<RoundSummary> h_sum;
     const int64_t nn = std::max<int64_t>(n, 1);
     d_tri.alloc(size_t(nn) * 9);
     d_cx.alloc(size_t(nn));
@@ -449,25 +746,25 @@ BuiltTree build_tree_gpu(const float* tri, int64_t ntri, const BuildParams& p, i
     d_sr.alloc(size_t(nn));
     d_pl.alloc(size_t(nn));
     d_pr.alloc(size_t(nn));
-    if (n > 0) check(cudaMemcpy(d_tri.p, tri, size_t(n) * 9 * sizeof(float), cudaMemcpyHostToDevice), "upload");
-    if (n > 0) k_prim_setup<<<grid(n), 256>>>(d_tri.p, n, d_cx.p, d_cy.p, d_cz.p, d_idx.p, d_pb.p);
-    check(cudaGetLastError(), "primitive setup");
+    d_scene.alloc(6);
+    d_sum.alloc(1);
+    h_scene.alloc(6);
+    h_sum.alloc(1);
 
     // Scene box (core/scene.cpp:146-154): union of the primitive boxes, enlarged by 0.1%.
-    std::vector<float> pb(size_t(nn) * 6);
-    if (n > 0) check(cudaMemcpy(pb.data(), d_pb.p, size_t(n) * 6 * sizeof(float), cudaMemcpyDeviceToHost), "boxes");
     Box scene;
-    for (int a = 0; a < 3; ++a) {
-        scene.mn[a] = FLT_MAX;
-        scene.mx[a] = -FLT_MAX;
-    }
-    for (int64_t i = 0; i < n; ++i)
-        for (int a = 0; a < 3; ++a) {
-            const float lo = pb[size_t(a) * n + i], hi = pb[size_t(3 + a) * n + i];
-            scene.mn[a] = (lo < scene.mn[a]) ? lo : scene.mn[a];
-            scene.mx[a] = (scene.mx[a] < hi) ? hi : scene.mx[a];
-        }
     {
+        empty_box(h_scene.p);
+        if (n > 0) {
+            check(cudaMemcpyAsync(d_tri.p, tri, size_t(n) * 9 * sizeof(float), cudaMemcpyHostToDevice, st), "upload");
+            k_prim_setup<<<grid(n), 256, 0, st>>>(d_tri.p, n, d_cx.p, d_cy.p, d_cz.p, d_idx.p, d_pb.p);
+            check(cudaMemcpyAsync(d_scene.p, h_scene.p, 6 * sizeof(int), cudaMemcpyHostToDevice, st), "scene box");
+            k_scene_box<<<std::min<unsigned>(grid(n), 148 * 8), 256, 0, st>>>(n, d_pb.p, d_scene.p);
+            check(cudaGetLastError(), "primitive setup");
+            check(cudaMemcpyAsync(h_scene.p, d_scene.p, 6 * sizeof(int), cudaMemcpyDeviceToHost, st), "scene box");
+            check(cudaStreamSynchronize(st), "primitive setup");
+        }
+        scene = box_from_images(h_scene.p);
         const float threshold = 0.001f;
         float delta[3];
         for (int k = 0; k < 3; ++k) delta[k] = (scene.mx[k] - scene.mn[k]) * threshold;
@@ -480,193 +777,100 @@ BuiltTree build_tree_gpu(const float* tri, int64_t ntri, const BuildParams& p, i
     if (n == 0) return t;
 
     size_t temp_bytes = 0;
-    cub::DeviceScan::ExclusiveSum(nullptr, temp_bytes, d_ml.p, d_sl.p, (int)n);
+    check(cub::DeviceScan::ExclusiveSum(nullptr, temp_bytes, d_ml.p, d_sl.p, (int)n, st), "scan size");
     d_temp.alloc(temp_bytes);
 
-    std::vector<ShapeNode> shape(1);
-    shape[0].off = 0;
-    shape[0].cnt = n;
-    int depth_max = 0;
-    // Nodes under construction, in order of their primitive ranges (disjoint), so
-    // the ranges split in a round come out sorted for the per-primitive lookup.
-    std::vector<NodeTask> active, next;
-    auto start_node = [&](std::vector<NodeTask>& into, int id, int depth, const Box& box) {
-        const ShapeNode& sn = shape[size_t(id)];
-        if (sn.cnt <= p.max_leaf || depth == p.max_depth) {  // splitNode's early return
-            depth_max = std::max(depth_max, depth);
-            return;
-        }
-        NodeTask nt;
-        nt.id = id;
-        nt.depth = depth;
-        nt.area = host_half_area(box);
-        nt.fifo[nt.tail++] = {sn.off, sn.off + sn.cnt};
-        into.push_back(nt);
-    };
-    start_node(active, 0, 1, scene);
-
-    std::vector<RangeIn> rin;
-    std::vector<RangeOut> rout;
-    std::vector<int> owner;
-    std::vector<int64_t> starts, ends;
-    while (!active.empty()) {
-        // One split per node: the front of its list, while SORT's loop would go on.
-        rin.clear();
-        owner.clear();
-        for (size_t k = 0; k < active.size(); ++k) {
-            NodeTask& nt = active[k];
-            if (nt.head == nt.tail || nt.total() >= W) continue;
-            const Range r = nt.fifo[nt.head++];
-            rin.push_back({r.s, r.e, nt.area, 0});
-            owner.push_back(int(k));
-        }
-        const int nr = int(rin.size());
-        if (nr > 0) {
-            starts.resize(size_t(nr));
-            ends.resize(size_t(nr));
-            for (int k = 0; k < nr; ++k) {
-                starts[size_t(k)] = rin[size_t(k)].s;
-                ends[size_t(k)] = rin[size_t(k)].e;
-            }
-            d_rt.alloc(size_t(nr));
-            d_in.alloc(size_t(nr));
-            d_out.alloc(size_t(nr));
-            d_starts.alloc(size_t(nr));
-            d_ends.alloc(size_t(nr));
-            check(cudaMemcpy(d_in.p, rin.data(), size_t(nr) * sizeof(RangeIn), cudaMemcpyHostToDevice), "ranges");
-            check(cudaMemcpy(d_starts.p, starts.data(), size_t(nr) * 8, cudaMemcpyHostToDevice), "ranges");
-            check(cudaMemcpy(d_ends.p, ends.data(), size_t(nr) * 8, cudaMemcpyHostToDevice), "ranges");
-            k_range_init<<<grid(nr, 128), 128>>>(nr, d_in.p, d_rt.p);
-            k_bounds<<<grid(n), 256>>>(n, d_starts.p, d_ends.p, nr, d_cx.p, d_cy.p, d_cz.p, d_rid.p, d_rt.p);
-            k_bin<<<grid(n), 256>>>(n, d_rid.p, d_cx.p, d_cy.p, d_cz.p, d_idx.p, d_pb.p, n, d_rt.p);
-            k_sweep<<<grid(nr, 128), 128>>>(nr, d_rt.p, p.max_leaf);
-            k_count_left<<<grid(n), 256>>>(n, d_rid.p, d_cx.p, d_cy.p, d_cz.p, d_rt.p);
-            k_misplaced<<<grid(n), 256>>>(n, d_rid.p, d_cx.p, d_cy.p, d_cz.p, d_rt.p, d_ml.p, d_mr.p);
-            check(cudaGetLastError(), "split kernels");
-            check(cub::DeviceScan::ExclusiveSum(d_temp.p, temp_bytes, d_ml.p, d_sl.p, (int)n), "scan");
-            check(cub::DeviceScan::ExclusiveSum(d_temp.p, temp_bytes, d_mr.p, d_sr.p, (int)n), "scan");
-            k_pairs<<<grid(n), 256>>>(n, d_rid.p, d_rt.p, d_ml.p, d_mr.p, d_sl.p, d_sr.p, d_pl.p, d_pr.p);
-            k_range_out<<<grid(nr, 128), 128>>>(nr, d_rt.p, d_out.p);
-            int last_sl = 0, last_ml = 0;
-            check(cudaMemcpy(&last_sl, d_sl.p + (n - 1), 4, cudaMemcpyDeviceToHost), "pairs");
-            check(cudaMemcpy(&last_ml, d_ml.p + (n - 1), 4, cudaMemcpyDeviceToHost), "pairs");
-            const int64_t pairs = int64_t(last_sl) + last_ml;
-            if (pairs > 0) k_swap<<<grid(pairs), 256>>>(pairs, d_pl.p, d_pr.p, d_cx.p, d_cy.p, d_cz.p, d_idx.p);
-            check(cudaGetLastError(), "partition kernels");
-            rout.resize(size_t(nr));
-            check(cudaMemcpy(rout.data(), d_out.p, size_t(nr) * sizeof(RangeOut), cudaMemcpyDeviceToHost), "results");
-            for (int k = 0; k < nr; ++k) {
-                NodeTask& nt = active[size_t(owner[size_t(k)])];
-                const RangeIn& x = rin[size_t(k)];
-                const int64_t mid = x.s + rout[size_t(k)].left;
-                if (!rout[size_t(k)].split || mid == x.s || mid == x.e) {
-                    nt.done[nt.ndone++] = {x.s, x.e};
-                } else {
-                    nt.fifo[nt.tail++] = {x.s, mid};
-                    nt.fifo[nt.tail++] = {mid, x.e};
-                }
-            }
-        }
-        // Nodes whose loop has ended become leaves, or hand their ranges on as
-        // children (SORT's child order: the remaining list, then the done list).
-        struct Kid {
-            int id, depth, parent, j;  // j: position among the parent's children
-        };
-        std::vector<Kid> kids;
-        next.clear();
-        for (NodeTask& nt : active) {
-            if (nt.head != nt.tail && nt.total() < W) {
-                next.push_back(nt);
-                continue;
-            }
-            if (nt.total() == 1) {
-                depth_max = std::max(depth_max, nt.depth);
-                continue;
-            }
-            Range rs[8];
-            int m = 0;
-            for (int q = nt.head; q < nt.tail; ++q) rs[m++] = nt.fifo[q];
-            for (int q = 0; q < nt.ndone; ++q) rs[m++] = nt.done[q];
-            const int first_kid = int(shape.size());
-            for (int q = 0; q < m; ++q) {
-                ShapeNode sn;
-                sn.off = rs[q].s;
-                sn.cnt = rs[q].e - rs[q].s;
-                shape[size_t(nt.id)].kid[shape[size_t(nt.id)].nkids++] = int(shape.size());
-                shape.push_back(sn);
-            }
-            // in range order for the sorted active list
-            int ord[8];
-            for (int q = 0; q < m; ++q) ord[q] = q;
-            std::sort(ord, ord + m, [&](int a, int b) { return rs[a].s < rs[b].s; });
-            for (int q = 0; q < m; ++q) {
-                kids.push_back({first_kid + ord[q], nt.depth + 1, nt.id, ord[q]});
-                next.emplace_back();  // placeholder
-                next.back().id = -1;
-            }
-        }
-        if (!kids.empty()) {
-            // Boxes of the new children (kids are in range order): their own SAH
-            // normaliser, and their parent's child boxes.
-            const int nk = int(kids.size());
-            starts.resize(size_t(nk));
-            ends.resize(size_t(nk));
-            for (int k = 0; k < nk; ++k) {
-                const ShapeNode& sn = shape[size_t(kids[size_t(k)].id)];
-                starts[size_t(k)] = sn.off;
-                ends[size_t(k)] = sn.off + sn.cnt;
-            }
-            std::vector<int> boxes(size_t(nk) * 6);
-            for (int k = 0; k < nk; ++k)
-                for (int a = 0; a < 3; ++a) {
-                    boxes[size_t(k) * 6 + a] = f2o(FLT_MAX);
-                    boxes[size_t(k) * 6 + 3 + a] = f2o(-FLT_MAX);
-                }
-            d_starts.alloc(size_t(nk));
-            d_ends.alloc(size_t(nk));
-            d_boxes.alloc(size_t(nk) * 6);
-            check(cudaMemcpy(d_starts.p, starts.data(), size_t(nk) * 8, cudaMemcpyHostToDevice), "kids");
-            check(cudaMemcpy(d_ends.p, ends.data(), size_t(nk) * 8, cudaMemcpyHostToDevice), "kids");
-            check(cudaMemcpy(d_boxes.p, boxes.data(), boxes.size() * 4, cudaMemcpyHostToDevice), "kids");
-            k_range_boxes<<<grid(n), 256>>>(n, d_starts.p, d_ends.p, nk, d_idx.p, d_pb.p, n, d_boxes.p);
-            check(cudaGetLastError(), "child boxes");
-            check(cudaMemcpy(boxes.data(), d_boxes.p, boxes.size() * 4, cudaMemcpyDeviceToHost), "kids");
-            std::vector<NodeTask> filled;
-            filled.reserve(next.size());
-            size_t kk = 0;
-            for (size_t q = 0; q < next.size(); ++q) {
-                if (next[q].id >= 0) {
-                    filled.push_back(next[q]);
-                    continue;
-                }
-                const Kid& kd = kids[kk];
-                const Box b = box_from_images(&boxes[kk * 6]);
-                ++kk;
-                shape[size_t(kd.parent)].kid_box[kd.j] = b;
-                start_node(filled, kd.id, kd.depth, b);
-            }
-            next.swap(filled);
-        }
-        active.swap(next);
+    // The root shape, and the root node unless splitNode returns at once.
+    int shape_count = 1;
+    d_shapes.alloc(size_t(std::max<int64_t>(1024, n / 4)));
+    {
+        DShape root{0, int32_t(n), -1, 0, {scene.mn[0], scene.mn[1], scene.mn[2]},
+                    {scene.mx[0], scene.mx[1], scene.mx[2]}};
+        check(cudaMemcpyAsync(d_shapes.p, &root, sizeof(root), cudaMemcpyHostToDevice, st), "root");
     }
-    t.depth = depth_max;
+    const bool root_node = n > p.max_leaf && p.max_depth != 1;
+    int na = root_node ? 1 : 0;
+    *h_sum.p = RoundSummary{0, 0, root_node ? 0 : 1, 0};
+    check(cudaMemcpyAsync(d_sum.p, h_sum.p, sizeof(RoundSummary), cudaMemcpyHostToDevice, st), "summary");
+    d_cur.alloc(4096);
+    d_next.alloc(4096);
+    if (root_node) {
+        DNode root{};
+        root.id = 0;
+        root.depth = 1;
+        root.area = host_half_area(scene);
+        root.tail = 1;
+        root.fifo[0] = DRange{0, int32_t(n), {scene.mn[0], scene.mn[1], scene.mn[2]},
+                              {scene.mx[0], scene.mx[1], scene.mx[2]}};
+        check(cudaMemcpyAsync(d_cur.p, &root, sizeof(root), cudaMemcpyHostToDevice, st), "root");
+    }
+    check(cudaStreamSynchronize(st), "root");
 
-    // Final permutation -> leaf order.
+    while (na > 0) {
+        d_rt.alloc(size_t(na));
+        d_starts.alloc(size_t(na));
+        d_ends.alloc(size_t(na));
+        d_cnt_next.alloc(size_t(na));
+        d_off_next.alloc(size_t(na));
+        d_cnt_shape.alloc(size_t(na));
+        d_off_shape.alloc(size_t(na));
+        k_node_ranges<<<grid(na, 128), 128, 0, st>>>(na, d_cur.p, d_rt.p, d_starts.p, d_ends.p);
+        k_bounds<<<grid(n), 256, 0, st>>>(n, d_starts.p, d_ends.p, na, d_cx.p, d_cy.p, d_cz.p, d_rid.p, d_rt.p);
+        k_bin<<<grid(n), 256, 0, st>>>(n, d_rid.p, d_cx.p, d_cy.p, d_cz.p, d_pb.p, d_rt.p);
+        k_sweep<<<grid(na, 128), 128, 0, st>>>(na, d_rt.p, p.max_leaf);
+        k_count_left<<<grid(n), 256, 0, st>>>(n, d_rid.p, d_cx.p, d_cy.p, d_cz.p, d_pb.p, d_rt.p);
+        k_misplaced<<<grid(n), 256, 0, st>>>(n, d_rid.p, d_cx.p, d_cy.p, d_cz.p, d_rt.p, d_ml.p, d_mr.p);
+        check(cudaGetLastError(), "split kernels");
+        check(cub::DeviceScan::ExclusiveSum(d_temp.p, temp_bytes, d_ml.p, d_sl.p, (int)n, st), "scan");
+        check(cub::DeviceScan::ExclusiveSum(d_temp.p, temp_bytes, d_mr.p, d_sr.p, (int)n, st), "scan");
+        k_pairs<<<grid(n), 256, 0, st>>>(n, d_rid.p, d_rt.p, d_ml.p, d_mr.p, d_sl.p, d_sr.p, d_pl.p, d_pr.p);
+        k_swap<<<grid((n + 1) / 2), 256, 0, st>>>(n, d_sl.p, d_ml.p, d_pl.p, d_pr.p, d_cx.p, d_cy.p, d_cz.p, d_pb.p,
+                                                  d_idx.p);
+        k_node_apply<<<grid(na, 128), 128, 0, st>>>(na, d_cur.p, d_rt.p, W, p.max_leaf, p.max_depth, d_cnt_next.p,
+                                                    d_cnt_shape.p, d_sum.p);
+        check(cudaGetLastError(), "partition kernels");
+        check(cub::DeviceScan::ExclusiveSum(d_temp.p, temp_bytes, d_cnt_next.p, d_off_next.p, na, st), "scan");
+        check(cub::DeviceScan::ExclusiveSum(d_temp.p, temp_bytes, d_cnt_shape.p, d_off_shape.p, na, st), "scan");
+        k_summary<<<1, 1, 0, st>>>(na, d_cnt_next.p, d_off_next.p, d_cnt_shape.p, d_off_shape.p, d_sum.p);
+        check(cudaMemcpyAsync(h_sum.p, d_sum.p, sizeof(RoundSummary), cudaMemcpyDeviceToHost, st), "summary");
+        check(cudaStreamSynchronize(st), "split round");
+        const RoundSummary s = *h_sum.p;
+        if (size_t(shape_count) + size_t(s.shapes) > d_shapes.n) {
+            DevBuf<DShape> bigger;
+            bigger.alloc(std::max(size_t(shape_count) + size_t(s.shapes), 2 * d_shapes.n));
+            check(cudaMemcpyAsync(bigger.p, d_shapes.p, size_t(shape_count) * sizeof(DShape),
+                                  cudaMemcpyDeviceToDevice, st),
+                  "grow shapes");
+            check(cudaStreamSynchronize(st), "grow shapes");
+            swap_bufs(d_shapes, bigger);
+        }
+        if (size_t(s.next) > d_next.n) d_next.alloc(std::max(size_t(s.next), 2 * d_next.n));
+        k_node_commit<<<grid(na, 128), 128, 0, st>>>(na, d_cur.p, d_off_next.p, d_off_shape.p, d_cnt_shape.p,
+                                                     shape_count, W, p.max_leaf, p.max_depth, d_shapes.p, d_next.p);
+        check(cudaGetLastError(), "node commit");
+        swap_bufs(d_cur, d_next);
+        shape_count += s.shapes;
+        na = s.next;
+    }
+    t.depth = h_sum.p->depth_max;
+
+    // Shapes and the final permutation (leaf order) to the host.
+    std::vector<DShape> shape(static_cast<size_t>(shape_count));
     std::vector<int32_t> order(static_cast<size_t>(n));
-    check(cudaMemcpy(order.data(), d_idx.p, size_t(n) * 4, cudaMemcpyDeviceToHost), "order");
-    t.order = order;
-    t.slot_box.resize(size_t(n));
+    check(cudaMemcpyAsync(shape.data(), d_shapes.p, shape.size() * sizeof(DShape), cudaMemcpyDeviceToHost, st),
+          "shapes");
+    check(cudaMemcpyAsync(order.data(), d_idx.p, size_t(n) * 4, cudaMemcpyDeviceToHost, st), "order");
+    check(cudaStreamSynchronize(st), "download");
     t.leaf_last.assign(size_t(n), 0);
-    for (int64_t i = 0; i < n; ++i) {
-        const int32_t q = order[size_t(i)];
-        Box& b = t.slot_box[size_t(i)];
-        for (int a = 0; a < 3; ++a) {
-            b.mn[a] = pb[size_t(a) * n + q];
-            b.mx[a] = pb[size_t(3 + a) * n + q];
-        }
-    }
+    t.order.swap(order);
     // Flatten exactly as build_tree numbers nodes: a node allocates its interior
     // children consecutively when it is filled, then fills them in order.
+    size_t interior_total = 0;
+    for (const DShape& sn : shape) interior_total += sn.nkids ? 1 : 0;
+    t.first_interior.reserve(interior_total);
+    t.child.reserve(interior_total * W);
+    t.lo.reserve(interior_total * 3 * W);
+    t.hi.reserve(interior_total * 3 * W);
     auto alloc = [&](int cnt) {
         const int32_t base = int32_t(t.first_interior.size());
         t.first_interior.resize(t.first_interior.size() + size_t(cnt), -1);
@@ -675,7 +879,7 @@ BuiltTree build_tree_gpu(const float* tri, int64_t ntri, const BuildParams& p, i
         t.hi.resize(t.hi.size() + size_t(cnt) * 3 * W, -FLT_MAX);
         return base;
     };
-    auto leaf = [&](const ShapeNode& sn) {
+    auto leaf = [&](const DShape& sn) {
         t.leaves++;
         t.leaf_last[size_t(sn.off + sn.cnt - 1)] = 1;
     };
@@ -690,28 +894,29 @@ BuiltTree build_tree_gpu(const float* tri, int64_t ntri, const BuildParams& p, i
     while (!stack.empty()) {
         const auto [sid, idx] = stack.back();
         stack.pop_back();
-        const ShapeNode sn = shape[size_t(sid)];
+        const DShape sn = shape[size_t(sid)];
         int interior = 0;
-        for (int j = 0; j < sn.nkids; ++j) interior += shape[size_t(sn.kid[j])].nkids ? 1 : 0;
+        for (int j = 0; j < sn.nkids; ++j) interior += shape[size_t(sn.first_kid + j)].nkids ? 1 : 0;
         const int32_t base = interior ? alloc(interior) : -1;
         t.first_interior[size_t(idx)] = base;
         int k = 0;
         std::pair<int, int32_t> sub[8];
         int nsub = 0;
         for (int j = 0; j < sn.nkids; ++j) {
-            const ShapeNode& kid = shape[size_t(sn.kid[j])];
+            const int kid_id = sn.first_kid + j;
+            const DShape& kid = shape[size_t(kid_id)];
             int32_t ref;
             if (kid.nkids == 0) {
                 ref = leaf_ref(kid.off);
                 leaf(kid);
             } else {
                 ref = base + k++;
-                sub[nsub++] = {sn.kid[j], ref};
+                sub[nsub++] = {kid_id, ref};
             }
             t.child[size_t(idx) * W + j] = ref;
             for (int a = 0; a < 3; ++a) {
-                t.lo[(size_t(idx) * 3 + a) * W + j] = sn.kid_box[j].mn[a];
-                t.hi[(size_t(idx) * 3 + a) * W + j] = sn.kid_box[j].mx[a];
+                t.lo[(size_t(idx) * 3 + a) * W + j] = kid.mn[a];
+                t.hi[(size_t(idx) * 3 + a) * W + j] = kid.mx[a];
             }
         }
         for (int q = nsub - 1; q >= 0; --q) stack.push_back(sub[q]);  // first child filled next
