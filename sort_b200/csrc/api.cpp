@@ -106,34 +106,40 @@ sg_status upload(sg_scene* s, const float* tri, int64_t ntri) {
         int32_t* ch = reinterpret_cast<int32_t*>(base + 6 * Q * 4);
         for (int j = 0; j < W; ++j) ch[j] = t.child[size_t(k) * W + j];
     }
-    std::vector<float4> tris(size_t(ntri + sg::kPadSlots) * 3);
-    std::memset(tris.data(), 0, tris.size() * sizeof(float4));
-    for (int64_t i = 0; i < ntri; ++i) {
-        const int32_t p = t.order[size_t(i)];
-        const float* v = tri + int64_t(p) * 9;
-        float4* dst = &tris[size_t(i) * 3];
-        int32_t last = t.leaf_last[size_t(i)];
-        dst[0] = make_float4(v[0], v[1], v[2], 0.0f);
-        std::memcpy(&dst[0].w, &p, 4);
-        dst[1] = make_float4(v[3], v[4], v[5], 0.0f);
-        std::memcpy(&dst[1].w, &last, 4);
-        dst[2] = make_float4(v[6], v[7], v[8], 0.0f);
-    }
-    const size_t nb = nodes.size() * sizeof(float4), tb = tris.size() * sizeof(float4);
+    const size_t nb = nodes.size() * sizeof(float4), tb = size_t(ntri + sg::kPadSlots) * 3 * sizeof(float4);
     cudaError_t e = cudaMalloc(&s->d_nodes, nb);
     if (e != cudaSuccess) return e == cudaErrorMemoryAllocation ? fail(SG_ERR_OUT_OF_MEMORY, "cudaMalloc(nodes) failed")
                                                                  : cuda_fail(e, "cudaMalloc(nodes)");
-    e = cudaMalloc(&s->d_tris, tb);
-    if (e != cudaSuccess) return e == cudaErrorMemoryAllocation ? fail(SG_ERR_OUT_OF_MEMORY, "cudaMalloc(triangles) failed")
-                                                                 : cuda_fail(e, "cudaMalloc(triangles)");
     if ((e = cudaMalloc(&s->d_err, sizeof(int))) != cudaSuccess) return cuda_fail(e, "cudaMalloc(status)");
     if ((e = cudaMalloc(&s->d_counters, sg_scene::kCounterSlots * sizeof(unsigned long long))) != cudaSuccess)
         return cuda_fail(e, "cudaMalloc(counters)");
     if ((e = cudaMemcpy(s->d_nodes, nodes.data(), nb, cudaMemcpyHostToDevice)) != cudaSuccess)
         return cuda_fail(e, "upload nodes");
-    if ((e = cudaMemcpy(s->d_tris, tris.data(), tb, cudaMemcpyHostToDevice)) != cudaSuccess)
-        return cuda_fail(e, "upload triangles");
     if ((e = cudaMemset(s->d_err, 0, sizeof(int))) != cudaSuccess) return cuda_fail(e, "clear status");
+    if (s->tree.d_tris) {  // the GPU builder wrote the records on the device
+        s->d_tris = s->tree.d_tris;
+        s->tree.d_tris = nullptr;
+    } else {
+        std::vector<float4> tris(size_t(ntri + sg::kPadSlots) * 3);
+        std::memset(tris.data(), 0, tris.size() * sizeof(float4));
+        for (int64_t i = 0; i < ntri; ++i) {
+            const int32_t p = t.order[size_t(i)];
+            const float* v = tri + int64_t(p) * 9;
+            float4* dst = &tris[size_t(i) * 3];
+            int32_t last = t.leaf_last[size_t(i)];
+            dst[0] = make_float4(v[0], v[1], v[2], 0.0f);
+            std::memcpy(&dst[0].w, &p, 4);
+            dst[1] = make_float4(v[3], v[4], v[5], 0.0f);
+            std::memcpy(&dst[1].w, &last, 4);
+            dst[2] = make_float4(v[6], v[7], v[8], 0.0f);
+        }
+        e = cudaMalloc(&s->d_tris, tb);
+        if (e != cudaSuccess)
+            return e == cudaErrorMemoryAllocation ? fail(SG_ERR_OUT_OF_MEMORY, "cudaMalloc(triangles) failed")
+                                                  : cuda_fail(e, "cudaMalloc(triangles)");
+        if ((e = cudaMemcpy(s->d_tris, tris.data(), tb, cudaMemcpyHostToDevice)) != cudaSuccess)
+            return cuda_fail(e, "upload triangles");
+    }
     s->device_bytes = int64_t(nb + tb);
     return SG_OK;
 }
@@ -143,6 +149,7 @@ void release(sg_scene* s) {
     DeviceGuard g(s->device);
     if (s->d_nodes) cudaFree(s->d_nodes);
     if (s->d_tris) cudaFree(s->d_tris);
+    if (s->tree.d_tris) cudaFree(s->tree.d_tris);  // a GPU build that was not adopted
     if (s->d_err) cudaFree(s->d_err);
     if (s->d_stats) cudaFree(s->d_stats);
     if (s->d_counters) cudaFree(s->d_counters);
@@ -271,7 +278,7 @@ sg_status sg_scene_create(const float* triangles, int64_t ntri, const sg_build_o
     s->build_seconds = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
     s->stack_need = std::max(1, s->tree.depth * (s->width - 1) + 1);
     if (s->stack_need > 256) {
-        delete s;
+        release(s);
         return fail(SG_ERR_LIMIT, "tree too deep for the traversal stack (depth*(width-1)+1 > 256)");
     }
     DeviceGuard g(s->device);

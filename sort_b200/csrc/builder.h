@@ -53,6 +53,10 @@ struct BuiltTree {
     std::vector<int32_t> first_interior;  // per node, -1 if none
     std::vector<int32_t> order;           // primitive index of each leaf slot (leaf order)
     std::vector<uint8_t> leaf_last;       // 1 on the last slot of every leaf
+    // Set by build_tree_gpu only: the triangle records of the device layout
+    // (layout.h), leaf order plus the zero pad slots, already on the build's
+    // device. The receiver owns it (cudaFree).
+    float4* d_tris = nullptr;
     int64_t leaves = 0;
     int64_t interior() const { return width ? int64_t(child.size()) / width : 0; }
 };

@@ -44,6 +44,7 @@
 #include <vector>
 
 #include "builder.h"
+#include "layout.h"
 
 namespace sg {
 namespace {
@@ -443,6 +444,19 @@ __global__ void k_swap(int64_t n, const int* __restrict__ sl, const int* __restr
     swap_at(cz, a, b);
     swap_at(idx, a, b);
     for (int q = 0; q < 6; ++q) swap_at(pb + q * n, a, b);
+}
+
+// Slot i of the device layout: {v0, primitive index}, {v1, last-in-leaf flag}, {v2, 0}.
+__global__ void k_leaf_tris(int64_t n, const float* __restrict__ tri, const int32_t* __restrict__ idx,
+                            const uint8_t* __restrict__ last, float4* __restrict__ out) {
+    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const int32_t p = idx[i];
+    const float* v = tri + int64_t(p) * 9;
+    const int32_t flag = last[i];
+    out[i * 3 + 0] = make_float4(v[0], v[1], v[2], __int_as_float(p));
+    out[i * 3 + 1] = make_float4(v[3], v[4], v[5], __int_as_float(flag));
+    out[i * 3 + 2] = make_float4(v[6], v[7], v[8], 0.0f);
 }
 
 void check(cudaError_t e, const char* what) {
@@ -921,6 +935,24 @@ BuiltTree build_tree_gpu(const float* tri, int64_t ntri, const BuildParams& p, i
         }
         for (int q = nsub - 1; q >= 0; --q) stack.push_back(sub[q]);  // first child filled next
     }
+
+    // The triangle records in leaf order, built where the triangles already are.
+    uint8_t* d_last = reinterpret_cast<uint8_t*>(d_rid.p);  // n bytes fit in the n-int buffer
+    check(cudaMemcpyAsync(d_last, t.leaf_last.data(), size_t(n), cudaMemcpyHostToDevice, st), "leaf flags");
+    const size_t tris_bytes = size_t(n + kPadSlots) * 3 * sizeof(float4);
+    float4* d_tris = nullptr;
+    check(cudaMalloc(&d_tris, tris_bytes), "cudaMalloc(triangles)");
+    cudaError_t e = cudaMemsetAsync(d_tris + size_t(n) * 3, 0, size_t(kPadSlots) * 3 * sizeof(float4), st);
+    if (e == cudaSuccess) {
+        k_leaf_tris<<<grid(n), 256, 0, st>>>(n, d_tri.p, d_idx.p, d_last, d_tris);
+        e = cudaGetLastError();
+    }
+    if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+    if (e != cudaSuccess) {
+        cudaFree(d_tris);
+        check(e, "triangle records");
+    }
+    t.d_tris = d_tris;
     return t;
 }
 
