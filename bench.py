@@ -22,7 +22,9 @@ Other workloads (--workload):
              batches per step: persistent multi-scene kernel under a captured
              CUDA graph (autotuned) vs one plain launch per batch;
   serve      4 resident path-tracing scenes, a Poisson stream of render
-             requests: the render server vs FIFO per-request renders.
+             requests: the render server vs FIFO per-request renders;
+  build      GPU build of the 21M-triangle OBVH (SORT's tree), one build per
+             step; reference arm: SORT's single-threaded Fbvh::Build.
 --nodes q8 times 8-bit child boxes (closest, raycast, pathtrace).
 """
 from __future__ import annotations
@@ -787,13 +789,132 @@ def run_serve(args):
         t.Release()
 
 
+BUILD_SAMPLE = (64, LEVEL)  # SORT's single-threaded build, timed on 64 of the 1,024 spheres (1,310,722 triangles)
+
+
+def build_config(extra=None):
+    cfg = {
+        "workload": "build_21m: BVH build of 1,024 level-5 icospheres + ground quad = 20,971,522 triangles as "
+                    "SORT's OBVH (width 8, depth 16, leaf 8) from host triangles; GPU builder (SG_BUILDER_GPU), "
+                    "the same tree as SORT's Fbvh::Build",
+        "scene_seed": 1,
+        "timing": "value: the library's clock around the whole build (triangle upload, GPU split rounds, "
+                  "host flattening); e2e: the create call (build + node upload) from host triangles",
+        "l2": "inputs larger than L2: 755 MB of triangles per build (no flush)",
+    }
+    if extra:
+        cfg.update(extra)
+    return cfg
+
+
+def sort_build_rate(threads_note=True):
+    """SORT's own Accelerator::Build (single-threaded, as SORT builds) on the bounded sample."""
+    from sort_b200 import scenes
+    from oracle.oracle import Reference, reference_available
+    if not reference_available():
+        return None
+    spheres, level = BUILD_SAMPLE
+    tri = scenes.sphere_field(spheres, level, seed=1)
+    ref = Reference()
+    secs = []
+    for _ in range(3):
+        tree = ref.build(tri, WIDTH, DEPTH, LEAF)
+        secs.append(tree.build_seconds())
+        del tree
+    rate = tri.shape[0] / statistics.median(secs) / 1e6
+    return {"value": round(rate, 3), "unit": "Mtriangles/s", "cores": 1, "kind": "reference",
+            "sample": f"{tri.shape[0]} triangles ({spheres} level-{level} icospheres + ground), median of 3 "
+                      "SORT Obvh::Build calls"}
+
+
+def run_build(args):
+    """build_21m: GPU builds of the 21M-triangle OBVH, one build per step."""
+    import torch
+
+    from sort_b200 import Obvh, _lib, scenes
+    from sort_b200.replicas import max_over_ranks
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.impl == "reference":
+        if rank != 0:
+            return
+        base = sort_build_rate()
+        if base is None:
+            print(json.dumps({"impl": "reference", "unavailable": "SORT reference library (oracle/_ref) not built"}))
+            return
+        print(json.dumps({
+            "impl": "reference", "metric": "Mtriangles/s BVH build", "value": base["value"],
+            "unit": "Mtriangles/s", "n_gpus": args.gpus, "steps": 3, "warmup": 0, "ms_per_step": None,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+            "data": "synthetic", "config": build_config({"sample": base["sample"]}), "cpu_baseline": base,
+            "e2e": {"value": base["value"], "unit": "Mtriangles/s", "h2d_bytes_per_step": 0,
+                    "d2h_bytes_per_step": 0}, "gpu_launches": 0}))
+        return
+    import torch.distributed as dist
+    torch.cuda.set_device(local)
+    device = torch.device("cuda", local)
+    if world > 1:
+        import datetime
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600), device_id=device)
+    tri = scenes.sphere_field(SPHERES, LEVEL, seed=1)
+    n = tri.shape[0]
+    build_s, create_s, info = [], [], None
+    with ClockSampler(local) as clocks:
+        for k in range(args.warmup + args.steps):
+            if world > 1:
+                dist.barrier()
+            acc = Obvh(max_node_depth=DEPTH, max_pri_in_leaf=LEAF, builder=_lib.SG_BUILDER_GPU, device=local)
+            t0 = time.perf_counter()
+            acc.Build(tri)
+            t1 = time.perf_counter()
+            info = acc.info()
+            acc.Release()
+            if k >= args.warmup:
+                build_s.append(info["build_seconds"])
+                create_s.append(t1 - t0)
+    mean_build = max_over_ranks(statistics.mean(build_s), device)
+    mean_create = max_over_ranks(statistics.mean(create_s), device)
+    if rank != 0:
+        if world > 1:
+            dist.destroy_process_group()
+        return
+    tris_bytes = (n + 8) * 48
+    node_bytes = info["device_bytes"] - tris_bytes
+    shapes = info["interior_nodes"] + info["leaves"]
+    out = {
+        "metric": "Mtriangles/s BVH build", "value": round(world * n / mean_build / 1e6, 3), "unit": "Mtriangles/s",
+        "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(1e3 * mean_build, 3),
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": build_config({"depth": info["depth"], "interior_nodes": info["interior_nodes"],
+                                "leaves": info["leaves"], "split_rounds": info["build_rounds"]}),
+        "e2e": {"value": round(world * n / mean_create / 1e6, 3), "unit": "Mtriangles/s",
+                "h2d_bytes_per_step": int(n * 36 + node_bytes), "d2h_bytes_per_step": int(n * 4 + shapes * 40)},
+        "gpu_launches": info["build_launches"] * args.steps,
+        "roofline": None,
+        "clocks": clocks.summary(),
+    }
+    if not args.no_cpu_baseline:
+        out["cpu_baseline"] = sort_build_rate()
+        host = Obvh(max_node_depth=DEPTH, max_pri_in_leaf=LEAF, builder=_lib.SG_BUILDER_HOST, device=local)
+        host.Build(tri)
+        out["host_builder"] = {"value": round(n / host.info()["build_seconds"] / 1e6, 3), "unit": "Mtriangles/s",
+                               "cores": os.cpu_count(), "note": "this library's multithreaded C++ builder"}
+        host.Release()
+    print(json.dumps(out))
+    if world > 1:
+        dist.destroy_process_group()
+
+
 def main():
     p = argparse.ArgumentParser()
     p.add_argument("--gpus", type=int, default=1)
     p.add_argument("--steps", type=int, default=200)
     p.add_argument("--warmup", type=int, default=5)
     p.add_argument("--impl", choices=["ours", "reference"], default="ours")
-    p.add_argument("--workload", choices=["closest", "raycast", "pathtrace", "batched", "serve"], default="closest")
+    p.add_argument("--workload", choices=["closest", "raycast", "pathtrace", "batched", "serve", "build"],
+                   default="closest")
     p.add_argument("--requests", type=int, default=120, help="serve workload: requests per run")
     p.add_argument("--path-slots", type=int, default=1 << 20, help="serve workload: server path pool")
     p.add_argument("--loads", type=float, nargs="*", default=[0.5, 0.8, 1.0],
@@ -807,6 +928,8 @@ def main():
     args = p.parse_args()
     if args.workload == "pathtrace":
         run_pathtrace(args)
+    elif args.workload == "build":
+        run_build(args)
     elif args.workload == "serve":
         if args.impl == "reference":
             print(json.dumps({"impl": "reference", "unavailable": "serve workload: SORT renders one image per "

@@ -122,7 +122,9 @@ typedef struct {
     int32_t valid;           /* Accelerator::GetIsValid */
     float bbox[6];           /* enlarged scene box: min xyz, max xyz */
     int64_t device_bytes;    /* HBM held by the tree (nodes + triangles) */
-    double build_seconds;    /* host build time */
+    double build_seconds;    /* build time (host clock, whole build) */
+    int32_t build_rounds;    /* SG_BUILDER_GPU: split rounds (0 for the host builder) */
+    int32_t build_launches;  /* SG_BUILDER_GPU: its own kernels launched (CUB's prefix sums not counted) */
 } sg_scene_info;
 
 /* Traversal launch schedule (results never depend on it). */

@@ -53,6 +53,10 @@ class _Tree:
     def depth(self) -> int:
         return int(self.api._depth(self.h))
 
+    def build_seconds(self) -> float:
+        """Duration of SORT's Accelerator::Build for this tree (reference library only)."""
+        return float(self.api.L.sortref_build_seconds(self.h))
+
     def bbox(self) -> np.ndarray:
         b = np.empty(6, np.float32)
         self.api._bbox(self.h, b.ctypes.data)
@@ -163,6 +167,8 @@ class Reference:
         L.sortref_scene_create_mat.argtypes = [ctypes.c_int, _vp, ctypes.c_int, _vp, ctypes.c_int, ctypes.c_int,
                                                ctypes.c_int]
         L.sortref_trace_multi.argtypes = [_vp, _vp, _i64, _vp, _vp, _vp, _vp, _vp, _vp, ctypes.c_int]
+        L.sortref_build_seconds.restype = ctypes.c_double
+        L.sortref_build_seconds.argtypes = [_vp]
         self.L = L
         self._free, self._topo, self._depth = L.sortref_scene_destroy, L.sortref_topology, L.sortref_depth
         self._bbox, self._closest, self._any = L.sortref_scene_bbox, L.sortref_trace_closest, L.sortref_trace_any

@@ -26,6 +26,7 @@
 #include <algorithm>
 #include <atomic>
 #include <cfloat>
+#include <chrono>
 #include <cmath>
 #include <cstdint>
 #include <cstring>
@@ -142,6 +143,7 @@ struct RefScene {
     std::unordered_map<const Primitive*, int32_t> index_of;
     std::vector<const Primitive*> prims;
     std::vector<std::unique_ptr<TaggedMaterial>> materials;
+    double build_seconds = 0.0;  // Accelerator::Build alone
 };
 
 }  // namespace
@@ -262,9 +264,13 @@ void* sortref_scene_create_mat(int width, const float* tri, int ntri, const int3
         rs->scene.m_accelerator.reset(harness_make_qbvh((unsigned)max_depth, (unsigned)max_leaf));
     else
         rs->scene.m_accelerator.reset(harness_make_obvh((unsigned)max_depth, (unsigned)max_leaf));
+    const auto t0 = std::chrono::steady_clock::now();
     rs->scene.m_accelerator->Build(rs->scene);
+    rs->build_seconds = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
     return rs;
 }
+
+double sortref_build_seconds(void* h) { return ((RefScene*)h)->build_seconds; }
 
 void* sortref_scene_create(int width, const float* tri, int ntri, int max_depth, int max_leaf) {
     return sortref_scene_create_mat(width, tri, ntri, nullptr, 0, max_depth, max_leaf);

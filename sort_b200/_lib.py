@@ -55,7 +55,8 @@ class SceneInfo(ctypes.Structure):
     _fields_ = [("triangles", ctypes.c_int64), ("interior_nodes", ctypes.c_int64), ("leaves", ctypes.c_int64),
                 ("depth", ctypes.c_int32), ("width", ctypes.c_int32), ("node_format", ctypes.c_int32),
                 ("valid", ctypes.c_int32), ("bbox", ctypes.c_float * 6), ("device_bytes", ctypes.c_int64),
-                ("build_seconds", ctypes.c_double)]
+                ("build_seconds", ctypes.c_double), ("build_rounds", ctypes.c_int32),
+                ("build_launches", ctypes.c_int32)]
 
 
 class MultiHits(ctypes.Structure):

@@ -257,7 +257,8 @@ class Accelerator:
         i = self._info
         return dict(triangles=i.triangles, interior_nodes=i.interior_nodes, leaves=i.leaves, depth=i.depth,
                     width=i.width, node_format=i.node_format, valid=bool(i.valid), bbox=tuple(i.bbox),
-                    device_bytes=i.device_bytes, build_seconds=i.build_seconds)
+                    device_bytes=i.device_bytes, build_seconds=i.build_seconds,
+                    build_rounds=i.build_rounds, build_launches=i.build_launches)
 
     def topology(self) -> np.ndarray:
         self._require()

@@ -323,6 +323,8 @@ sg_status sg_scene_info_get(const sg_scene* s, sg_scene_info* info) {
     }
     info->device_bytes = s->device_bytes;
     info->build_seconds = s->build_seconds;
+    info->build_rounds = s->tree.rounds;
+    info->build_launches = s->tree.launches;
     return SG_OK;
 }
 

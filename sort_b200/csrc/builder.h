@@ -57,6 +57,7 @@ struct BuiltTree {
     // (layout.h), leaf order plus the zero pad slots, already on the build's
     // device. The receiver owns it (cudaFree).
     float4* d_tris = nullptr;
+    int rounds = 0, launches = 0;  // build_tree_gpu's split rounds and kernel launches
     int64_t leaves = 0;
     int64_t interior() const { return width ? int64_t(child.size()) / width : 0; }
 };

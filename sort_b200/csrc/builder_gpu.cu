@@ -38,7 +38,9 @@
 
 #include <algorithm>
 #include <cfloat>
+#include <cstdint>
 #include <cstring>
+#include <mutex>
 #include <stdexcept>
 #include <string>
 #include <vector>
@@ -77,6 +79,16 @@ struct RangeTask {
     int split;           // 1 = partition this range
     unsigned left;       // primitives passing the predicate
     int half_box[2][6];  // primitive boxes of the left (passing) and right halves
+};
+
+// Device-resident build state: the rounds need no host round trip.
+struct BuildState {
+    int na;         // nodes under construction this round (= ranges split)
+    int shapes;     // shape nodes written so far
+    int depth_max;  // Fbvh::m_depth
+    int rounds;     // rounds that split something
+    int next;       // this round's results, consumed by k_advance
+    int new_shapes;
 };
 
 __device__ __forceinline__ int find_range(const int64_t* __restrict__ starts, const int64_t* __restrict__ ends,
@@ -176,13 +188,14 @@ __global__ void __launch_bounds__(256) k_scene_box(int64_t n, const float* __res
 
 // Range id of every primitive (-1 outside the round's ranges) and centroid bounds.
 __global__ void __launch_bounds__(256) k_bounds(int64_t n, const int64_t* __restrict__ starts,
-                                                const int64_t* __restrict__ ends, int nr, const float* __restrict__ cx,
+                                                const int64_t* __restrict__ ends, const BuildState* __restrict__ bs,
+                                                const float* __restrict__ cx,
                                                 const float* __restrict__ cy, const float* __restrict__ cz,
                                                 int* __restrict__ rid, RangeTask* __restrict__ rt) {
     __shared__ int sr, sbox[6];
     const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     const bool in = i < n;
-    const int r = in ? find_range(starts, ends, nr, i) : -1;
+    const int r = in ? find_range(starts, ends, bs->na, i) : -1;
     if (in) rid[i] = r;
     if (threadIdx.x == 0) empty_box(sbox);
     const bool one = block_in_one_range(r, sr);
@@ -281,9 +294,9 @@ __global__ void __launch_bounds__(256) k_bin(int64_t n, const int* __restrict__ 
 }
 
 // The SAH sweep of pick_best_split and splitNode's decision, one thread per range.
-__global__ void k_sweep(int nr, RangeTask* __restrict__ rt, int max_leaf) {
+__global__ void k_sweep(const BuildState* __restrict__ bs, RangeTask* __restrict__ rt, int max_leaf) {
     const int r = blockIdx.x * blockDim.x + threadIdx.x;
-    if (r >= nr) return;
+    if (r >= bs->na) return;
     RangeTask& t = rt[r];
     const unsigned n = (unsigned)(t.e - t.s);
     t.split = 0;
@@ -463,20 +476,70 @@ void check(cudaError_t e, const char* what) {
     if (e != cudaSuccess) throw std::runtime_error(std::string("GPU build: ") + what + ": " + cudaGetErrorString(e));
 }
 
+// Scratch memory: a private stream-ordered pool per device. Builds allocate
+// and free on their stream without synchronising the device, and a build
+// reuses the memory the previous one mapped (up to kKeepBytes stay mapped
+// between builds), so back-to-back scene builds do not pay for the mapping.
+constexpr uint64_t kKeepBytes = uint64_t(16) << 30;
+
+cudaMemPool_t scratch_pool(int device) {
+    static std::mutex lock;
+    static std::vector<cudaMemPool_t> pools;
+    std::lock_guard<std::mutex> g(lock);
+    if (device < 0) throw std::invalid_argument("device out of range");
+    if (pools.size() <= size_t(device)) pools.resize(size_t(device) + 1, nullptr);
+    if (!pools[size_t(device)]) {
+        cudaMemPoolProps props{};
+        props.allocType = cudaMemAllocationTypePinned;
+        props.location.type = cudaMemLocationTypeDevice;
+        props.location.id = device;
+        cudaMemPool_t pool = nullptr;
+        check(cudaMemPoolCreate(&pool, &props), "cudaMemPoolCreate");
+        uint64_t keep = UINT64_MAX;  // release only when a build ends (trim below)
+        check(cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep), "pool threshold");
+        pools[size_t(device)] = pool;
+    }
+    return pools[size_t(device)];
+}
+
+// The pool and stream that DevBufs declared during a build allocate on.
+struct Scratch {
+    cudaMemPool_t pool = nullptr;
+    cudaStream_t st = nullptr;
+};
+thread_local Scratch scratch;
+
+// Binds DevBufs to (pool, stream) for its lifetime; when it ends (after the
+// DevBufs declared later have freed), waits for the stream and trims the pool.
+struct ScratchScope {
+    Scratch saved;
+    ScratchScope(cudaMemPool_t pool, cudaStream_t st) : saved(scratch) { scratch = Scratch{pool, st}; }
+    ~ScratchScope() {
+        cudaStreamSynchronize(scratch.st);
+        cudaMemPoolTrimTo(scratch.pool, kKeepBytes);
+        scratch = saved;
+    }
+};
+
 template <class T>
 struct DevBuf {
     T* p = nullptr;
     size_t n = 0;
+    cudaMemPool_t pool = scratch.pool;
+    cudaStream_t st = scratch.st;
+    // Grows by at least half its size; the old contents are not kept.
     void alloc(size_t count) {
         if (count <= n) return;
-        if (p) cudaFree(p);
+        count = std::max(count, n + n / 2);
+        if (p) cudaFreeAsync(p, st);
         p = nullptr;
         n = 0;
-        check(cudaMalloc(&p, std::max<size_t>(count, 1) * sizeof(T)), "cudaMalloc");
+        check(cudaMallocFromPoolAsync(reinterpret_cast<void**>(&p), std::max<size_t>(count, 1) * sizeof(T), pool, st),
+              "device allocation");
         n = count;
     }
     ~DevBuf() {
-        if (p) cudaFree(p);
+        if (p) cudaFreeAsync(p, st);
     }
 };
 
@@ -504,13 +567,15 @@ struct DRange {
     float mn[3], mx[3];
 };
 
-// A node under construction: SORT's to_split list (fifo) and done list.
+// A node under construction: SORT's to_split list (fifo) and done list. The
+// list holds at most W ranges at a time (fewer than W before a split, one
+// more after it), so the fifo is a ring of 8 indexed by running counters.
 struct DNode {
     int32_t id;  // shape index
     int32_t depth;
     float area;  // half_area of the node's box (SAH normaliser)
     int32_t head, tail, ndone;
-    DRange fifo[15];  // 1 + 2 * (W - 1) entries at most
+    DRange fifo[8];
     DRange done[8];
 };
 
@@ -518,13 +583,6 @@ struct DNode {
 struct DShape {
     int32_t off, cnt, first_kid, nkids;
     float mn[3], mx[3];  // box of the primitive range (the parent's child box)
-};
-
-struct RoundSummary {
-    int next;    // nodes under construction in the next round
-    int shapes;  // shape nodes this round adds
-    int depth_max;
-    int pad;
 };
 
 __device__ __forceinline__ bool starts_node(const DRange& x, int depth, int max_leaf, int max_depth) {
@@ -543,12 +601,12 @@ __device__ __forceinline__ DRange make_range(int32_t s, int32_t e, const int (&i
 }
 
 // The front range of every node is split this round (range r belongs to node r).
-__global__ void k_node_ranges(int na, const DNode* __restrict__ nodes, RangeTask* __restrict__ rt,
-                              int64_t* __restrict__ starts, int64_t* __restrict__ ends) {
+__global__ void k_node_ranges(const BuildState* __restrict__ bs, const DNode* __restrict__ nodes,
+                              RangeTask* __restrict__ rt, int64_t* __restrict__ starts, int64_t* __restrict__ ends) {
     const int r = blockIdx.x * blockDim.x + threadIdx.x;
-    if (r >= na) return;
+    if (r >= bs->na) return;
     const DNode& nd = nodes[r];
-    const DRange& x = nd.fifo[nd.head];
+    const DRange& x = nd.fifo[nd.head & 7];
     RangeTask& t = rt[r];
     t.s = starts[r] = x.s;
     t.e = ends[r] = x.e;
@@ -568,21 +626,21 @@ __global__ void k_node_ranges(int na, const DNode* __restrict__ nodes, RangeTask
 
 // Applies the round's split to every node (SORT's loop body) and counts what
 // the node hands to the next round: itself, or its children that are nodes.
-__global__ void k_node_apply(int na, DNode* __restrict__ nodes, const RangeTask* __restrict__ rt, int W,
-                             int max_leaf, int max_depth, int* __restrict__ cnt_next, int* __restrict__ cnt_shape,
-                             RoundSummary* __restrict__ sum) {
+__global__ void k_node_apply(BuildState* __restrict__ bs, DNode* __restrict__ nodes, const RangeTask* __restrict__ rt,
+                             int W, int max_leaf, int max_depth, int* __restrict__ cnt_next,
+                             int* __restrict__ cnt_shape) {
     const int r = blockIdx.x * blockDim.x + threadIdx.x;
-    if (r >= na) return;
+    if (r >= bs->na) return;
     DNode& nd = nodes[r];
     const RangeTask& t = rt[r];
-    const DRange x = nd.fifo[nd.head];
+    const DRange x = nd.fifo[nd.head & 7];
     const int32_t mid = x.s + int32_t(t.left);
     int head = nd.head + 1, tail = nd.tail, ndone = nd.ndone;
     if (!t.split || mid == x.s || mid == x.e) {
         nd.done[ndone++] = x;
     } else {
-        nd.fifo[tail++] = make_range(x.s, mid, t.half_box[0]);
-        nd.fifo[tail++] = make_range(mid, x.e, t.half_box[1]);
+        nd.fifo[tail++ & 7] = make_range(x.s, mid, t.half_box[0]);
+        nd.fifo[tail++ & 7] = make_range(mid, x.e, t.half_box[1]);
     }
     nd.head = head;
     nd.tail = tail;
@@ -592,12 +650,12 @@ __global__ void k_node_apply(int na, DNode* __restrict__ nodes, const RangeTask*
     if (head != tail && total < W) {
         next = 1;
     } else if (total == 1) {
-        atomicMax(&sum->depth_max, nd.depth);
+        atomicMax(&bs->depth_max, nd.depth);
     } else {
         shapes = total;
         int kid_max = 0;
         for (int q = head; q < tail; ++q) {
-            if (starts_node(nd.fifo[q], nd.depth + 1, max_leaf, max_depth))
+            if (starts_node(nd.fifo[q & 7], nd.depth + 1, max_leaf, max_depth))
                 ++next;
             else
                 kid_max = nd.depth + 1;
@@ -608,28 +666,29 @@ __global__ void k_node_apply(int na, DNode* __restrict__ nodes, const RangeTask*
             else
                 kid_max = nd.depth + 1;
         }
-        if (kid_max) atomicMax(&sum->depth_max, kid_max);
+        if (kid_max) atomicMax(&bs->depth_max, kid_max);
     }
     cnt_next[r] = next;
     cnt_shape[r] = shapes;
 }
 
-__global__ void k_summary(int na, const int* __restrict__ cnt_next, const int* __restrict__ off_next,
-                          const int* __restrict__ cnt_shape, const int* __restrict__ off_shape,
-                          RoundSummary* __restrict__ sum) {
-    sum->next = off_next[na - 1] + cnt_next[na - 1];
-    sum->shapes = off_shape[na - 1] + cnt_shape[na - 1];
+__global__ void k_summary(BuildState* __restrict__ bs, const int* __restrict__ cnt_next,
+                          const int* __restrict__ off_next, const int* __restrict__ cnt_shape,
+                          const int* __restrict__ off_shape) {
+    const int na = bs->na;
+    bs->next = na > 0 ? off_next[na - 1] + cnt_next[na - 1] : 0;
+    bs->new_shapes = na > 0 ? off_shape[na - 1] + cnt_shape[na - 1] : 0;
 }
 
 // Finished nodes write their children (SORT's child order: the remaining list,
 // then the done list) as shape nodes; the next round's nodes are the
 // continuing ones and the new children, in primitive-range order.
-__global__ void k_node_commit(int na, const DNode* __restrict__ cur, const int* __restrict__ off_next,
-                              const int* __restrict__ off_shape, const int* __restrict__ cnt_shape, int shape_base,
-                              int W, int max_leaf, int max_depth, DShape* __restrict__ shapes,
-                              DNode* __restrict__ next) {
+__global__ void k_node_commit(const BuildState* __restrict__ bs, const DNode* __restrict__ cur,
+                              const int* __restrict__ off_next, const int* __restrict__ off_shape,
+                              const int* __restrict__ cnt_shape, int W, int max_leaf, int max_depth,
+                              DShape* __restrict__ shapes, DNode* __restrict__ next) {
     const int r = blockIdx.x * blockDim.x + threadIdx.x;
-    if (r >= na) return;
+    if (r >= bs->na) return;
     const DNode& nd = cur[r];
     const int total = (nd.tail - nd.head) + nd.ndone;
     int o = off_next[r];
@@ -639,12 +698,12 @@ __global__ void k_node_commit(int na, const DNode* __restrict__ cur, const int* 
     }
     const int m = cnt_shape[r];
     if (m == 0) return;  // a single range: the node is a leaf
-    const int first = shape_base + off_shape[r];
+    const int first = bs->shapes + off_shape[r];
     shapes[nd.id].first_kid = first;
     shapes[nd.id].nkids = m;
     DRange ks[8];
     int k = 0;
-    for (int q = nd.head; q < nd.tail; ++q) ks[k++] = nd.fifo[q];
+    for (int q = nd.head; q < nd.tail; ++q) ks[k++] = nd.fifo[q & 7];
     for (int q = 0; q < nd.ndone; ++q) ks[k++] = nd.done[q];
     int ord[8];
     for (int q = 0; q < m; ++q) {
@@ -677,6 +736,13 @@ __global__ void k_node_commit(int na, const DNode* __restrict__ cur, const int* 
         c.ndone = 0;
         c.fifo[0] = x;
     }
+}
+
+__global__ void k_advance(BuildState* __restrict__ bs) {
+    if (bs->na > 0) ++bs->rounds;
+    bs->shapes += bs->new_shapes;
+    bs->na = bs->next;
+    bs->next = bs->new_shapes = 0;
 }
 
 unsigned grid(int64_t n, int t = 256) { return (unsigned)std::max<int64_t>(1, (n + t - 1) / t); }
@@ -733,6 +799,7 @@ BuiltTree build_tree_gpu(const float* tri, int64_t ntri, const BuildParams& p, i
     } restore{prev};
     Stream stream;
     const cudaStream_t st = stream.s;
+    ScratchScope scope(scratch_pool(device), st);  // declared before every DevBuf: outlives them
 
     DevBuf<float> d_tri, d_cx, d_cy, d_cz, d_pb;
     DevBuf<int32_t> d_idx;
@@ -742,10 +809,10 @@ BuiltTree build_tree_gpu(const float* tri, int64_t ntri, const BuildParams& p, i
     DevBuf<DNode> d_cur, d_next;
     DevBuf<DShape> d_shapes;
     DevBuf<int> d_cnt_next, d_off_next, d_cnt_shape, d_off_shape;
-    DevBuf<RoundSummary> d_sum;
+    DevBuf<BuildState> d_state;
     DevBuf<unsigned char> d_temp;
     PinnedBuf<int> h_scene;
-    PinnedBuf<RoundSummary> h_sum;
+    PinnedBuf<BuildState> h_state;
     const int64_t nn = std::max<int64_t>(n, 1);
     d_tri.alloc(size_t(nn) * 9);
     d_cx.alloc(size_t(nn));
@@ -761,9 +828,9 @@ BuiltTree build_tree_gpu(const float* tri, int64_t ntri, const BuildParams& p, i
     d_pl.alloc(size_t(nn));
     d_pr.alloc(size_t(nn));
     d_scene.alloc(6);
-    d_sum.alloc(1);
+    d_state.alloc(1);
     h_scene.alloc(6);
-    h_sum.alloc(1);
+    h_state.alloc(1);
 
     // Scene box (core/scene.cpp:146-154): union of the primitive boxes, enlarged by 0.1%.
     Box scene;
@@ -790,24 +857,39 @@ BuiltTree build_tree_gpu(const float* tri, int64_t ntri, const BuildParams& p, i
     t.scene = scene;
     if (n == 0) return t;
 
-    size_t temp_bytes = 0;
+    // Node-sized buffers at their bounds: nodes under construction own disjoint
+    // ranges of more than max_leaf primitives; the tree has fewer than 2n nodes.
+    const int64_t cap = std::min<int64_t>(n, n / (int64_t(p.max_leaf) + 1) + 1);
+    d_cur.alloc(size_t(cap));
+    d_next.alloc(size_t(cap));
+    d_rt.alloc(size_t(cap));
+    d_starts.alloc(size_t(cap));
+    d_ends.alloc(size_t(cap));
+    d_cnt_next.alloc(size_t(cap));
+    d_off_next.alloc(size_t(cap));
+    d_cnt_shape.alloc(size_t(cap));
+    d_off_shape.alloc(size_t(cap));
+    d_shapes.alloc(size_t(2 * n));
+    // The node prefix sums run over all cap entries: the ones past a round's
+    // node count must hold small values (zero, or counts of earlier rounds).
+    check(cudaMemsetAsync(d_cnt_next.p, 0, size_t(cap) * sizeof(int), st), "clear counts");
+    check(cudaMemsetAsync(d_cnt_shape.p, 0, size_t(cap) * sizeof(int), st), "clear counts");
+
+    size_t temp_bytes = 0, temp_nodes = 0;
     check(cub::DeviceScan::ExclusiveSum(nullptr, temp_bytes, d_ml.p, d_sl.p, (int)n, st), "scan size");
+    check(cub::DeviceScan::ExclusiveSum(nullptr, temp_nodes, d_cnt_next.p, d_off_next.p, (int)cap, st), "scan size");
+    temp_bytes = std::max(temp_bytes, temp_nodes);
     d_temp.alloc(temp_bytes);
 
     // The root shape, and the root node unless splitNode returns at once.
-    int shape_count = 1;
-    d_shapes.alloc(size_t(std::max<int64_t>(1024, n / 4)));
     {
         DShape root{0, int32_t(n), -1, 0, {scene.mn[0], scene.mn[1], scene.mn[2]},
                     {scene.mx[0], scene.mx[1], scene.mx[2]}};
         check(cudaMemcpyAsync(d_shapes.p, &root, sizeof(root), cudaMemcpyHostToDevice, st), "root");
     }
     const bool root_node = n > p.max_leaf && p.max_depth != 1;
-    int na = root_node ? 1 : 0;
-    *h_sum.p = RoundSummary{0, 0, root_node ? 0 : 1, 0};
-    check(cudaMemcpyAsync(d_sum.p, h_sum.p, sizeof(RoundSummary), cudaMemcpyHostToDevice, st), "summary");
-    d_cur.alloc(4096);
-    d_next.alloc(4096);
+    *h_state.p = BuildState{root_node ? 1 : 0, 1, root_node ? 0 : 1, 0, 0, 0};
+    check(cudaMemcpyAsync(d_state.p, h_state.p, sizeof(BuildState), cudaMemcpyHostToDevice, st), "state");
     if (root_node) {
         DNode root{};
         root.id = 0;
@@ -820,53 +902,52 @@ BuiltTree build_tree_gpu(const float* tri, int64_t ntri, const BuildParams& p, i
     }
     check(cudaStreamSynchronize(st), "root");
 
-    while (na > 0) {
-        d_rt.alloc(size_t(na));
-        d_starts.alloc(size_t(na));
-        d_ends.alloc(size_t(na));
-        d_cnt_next.alloc(size_t(na));
-        d_off_next.alloc(size_t(na));
-        d_cnt_shape.alloc(size_t(na));
-        d_off_shape.alloc(size_t(na));
-        k_node_ranges<<<grid(na, 128), 128, 0, st>>>(na, d_cur.p, d_rt.p, d_starts.p, d_ends.p);
-        k_bounds<<<grid(n), 256, 0, st>>>(n, d_starts.p, d_ends.p, na, d_cx.p, d_cy.p, d_cz.p, d_rid.p, d_rt.p);
-        k_bin<<<grid(n), 256, 0, st>>>(n, d_rid.p, d_cx.p, d_cy.p, d_cz.p, d_pb.p, d_rt.p);
-        k_sweep<<<grid(na, 128), 128, 0, st>>>(na, d_rt.p, p.max_leaf);
-        k_count_left<<<grid(n), 256, 0, st>>>(n, d_rid.p, d_cx.p, d_cy.p, d_cz.p, d_pb.p, d_rt.p);
-        k_misplaced<<<grid(n), 256, 0, st>>>(n, d_rid.p, d_cx.p, d_cy.p, d_cz.p, d_rt.p, d_ml.p, d_mr.p);
-        check(cudaGetLastError(), "split kernels");
-        check(cub::DeviceScan::ExclusiveSum(d_temp.p, temp_bytes, d_ml.p, d_sl.p, (int)n, st), "scan");
-        check(cub::DeviceScan::ExclusiveSum(d_temp.p, temp_bytes, d_mr.p, d_sr.p, (int)n, st), "scan");
-        k_pairs<<<grid(n), 256, 0, st>>>(n, d_rid.p, d_rt.p, d_ml.p, d_mr.p, d_sl.p, d_sr.p, d_pl.p, d_pr.p);
-        k_swap<<<grid((n + 1) / 2), 256, 0, st>>>(n, d_sl.p, d_ml.p, d_pl.p, d_pr.p, d_cx.p, d_cy.p, d_cz.p, d_pb.p,
-                                                  d_idx.p);
-        k_node_apply<<<grid(na, 128), 128, 0, st>>>(na, d_cur.p, d_rt.p, W, p.max_leaf, p.max_depth, d_cnt_next.p,
-                                                    d_cnt_shape.p, d_sum.p);
-        check(cudaGetLastError(), "partition kernels");
-        check(cub::DeviceScan::ExclusiveSum(d_temp.p, temp_bytes, d_cnt_next.p, d_off_next.p, na, st), "scan");
-        check(cub::DeviceScan::ExclusiveSum(d_temp.p, temp_bytes, d_cnt_shape.p, d_off_shape.p, na, st), "scan");
-        k_summary<<<1, 1, 0, st>>>(na, d_cnt_next.p, d_off_next.p, d_cnt_shape.p, d_off_shape.p, d_sum.p);
-        check(cudaMemcpyAsync(h_sum.p, d_sum.p, sizeof(RoundSummary), cudaMemcpyDeviceToHost, st), "summary");
-        check(cudaStreamSynchronize(st), "split round");
-        const RoundSummary s = *h_sum.p;
-        if (size_t(shape_count) + size_t(s.shapes) > d_shapes.n) {
-            DevBuf<DShape> bigger;
-            bigger.alloc(std::max(size_t(shape_count) + size_t(s.shapes), 2 * d_shapes.n));
-            check(cudaMemcpyAsync(bigger.p, d_shapes.p, size_t(shape_count) * sizeof(DShape),
-                                  cudaMemcpyDeviceToDevice, st),
-                  "grow shapes");
-            check(cudaStreamSynchronize(st), "grow shapes");
-            swap_bufs(d_shapes, bigger);
+    // Rounds are queued in groups without a host round trip (a round with no
+    // node left does no work); the host reads the state after each group. A
+    // node splits at most W - 1 times and the depth is capped, which bounds
+    // the rounds.
+    constexpr int kGroup = 8;
+    const int64_t max_rounds = int64_t(W - 1) * p.max_depth + 1;
+    const unsigned ng = grid(cap, 128);
+    int64_t queued = 0;
+    while (root_node) {
+        for (int g = 0; g < kGroup; ++g) {
+            k_node_ranges<<<ng, 128, 0, st>>>(d_state.p, d_cur.p, d_rt.p, d_starts.p, d_ends.p);
+            k_bounds<<<grid(n), 256, 0, st>>>(n, d_starts.p, d_ends.p, d_state.p, d_cx.p, d_cy.p, d_cz.p, d_rid.p,
+                                              d_rt.p);
+            k_bin<<<grid(n), 256, 0, st>>>(n, d_rid.p, d_cx.p, d_cy.p, d_cz.p, d_pb.p, d_rt.p);
+            k_sweep<<<ng, 128, 0, st>>>(d_state.p, d_rt.p, p.max_leaf);
+            k_count_left<<<grid(n), 256, 0, st>>>(n, d_rid.p, d_cx.p, d_cy.p, d_cz.p, d_pb.p, d_rt.p);
+            k_misplaced<<<grid(n), 256, 0, st>>>(n, d_rid.p, d_cx.p, d_cy.p, d_cz.p, d_rt.p, d_ml.p, d_mr.p);
+            check(cudaGetLastError(), "split kernels");
+            check(cub::DeviceScan::ExclusiveSum(d_temp.p, temp_bytes, d_ml.p, d_sl.p, (int)n, st), "scan");
+            check(cub::DeviceScan::ExclusiveSum(d_temp.p, temp_bytes, d_mr.p, d_sr.p, (int)n, st), "scan");
+            k_pairs<<<grid(n), 256, 0, st>>>(n, d_rid.p, d_rt.p, d_ml.p, d_mr.p, d_sl.p, d_sr.p, d_pl.p, d_pr.p);
+            k_swap<<<grid((n + 1) / 2), 256, 0, st>>>(n, d_sl.p, d_ml.p, d_pl.p, d_pr.p, d_cx.p, d_cy.p, d_cz.p,
+                                                      d_pb.p, d_idx.p);
+            k_node_apply<<<ng, 128, 0, st>>>(d_state.p, d_cur.p, d_rt.p, W, p.max_leaf, p.max_depth, d_cnt_next.p,
+                                             d_cnt_shape.p);
+            check(cudaGetLastError(), "partition kernels");
+            check(cub::DeviceScan::ExclusiveSum(d_temp.p, temp_bytes, d_cnt_next.p, d_off_next.p, (int)cap, st),
+                  "scan");
+            check(cub::DeviceScan::ExclusiveSum(d_temp.p, temp_bytes, d_cnt_shape.p, d_off_shape.p, (int)cap, st),
+                  "scan");
+            k_summary<<<1, 1, 0, st>>>(d_state.p, d_cnt_next.p, d_off_next.p, d_cnt_shape.p, d_off_shape.p);
+            k_node_commit<<<ng, 128, 0, st>>>(d_state.p, d_cur.p, d_off_next.p, d_off_shape.p, d_cnt_shape.p, W,
+                                              p.max_leaf, p.max_depth, d_shapes.p, d_next.p);
+            k_advance<<<1, 1, 0, st>>>(d_state.p);
+            check(cudaGetLastError(), "node commit");
+            swap_bufs(d_cur, d_next);
         }
-        if (size_t(s.next) > d_next.n) d_next.alloc(std::max(size_t(s.next), 2 * d_next.n));
-        k_node_commit<<<grid(na, 128), 128, 0, st>>>(na, d_cur.p, d_off_next.p, d_off_shape.p, d_cnt_shape.p,
-                                                     shape_count, W, p.max_leaf, p.max_depth, d_shapes.p, d_next.p);
-        check(cudaGetLastError(), "node commit");
-        swap_bufs(d_cur, d_next);
-        shape_count += s.shapes;
-        na = s.next;
+        queued += kGroup;
+        check(cudaMemcpyAsync(h_state.p, d_state.p, sizeof(BuildState), cudaMemcpyDeviceToHost, st), "state");
+        check(cudaStreamSynchronize(st), "split rounds");
+        if (h_state.p->na == 0) break;
+        if (queued > max_rounds) throw std::runtime_error("GPU build: the split rounds did not finish");
     }
-    t.depth = h_sum.p->depth_max;
+    const BuildState fin = *h_state.p;
+    const int shape_count = fin.shapes;
+    t.depth = fin.depth_max;
 
     // Shapes and the final permutation (leaf order) to the host.
     std::vector<DShape> shape(static_cast<size_t>(shape_count));
@@ -953,6 +1034,10 @@ BuiltTree build_tree_gpu(const float* tri, int64_t ntri, const BuildParams& p, i
         check(e, "triangle records");
     }
     t.d_tris = d_tris;
+    // This file's kernels: setup and scene box, 13 per queued round, the triangle
+    // records (the prefix sums are CUB's, four per round, not counted).
+    t.rounds = fin.rounds;
+    t.launches = int(3 + 13 * queued);
     return t;
 }
 
