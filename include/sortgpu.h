@@ -201,8 +201,8 @@ sg_status sg_trace_any_host(const sg_scene* scene, const float* rays8, int64_t n
 
 /* sg_trace_closest_host without any device allocation. No counterpart in SORT:
  * it exists for callers that must not call cudaMalloc while they query (a
- * stream under graph capture, a host that owns the GPU memory budget, a
- * real-time loop). Rays and hits are staged in a 24 MiB array compiled into
+ * host that owns the whole GPU memory budget, a real-time loop that must not
+ * take the allocator's locks or wait on an implicit synchronisation). Rays and hits are staged in a 24 MiB array compiled into
  * the library, held on every GPU that loads it until exit; at most 524,288 rays
  * per call (SG_ERR_LIMIT beyond). All calls share that array, so calls whose
  * work overlaps on the GPU race. The first call on a device looks up the

@@ -1,10 +1,10 @@
 // sg_trace_closest_host_static: the host-buffer closest-hit query without any
 // device allocation.
 //
-// Some callers cannot call cudaMalloc at query time: code running while a CUDA
-// stream is being captured into a graph, hosts that hand the whole GPU memory
-// budget to their own allocator up front, or real-time loops that must not
-// take the allocator's locks or trigger an implicit device synchronisation.
+// Some callers cannot call cudaMalloc at query time: hosts that hand the whole
+// GPU memory budget to their own allocator up front, so nothing is left for a
+// library to take, or real-time loops that must not take the allocator's locks
+// or trigger the implicit device synchronisation a cudaFree brings.
 // sg_trace_closest_host stages rays and hits in a device buffer it grows with
 // cudaMalloc on demand; this entry point stages them in a fixed array compiled
 // into the library instead, so a call allocates and frees nothing.

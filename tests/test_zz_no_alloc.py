@@ -1,8 +1,8 @@
 """sg_trace_closest_host_static: the allocation-free host-buffer query.
 
-Callers that cannot call cudaMalloc while they query (a stream being captured
-into a graph, a host that owns the whole GPU memory budget, a real-time loop)
-use this entry point; it stages rays and hits in an array compiled into the
+Callers that cannot call cudaMalloc while they query (a host that owns the
+whole GPU memory budget, a real-time loop that must not take the allocator's
+locks) use this entry point; it stages rays and hits in an array compiled into the
 library. Its results must equal sg_trace_closest_host's bit for bit, on two
 calls in a row (the second call reuses the array the first one left behind).
 This file is collected last.
