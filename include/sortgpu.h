@@ -38,6 +38,14 @@
  *                     the same queries on host buffers, with the host<->device
  *                     copies done inside the call (what a caller that holds rays in
  *                     host memory, like SORT's integrators, binds).
+ *   sg_trace_multi / sg_trace_multi_host
+ *                     Accelerator::GetIntersect(const Ray&, BSSRDFIntersections&,
+ *                     RenderContext&, StringID) (accel/accelerator.h:122), the
+ *                     BSSRDF probe query, for a batch.
+ *   sg_trace_attenuation / sg_trace_attenuation_host
+ *                     Scene::GetAttenuation (core/scene.cpp:192-208) with
+ *                     Accelerator::GetAttenuation (accel/accelerator.cpp:26-69) on
+ *                     scenes with transparent materials (ENABLE_TRANSPARENT_SHADOW).
  *
  * Semantics carried over from SORT:
  *   - hit identity is the primitive's index in input order (SORT returns a
@@ -186,6 +194,30 @@ sg_status sg_trace_multi(const sg_scene* scene, const sg_rays* rays, int64_t n, 
 sg_status sg_scene_set_materials(sg_scene* scene, const int32_t* material, int64_t n);
 sg_status sg_trace_multi_host(const sg_scene* scene, const float* rays8, int64_t n, const int32_t* ray_material,
                               int32_t* count, int32_t* prim, float* t, float* u, float* v);
+
+/* Transparent-shadow query: Scene::GetAttenuation (core/scene.cpp:192-208)
+ * over Accelerator::GetAttenuation (accel/accelerator.cpp:26-69) and Fbvh's
+ * query_shadow traversal (accel/fast_bvh.hpp:345-370). Per ray, from its
+ * [tmin, tmax] segment: find the nearest hit, leaving early when a SIMD pack's
+ * nearest hit is on an opaque material (then the attenuation is 0); on a
+ * transparent hit multiply by the material's transparency (a black one is
+ * returned as it is) and restart at the hit point with tmin 0.001 and
+ * tmax - t; no hit ends the loop. attenuation[0..n), [n..2n), [2n..3n): r, g, b.
+ * Primitive materials come from sg_scene_set_materials; materials[nmat] is a
+ * device array for sg_trace_attenuation, a host array for the _host form. A
+ * ray that crosses more than 4096 transparent surfaces stops there (reported
+ * as SG_ERR_LIMIT); a primitive material id outside [0, nmat) counts as opaque
+ * (reported as SG_ERR_INVALID_ARGUMENT). The _host form reports both; the
+ * device form records them in the scene's status word, which the next
+ * host-buffer call on that scene reports. */
+typedef struct {
+    int32_t transparent; /* MaterialBase::HasTransparency (material/material.h:100) */
+    float rgb[3];        /* MaterialBase::EvaluateTransparency (material/material.h:85), constant per material */
+} sg_transparency;
+sg_status sg_trace_attenuation(const sg_scene* scene, const sg_rays* rays, int64_t n, const sg_transparency* materials,
+                               int32_t nmat, float* attenuation, void* stream);
+sg_status sg_trace_attenuation_host(const sg_scene* scene, const float* rays8, int64_t n,
+                                    const sg_transparency* materials, int32_t nmat, float* attenuation);
 
 /* Counts over one batch (synchronises the stream): interior nodes box-tested and
  * primitives tested, the latter counted per leaf entered as SORT's

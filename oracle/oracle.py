@@ -53,6 +53,14 @@ class _Tree:
     def depth(self) -> int:
         return int(self.api._depth(self.h))
 
+    def attenuation(self, rays: np.ndarray, threads: int = 0) -> np.ndarray:
+        """Scene::GetAttenuation per ray (reference library only): (3, n) rgb."""
+        r = np.ascontiguousarray(rays, np.float32)
+        n = r.shape[1]
+        out = np.empty((3, n), np.float32)
+        self.api.L.sortref_trace_attenuation(self.h, r.ctypes.data, n, out.ctypes.data, threads or os.cpu_count())
+        return out
+
     def build_seconds(self) -> float:
         """Duration of SORT's Accelerator::Build for this tree (reference library only)."""
         return float(self.api.L.sortref_build_seconds(self.h))
@@ -169,6 +177,10 @@ class Reference:
         L.sortref_trace_multi.argtypes = [_vp, _vp, _i64, _vp, _vp, _vp, _vp, _vp, _vp, ctypes.c_int]
         L.sortref_build_seconds.restype = ctypes.c_double
         L.sortref_build_seconds.argtypes = [_vp]
+        L.sortref_scene_create_transparent.restype = _vp
+        L.sortref_scene_create_transparent.argtypes = [ctypes.c_int, _vp, ctypes.c_int, _vp, ctypes.c_int, _vp, _vp,
+                                                       ctypes.c_int, ctypes.c_int]
+        L.sortref_trace_attenuation.argtypes = [_vp, _vp, _i64, _vp, ctypes.c_int]
         self.L = L
         self._free, self._topo, self._depth = L.sortref_scene_destroy, L.sortref_topology, L.sortref_depth
         self._bbox, self._closest, self._any = L.sortref_scene_bbox, L.sortref_trace_closest, L.sortref_trace_any
@@ -181,6 +193,22 @@ class Reference:
         m = np.ascontiguousarray(mat_of_tri, np.int32)
         h = self.L.sortref_scene_create_mat(width, tri.ctypes.data, tri.shape[0], m.ctypes.data, int(nmat),
                                             max_depth, max_leaf)
+        if not h:
+            raise ValueError("reference build failed")
+        return _Tree(self, h, width, tri.shape[0])
+
+    def build_transparent(self, tri: np.ndarray, mat_of_tri: np.ndarray, transparent, rgb, width: int,
+                          max_depth: int = 16, max_leaf: int = 8) -> _Tree:
+        """A tree whose materials 0..nmat-1 carry a HasTransparency flag and a
+        constant transparency (for the transparent-shadow query)."""
+        tri = np.ascontiguousarray(tri, np.float32).reshape(-1, 9)
+        m = np.ascontiguousarray(mat_of_tri, np.int32)
+        flags = np.ascontiguousarray(transparent, np.int32).reshape(-1)
+        col = np.ascontiguousarray(rgb, np.float32).reshape(-1, 3)
+        if col.shape[0] != flags.size:
+            raise ValueError("one flag and one rgb triple per material")
+        h = self.L.sortref_scene_create_transparent(width, tri.ctypes.data, tri.shape[0], m.ctypes.data, flags.size,
+                                                    flags.ctypes.data, col.ctypes.data, max_depth, max_leaf)
         if not h:
             raise ValueError("reference build failed")
         return _Tree(self, h, width, tri.shape[0])

@@ -75,15 +75,25 @@ public:
 
 OpaqueMaterial g_opaque;
 
-// Opaque material with its own unique id, for the BSSRDF multi-hit query,
-// which keeps only hits on primitives of one material (by GetUniqueID).
+// Material with its own unique id, for the BSSRDF multi-hit query, which keeps
+// only hits on primitives of one material (by GetUniqueID), and for the
+// transparent-shadow query: a transparent material answers HasTransparency and
+// EvaluateTransparency with a constant, in place of the TSL shader's value
+// (material/material.h:159-165, 189-191).
 class TaggedMaterial : public OpaqueMaterial {
 public:
-    explicit TaggedMaterial(sid_t id) : m_id(id) {}
+    explicit TaggedMaterial(sid_t id, bool transparent = false, Spectrum transparency = Spectrum(0.0f))
+        : m_id(id), m_transparent(transparent), m_transparency(transparency) {}
     StringID GetUniqueID() const override { return StringID(m_id); }
+    bool HasTransparency() const override { return m_transparent; }
+    Spectrum EvaluateTransparency(const SurfaceInteraction&) const override {
+        return m_transparent ? m_transparency : Spectrum(0.0f);
+    }
 
 private:
     sid_t m_id;
+    bool m_transparent;
+    Spectrum m_transparency;
 };
 
 // Material index k of a harness scene maps to unique id kMaterialIdBase + k.
@@ -225,14 +235,18 @@ extern "C" {
 // Build SORT's QBVH (width 4) or OBVH (width 8) over ntri triangles given as
 // 9 floats each (v0, v1, v2). max_depth / max_leaf are Fbvh's m_maxNodeDepth /
 // m_maxPriInLeaf (accel/fast_bvh.h:176-181, read from the scene stream in SORT).
-void* sortref_scene_create_mat(int width, const float* tri, int ntri, const int32_t* mat_of_tri, int nmat,
-                               int max_depth, int max_leaf) {
+void* sortref_scene_create_transparent(int width, const float* tri, int ntri, const int32_t* mat_of_tri, int nmat,
+                                       const int32_t* transparent, const float* rgb, int max_depth, int max_leaf) {
     if ((width != 4 && width != 8) || ntri < 0 || nmat < 0) return nullptr;
     auto* rs = new RefScene();
     rs->width = width;
     std::vector<MaterialBase*> mats;
     if (mat_of_tri) {
-        for (int k = 0; k < nmat; ++k) rs->materials.push_back(std::make_unique<TaggedMaterial>(kMaterialIdBase + k));
+        for (int k = 0; k < nmat; ++k) {
+            const bool tr = transparent && transparent[k];
+            const Spectrum c = rgb ? Spectrum(rgb[3 * k], rgb[3 * k + 1], rgb[3 * k + 2]) : Spectrum(0.0f);
+            rs->materials.push_back(std::make_unique<TaggedMaterial>(kMaterialIdBase + k, tr, c));
+        }
         mats.resize((size_t)ntri);
         for (int i = 0; i < ntri; ++i) {
             if (mat_of_tri[i] < 0 || mat_of_tri[i] >= nmat) {
@@ -271,6 +285,12 @@ void* sortref_scene_create_mat(int width, const float* tri, int ntri, const int3
 }
 
 double sortref_build_seconds(void* h) { return ((RefScene*)h)->build_seconds; }
+
+void* sortref_scene_create_mat(int width, const float* tri, int ntri, const int32_t* mat_of_tri, int nmat,
+                               int max_depth, int max_leaf) {
+    return sortref_scene_create_transparent(width, tri, ntri, mat_of_tri, nmat, nullptr, nullptr, max_depth,
+                                            max_leaf);
+}
 
 void* sortref_scene_create(int width, const float* tri, int ntri, int max_depth, int max_leaf) {
     return sortref_scene_create_mat(width, tri, ntri, nullptr, 0, max_depth, max_leaf);
@@ -388,6 +408,32 @@ void sortref_trace_any(void* h, const float* rays, int64_t n, uint8_t* occluded,
         bool blocked = false;
         if (valid) blocked = acc->GetAttenuation(r, att, rc, nullptr) && att.IsBlack();
         occluded[i] = blocked ? 1 : 0;
+    });
+}
+
+// Scene::GetAttenuation (core/scene.cpp:192-208), restated over SORT's own
+// Accelerator::GetAttenuation (accel/accelerator.cpp:26-69, no medium): rgb
+// planes [0,n), [n,2n), [2n,3n).
+void sortref_trace_attenuation(void* h, const float* rays, int64_t n, float* out, int nthreads) {
+    RefScene* rs = (RefScene*)h;
+    const Accelerator* acc = rs->scene.m_accelerator.get();
+    const bool valid = acc->GetIsValid();
+    parallel_chunks(n, nthreads, [&](RenderContext& rc, int64_t i) {
+        Ray ray(Point(rays[i], rays[n + i], rays[2 * n + i]), Vector(rays[3 * n + i], rays[4 * n + i], rays[5 * n + i]),
+                0, rays[6 * n + i], rays[7 * n + i]);
+        Spectrum attenuation(1.0f);
+        while (valid && !attenuation.IsBlack()) {
+            Spectrum att;
+            if (!acc->GetAttenuation(ray, att, rc, nullptr)) break;
+            if (att.IsBlack()) {
+                attenuation = att;
+                break;
+            }
+            attenuation *= att;
+        }
+        out[i] = attenuation.r;
+        out[n + i] = attenuation.g;
+        out[2 * n + i] = attenuation.b;
     });
 }
 

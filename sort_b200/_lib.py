@@ -64,6 +64,10 @@ class MultiHits(ctypes.Structure):
                 ("v", ctypes.c_void_p)]
 
 
+class Transparency(ctypes.Structure):
+    _fields_ = [("transparent", ctypes.c_int32), ("rgb", ctypes.c_float * 3)]
+
+
 class Batch(ctypes.Structure):
     _fields_ = [("scene", ctypes.c_void_p), ("rays", ctypes.c_void_p), ("stride", ctypes.c_int64),
                 ("n", ctypes.c_int64), ("any", ctypes.c_int32), ("reserved", ctypes.c_int32), ("hits", Hits),
@@ -140,6 +144,8 @@ _SIGNATURES = {
     "sg_trace_multi": (ctypes.c_int, [_vp, ctypes.POINTER(Rays), _i64, _vp, _vp, ctypes.POINTER(MultiHits), _vp]),
     "sg_scene_set_materials": (ctypes.c_int, [_vp, _vp, _i64]),
     "sg_trace_multi_host": (ctypes.c_int, [_vp, _vp, _i64, _vp, _vp, _vp, _vp, _vp, _vp]),
+    "sg_trace_attenuation": (ctypes.c_int, [_vp, ctypes.POINTER(Rays), _i64, _vp, ctypes.c_int32, _vp, _vp]),
+    "sg_trace_attenuation_host": (ctypes.c_int, [_vp, _vp, _i64, _vp, ctypes.c_int32, _vp]),
     "sg_probe_l2_read_gbs": (ctypes.c_int, [ctypes.c_int32, _i64, ctypes.c_int32, ctypes.POINTER(ctypes.c_double)]),
     "sg_last_error": (ctypes.c_char_p, []),
     "sg_version": (ctypes.c_char_p, []),

@@ -214,6 +214,43 @@ class Accelerator:
                                               rm.data_ptr(), ctypes.byref(h), s))
         return count, prim, t, u, v
 
+    def SetMaterials(self, prim_material) -> None:
+        """The material id of every primitive (int32, input order), kept on the
+        device for the queries that depend on materials."""
+        self._require()
+        m = np.ascontiguousarray(np.asarray(prim_material, dtype=np.int32).reshape(-1))
+        _lib.check(_lib.load().sg_scene_set_materials(self._h, m.ctypes.data, m.size))
+
+    @staticmethod
+    def transparency_table(transparent, rgb) -> np.ndarray:
+        """The sg_transparency array for per-material flags and rgb triples."""
+        flags = np.asarray(transparent, dtype=np.int32).reshape(-1)
+        col = np.asarray(rgb, dtype=np.float32).reshape(-1, 3)
+        if col.shape[0] != flags.size:
+            raise ValueError("one transparency flag and one rgb triple per material")
+        table = np.zeros(flags.size, dtype=[("transparent", np.int32), ("rgb", np.float32, 3)])
+        table["transparent"] = flags
+        table["rgb"] = col
+        return table
+
+    def GetAttenuationTransparent(self, rays, transparent, rgb, stream=None):
+        """SORT's Scene::GetAttenuation (core/scene.cpp:192-208) with transparent
+        materials, for a CUDA ray batch: per material a HasTransparency flag and a
+        constant EvaluateTransparency rgb; primitive materials from SetMaterials.
+        Returns a (3, n) float32 tensor (r, g, b rows)."""
+        self._require()
+        torch = _torch()
+        rays = rays.contiguous()
+        n = rays.shape[1]
+        dev = rays.device
+        table = self.transparency_table(transparent, rgb)
+        d_table = torch.from_numpy(table.view(np.uint8).copy()).to(dev)
+        out = torch.empty((3, n), dtype=torch.float32, device=dev)
+        s = stream if stream is not None else torch.cuda.current_stream(dev).cuda_stream
+        _lib.check(_lib.load().sg_trace_attenuation(self._h, ctypes.byref(self._ray_struct(rays)), n,
+                                                    d_table.data_ptr(), table.size, out.data_ptr(), s))
+        return out
+
     def TraceStats(self, rays, any_hit: bool = False, stream=None):
         """(interior nodes tested, primitives tested) summed over a CUDA ray batch,
         counted as SORT's traversal statistics count them."""

@@ -184,13 +184,20 @@ unsigned long long* next_counter(const sg_scene* cs) {
     return s->d_counters + k;
 }
 
+// Status word bits: 1 traversal stack bound (cannot happen when the stack
+// holds depth*(W-1)+1 entries), 2 attenuation layer limit, 4 primitive
+// material id outside the caller's table. Reading a set word clears it.
 sg_status check_status_word(const sg_scene* s, cudaStream_t st) {
     int h = 0;
     cudaError_t e = cudaMemcpyAsync(&h, s->d_err, sizeof(int), cudaMemcpyDeviceToHost, st);
     if (e == cudaSuccess) e = cudaStreamSynchronize(st);
     if (e != cudaSuccess) return cuda_fail(e, "read traversal status");
-    if (h != 0) return fail(SG_ERR_INTERNAL, "traversal stack bound exceeded");
-    return SG_OK;
+    if (h == 0) return SG_OK;
+    if ((e = cudaMemsetAsync(s->d_err, 0, sizeof(int), st)) == cudaSuccess) e = cudaStreamSynchronize(st);
+    if (e != cudaSuccess) return cuda_fail(e, "clear traversal status");
+    if (h & 1) return fail(SG_ERR_INTERNAL, "traversal stack bound exceeded");
+    if (h & 4) return fail(SG_ERR_INVALID_ARGUMENT, "primitive material id outside the material table");
+    return fail(SG_ERR_LIMIT, "a ray crossed more than 4096 transparent surfaces");
 }
 
 }  // namespace
@@ -198,6 +205,8 @@ sg_status check_status_word(const sg_scene* s, cudaStream_t st) {
 namespace sg {
 
 sg_status set_error(sg_status s, const char* msg) { return fail(s, msg); }
+
+const int32_t* scene_materials(const sg_scene* s) { return s ? s->d_material : nullptr; }
 
 sg_status scene_launch(const sg_scene* s, bool any, TraceLaunch* L, DevTree* tree, int* device) {
     if (!s || !L || !tree || !device) return fail(SG_ERR_INVALID_ARGUMENT, "NULL argument");
@@ -558,6 +567,52 @@ sg_status sg_trace_multi_host(const sg_scene* cs, const float* rays8, int64_t n,
         (e = cudaMemcpyAsync(t, h.t, N * 16, cudaMemcpyDeviceToHost, st)) != cudaSuccess ||
         (u && (e = cudaMemcpyAsync(u, h.u, N * 16, cudaMemcpyDeviceToHost, st)) != cudaSuccess) ||
         (v && (e = cudaMemcpyAsync(v, h.v, N * 16, cudaMemcpyDeviceToHost, st)) != cudaSuccess))
+        return cuda_fail(e, "copy results to host");
+    if ((e = cudaStreamSynchronize(st)) != cudaSuccess) return cuda_fail(e, "synchronize");
+    return check_status_word(s, st);
+}
+
+sg_status sg_trace_attenuation_host(const sg_scene* cs, const float* rays8, int64_t n,
+                                    const sg_transparency* materials, int32_t nmat, float* attenuation) {
+    if (!cs || !rays8 || !attenuation) return fail(SG_ERR_INVALID_ARGUMENT, "NULL argument");
+    if (n < 0 || nmat < 0) return fail(SG_ERR_INVALID_ARGUMENT, "negative count");
+    if (nmat > 0 && !materials) return fail(SG_ERR_INVALID_ARGUMENT, "NULL material table");
+    if (n == 0) return SG_OK;
+    sg_scene* s = const_cast<sg_scene*>(cs);
+    if (!s->d_material) return fail(SG_ERR_INVALID_ARGUMENT, "no primitive materials (sg_scene_set_materials)");
+    std::lock_guard<std::mutex> lock(s->scratch_lock);
+    DeviceGuard g(s->device);
+    if (!g.ok) return fail(SG_ERR_CUDA, "cudaSetDevice failed");
+    cudaError_t e;
+    if (!s->stream && (e = cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking)) != cudaSuccess)
+        return cuda_fail(e, "cudaStreamCreate");
+    // rays 32 B and attenuation 12 B per ray, then the material table
+    auto al = [](size_t x) { return (x + 255) & ~size_t(255); };
+    const size_t N = size_t(n), M = size_t(nmat);
+    const size_t need = al(N * 32) + al(N * 12) + al(std::max<size_t>(M, 1) * sizeof(sg_transparency));
+    if (s->scratch_bytes < need) {
+        if (s->d_scratch) cudaFree(s->d_scratch);
+        s->d_scratch = nullptr;
+        s->scratch_bytes = 0;
+        if ((e = cudaMalloc(&s->d_scratch, need)) != cudaSuccess) return cuda_fail(e, "cudaMalloc(scratch)");
+        s->scratch_bytes = need;
+    }
+    char* b = static_cast<char*>(s->d_scratch);
+    float* d_rays = reinterpret_cast<float*>(b);
+    b += al(N * 32);
+    float* d_att = reinterpret_cast<float*>(b);
+    b += al(N * 12);
+    sg_transparency* d_mats = reinterpret_cast<sg_transparency*>(b);
+    cudaStream_t st = s->stream;
+    if ((e = cudaMemcpyAsync(d_rays, rays8, N * 32, cudaMemcpyHostToDevice, st)) != cudaSuccess ||
+        (M && (e = cudaMemcpyAsync(d_mats, materials, M * sizeof(sg_transparency), cudaMemcpyHostToDevice, st)) !=
+                  cudaSuccess))
+        return cuda_fail(e, "copy rays to device");
+    const sg_rays r{d_rays, d_rays + n, d_rays + 2 * n, d_rays + 3 * n, d_rays + 4 * n, d_rays + 5 * n, d_rays + 6 * n,
+                    d_rays + 7 * n};
+    sg_status status = sg_trace_attenuation(s, &r, n, d_mats, nmat, d_att, st);
+    if (status != SG_OK) return status;
+    if ((e = cudaMemcpyAsync(attenuation, d_att, N * 12, cudaMemcpyDeviceToHost, st)) != cudaSuccess)
         return cuda_fail(e, "copy results to host");
     if ((e = cudaStreamSynchronize(st)) != cudaSuccess) return cuda_fail(e, "synchronize");
     return check_status_word(s, st);

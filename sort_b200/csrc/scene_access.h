@@ -16,6 +16,9 @@ sg_status set_error(sg_status s, const char* msg);
 // persistent-schedule counter slot) and the device tree of scene s.
 sg_status scene_launch(const sg_scene* s, bool any, TraceLaunch* L, DevTree* tree, int* device);
 
+// The per-primitive material ids of scene s on its device (sg_scene_set_materials), or NULL.
+const int32_t* scene_materials(const sg_scene* s);
+
 // Synchronises st and reports the traversal status word of scene s.
 sg_status scene_status(const sg_scene* s, cudaStream_t st);
 

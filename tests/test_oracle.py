@@ -74,3 +74,12 @@ def test_reference_multi_reproduces_golden(reference, width):
     count, prim, t, u, v = tree.multi(z["rays"], z["ray_mat"])
     assert np.array_equal(count, z[f"count{width}"]) and np.array_equal(prim, z[f"prim{width}"])
     assert same_bits(t, z[f"t{width}"]) and same_bits(u, z[f"u{width}"]) and same_bits(v, z[f"v{width}"])
+
+
+@pytest.mark.parametrize("width", [4, 8])
+@pytest.mark.parametrize("assign", ["by_sphere", "per_tri"])
+def test_reference_attenuation_reproduces_golden(reference, width, assign):
+    """The committed transparent-shadow fixture is what SORT's code returns (pins it)."""
+    z = golden("attenuation")
+    tree = reference.build_transparent(z["triangles"], z[assign], z["transparent"], z["rgb"], width)
+    assert same_bits(tree.attenuation(z["rays"]), z[f"att{width}_{assign}"])
