@@ -52,6 +52,7 @@ TRI_BYTES = 36                  # 9 floats per triangle test
 RAY_IN, HIT_OUT = 32, 16
 CPU_SAMPLE = 262_144            # rays per CPU-baseline step
 NODE_FORMATS = {"fp32": 0, "q8": 1}
+BUILDERS = {"host": 0, "gpu": 1, "lbvh": 2}  # host / gpu: SORT's tree; lbvh: Morton-order tree
 
 
 def workload_config(extra=None):
@@ -233,7 +234,8 @@ def run_ours(args):
         from sort_b200 import Qbvh
         width = 4
         tri = scenes.sphere_field(64, 3, seed=1)
-        acc = Qbvh(DEPTH, LEAF, node_format=NODE_FORMATS[args.nodes], device=local)
+        acc = Qbvh(DEPTH, LEAF, node_format=NODE_FORMATS[args.nodes], device=local,
+                   builder=BUILDERS[args.builder or "host"])
         acc.Build(tri)
         diffuse = scenes.camera_rays(1024, 1024, seed=7 + rank)
         h = acc.GetIntersect(torch.from_numpy(diffuse).to(device))
@@ -242,7 +244,8 @@ def run_ours(args):
     else:
         width = WIDTH
         tri = scenes.sphere_field(SPHERES, LEVEL, seed=1)
-        acc = Obvh(DEPTH, LEAF, node_format=NODE_FORMATS[args.nodes], device=local)
+        acc = Obvh(DEPTH, LEAF, node_format=NODE_FORMATS[args.nodes], device=local,
+                   builder=BUILDERS[args.builder or "host"])
         acc.Build(tri)
         diffuse, shadow = make_rays(acc, tri, rank, device)
     info = acc.info()
@@ -253,7 +256,7 @@ def run_ours(args):
     # SORT's traversal counters on these rays -> algorithmic bytes per ray. The
     # counts are SORT's (FP32 boxes), whatever node format is timed.
     parity = None
-    if args.nodes == "fp32":
+    if args.nodes == "fp32" and args.builder != "lbvh":
         node_tests, prim_tests = acc.TraceStats(d_diff, False)
         a_nodes, a_prims = acc.TraceStats(d_shad, True)
     else:
@@ -348,7 +351,9 @@ def run_ours(args):
             "warmup": args.warmup, "ms_per_step": round(ms_max / args.steps, 4), "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded procedural scene)",
             "config": (raycast_config if width == 4 else workload_config)(
-                {"nodes": args.nodes} if args.nodes != "fp32" else {}) | (
+                ({"nodes": args.nodes} if args.nodes != "fp32" else {}) |
+                ({"tree": "LBVH (Morton-order wide BVH built on the GPU; algorithmic bytes counted on SORT's tree)"}
+                 if args.builder == "lbvh" else {})) | (
                 {"parallelism": f"replicas x{world}", "build_seconds": round(info["build_seconds"], 2),
                                        "tree_device_bytes": info["device_bytes"]}),
             "roofline": {"bound": bound, "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
@@ -792,14 +797,17 @@ def run_serve(args):
 BUILD_SAMPLE = (64, LEVEL)  # SORT's single-threaded build, timed on 64 of the 1,024 spheres (1,310,722 triangles)
 
 
-def build_config(extra=None):
+def build_config(extra=None, builder="gpu"):
+    tree = {"gpu": "GPU builder (SG_BUILDER_GPU), the same tree as SORT's Fbvh::Build",
+            "host": "this library's host builder, the same tree as SORT's Fbvh::Build",
+            "lbvh": "Morton-order wide BVH built on the GPU (SG_BUILDER_LBVH), not SORT's tree"}[builder]
     cfg = {
-        "workload": "build_21m: BVH build of 1,024 level-5 icospheres + ground quad = 20,971,522 triangles as "
-                    "SORT's OBVH (width 8, depth 16, leaf 8) from host triangles; GPU builder (SG_BUILDER_GPU), "
-                    "the same tree as SORT's Fbvh::Build",
+        "workload": "build_21m: BVH build of 1,024 level-5 icospheres + ground quad = 20,971,522 triangles, "
+                    f"width 8, leaf 8, from host triangles; {tree}",
         "scene_seed": 1,
-        "timing": "value: the library's clock around the whole build (triangle upload, GPU split rounds, "
-                  "host flattening); e2e: the create call (build + node upload) from host triangles",
+        "timing": "value: the library's clock around the whole build (triangle upload, GPU passes, and for "
+                  "SORT's tree the host flattening); e2e: the create call (build + node upload) from host "
+                  "triangles",
         "l2": "inputs larger than L2: 755 MB of triangles per build (no flush)",
     }
     if extra:
@@ -865,7 +873,8 @@ def run_build(args):
         for k in range(args.warmup + args.steps):
             if world > 1:
                 dist.barrier()
-            acc = Obvh(max_node_depth=DEPTH, max_pri_in_leaf=LEAF, builder=_lib.SG_BUILDER_GPU, device=local)
+            acc = Obvh(max_node_depth=DEPTH, max_pri_in_leaf=LEAF, builder=BUILDERS[args.builder or "gpu"],
+                       device=local)
             t0 = time.perf_counter()
             acc.Build(tri)
             t1 = time.perf_counter()
@@ -882,17 +891,21 @@ def run_build(args):
         return
     tris_bytes = (n + 8) * 48
     node_bytes = info["device_bytes"] - tris_bytes
+    lbvh = args.builder == "lbvh"
     shapes = info["interior_nodes"] + info["leaves"]
     out = {
         "metric": "Mtriangles/s BVH build", "value": round(world * n / mean_build / 1e6, 3), "unit": "Mtriangles/s",
         "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(1e3 * mean_build, 3),
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
         "config": build_config({"depth": info["depth"], "interior_nodes": info["interior_nodes"],
-                                "leaves": info["leaves"], "split_rounds": info["build_rounds"]}),
+                                "leaves": info["leaves"], "rounds": info["build_rounds"]}, args.builder or "gpu"),
         "e2e": {"value": round(world * n / mean_create / 1e6, 3), "unit": "Mtriangles/s",
-                "h2d_bytes_per_step": int(n * 36 + node_bytes), "d2h_bytes_per_step": int(n * 4 + shapes * 40)},
+                "h2d_bytes_per_step": int(n * 36 + (0 if lbvh else node_bytes)),
+                "d2h_bytes_per_step": int(16 * info["build_rounds"] if lbvh else n * 4 + shapes * 40)},
         "gpu_launches": info["build_launches"] * args.steps,
         "roofline": None,
+        **({"tree": "LBVH: Morton-order wide BVH built on the GPU, not SORT's tree (same hits except near-ties "
+                    "and box-grazing rays)"} if lbvh else {}),
         "clocks": clocks.summary(),
     }
     if not args.no_cpu_baseline:
@@ -923,6 +936,9 @@ def main():
     p.add_argument("--batch-seed", type=int, default=7, help="batched workload: seed of the batch list")
     p.add_argument("--sample", type=int, default=CPU_SAMPLE)
     p.add_argument("--no-cpu-baseline", action="store_true")
+    p.add_argument("--builder", choices=sorted(BUILDERS), default=None,
+                   help="tree builder: host/gpu build SORT's tree (closest default host), lbvh the Morton-order "
+                        "tree (build workload default gpu)")
     p.add_argument("--nodes", choices=sorted(NODE_FORMATS), default="fp32",
                    help="child-box format of the timed tree (q8: 8-bit, outward-rounded)")
     args = p.parse_args()

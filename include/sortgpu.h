@@ -92,13 +92,21 @@ typedef struct {
     int32_t node_format;    /* sg_node_format */
     int32_t device;         /* CUDA device ordinal the tree lives on */
     int32_t build_threads;  /* host threads for the build, 0 = all */
-    int32_t builder;        /* sg_builder: where the (same) tree is built */
+    int32_t builder;        /* sg_builder: which builder makes the tree */
 } sg_build_opts;
 
-/* Both builders produce SORT's Fbvh tree (same topology, leaf order, boxes). */
+/* SG_BUILDER_HOST and SG_BUILDER_GPU produce SORT's Fbvh tree (same
+ * topology, leaf order, boxes). SG_BUILDER_LBVH builds a wide BVH in Morton
+ * order entirely on the device, for fast scene admission: not SORT's tree (the
+ * same hits and distances except near-ties, where two triangles are hit within
+ * 1e-6 of each other and a rounded box entry distance decides which one is
+ * kept, and rays whose slab test misses the hit triangle's own box by
+ * rounding, so that finding it depends on the leaf boxes), FP32 nodes only,
+ * max_depth ignored, no topology export. */
 typedef enum {
     SG_BUILDER_HOST = 0, /* host threads, one subtree per thread below the top */
-    SG_BUILDER_GPU = 1   /* data-parallel passes on the scene's device */
+    SG_BUILDER_GPU = 1,  /* data-parallel passes on the scene's device */
+    SG_BUILDER_LBVH = 2  /* Morton-order wide BVH on the scene's device */
 } sg_builder;
 
 /* Structure-of-arrays ray batch: n entries in each array. */
@@ -131,8 +139,8 @@ typedef struct {
     float bbox[6];           /* enlarged scene box: min xyz, max xyz */
     int64_t device_bytes;    /* HBM held by the tree (nodes + triangles) */
     double build_seconds;    /* build time (host clock, whole build) */
-    int32_t build_rounds;    /* SG_BUILDER_GPU: split rounds (0 for the host builder) */
-    int32_t build_launches;  /* SG_BUILDER_GPU: its own kernels launched (CUB's prefix sums not counted) */
+    int32_t build_rounds;    /* GPU builders: split rounds (SG_BUILDER_GPU) or wide-tree levels (LBVH); 0 on the host */
+    int32_t build_launches;  /* GPU builders: their own kernels launched (CUB's scans and sorts not counted) */
 } sg_scene_info;
 
 /* Traversal launch schedule (results never depend on it). */

@@ -37,6 +37,7 @@ class BuildOpts(ctypes.Structure):
 
 SG_BUILDER_HOST = 0
 SG_BUILDER_GPU = 1
+SG_BUILDER_LBVH = 2
 
 
 class Rays(ctypes.Structure):

@@ -90,13 +90,15 @@ sg_status upload(sg_scene* s, const float* tri, int64_t ntri) {
     const int f4 = W == 8 ? sg::NodeShape<8>::kF4 : sg::NodeShape<4>::kF4;
     const int64_t nn = t.interior();
     std::vector<float4> nodes;
-    if (s->node_format == SG_NODES_QUANT8) {
+    const bool adopt = t.d_nodes != nullptr;  // the LBVH builder wrote the nodes on the device
+    if (adopt) {
+    } else if (s->node_format == SG_NODES_QUANT8) {
         sg::quantize_nodes(t, nodes);
     } else {
         nodes.assign(size_t(std::max<int64_t>(nn, 1)) * f4, make_float4(0.0f, 0.0f, 0.0f, 0.0f));
     }
     const int Q = W / 4;  // float4 per plane
-    for (int64_t k = 0; s->node_format == SG_NODES_FP32 && k < nn; ++k) {
+    for (int64_t k = 0; !adopt && s->node_format == SG_NODES_FP32 && k < nn; ++k) {
         float* base = reinterpret_cast<float*>(&nodes[size_t(k) * f4]);
         for (int a = 0; a < 3; ++a)
             for (int j = 0; j < W; ++j) {
@@ -106,14 +108,20 @@ sg_status upload(sg_scene* s, const float* tri, int64_t ntri) {
         int32_t* ch = reinterpret_cast<int32_t*>(base + 6 * Q * 4);
         for (int j = 0; j < W; ++j) ch[j] = t.child[size_t(k) * W + j];
     }
-    const size_t nb = nodes.size() * sizeof(float4), tb = size_t(ntri + sg::kPadSlots) * 3 * sizeof(float4);
-    cudaError_t e = cudaMalloc(&s->d_nodes, nb);
-    if (e != cudaSuccess) return e == cudaErrorMemoryAllocation ? fail(SG_ERR_OUT_OF_MEMORY, "cudaMalloc(nodes) failed")
-                                                                 : cuda_fail(e, "cudaMalloc(nodes)");
+    const size_t nb = adopt ? size_t(nn) * f4 * sizeof(float4) : nodes.size() * sizeof(float4),
+                 tb = size_t(ntri + sg::kPadSlots) * 3 * sizeof(float4);
+    cudaError_t e = cudaSuccess;
+    if (adopt) {
+        s->d_nodes = s->tree.d_nodes;
+        s->tree.d_nodes = nullptr;
+    } else if ((e = cudaMalloc(&s->d_nodes, nb)) != cudaSuccess) {
+        return e == cudaErrorMemoryAllocation ? fail(SG_ERR_OUT_OF_MEMORY, "cudaMalloc(nodes) failed")
+                                              : cuda_fail(e, "cudaMalloc(nodes)");
+    }
     if ((e = cudaMalloc(&s->d_err, sizeof(int))) != cudaSuccess) return cuda_fail(e, "cudaMalloc(status)");
     if ((e = cudaMalloc(&s->d_counters, sg_scene::kCounterSlots * sizeof(unsigned long long))) != cudaSuccess)
         return cuda_fail(e, "cudaMalloc(counters)");
-    if ((e = cudaMemcpy(s->d_nodes, nodes.data(), nb, cudaMemcpyHostToDevice)) != cudaSuccess)
+    if (!adopt && (e = cudaMemcpy(s->d_nodes, nodes.data(), nb, cudaMemcpyHostToDevice)) != cudaSuccess)
         return cuda_fail(e, "upload nodes");
     if ((e = cudaMemset(s->d_err, 0, sizeof(int))) != cudaSuccess) return cuda_fail(e, "clear status");
     if (s->tree.d_tris) {  // the GPU builder wrote the records on the device
@@ -150,6 +158,7 @@ void release(sg_scene* s) {
     if (s->d_nodes) cudaFree(s->d_nodes);
     if (s->d_tris) cudaFree(s->d_tris);
     if (s->tree.d_tris) cudaFree(s->tree.d_tris);  // a GPU build that was not adopted
+    if (s->tree.d_nodes) cudaFree(s->tree.d_nodes);
     if (s->d_err) cudaFree(s->d_err);
     if (s->d_stats) cudaFree(s->d_stats);
     if (s->d_counters) cudaFree(s->d_counters);
@@ -264,14 +273,20 @@ sg_status sg_scene_create(const float* triangles, int64_t ntri, const sg_build_o
     bp.max_depth = opts->max_depth;
     bp.max_leaf = opts->max_leaf;
     bp.threads = opts->build_threads;
-    if (opts->builder != SG_BUILDER_HOST && opts->builder != SG_BUILDER_GPU) {
+    if (opts->builder != SG_BUILDER_HOST && opts->builder != SG_BUILDER_GPU && opts->builder != SG_BUILDER_LBVH) {
         delete s;
         return fail(SG_ERR_INVALID_ARGUMENT, "unknown builder");
+    }
+    if (opts->builder == SG_BUILDER_LBVH && opts->node_format != SG_NODES_FP32) {
+        delete s;
+        return fail(SG_ERR_UNSUPPORTED, "SG_BUILDER_LBVH writes FP32 nodes only");
     }
     const auto t0 = std::chrono::steady_clock::now();
     try {
         if (opts->builder == SG_BUILDER_GPU)
             s->tree = sg::build_tree_gpu(triangles, ntri, bp, opts->device);
+        else if (opts->builder == SG_BUILDER_LBVH)
+            s->tree = sg::build_tree_lbvh(triangles, ntri, bp, opts->device);
         else
             s->tree = sg::build_tree(triangles, ntri, bp);
     } catch (const std::bad_alloc&) {
@@ -319,7 +334,7 @@ sg_status sg_scene_destroy(sg_scene* s) {
 sg_status sg_scene_info_get(const sg_scene* s, sg_scene_info* info) {
     if (!s || !info) return fail(SG_ERR_INVALID_ARGUMENT, "NULL argument");
     std::memset(info, 0, sizeof(*info));
-    info->triangles = int64_t(s->tree.order.size());
+    info->triangles = s->tree.triangles();
     info->interior_nodes = s->tree.interior();
     info->leaves = s->tree.leaves;
     info->depth = s->tree.depth;
@@ -339,6 +354,7 @@ sg_status sg_scene_info_get(const sg_scene* s, sg_scene_info* info) {
 
 sg_status sg_scene_topology(const sg_scene* s, int32_t* out, int64_t cap, int64_t* written) {
     if (!s || !written) return fail(SG_ERR_INVALID_ARGUMENT, "NULL argument");
+    if (!s->tree.host_arrays()) return fail(SG_ERR_UNSUPPORTED, "an SG_BUILDER_LBVH tree has no topology export");
     std::vector<int32_t> v;
     sg::tree_topology(s->tree, v);
     *written = int64_t(v.size());
@@ -503,7 +519,7 @@ static sg_status host_trace(const sg_scene* cs, const float* rays8, int64_t n, i
 
 sg_status sg_scene_set_materials(sg_scene* s, const int32_t* material, int64_t n) {
     if (!s || (n > 0 && !material)) return fail(SG_ERR_INVALID_ARGUMENT, "NULL argument");
-    if (n != int64_t(s->tree.order.size())) return fail(SG_ERR_INVALID_ARGUMENT, "one material per primitive");
+    if (n != s->tree.triangles()) return fail(SG_ERR_INVALID_ARGUMENT, "one material per primitive");
     std::lock_guard<std::mutex> lock(s->scratch_lock);
     DeviceGuard g(s->device);
     if (!g.ok) return fail(SG_ERR_CUDA, "cudaSetDevice failed");

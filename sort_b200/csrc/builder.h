@@ -57,9 +57,17 @@ struct BuiltTree {
     // (layout.h), leaf order plus the zero pad slots, already on the build's
     // device. The receiver owns it (cudaFree).
     float4* d_tris = nullptr;
-    int rounds = 0, launches = 0;  // build_tree_gpu's split rounds and kernel launches
+    // Set by build_tree_lbvh only: the interior nodes already in the device
+    // layout (layout.h, FP32 boxes), n_interior of them, owned like d_tris. Its
+    // host arrays (child, lo, hi, first_interior, order, leaf_last) stay empty;
+    // n_tri and n_interior give the sizes.
+    float4* d_nodes = nullptr;
+    int64_t n_interior = -1, n_tri = -1;
+    int rounds = 0, launches = 0;  // GPU builders: rounds (levels) and their own kernel launches
     int64_t leaves = 0;
-    int64_t interior() const { return width ? int64_t(child.size()) / width : 0; }
+    int64_t interior() const { return n_interior >= 0 ? n_interior : (width ? int64_t(child.size()) / width : 0); }
+    int64_t triangles() const { return n_tri >= 0 ? n_tri : int64_t(order.size()); }
+    bool host_arrays() const { return n_interior < 0; }
 };
 
 // Builds over ntri triangles, 9 floats each (v0, v1, v2). Throws
@@ -70,6 +78,12 @@ BuiltTree build_tree(const float* tri, int64_t ntri, const BuildParams& p);
 // (builder_gpu.cu). Throws std::invalid_argument on bad input and
 // std::runtime_error on a CUDA error.
 BuiltTree build_tree_gpu(const float* tri, int64_t ntri, const BuildParams& p, int device);
+
+// A wide BVH in Morton order (LBVH), built entirely on the GPU: not SORT's
+// tree (same hits except near-ties and rays whose slab test misses the hit
+// triangle's own box by rounding), for fast scene admission.
+// max_depth does not apply. The result has no host arrays (host_arrays()).
+BuiltTree build_tree_lbvh(const float* tri, int64_t ntri, const BuildParams& p, int device);
 
 // 8-bit node format (quantize.cpp): one record per interior node in the layout
 // layout.h describes; every decoded child box contains the FP32 box.

@@ -1,0 +1,132 @@
+"""SG_BUILDER_LBVH: the Morton-order wide BVH built on the GPU.
+
+Its tree is not SORT's, so the bar is the one for a different tree over the
+same triangles: every ray's closest distance equals the one through SORT's
+tree (the host builder's) bit for bit, the primitive is the same unless two
+triangles are hit at exactly that distance, and the any-hit answer is the
+same. Two exceptions come from the box arithmetic, not from a fault of either
+tree. Near-ties: when two triangles are hit within 1e-6 (relative) of each
+other, a box entry distance that rounds above the first hit found culls the
+other, so each tree may keep a different one. And a ray that
+SORT's slab test (with its 1e-5 clamp of direction components,
+simd/simd_ray_utils.h:61-64, and simd/simd_bbox.h:47-109) sends past a
+triangle's own box by rounding reaches that triangle only through a larger
+leaf box, so whether it is found depends on which triangles share its leaf;
+such rays may differ, and the test checks that every difference is one.
+Scenes cover ties and degenerate triangles (the golden edge scene), tiny and
+empty scenes, leaf sizes 1 to 16, and both widths.
+"""
+import numpy as np
+import pytest
+
+from conftest import golden, same_bits
+
+pytestmark = pytest.mark.gpu
+torch = pytest.importorskip("torch")
+
+
+def _pair(tri, width, **kw):
+    from sort_b200 import Obvh, Qbvh, _lib
+    cls = Qbvh if width == 4 else Obvh
+    ref = cls(builder=_lib.SG_BUILDER_HOST, **kw)
+    ref.Build(tri)
+    lb = cls(builder=_lib.SG_BUILDER_LBVH, **kw)
+    lb.Build(tri)
+    return ref, lb
+
+
+def _own_box_missed(tri, prim, rays, i):
+    """SORT's slab test of ray i against triangle prim's own box (float32,
+    multiply and add rounded separately, |d| < 1e-5 clamped): True if it fails."""
+    f = np.float32
+    v = np.asarray(tri[prim], f).reshape(3, 3)
+    lo, hi = v.min(0), v.max(0)
+    o = rays[0:3, i].astype(f)
+    d = rays[3:6, i].astype(f)
+    d = np.where(np.abs(d) < f(1e-5), np.where(d < 0, f(-1e-5), f(1e-5)), d).astype(f)
+    rcp = (f(1) / d).astype(f)
+    t1 = ((lo - o).astype(f) * rcp).astype(f)
+    t2 = ((hi - o).astype(f) * rcp).astype(f)
+    tmin = max(f(rays[6, i]), np.minimum(t1, t2).max())
+    tmax = min(f(rays[7, i]), np.maximum(t1, t2).min())
+    return not tmin <= tmax
+
+
+def _same_hits(tri, ref, lb, rays, check_ties=True):
+    from oracle.oracle import Port
+    r = np.ascontiguousarray(rays)
+    d = torch.from_numpy(r).cuda()
+    ha, hb = ref.GetIntersect(d), lb.GetIntersect(d)
+    pa, pb = ha.prim.cpu().numpy(), hb.prim.cpu().numpy()
+    ta, tb = ha.t.cpu().numpy(), hb.t.cpu().numpy()
+    moved = np.nonzero(ta.view(np.int32) != tb.view(np.int32))[0]
+    for i in moved:  # a near-tie, or the nearer hit's own box is missed by the slab test
+        near_tie = pa[i] >= 0 and pb[i] >= 0 and abs(float(ta[i]) - float(tb[i])) <= 1e-6 * float(min(ta[i], tb[i]))
+        p = pa[i] if ta[i] < tb[i] else pb[i]
+        assert near_tie or (p >= 0 and _own_box_missed(tri, int(p), r, int(i))), \
+            f"ray {i}: {pa[i]}@{ta[i]} vs {pb[i]}@{tb[i]}"
+    assert moved.size <= max(10, rays.shape[1] // 1000)
+    same_t = np.ones(rays.shape[1], bool)
+    same_t[moved] = False
+    diff = np.nonzero((pa != pb) & same_t)[0]
+    if check_ties and diff.size:
+        port = Port()
+        for i in diff[:50]:  # a tie: both triangles give the reported distance
+            assert np.float32(port.tri_t(tri, int(pa[i]), r, int(i))) == ta[i]
+            assert np.float32(port.tri_t(tri, int(pb[i]), r, int(i))) == ta[i]
+    oa, ob = ref.GetAttenuation(d).cpu().numpy(), lb.GetAttenuation(d).cpu().numpy()
+    assert np.array_equal(oa[same_t], ob[same_t])
+
+
+@pytest.mark.parametrize("width", [4, 8])
+def test_lbvh_sphere_fields(width):
+    assert torch.cuda.is_available(), "GPU test needs a CUDA device"
+    from sort_b200 import scenes
+    for spheres, level, seed in ((64, 3, 1), (256, 4, 2)):
+        tri = scenes.sphere_field(spheres, level, seed=seed)
+        rays = np.concatenate([scenes.camera_rays(256, 256, seed=3), scenes.random_rays(50_000, seed=4)], axis=1)
+        ref, lb = _pair(tri, width)
+        _same_hits(tri, ref, lb, rays)
+        info = lb.info()
+        assert info["triangles"] == tri.shape[0] and info["leaves"] > 0 and info["interior_nodes"] > 0
+        assert info["bbox"] == ref.info()["bbox"]
+
+
+@pytest.mark.parametrize("width", [4, 8])
+@pytest.mark.parametrize("leaf", [1, 3, 8, 16])
+def test_lbvh_edge_scene(width, leaf):
+    z = golden("edges")
+    ref, lb = _pair(z["triangles"], width, max_pri_in_leaf=leaf)
+    _same_hits(z["triangles"], ref, lb, z["rays"])
+
+
+def test_lbvh_random_soup_and_tiny_scenes():
+    from sort_b200 import scenes
+    rng = np.random.default_rng(7)
+    c = rng.uniform(-5, 5, (20000, 1, 3))
+    tri = (c + rng.normal(0, 0.5, (20000, 3, 3))).astype(np.float32).reshape(-1, 9)
+    tri[::5] = np.round(tri[::5])  # repeated coordinates: equal Morton codes
+    rays = scenes.random_rays(20000, seed=8, box=8.0, axis_fraction=0.2)
+    for width in (4, 8):
+        ref, lb = _pair(tri, width)
+        _same_hits(tri, ref, lb, rays)
+        for k in (1, 2, 9, 17):
+            ref, lb = _pair(tri[:k], width)
+            _same_hits(tri[:k], ref, lb, rays[:, :2000])
+
+
+def test_lbvh_limits_are_reported():
+    from sort_b200 import Obvh, _lib, scenes
+    tri = scenes.sphere_field(8, 2, seed=9)
+    acc = Obvh(builder=_lib.SG_BUILDER_LBVH)
+    acc.Build(tri)
+    with pytest.raises(_lib.SortGpuError) as ex:
+        acc.topology()
+    assert ex.value.status == 4  # SG_ERR_UNSUPPORTED
+    q8 = Obvh(builder=_lib.SG_BUILDER_LBVH, node_format=_lib.SG_NODES_QUANT8)
+    with pytest.raises(_lib.SortGpuError) as ex:
+        q8.Build(tri)
+    assert ex.value.status == 4
+    empty = Obvh(builder=_lib.SG_BUILDER_LBVH)
+    empty.Build(np.zeros((0, 9), np.float32))
+    assert not empty.GetIsValid()
