@@ -161,6 +161,19 @@ typedef struct sg_scene sg_scene;
 void sg_default_build_opts(sg_build_opts* opts);
 
 sg_status sg_scene_create(const float* triangles, int64_t ntri, const sg_build_opts* opts, sg_scene** out);
+
+/* A scene of triangles and hair line segments: SORT's Line shapes as a
+ * HairVisual makes them (entity/visual.cpp:41-97, shape/line.cpp), tested with
+ * Line4/8's ray-line test (simd/simd_line.h:232-330). lines: 10 floats per
+ * segment in world space: p0 xyz, p1 xyz, v0, v1 (texture v at the two ends),
+ * w0, w1 (half widths at the two ends). Primitive indices: the triangles
+ * 0 .. ntri-1, then the lines ntri .. ntri+nlines-1 (a mesh visual followed by
+ * a hair visual in SORT's primitive order). A line hit reports u = 1 and SORT's
+ * v. Such a scene answers sg_trace_closest / sg_trace_any and their _host
+ * forms; the other queries return SG_ERR_UNSUPPORTED, and so does
+ * SG_BUILDER_LBVH. sg_scene_info's triangle count is the primitive count. */
+sg_status sg_scene_create_hair(const float* triangles, int64_t ntri, const float* lines, int64_t nlines,
+                               const sg_build_opts* opts, sg_scene** out);
 sg_status sg_scene_destroy(sg_scene* scene);
 sg_status sg_scene_info_get(const sg_scene* scene, sg_scene_info* info);
 sg_status sg_scene_topology(const sg_scene* scene, int32_t* out, int64_t cap, int64_t* written);
@@ -169,6 +182,11 @@ sg_status sg_scene_topology(const sg_scene* scene, int32_t* out, int64_t cap, in
  * out = NULL / cap = 0 to learn the size (returns SG_ERR_LIMIT and sets written). */
 sg_status sg_build_topology_host(const float* triangles, int64_t ntri, const sg_build_opts* opts, int32_t* out,
                                  int64_t cap, int64_t* written, int32_t* depth);
+/* The same for a scene with hair segments (as sg_scene_create_hair takes
+ * them): SORT's tree over the triangles and the lines' boxes. */
+sg_status sg_build_topology_host_hair(const float* triangles, int64_t ntri, const float* lines, int64_t nlines,
+                                      const sg_build_opts* opts, int32_t* out, int64_t cap, int64_t* written,
+                                      int32_t* depth);
 
 sg_status sg_scene_set_tuning(sg_scene* scene, const sg_trace_tuning* tuning);
 sg_status sg_scene_get_tuning(const sg_scene* scene, sg_trace_tuning* tuning);

@@ -181,6 +181,9 @@ class Reference:
         L.sortref_scene_create_transparent.argtypes = [ctypes.c_int, _vp, ctypes.c_int, _vp, ctypes.c_int, _vp, _vp,
                                                        ctypes.c_int, ctypes.c_int]
         L.sortref_trace_attenuation.argtypes = [_vp, _vp, _i64, _vp, ctypes.c_int]
+        L.sortref_scene_create_hair.restype = _vp
+        L.sortref_scene_create_hair.argtypes = [ctypes.c_int, _vp, ctypes.c_int, _vp, ctypes.c_int, ctypes.c_int,
+                                                ctypes.c_int]
         self.L = L
         self._free, self._topo, self._depth = L.sortref_scene_destroy, L.sortref_topology, L.sortref_depth
         self._bbox, self._closest, self._any = L.sortref_scene_bbox, L.sortref_trace_closest, L.sortref_trace_any
@@ -212,6 +215,17 @@ class Reference:
         if not h:
             raise ValueError("reference build failed")
         return _Tree(self, h, width, tri.shape[0])
+
+    def build_hair(self, tri: np.ndarray, lines: np.ndarray, width: int, max_depth: int = 16,
+                   max_leaf: int = 8) -> _Tree:
+        """Triangles followed by hair segments (m, 10): p0, p1, v0, v1, w0, w1."""
+        tri = np.ascontiguousarray(tri, np.float32).reshape(-1, 9)
+        ln = np.ascontiguousarray(lines, np.float32).reshape(-1, 10)
+        h = self.L.sortref_scene_create_hair(width, tri.ctypes.data, tri.shape[0], ln.ctypes.data, ln.shape[0],
+                                             max_depth, max_leaf)
+        if not h:
+            raise ValueError("reference build failed")
+        return _Tree(self, h, width, tri.shape[0] + ln.shape[0])
 
     def build(self, tri: np.ndarray, width: int, max_depth: int = 16, max_leaf: int = 8) -> _Tree:
         tri = np.ascontiguousarray(tri, np.float32).reshape(-1, 9)

@@ -47,6 +47,7 @@
 #include "core/render_context.h"
 #include "math/interaction.h"
 #include "scatteringevent/bssrdf/bssrdf.h"
+#include "shape/line.h"
 #undef private
 #undef protected
 
@@ -136,12 +137,39 @@ public:
     }
 };
 
+// Hair line segments as SORT's HairVisual makes them (entity/visual.cpp:41-102):
+// one Line per segment, its transform applied (the identity here: the segments
+// are given in world space), one Primitive per Line.
+class HarnessHair : public Visual {
+public:
+    void Fill(const float* seg, int n) {
+        for (int i = 0; i < n; ++i) {
+            const float* s = seg + (size_t)i * 10;
+            m_lines.push_back(std::make_unique<Line>(Point(s[0], s[1], s[2]), Point(s[3], s[4], s[5]), s[6], s[7],
+                                                     s[8], s[9], -1));
+            m_lines.back()->SetTransform(Transform());
+            m_primitives.push_back(std::make_unique<Primitive>(nullptr, &g_opaque, m_lines.back().get()));
+        }
+    }
+    void Serialize(IStreamBase&) override {}
+    void ApplyTransform(const Transform&) override {}
+
+private:
+    std::vector<std::unique_ptr<Line>> m_lines;
+};
+
 class HarnessEntity : public Entity {
 public:
     void Serialize(IStreamBase&) override {}
     HarnessVisual* AddVisual() {
         auto v = std::make_unique<HarnessVisual>();
         HarnessVisual* raw = v.get();
+        m_visuals.push_back(std::move(v));
+        return raw;
+    }
+    HarnessHair* AddHair() {
+        auto v = std::make_unique<HarnessHair>();
+        HarnessHair* raw = v.get();
         m_visuals.push_back(std::move(v));
         return raw;
     }
@@ -235,9 +263,10 @@ extern "C" {
 // Build SORT's QBVH (width 4) or OBVH (width 8) over ntri triangles given as
 // 9 floats each (v0, v1, v2). max_depth / max_leaf are Fbvh's m_maxNodeDepth /
 // m_maxPriInLeaf (accel/fast_bvh.h:176-181, read from the scene stream in SORT).
-void* sortref_scene_create_transparent(int width, const float* tri, int ntri, const int32_t* mat_of_tri, int nmat,
-                                       const int32_t* transparent, const float* rgb, int max_depth, int max_leaf) {
-    if ((width != 4 && width != 8) || ntri < 0 || nmat < 0) return nullptr;
+static void* make_ref_scene(int width, const float* tri, int ntri, const float* lines, int nlines,
+                            const int32_t* mat_of_tri, int nmat, const int32_t* transparent, const float* rgb,
+                            int max_depth, int max_leaf) {
+    if ((width != 4 && width != 8) || ntri < 0 || nmat < 0 || nlines < 0) return nullptr;
     auto* rs = new RefScene();
     rs->width = width;
     std::vector<MaterialBase*> mats;
@@ -259,6 +288,7 @@ void* sortref_scene_create_transparent(int width, const float* tri, int ntri, co
     auto entity = std::make_unique<HarnessEntity>();
     HarnessVisual* visual = entity->AddVisual();
     visual->Fill(tri, ntri, mat_of_tri ? mats.data() : nullptr);
+    if (nlines > 0) entity->AddHair()->Fill(lines, nlines);
     rs->scene.m_entities.push_back(std::move(entity));
 
     ScenePrimitiveIterator iter(rs->scene);
@@ -285,6 +315,18 @@ void* sortref_scene_create_transparent(int width, const float* tri, int ntri, co
 }
 
 double sortref_build_seconds(void* h) { return ((RefScene*)h)->build_seconds; }
+
+void* sortref_scene_create_transparent(int width, const float* tri, int ntri, const int32_t* mat_of_tri, int nmat,
+                                       const int32_t* transparent, const float* rgb, int max_depth, int max_leaf) {
+    return make_ref_scene(width, tri, ntri, nullptr, 0, mat_of_tri, nmat, transparent, rgb, max_depth, max_leaf);
+}
+
+// Triangles followed by hair segments (10 floats each: p0, p1, v0, v1, w0, w1),
+// all opaque; primitive order: the triangles, then the lines.
+void* sortref_scene_create_hair(int width, const float* tri, int ntri, const float* lines, int nlines, int max_depth,
+                                int max_leaf) {
+    return make_ref_scene(width, tri, ntri, lines, nlines, nullptr, 0, nullptr, nullptr, max_depth, max_leaf);
+}
 
 void* sortref_scene_create_mat(int width, const float* tri, int ntri, const int32_t* mat_of_tri, int nmat,
                                int max_depth, int max_leaf) {

@@ -33,6 +33,13 @@ void export_node(const HarnessIndexMap& idx, const Node* node, std::vector<int32
                 out.push_back(idx.at(p));
                 ++n;
             }
+        for (unsigned i = 0; i < node->line_cnt; ++i)  // then the line packs, as the leaf tests them
+            for (int l = 0; l < SIMD_CHANNEL; ++l) {
+                const Primitive* p = node->line_list[i].m_ori_pri[l];
+                if (!p) continue;
+                out.push_back(idx.at(p));
+                ++n;
+            }
         for (const Primitive* p : node->other_list) {
             out.push_back(idx.at(p));
             ++n;

@@ -123,11 +123,14 @@ _SIGNATURES = {
                                            ctypes.POINTER(BatchTuning), _vp]),
     "sg_default_build_opts": (None, [ctypes.POINTER(BuildOpts)]),
     "sg_scene_create": (ctypes.c_int, [_vp, _i64, ctypes.POINTER(BuildOpts), ctypes.POINTER(_vp)]),
+    "sg_scene_create_hair": (ctypes.c_int, [_vp, _i64, _vp, _i64, ctypes.POINTER(BuildOpts), ctypes.POINTER(_vp)]),
     "sg_scene_destroy": (ctypes.c_int, [_vp]),
     "sg_scene_info_get": (ctypes.c_int, [_vp, ctypes.POINTER(SceneInfo)]),
     "sg_scene_topology": (ctypes.c_int, [_vp, _vp, _i64, ctypes.POINTER(_i64)]),
     "sg_build_topology_host": (ctypes.c_int, [_vp, _i64, ctypes.POINTER(BuildOpts), _vp, _i64,
                                               ctypes.POINTER(_i64), ctypes.POINTER(ctypes.c_int32)]),
+    "sg_build_topology_host_hair": (ctypes.c_int, [_vp, _i64, _vp, _i64, ctypes.POINTER(BuildOpts), _vp, _i64,
+                                                   ctypes.POINTER(_i64), ctypes.POINTER(ctypes.c_int32)]),
     "sg_scene_set_tuning": (ctypes.c_int, [_vp, ctypes.POINTER(Tuning)]),
     "sg_scene_get_tuning": (ctypes.c_int, [_vp, ctypes.POINTER(Tuning)]),
     "sg_trace_closest": (ctypes.c_int, [_vp, ctypes.POINTER(Rays), _i64, ctypes.POINTER(Hits), _vp]),

@@ -42,14 +42,19 @@ class Hits:
 
 
 class Scene:
-    """Triangle soup in primitive order (SORT's ScenePrimitiveIterator order)."""
+    """Triangle soup in primitive order (SORT's ScenePrimitiveIterator order),
+    optionally followed by hair line segments: (m, 10) float32 rows of p0 xyz,
+    p1 xyz, v0, v1, w0, w1 (half widths), in world space, primitive indices
+    after the triangles."""
 
-    def __init__(self, triangles):
+    def __init__(self, triangles, lines=None):
         tri = np.ascontiguousarray(np.asarray(triangles, dtype=np.float32).reshape(-1, 9))
         self.triangles = tri
+        self.lines = None if lines is None else np.ascontiguousarray(
+            np.asarray(lines, dtype=np.float32).reshape(-1, 10))
 
     def GetPrimitiveCount(self) -> int:
-        return int(self.triangles.shape[0])
+        return int(self.triangles.shape[0]) + (0 if self.lines is None else int(self.lines.shape[0]))
 
 
 def _torch():
@@ -96,11 +101,17 @@ class Accelerator:
 
     # -- build ----------------------------------------------------------------------
     def Build(self, scene) -> None:
-        tri = scene.triangles if isinstance(scene, Scene) else Scene(scene).triangles
+        sc = scene if isinstance(scene, Scene) else Scene(scene)
+        tri = sc.triangles
         self.Release()
         lib = _lib.load()
         h = ctypes.c_void_p()
-        _lib.check(lib.sg_scene_create(tri.ctypes.data, tri.shape[0], ctypes.byref(self._opts()), ctypes.byref(h)))
+        if sc.lines is None:
+            _lib.check(lib.sg_scene_create(tri.ctypes.data, tri.shape[0], ctypes.byref(self._opts()),
+                                           ctypes.byref(h)))
+        else:
+            _lib.check(lib.sg_scene_create_hair(tri.ctypes.data, tri.shape[0], sc.lines.ctypes.data,
+                                                sc.lines.shape[0], ctypes.byref(self._opts()), ctypes.byref(h)))
         self._h = h
         info = _lib.SceneInfo()
         _lib.check(lib.sg_scene_info_get(h, ctypes.byref(info)))
@@ -317,20 +328,29 @@ class Obvh(Accelerator):
     WIDTH = 8
 
 
-def build_topology_host(triangles, width: int, max_depth: int = 16, max_leaf: int = 8, threads: int = 0):
-    """Build on the host only and return (topology stream, depth); needs no GPU."""
+def build_topology_host(triangles, width: int, max_depth: int = 16, max_leaf: int = 8, threads: int = 0,
+                        lines=None):
+    """Build on the host only and return (topology stream, depth); needs no GPU.
+    With hair segments (lines, (m, 10)), they follow the triangles."""
     lib = _lib.load()
     tri = np.ascontiguousarray(np.asarray(triangles, np.float32).reshape(-1, 9))
+    ln = None if lines is None else np.ascontiguousarray(np.asarray(lines, np.float32).reshape(-1, 10))
     o = _lib.BuildOpts()
     lib.sg_default_build_opts(ctypes.byref(o))
     o.width, o.max_depth, o.max_leaf, o.build_threads = width, max_depth, max_leaf, threads
     need = ctypes.c_int64(0)
     depth = ctypes.c_int32(0)
-    st = lib.sg_build_topology_host(tri.ctypes.data, tri.shape[0], ctypes.byref(o), None, 0, ctypes.byref(need),
-                                    ctypes.byref(depth))
+
+    def call(out, cap):
+        if ln is None:
+            return lib.sg_build_topology_host(tri.ctypes.data, tri.shape[0], ctypes.byref(o), out, cap,
+                                              ctypes.byref(need), ctypes.byref(depth))
+        return lib.sg_build_topology_host_hair(tri.ctypes.data, tri.shape[0], ln.ctypes.data, ln.shape[0],
+                                               ctypes.byref(o), out, cap, ctypes.byref(need), ctypes.byref(depth))
+
+    st = call(None, 0)
     if st not in (_lib.SG_OK, 5):
         _lib.check(st)
     out = np.empty(max(need.value, 1), np.int32)
-    _lib.check(lib.sg_build_topology_host(tri.ctypes.data, tri.shape[0], ctypes.byref(o), out.ctypes.data, out.size,
-                                          ctypes.byref(need), ctypes.byref(depth)))
+    _lib.check(call(out.ctypes.data, out.size))
     return out[:need.value], depth.value

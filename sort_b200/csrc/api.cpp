@@ -17,6 +17,7 @@
 #include <vector>
 
 #include "builder.h"
+#include "hair.h"
 #include "trace_kernels.h"
 
 namespace {
@@ -80,11 +81,17 @@ struct sg_scene {
     cudaEvent_t in_done[kMaxChunks] = {};
     cudaEvent_t trace_done[kMaxChunks] = {};
     int32_t* d_material = nullptr;  // per primitive, for sg_trace_multi_host (sg_scene_set_materials)
+    float4* d_lines = nullptr;      // hair line records (hair.h), primitives ntri .. ntri + n_lines - 1
+    int64_t n_lines = 0;
 };
 
 namespace {
 
-sg_status upload(sg_scene* s, const float* tri, int64_t ntri) {
+// Slot records in leaf order (layout.h); with hair lines (line_recs, 20 floats
+// each, primitives ntri ..), a leaf's triangles come before its lines, each in
+// leaf order, as SORT tests its triangle packs before its line packs.
+sg_status upload(sg_scene* s, const float* tri, int64_t ntri, const std::vector<float>& line_recs = {},
+                 int64_t nlines = 0) {
     const sg::BuiltTree& t = s->tree;
     const int W = t.width;
     const int f4 = W == 8 ? sg::NodeShape<8>::kF4 : sg::NodeShape<4>::kF4;
@@ -109,7 +116,8 @@ sg_status upload(sg_scene* s, const float* tri, int64_t ntri) {
         for (int j = 0; j < W; ++j) ch[j] = t.child[size_t(k) * W + j];
     }
     const size_t nb = adopt ? size_t(nn) * f4 * sizeof(float4) : nodes.size() * sizeof(float4),
-                 tb = size_t(ntri + sg::kPadSlots) * 3 * sizeof(float4);
+                 tb = size_t(ntri + nlines + sg::kPadSlots) * 3 * sizeof(float4) +
+                      size_t(nlines) * sg::kLineF4 * sizeof(float4);
     cudaError_t e = cudaSuccess;
     if (adopt) {
         s->d_nodes = s->tree.d_nodes;
@@ -128,25 +136,56 @@ sg_status upload(sg_scene* s, const float* tri, int64_t ntri) {
         s->d_tris = s->tree.d_tris;
         s->tree.d_tris = nullptr;
     } else {
-        std::vector<float4> tris(size_t(ntri + sg::kPadSlots) * 3);
+        const int64_t nall = ntri + nlines;
+        std::vector<float4> tris(size_t(nall + sg::kPadSlots) * 3);
         std::memset(tris.data(), 0, tris.size() * sizeof(float4));
-        for (int64_t i = 0; i < ntri; ++i) {
-            const int32_t p = t.order[size_t(i)];
-            const float* v = tri + int64_t(p) * 9;
-            float4* dst = &tris[size_t(i) * 3];
-            int32_t last = t.leaf_last[size_t(i)];
-            dst[0] = make_float4(v[0], v[1], v[2], 0.0f);
+        auto put = [&](int64_t slot, int32_t p, int32_t last) {
+            float4* dst = &tris[size_t(slot) * 3];
+            if (p < ntri) {
+                const float* v = tri + int64_t(p) * 9;
+                dst[0] = make_float4(v[0], v[1], v[2], 0.0f);
+                dst[1] = make_float4(v[3], v[4], v[5], 0.0f);
+                dst[2] = make_float4(v[6], v[7], v[8], 0.0f);
+            } else {
+                const int32_t line = int32_t(p - ntri), kind = sg::kLineSlot;
+                std::memcpy(&dst[2].x, &line, 4);
+                std::memcpy(&dst[2].w, &kind, 4);
+            }
             std::memcpy(&dst[0].w, &p, 4);
-            dst[1] = make_float4(v[3], v[4], v[5], 0.0f);
             std::memcpy(&dst[1].w, &last, 4);
-            dst[2] = make_float4(v[6], v[7], v[8], 0.0f);
+        };
+        if (nlines == 0) {
+            for (int64_t i = 0; i < ntri; ++i) put(i, t.order[size_t(i)], t.leaf_last[size_t(i)]);
+        } else {
+            for (int64_t b = 0; b < nall;) {  // one leaf: slots b .. e
+                int64_t e = b;
+                while (!t.leaf_last[size_t(e)]) ++e;
+                int64_t k = b;
+                for (int pass = 0; pass < 2; ++pass)
+                    for (int64_t i = b; i <= e; ++i) {
+                        const int32_t p = t.order[size_t(i)];
+                        if ((p >= ntri) != (pass == 1)) continue;
+                        const int64_t slot = k++;
+                        put(slot, p, slot == e ? 1 : 0);
+                    }
+                b = e + 1;
+            }
         }
-        e = cudaMalloc(&s->d_tris, tb);
+        const size_t tbytes = tris.size() * sizeof(float4);
+        e = cudaMalloc(&s->d_tris, tbytes);
         if (e != cudaSuccess)
             return e == cudaErrorMemoryAllocation ? fail(SG_ERR_OUT_OF_MEMORY, "cudaMalloc(triangles) failed")
                                                   : cuda_fail(e, "cudaMalloc(triangles)");
-        if ((e = cudaMemcpy(s->d_tris, tris.data(), tb, cudaMemcpyHostToDevice)) != cudaSuccess)
+        if ((e = cudaMemcpy(s->d_tris, tris.data(), tbytes, cudaMemcpyHostToDevice)) != cudaSuccess)
             return cuda_fail(e, "upload triangles");
+        if (nlines > 0) {
+            if ((e = cudaMalloc(&s->d_lines, line_recs.size() * sizeof(float))) != cudaSuccess)
+                return cuda_fail(e, "cudaMalloc(lines)");
+            if ((e = cudaMemcpy(s->d_lines, line_recs.data(), line_recs.size() * sizeof(float),
+                                cudaMemcpyHostToDevice)) != cudaSuccess)
+                return cuda_fail(e, "upload lines");
+            s->n_lines = nlines;
+        }
     }
     s->device_bytes = int64_t(nb + tb);
     return SG_OK;
@@ -159,6 +198,7 @@ void release(sg_scene* s) {
     if (s->d_tris) cudaFree(s->d_tris);
     if (s->tree.d_tris) cudaFree(s->tree.d_tris);  // a GPU build that was not adopted
     if (s->tree.d_nodes) cudaFree(s->tree.d_nodes);
+    if (s->d_lines) cudaFree(s->d_lines);
     if (s->d_err) cudaFree(s->d_err);
     if (s->d_stats) cudaFree(s->d_stats);
     if (s->d_counters) cudaFree(s->d_counters);
@@ -219,6 +259,7 @@ const int32_t* scene_materials(const sg_scene* s) { return s ? s->d_material : n
 
 sg_status scene_launch(const sg_scene* s, bool any, TraceLaunch* L, DevTree* tree, int* device) {
     if (!s || !L || !tree || !device) return fail(SG_ERR_INVALID_ARGUMENT, "NULL argument");
+    if (s->d_lines) return fail(SG_ERR_UNSUPPORTED, "a scene with hair lines answers the closest-hit and any-hit queries only");
     L->width = s->width;
     L->any = any;
     L->stack_need = s->stack_need;
@@ -248,11 +289,20 @@ void sg_default_build_opts(sg_build_opts* o) {
     o->builder = SG_BUILDER_HOST;
 }
 
-sg_status sg_scene_create(const float* triangles, int64_t ntri, const sg_build_opts* opts, sg_scene** out) {
+}  // extern "C"
+
+namespace {
+
+sg_status create_scene(const float* triangles, int64_t ntri, const float* lines, int64_t nlines,
+                       const sg_build_opts* opts, sg_scene** out) {
     if (!out) return fail(SG_ERR_INVALID_ARGUMENT, "out is NULL");
     *out = nullptr;
     if (!opts) return fail(SG_ERR_INVALID_ARGUMENT, "opts is NULL");
     if (ntri < 0 || (ntri > 0 && !triangles)) return fail(SG_ERR_INVALID_ARGUMENT, "bad triangle buffer");
+    if (nlines < 0 || (nlines > 0 && !lines)) return fail(SG_ERR_INVALID_ARGUMENT, "bad line buffer");
+    if (nlines > 0 && opts->builder == SG_BUILDER_LBVH)
+        return fail(SG_ERR_UNSUPPORTED, "SG_BUILDER_LBVH builds triangle scenes only");
+    if (ntri + nlines >= int64_t(0x7fffffff)) return fail(SG_ERR_LIMIT, "more than 2^31-2 primitives");
     if (opts->width != 4 && opts->width != 8) return fail(SG_ERR_INVALID_ARGUMENT, "width must be 4 or 8");
     if (opts->max_leaf < 1 || opts->max_depth < 1) return fail(SG_ERR_INVALID_ARGUMENT, "max_leaf/max_depth < 1");
     if (opts->node_format != SG_NODES_FP32 && opts->node_format != SG_NODES_QUANT8)
@@ -273,6 +323,18 @@ sg_status sg_scene_create(const float* triangles, int64_t ntri, const sg_build_o
     bp.max_depth = opts->max_depth;
     bp.max_leaf = opts->max_leaf;
     bp.threads = opts->build_threads;
+    // Hair lines: SORT's per-line constants and boxes (hair_setup.cpp).
+    std::vector<float> line_recs, line_boxes;
+    try {
+        line_recs.resize(size_t(nlines) * 20);
+        line_boxes.resize(size_t(nlines) * 6);
+    } catch (const std::bad_alloc&) {
+        delete s;
+        return fail(SG_ERR_OUT_OF_MEMORY, "host allocation failed");
+    }
+    for (int64_t k = 0; k < nlines; ++k) sg::line_setup(lines + k * 10, &line_recs[size_t(k) * 20], &line_boxes[size_t(k) * 6]);
+    bp.extra_boxes = line_boxes.data();
+    bp.nextra = nlines;
     if (opts->builder != SG_BUILDER_HOST && opts->builder != SG_BUILDER_GPU && opts->builder != SG_BUILDER_LBVH) {
         delete s;
         return fail(SG_ERR_INVALID_ARGUMENT, "unknown builder");
@@ -312,7 +374,7 @@ sg_status sg_scene_create(const float* triangles, int64_t ntri, const sg_build_o
     }
     sg_status st;
     try {
-        st = upload(s, triangles, ntri);
+        st = upload(s, triangles, ntri, line_recs, nlines);
     } catch (const std::bad_alloc&) {
         st = fail(SG_ERR_OUT_OF_MEMORY, "host memory exhausted during upload");
     }
@@ -324,6 +386,19 @@ sg_status sg_scene_create(const float* triangles, int64_t ntri, const sg_build_o
     std::vector<float>().swap(s->tree.hi);
     *out = s;
     return SG_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+sg_status sg_scene_create(const float* triangles, int64_t ntri, const sg_build_opts* opts, sg_scene** out) {
+    return create_scene(triangles, ntri, nullptr, 0, opts, out);
+}
+
+sg_status sg_scene_create_hair(const float* triangles, int64_t ntri, const float* lines, int64_t nlines,
+                               const sg_build_opts* opts, sg_scene** out) {
+    return create_scene(triangles, ntri, lines, nlines, opts, out);
 }
 
 sg_status sg_scene_destroy(sg_scene* s) {
@@ -365,8 +440,15 @@ sg_status sg_scene_topology(const sg_scene* s, int32_t* out, int64_t cap, int64_
 
 sg_status sg_build_topology_host(const float* triangles, int64_t ntri, const sg_build_opts* opts, int32_t* out,
                                  int64_t cap, int64_t* written, int32_t* depth) {
+    return sg_build_topology_host_hair(triangles, ntri, nullptr, 0, opts, out, cap, written, depth);
+}
+
+sg_status sg_build_topology_host_hair(const float* triangles, int64_t ntri, const float* lines, int64_t nlines,
+                                      const sg_build_opts* opts, int32_t* out, int64_t cap, int64_t* written,
+                                      int32_t* depth) {
     if (!opts || !written) return fail(SG_ERR_INVALID_ARGUMENT, "NULL argument");
     if (ntri < 0 || (ntri > 0 && !triangles)) return fail(SG_ERR_INVALID_ARGUMENT, "bad triangle buffer");
+    if (nlines < 0 || (nlines > 0 && !lines)) return fail(SG_ERR_INVALID_ARGUMENT, "bad line buffer");
     sg::BuildParams bp;
     bp.width = opts->width;
     bp.max_depth = opts->max_depth;
@@ -374,6 +456,10 @@ sg_status sg_build_topology_host(const float* triangles, int64_t ntri, const sg_
     bp.threads = opts->build_threads;
     std::vector<int32_t> v;
     try {
+        std::vector<float> rec(size_t(nlines) * 20), boxes(size_t(nlines) * 6);
+        for (int64_t k = 0; k < nlines; ++k) sg::line_setup(lines + k * 10, &rec[size_t(k) * 20], &boxes[size_t(k) * 6]);
+        bp.extra_boxes = boxes.data();
+        bp.nextra = nlines;
         const sg::BuiltTree t = sg::build_tree(triangles, ntri, bp);
         sg::tree_topology(t, v);
         if (depth) *depth = t.depth;
@@ -416,7 +502,8 @@ static sg_status trace_common(const sg_scene* s, const sg_rays* rays, int64_t n,
     }
     L.err = s->d_err;
     L.counter = next_counter(s);
-    const cudaError_t e = sg::launch_trace_fp32(L, dev_tree(s), r, n, st);
+    const cudaError_t e = s->d_lines ? sg::launch_trace_hair(L, dev_tree(s), s->d_lines, r, n, st)
+                                     : sg::launch_trace_fp32(L, dev_tree(s), r, n, st);
     if (e != cudaSuccess) return cuda_fail(e, "traversal launch");
     return SG_OK;
 }
@@ -641,6 +728,7 @@ sg_status sg_trace_stats(const sg_scene* cs, const sg_rays* rays, int64_t n, int
     if (!rays->ox || !rays->oy || !rays->oz || !rays->dx || !rays->dy || !rays->dz || !rays->tmin || !rays->tmax)
         return fail(SG_ERR_INVALID_ARGUMENT, "NULL ray array");
     *node_tests = *prim_tests = 0;
+    if (cs->d_lines) return fail(SG_ERR_UNSUPPORTED, "traversal statistics cover triangle scenes only");
     if (n == 0) return SG_OK;
     sg_scene* s = const_cast<sg_scene*>(cs);
     std::lock_guard<std::mutex> lock(s->scratch_lock);

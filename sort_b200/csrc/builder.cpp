@@ -257,10 +257,12 @@ struct Flattener {
 
 }  // namespace
 
-BuiltTree build_tree(const float* tri, int64_t ntri, const BuildParams& p) {
+BuiltTree build_tree(const float* tri, int64_t ntri_in, const BuildParams& p) {
     if (p.width != 4 && p.width != 8) throw std::invalid_argument("width must be 4 or 8");
     if (p.max_leaf < 1 || p.max_depth < 1) throw std::invalid_argument("max_leaf and max_depth must be >= 1");
-    if (ntri < 0 || ntri >= int64_t(0x7fffffff)) throw std::invalid_argument("triangle count out of range");
+    if (p.nextra < 0 || (p.nextra > 0 && !p.extra_boxes)) throw std::invalid_argument("bad extra primitive boxes");
+    const int64_t ntri = ntri_in + p.nextra;  // every primitive: triangles, then the extra ones
+    if (ntri_in < 0 || ntri >= int64_t(0x7fffffff)) throw std::invalid_argument("triangle count out of range");
     BuiltTree t;
     t.width = p.width;
     const int nthreads = p.threads > 0 ? p.threads : int(std::max(1u, std::thread::hardware_concurrency()));
@@ -278,7 +280,15 @@ BuiltTree build_tree(const float* tri, int64_t ntri, const BuildParams& p) {
             pool.emplace_back([&, s, e]() {
                 for (int64_t i = s; i < e; ++i) {
                     Box b = empty_box();
-                    for (int k = 0; k < 3; ++k) add_point(b, tri + i * 9 + 3 * k);
+                    if (i < ntri_in) {
+                        for (int k = 0; k < 3; ++k) add_point(b, tri + i * 9 + 3 * k);
+                    } else {  // Line::GetBBox (shape/line.cpp:98-106), computed by the caller
+                        const float* x = p.extra_boxes + (i - ntri_in) * 6;
+                        for (int k = 0; k < 3; ++k) {
+                            b.mn[k] = x[k];
+                            b.mx[k] = x[3 + k];
+                        }
+                    }
                     pbox[size_t(i)] = b;
                     Prim& pr = prims[size_t(i)];
                     for (int k = 0; k < 3; ++k) pr.c[k] = (b.mx[k] + b.mn[k]) * 0.5f;
@@ -300,6 +310,7 @@ BuiltTree build_tree(const float* tri, int64_t ntri, const BuildParams& p) {
         }
     }
     t.scene = scene;
+    if (p.nextra > 0) t.first_extra = ntri_in;
     if (ntri == 0) return t;
 
     Ctx c;
@@ -335,14 +346,17 @@ void topo_rec(const BuiltTree& t, int32_t ref, std::vector<int32_t>& out) {
         out.push_back(0);
         const size_t cnt_pos = out.size();
         out.push_back(0);
-        int64_t i = leaf_begin(ref);
+        const int64_t b = leaf_begin(ref);
+        int64_t e = b;
+        while (!t.leaf_last[size_t(e)]) ++e;
         int32_t n = 0;
-        for (;;) {
-            out.push_back(t.order[size_t(i)]);
-            ++n;
-            if (t.leaf_last[size_t(i)]) break;
-            ++i;
-        }
+        for (int pass = 0; pass < (t.first_extra >= 0 ? 2 : 1); ++pass)  // triangles, then the others
+            for (int64_t i = b; i <= e; ++i) {
+                const bool extra = t.first_extra >= 0 && t.order[size_t(i)] >= t.first_extra;
+                if (extra != (pass == 1)) continue;
+                out.push_back(t.order[size_t(i)]);
+                ++n;
+            }
         out[cnt_pos] = n;
         return;
     }

@@ -36,6 +36,11 @@ struct BuildParams {
     int max_depth = 16;
     int max_leaf = 8;
     int threads = 0;  // 0 = hardware_concurrency
+    // Primitives after the triangles (hair lines): their boxes, 6 floats each
+    // (min xyz, max xyz), primitive indices ntri .. ntri + nextra - 1. SORT's
+    // split rules see every primitive as its box and the box centre.
+    const float* extra_boxes = nullptr;
+    int64_t nextra = 0;
 };
 
 // Flat tree. Interior node k owns child[k*W + j] and, for child j on axis a,
@@ -63,6 +68,10 @@ struct BuiltTree {
     // n_tri and n_interior give the sizes.
     float4* d_nodes = nullptr;
     int64_t n_interior = -1, n_tri = -1;
+    // Primitives from first_extra on are not triangles (hair lines); -1: none.
+    // A leaf tests its triangles before them, as SORT's leaf tests its triangle
+    // packs before its line packs.
+    int64_t first_extra = -1;
     int rounds = 0, launches = 0;  // GPU builders: rounds (levels) and their own kernel launches
     int64_t leaves = 0;
     int64_t interior() const { return n_interior >= 0 ? n_interior : (width ? int64_t(child.size()) / width : 0); }

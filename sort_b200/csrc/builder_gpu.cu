@@ -610,7 +610,10 @@ BuiltTree build_tree_gpu(const float* tri, int64_t ntri, const BuildParams& p, i
     if (p.max_leaf < 1 || p.max_depth < 1) throw std::invalid_argument("max_leaf and max_depth must be >= 1");
     if (ntri < 0 || ntri >= int64_t(0x7fffffff)) throw std::invalid_argument("triangle count out of range");
     const int W = p.width;
-    const int64_t n = ntri;
+    if (p.nextra < 0 || (p.nextra > 0 && !p.extra_boxes)) throw std::invalid_argument("bad extra primitive boxes");
+    const int64_t nt = ntri;           // triangles
+    const int64_t n = ntri + p.nextra;  // every primitive
+    if (n >= int64_t(0x7fffffff)) throw std::invalid_argument("primitive count out of range");
     BuiltTree t;
     t.width = W;
     int prev = -1;
@@ -639,7 +642,8 @@ BuiltTree build_tree_gpu(const float* tri, int64_t ntri, const BuildParams& p, i
     PinnedBuf<int> h_scene;
     PinnedBuf<BuildState> h_state;
     const int64_t nn = std::max<int64_t>(n, 1);
-    d_tri.alloc(size_t(nn) * 9);
+    d_tri.alloc(size_t(std::max<int64_t>(nt, 1)) * 9);
+    DevBuf<float> d_extra;
     d_cx.alloc(size_t(nn));
     d_cy.alloc(size_t(nn));
     d_cz.alloc(size_t(nn));
@@ -662,8 +666,19 @@ BuiltTree build_tree_gpu(const float* tri, int64_t ntri, const BuildParams& p, i
     {
         empty_box(h_scene.p);
         if (n > 0) {
-            check(cudaMemcpyAsync(d_tri.p, tri, size_t(n) * 9 * sizeof(float), cudaMemcpyHostToDevice, st), "upload");
-            k_prim_setup<<<grid(n), 256, 0, st>>>(d_tri.p, n, d_cx.p, d_cy.p, d_cz.p, d_idx.p, d_pb.p);
+            if (nt > 0) {
+                check(cudaMemcpyAsync(d_tri.p, tri, size_t(nt) * 9 * sizeof(float), cudaMemcpyHostToDevice, st),
+                      "upload");
+                k_prim_setup<<<grid(nt), 256, 0, st>>>(d_tri.p, nt, n, d_cx.p, d_cy.p, d_cz.p, d_idx.p, d_pb.p);
+            }
+            if (p.nextra > 0) {
+                d_extra.alloc(size_t(p.nextra) * 6);
+                check(cudaMemcpyAsync(d_extra.p, p.extra_boxes, size_t(p.nextra) * 6 * sizeof(float),
+                                      cudaMemcpyHostToDevice, st),
+                      "upload boxes");
+                k_box_setup<<<grid(p.nextra), 256, 0, st>>>(d_extra.p, nt, p.nextra, n, d_cx.p, d_cy.p, d_cz.p,
+                                                            d_idx.p, d_pb.p);
+            }
             check(cudaMemcpyAsync(d_scene.p, h_scene.p, 6 * sizeof(int), cudaMemcpyHostToDevice, st), "scene box");
             k_scene_box<<<std::min<unsigned>(grid(n), 148 * 8), 256, 0, st>>>(n, d_pb.p, d_scene.p);
             check(cudaGetLastError(), "primitive setup");
@@ -680,6 +695,7 @@ BuiltTree build_tree_gpu(const float* tri, int64_t ntri, const BuildParams& p, i
         }
     }
     t.scene = scene;
+    if (p.nextra > 0) t.first_extra = nt;
     if (n == 0) return t;
 
     // Node-sized buffers at their bounds: nodes under construction own disjoint
@@ -842,6 +858,11 @@ BuiltTree build_tree_gpu(const float* tri, int64_t ntri, const BuildParams& p, i
         for (int q = nsub - 1; q >= 0; --q) stack.push_back(sub[q]);  // first child filled next
     }
 
+    // This file's kernels: setup and scene box, 13 per queued round, the triangle
+    // records (the prefix sums are CUB's, four per round, not counted).
+    t.rounds = int(fin.rounds);
+    t.launches = int(3 + 13 * queued);
+    if (p.nextra > 0) return t;  // mixed primitives: the scene writes its slot records on the host
     // The triangle records in leaf order, built where the triangles already are.
     uint8_t* d_last = reinterpret_cast<uint8_t*>(d_rid.p);  // n bytes fit in the n-int buffer
     check(cudaMemcpyAsync(d_last, t.leaf_last.data(), size_t(n), cudaMemcpyHostToDevice, st), "leaf flags");
@@ -859,10 +880,6 @@ BuiltTree build_tree_gpu(const float* tri, int64_t ntri, const BuildParams& p, i
         check(e, "triangle records");
     }
     t.d_tris = d_tris;
-    // This file's kernels: setup and scene box, 13 per queued round, the triangle
-    // records (the prefix sums are CUB's, four per round, not counted).
-    t.rounds = fin.rounds;
-    t.launches = int(3 + 13 * queued);
     return t;
 }
 

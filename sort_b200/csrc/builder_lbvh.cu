@@ -294,6 +294,7 @@ BuiltTree build_tree_lbvh(const float* tri, int64_t ntri, const BuildParams& p, 
     if (p.width != 4 && p.width != 8) throw std::invalid_argument("width must be 4 or 8");
     if (p.max_leaf < 1) throw std::invalid_argument("max_leaf must be >= 1");
     if (ntri < 0 || ntri >= int64_t(0x7fffffff)) throw std::invalid_argument("triangle count out of range");
+    if (p.nextra != 0) throw std::invalid_argument("the LBVH builder takes triangles only");
     const int W = p.width;
     const int F4 = W == 8 ? NodeShape<8>::kF4 : NodeShape<4>::kF4;
     const int64_t n = ntri;
@@ -341,7 +342,7 @@ BuiltTree build_tree_lbvh(const float* tri, int64_t ntri, const BuildParams& p, 
     empty_box(h_box.p + 6);
     if (n > 0) {
         check(cudaMemcpyAsync(d_tri.p, tri, size_t(n) * 9 * sizeof(float), cudaMemcpyHostToDevice, st), "upload");
-        k_prim_setup<<<grid(n), 256, 0, st>>>(d_tri.p, n, d_cx.p, d_cy.p, d_cz.p, d_idx.p, d_pb.p);
+        k_prim_setup<<<grid(n), 256, 0, st>>>(d_tri.p, n, n, d_cx.p, d_cy.p, d_cz.p, d_idx.p, d_pb.p);
         check(cudaMemcpyAsync(d_box.p, h_box.p, 12 * sizeof(int), cudaMemcpyHostToDevice, st), "boxes");
         const unsigned gb = std::min<unsigned>(grid(n), 148 * 8);
         k_scene_box<<<gb, 256, 0, st>>>(n, d_pb.p, d_box.p);

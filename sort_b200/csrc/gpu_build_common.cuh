@@ -155,10 +155,13 @@ __device__ __forceinline__ void atomic_box(int* dst, const int (&v)[6]) {
     }
 }
 
-__global__ void k_prim_setup(const float* __restrict__ tri, int64_t n, float* __restrict__ cx, float* __restrict__ cy,
-                             float* __restrict__ cz, int32_t* __restrict__ idx, float* __restrict__ pb) {
+// Boxes, centroids and identity indices of the first `count` primitives
+// (triangles); box planes and centroid arrays have `stride` entries.
+__global__ void k_prim_setup(const float* __restrict__ tri, int64_t count, int64_t stride, float* __restrict__ cx,
+                             float* __restrict__ cy, float* __restrict__ cz, int32_t* __restrict__ idx,
+                             float* __restrict__ pb) {
     const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= n) return;
+    if (i >= count) return;
     float mn[3] = {FLT_MAX, FLT_MAX, FLT_MAX}, mx[3] = {-FLT_MAX, -FLT_MAX, -FLT_MAX};
     for (int k = 0; k < 3; ++k)  // BBox::Union(const Point&) per vertex (math/bbox.cpp:106-113)
         for (int a = 0; a < 3; ++a) {
@@ -167,8 +170,29 @@ __global__ void k_prim_setup(const float* __restrict__ tri, int64_t n, float* __
             if (p > mx[a]) mx[a] = p;
         }
     for (int a = 0; a < 3; ++a) {
-        pb[a * n + i] = mn[a];
-        pb[(3 + a) * n + i] = mx[a];
+        pb[a * stride + i] = mn[a];
+        pb[(3 + a) * stride + i] = mx[a];
+    }
+    cx[i] = __fmul_rn(__fadd_rn(mx[0], mn[0]), 0.5f);
+    cy[i] = __fmul_rn(__fadd_rn(mx[1], mn[1]), 0.5f);
+    cz[i] = __fmul_rn(__fadd_rn(mx[2], mn[2]), 0.5f);
+    idx[i] = (int32_t)i;
+}
+
+// The same for primitives given as boxes (6 floats: min xyz, max xyz), at
+// indices first .. first + count - 1.
+__global__ void k_box_setup(const float* __restrict__ boxes, int64_t first, int64_t count, int64_t stride,
+                            float* __restrict__ cx, float* __restrict__ cy, float* __restrict__ cz,
+                            int32_t* __restrict__ idx, float* __restrict__ pb) {
+    const int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= count) return;
+    const int64_t i = first + k;
+    float mn[3], mx[3];
+    for (int a = 0; a < 3; ++a) {
+        mn[a] = boxes[k * 6 + a];
+        mx[a] = boxes[k * 6 + 3 + a];
+        pb[a * stride + i] = mn[a];
+        pb[(3 + a) * stride + i] = mx[a];
     }
     cx[i] = __fmul_rn(__fadd_rn(mx[0], mn[0]), 0.5f);
     cy[i] = __fmul_rn(__fadd_rn(mx[1], mn[1]), 0.5f);

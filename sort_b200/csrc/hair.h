@@ -1,0 +1,30 @@
+// Hair line segments: the per-line record the traversal reads and its set-up.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstdint>
+
+#include "layout.h"
+
+namespace sg {
+
+// A line's record, 5 float4 per line in primitive order:
+//   [m00 m01 m02 m03] [m10 m11 m12 m13] [m20 m21 m22 m23]  world-to-line matrix rows
+//   [w0 w1 length (w1-w0)/length] [v0 v1 0 0]
+// A leaf slot that holds a line is {0, 0, 0, primitive index},
+// {0, 0, 0, last-in-leaf flag}, {line index, 0, 0, kLineSlot} (int bits).
+constexpr int kLineF4 = 5;
+constexpr int32_t kLineSlot = 1;
+
+// One segment in world space, 10 floats (p0 xyz, p1 xyz, v0, v1, w0, w1
+// half widths): its record (20 floats) and its box (min xyz, max xyz).
+void line_setup(const float* segment10, float* record20, float* box6);
+
+struct TraceLaunch;
+// Closest-hit or any-hit (L.any) over a tree whose leaves hold triangles and
+// lines (hair.cu).
+cudaError_t launch_trace_hair(const TraceLaunch& L, const DevTree& tr, const float4* lines, const DevRays& rays,
+                              int64_t n, cudaStream_t s);
+
+}  // namespace sg

@@ -1,0 +1,94 @@
+// Hair line set-up on the host: what SORT computes once per Line before any
+// ray is traced (shape/line.cpp:117-135 Line::SetTransform, 98-106
+// Line::GetBBox), in SORT's operation order (this file is compiled without
+// floating-point contraction, as SORT is), so the per-line constants and boxes
+// are bit-identical to SORT's.
+//
+// SORT's HairVisual builds its lines in object space and applies the entity's
+// transform (entity/visual.cpp:41-102); the lines given here are already in
+// world space, so the transform is the identity, which SORT still applies
+// through Matrix::TransformPoint (a -0 coordinate becomes +0).
+#include "hair.h"
+
+#include <cmath>
+
+namespace sg {
+namespace {
+
+struct V3 {
+    float x, y, z;
+};
+
+// Matrix::TransformPoint (math/matrix.cpp:70-82) for a matrix whose last row is
+// (0, 0, 0, 1): w is 1 for finite input.
+V3 transform_point(const float (&m)[12], const V3& p) {
+    V3 r;
+    r.x = p.x * m[0] + p.y * m[1] + p.z * m[2] + m[3];
+    r.y = p.x * m[4] + p.y * m[5] + p.z * m[6] + m[7];
+    r.z = p.x * m[8] + p.y * m[9] + p.z * m[10] + m[11];
+    const float w = p.x * 0.0f + p.y * 0.0f + p.z * 0.0f + 1.0f;
+    if (w != 1.0f) {  // Point / w, only for non-finite input
+        r.x /= w;
+        r.y /= w;
+        r.z /= w;
+    }
+    return r;
+}
+
+// normalize (math/vector3.h:163-168).
+V3 normalize(const V3& v) {
+    const float len = std::sqrt(v.x * v.x + v.y * v.y + v.z * v.z);
+    if (len == 0.0f) return v;
+    return V3{v.x / len, v.y / len, v.z / len};
+}
+
+}  // namespace
+
+void line_setup(const float* in, float* rec, float* box) {
+    const V3 p0{in[0], in[1], in[2]}, p1{in[3], in[4], in[5]};
+    const float v0 = in[6], v1 = in[7], w0 = in[8], w1 = in[9];
+    static const float identity[12] = {1.0f, 0.0f, 0.0f, 0.0f, 0.0f, 1.0f, 0.0f, 0.0f, 0.0f, 0.0f, 1.0f, 0.0f};
+    const V3 gp0 = transform_point(identity, p0), gp1 = transform_point(identity, p1);
+    const V3 y = normalize(V3{gp1.x - gp0.x, gp1.y - gp0.y, gp1.z - gp0.z});
+    // coordinateSystem (math/vector3.h:171-180)
+    V3 x;
+    if (std::fabs(y.x) > std::fabs(y.y)) {
+        const float inv = 1.0f / sqrtf(y.x * y.x + y.z * y.z);
+        x = V3{-y.z * inv, 0.0f, y.x * inv};
+    } else {
+        const float inv = 1.0f / sqrtf(y.y * y.y + y.z * y.z);
+        x = V3{0.0f, y.z * inv, -y.y * inv};
+    }
+    const V3 z{y.y * x.z - y.z * x.y, y.z * x.x - y.x * x.z, y.x * x.y - y.y * x.x};  // cross(y, x)
+    float m[12] = {x.x, x.y, x.z, -(x.x * gp0.x + x.y * gp0.y + x.z * gp0.z),
+                   y.x, y.y, y.z, -(y.x * gp0.x + y.y * gp0.y + y.z * gp0.z),
+                   z.x, z.y, z.z, -(z.x * gp0.x + z.y * gp0.y + z.z * gp0.z)};
+    const V3 lp0 = transform_point(m, gp0), lp1 = transform_point(m, gp1);
+    const float length = lp1.y - lp0.y;
+    for (int k = 0; k < 12; ++k) rec[k] = m[k];
+    rec[12] = w0;
+    rec[13] = w1;
+    rec[14] = length;
+    rec[15] = (w1 - w0) / length;  // formed per test by intersectLine_Inner (simd/simd_line.h:239)
+    rec[16] = v0;
+    rec[17] = v1;
+    rec[18] = 0.0f;
+    rec[19] = 0.0f;
+    // Line::GetBBox: BBox() then Union(gp0), Union(gp1) (math/bbox.cpp:106-113), Expend(max(w0, w1)).
+    float mn[3] = {3.402823466e+38f, 3.402823466e+38f, 3.402823466e+38f};
+    float mx[3] = {-3.402823466e+38f, -3.402823466e+38f, -3.402823466e+38f};
+    for (const V3& p : {gp0, gp1}) {
+        const float c[3] = {p.x, p.y, p.z};
+        for (int a = 0; a < 3; ++a) {
+            if (c[a] < mn[a]) mn[a] = c[a];
+            if (c[a] > mx[a]) mx[a] = c[a];
+        }
+    }
+    const float grow = w0 < w1 ? w1 : w0;  // std::max(w0, w1)
+    for (int a = 0; a < 3; ++a) {
+        box[a] = mn[a] - grow;
+        box[3 + a] = mx[a] + grow;
+    }
+}
+
+}  // namespace sg

@@ -270,3 +270,29 @@ def pt_scene(spheres: int, level: int, seed: int = 1, mat_seed: int = 5, light: 
     tri_gpu = np.ascontiguousarray(np.concatenate([tri, light_triangles(light)]))
     mat_gpu = np.concatenate([mat_of_tri, np.array([-1, -1], np.int32)])
     return tri, mat_of_tri, mats, light, tri_gpu, mat_gpu
+
+
+def hair_strands(strands: int, steps: int = 8, seed: int = 13, box: float = 10.0, length: float = 3.0,
+                 width_bottom: float = 0.05, width_tip: float = 0.01) -> np.ndarray:
+    """Hair segments (strands * steps, 10) float32: p0 xyz, p1 xyz, v0, v1, w0, w1.
+
+    Each strand grows from a random root in the box with a random bend; its
+    segments get widths and v as SORT's HairVisual derives them from the
+    cumulative length (entity/visual.cpp:58-94: width from bottom to tip, v
+    from 0 to 1, both interpolated by the length fraction)."""
+    rng = np.random.default_rng(seed)
+    out = np.zeros((strands * steps, 10), np.float32)
+    for s in range(strands):
+        p = [rng.uniform(-box, box, 3).astype(np.float32)]
+        d = rng.normal(size=3)
+        d /= np.linalg.norm(d)
+        for _ in range(steps):
+            d = d + rng.normal(scale=0.35, size=3)
+            d /= np.linalg.norm(d)
+            p.append((p[-1] + d * (length / steps) * rng.uniform(0.5, 1.5)).astype(np.float32))
+        seg = np.array([np.linalg.norm(p[j + 1].astype(np.float64) - p[j]) for j in range(steps)])
+        frac = np.concatenate([[0.0], np.cumsum(seg) / seg.sum()])
+        w = width_bottom * (1.0 - frac) + width_tip * frac
+        for j in range(steps):
+            out[s * steps + j] = (*p[j], *p[j + 1], frac[j], frac[j + 1], w[j], w[j + 1])
+    return out

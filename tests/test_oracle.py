@@ -83,3 +83,14 @@ def test_reference_attenuation_reproduces_golden(reference, width, assign):
     z = golden("attenuation")
     tree = reference.build_transparent(z["triangles"], z[assign], z["transparent"], z["rgb"], width)
     assert same_bits(tree.attenuation(z["rays"]), z[f"att{width}_{assign}"])
+
+
+@pytest.mark.parametrize("width", [4, 8])
+def test_reference_hair_reproduces_golden(reference, width):
+    """The committed hair fixture is what SORT's code returns (pins it)."""
+    z = golden("hair")
+    tree = reference.build_hair(z["triangles"], z["lines"], width)
+    prim, t, u, v = tree.closest(z["rays"])
+    assert np.array_equal(prim, z[f"prim{width}"]) and same_bits(t, z[f"t{width}"])
+    assert same_bits(u, z[f"u{width}"]) and same_bits(v, z[f"v{width}"])
+    assert np.array_equal(tree.any(z["rays"]), z[f"occ{width}"])
