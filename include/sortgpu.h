@@ -174,6 +174,68 @@ sg_status sg_scene_create(const float* triangles, int64_t ntri, const sg_build_o
  * SG_BUILDER_LBVH. sg_scene_info's triangle count is the primitive count. */
 sg_status sg_scene_create_hair(const float* triangles, int64_t ntri, const float* lines, int64_t nlines,
                                const sg_build_opts* opts, sg_scene** out);
+
+/* SORT's binary scene stream (what the Blender exporter writes and
+ * ImageEvaluation loads, work/image_evaluation/image_evaluation.cpp:62-108),
+ * read for the GPU path: the configuration with the integrator's parameters
+ * (loadConfig, 354-377), the material section (MatManager::ParseMatFile,
+ * material/matmanager.cpp:50-270: names and flags are kept, TSL shader graphs
+ * and resources are read past), the entities (Scene::LoadScene,
+ * core/scene.cpp:112-180: meshes and hair with their transforms, the camera,
+ * area lights; other lights are counted) and the accelerator. Triangles are in
+ * world space (Mesh::ApplyTransform); hair segments as HairVisual makes them
+ * (entity/visual.cpp:41-97). StringIDs are SORT's 32-bit hashes of the class
+ * names. Unknown classes or a broken stream: SG_ERR_UNSUPPORTED. */
+typedef struct sg_stream sg_stream;
+typedef struct {
+    int32_t version, threads, spp, image_width, image_height;
+    float clamp;
+    uint32_t integrator;     /* StringID of the integrator class (PathTracing, ...) */
+    int32_t max_depth;       /* Integrator::max_recursive_depth */
+    int32_t bssrdf_bounces;  /* PathTracing */
+    float ao_max_distance;   /* AmbientOcclusion */
+    int32_t mis;             /* BidirPathTracing, LightTracing */
+    int32_t ir_path_sets, ir_paths;
+    float ir_min_distance;   /* InstantRadiosity */
+    int64_t triangles, lines;
+    int32_t materials, area_lights, other_lights, has_camera, volumes;
+    uint32_t accelerator;    /* StringID of the accelerator class (Qbvh, Obvh, ...) */
+    int32_t accel_max_depth, accel_max_leaf;
+    int64_t entity_offset;   /* byte offset of the entity section ("verification bits") */
+} sg_stream_info;
+typedef struct {
+    float eye[3], up[3], target[3];
+    int32_t image_width, image_height;
+    float lens_radius, sensor_w, sensor_h;
+    int32_t aspect_fit;
+    float aspect_ratio_w, aspect_ratio_h, fov;
+} sg_stream_camera; /* PerspectiveCameraEntity::Serialize (entity/camera_entity.cpp:21-33) */
+typedef struct {
+    float light2world[16]; /* as streamed (SORT removes the scale afterwards, entity/light_entity.cpp:99-106) */
+    float energy;
+    float intensity[3];
+    uint32_t shape;        /* StringID: SQUARE, RECTANGLE or DISK */
+    float size_x, size_y;  /* SQUARE: size_x; RECTANGLE: both; DISK: size_x is the radius */
+} sg_stream_area_light;
+sg_status sg_stream_open(const char* path, sg_stream** out);
+sg_status sg_stream_info_get(const sg_stream* stream, sg_stream_info* info);
+/* 9 floats per triangle (world space) and its material index (-1: none). */
+sg_status sg_stream_triangles(const sg_stream* stream, float* triangles, int32_t* material);
+/* 10 floats per hair segment in world space (as sg_scene_create_hair takes
+ * them) and its material index. */
+sg_status sg_stream_lines(const sg_stream* stream, float* lines, int32_t* material);
+sg_status sg_stream_camera_get(const sg_stream* stream, sg_stream_camera* camera);
+sg_status sg_stream_area_light_get(const sg_stream* stream, int32_t index, sg_stream_area_light* light);
+/* Name (NUL-terminated, cap bytes available) and flags (bit 0: a transparency
+ * node, bit 1: an SSS node) of material `index` in the stream's order. */
+sg_status sg_stream_material(const sg_stream* stream, int32_t index, char* name, int64_t cap, int32_t* flags);
+/* The stream's scene as an sg_scene: its triangles, then its hair segments
+ * (their entity's transform applied as SORT's Line::SetTransform applies it).
+ * opts NULL: the stream's accelerator (Obvh: width 8, Qbvh: width 4, with
+ * their depth and leaf size; any other class: SORT's fallback, a QBVH with
+ * default parameters). */
+sg_status sg_stream_scene_create(const sg_stream* stream, const sg_build_opts* opts, sg_scene** out);
+sg_status sg_stream_close(sg_stream* stream);
 sg_status sg_scene_destroy(sg_scene* scene);
 sg_status sg_scene_info_get(const sg_scene* scene, sg_scene_info* info);
 sg_status sg_scene_topology(const sg_scene* scene, int32_t* out, int64_t cap, int64_t* written);

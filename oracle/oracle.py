@@ -181,6 +181,8 @@ class Reference:
         L.sortref_scene_create_transparent.argtypes = [ctypes.c_int, _vp, ctypes.c_int, _vp, ctypes.c_int, _vp, _vp,
                                                        ctypes.c_int, ctypes.c_int]
         L.sortref_trace_attenuation.argtypes = [_vp, _vp, _i64, _vp, ctypes.c_int]
+        L.sortref_scene_from_stream.restype = _vp
+        L.sortref_scene_from_stream.argtypes = [ctypes.c_char_p, _i64, ctypes.c_int, ctypes.c_int, ctypes.c_int]
         L.sortref_scene_create_hair.restype = _vp
         L.sortref_scene_create_hair.argtypes = [ctypes.c_int, _vp, ctypes.c_int, _vp, ctypes.c_int, ctypes.c_int,
                                                 ctypes.c_int]
@@ -215,6 +217,14 @@ class Reference:
         if not h:
             raise ValueError("reference build failed")
         return _Tree(self, h, width, tri.shape[0])
+
+    def build_from_stream(self, path: str, entity_offset: int, ntri: int, width: int, max_depth: int = 16,
+                          max_leaf: int = 8) -> _Tree:
+        """SORT's own visuals deserialized from a scene stream's entity section, then its tree."""
+        h = self.L.sortref_scene_from_stream(str(path).encode(), entity_offset, width, max_depth, max_leaf)
+        if not h:
+            raise ValueError("reference could not read the stream")
+        return _Tree(self, h, width, ntri)
 
     def build_hair(self, tri: np.ndarray, lines: np.ndarray, width: int, max_depth: int = 16,
                    max_leaf: int = 8) -> _Tree:

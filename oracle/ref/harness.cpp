@@ -48,6 +48,7 @@
 #include "math/interaction.h"
 #include "scatteringevent/bssrdf/bssrdf.h"
 #include "shape/line.h"
+#include "stream/fstream.h"
 #undef private
 #undef protected
 
@@ -167,6 +168,7 @@ public:
         m_visuals.push_back(std::move(v));
         return raw;
     }
+    void Push(std::unique_ptr<Visual> v) { m_visuals.push_back(std::move(v)); }
     HarnessHair* AddHair() {
         auto v = std::make_unique<HarnessHair>();
         HarnessHair* raw = v.get();
@@ -319,6 +321,109 @@ double sortref_build_seconds(void* h) { return ((RefScene*)h)->build_seconds; }
 void* sortref_scene_create_transparent(int width, const float* tri, int ntri, const int32_t* mat_of_tri, int nmat,
                                        const int32_t* transparent, const float* rgb, int max_depth, int max_leaf) {
     return make_ref_scene(width, tri, ntri, nullptr, 0, mat_of_tri, nmat, transparent, rgb, max_depth, max_leaf);
+}
+
+// The entity section of a SORT scene stream, from byte `offset` (its
+// "verification bits"), read with SORT's own IFileStream and visuals: each
+// VisualEntity's transform (VisualEntity::Serialize, entity/visual_entity.h:
+// 31-43) with its MeshVisual / HairVisual Serialize and ApplyTransform
+// (entity/visual.cpp). Cameras and lights are read past with their fields
+// (entity/camera_entity.cpp:21-33, entity/light_entity.cpp:25-150). Then the
+// accelerator of the given width over the primitives in SORT's order.
+void* sortref_scene_from_stream(const char* path, int64_t offset, int width, int max_depth, int max_leaf) {
+    if (width != 4 && width != 8) return nullptr;
+    IFileStream file(path);
+    IStreamBase& stream = file;  // the composite readers (StringID, Point, Transform) live on the base
+    std::vector<char> skip((size_t)offset);
+    if (offset > 0) stream.Load(skip.data(), (int)offset);
+    StringID check;
+    stream >> check;
+    if (!(check == StringID("verification bits"))) return nullptr;
+    auto* rs = new RefScene();
+    rs->width = width;
+    auto entity = std::make_unique<HarnessEntity>();
+    for (;;) {
+        StringID cls;
+        stream >> cls;
+        if (cls == StringID("End of Entities")) break;
+        if (cls == StringID("VisualEntity")) {
+            Transform xf;
+            stream >> xf;
+            unsigned cnt = 0;
+            stream >> cnt;
+            while (cnt-- > 0) {
+                StringID vc;
+                stream >> vc;
+                std::unique_ptr<Visual> v;
+                if (vc == StringID("MeshVisual"))
+                    v = std::make_unique<MeshVisual>();
+                else if (vc == StringID("HairVisual"))
+                    v = std::make_unique<HairVisual>();
+                else {
+                    delete rs;
+                    return nullptr;
+                }
+                v->Serialize(stream);
+                v->ApplyTransform(xf);
+                entity->Push(std::move(v));
+            }
+        } else if (cls == StringID("PerspectiveCameraEntity")) {
+            Point eye, target;
+            Vector up;
+            unsigned w, h;
+            float lens, sw, sh, arw, arh, fov;
+            int fit;
+            stream >> eye >> up >> target >> w >> h >> lens >> sw >> sh >> fit >> arw >> arh >> fov;
+        } else if (cls == StringID("AreaLightEntity")) {
+            Transform xf;
+            float energy;
+            Spectrum in;
+            StringID shape;
+            stream >> xf >> energy >> in >> shape;
+            float a, b;
+            if (shape == StringID("RECTANGLE"))
+                stream >> a >> b;
+            else
+                stream >> a;
+        } else if (cls == StringID("PointLightEntity") || cls == StringID("DirLightEntity") ||
+                   cls == StringID("SpotLightEntity")) {
+            Transform xf;
+            float energy;
+            Spectrum in;
+            stream >> xf >> energy >> in;
+            if (cls == StringID("SpotLightEntity")) {
+                float a, b;
+                stream >> a >> b;
+            }
+        } else if (cls == StringID("SkyLightEntity")) {
+            Transform xf;
+            float intensity;
+            Spectrum color;
+            std::string file;
+            stream >> xf >> intensity >> color >> file;
+        } else {
+            delete rs;
+            return nullptr;
+        }
+    }
+    rs->scene.m_entities.push_back(std::move(entity));
+    ScenePrimitiveIterator iter(rs->scene);
+    int32_t idx = 0;
+    while (auto p = iter.Next()) {
+        rs->index_of[p] = idx++;
+        rs->prims.push_back(p);
+        rs->scene.m_bbox.Union(p->GetBBox());
+    }
+    static const auto threshold = 0.001f;  // core/scene.cpp:150-154
+    auto delta = (rs->scene.m_bbox.m_Max - rs->scene.m_bbox.m_Min) * threshold;
+    rs->scene.m_bbox.m_Min -= delta;
+    rs->scene.m_bbox.m_Max += delta;
+    if (width == 4)
+        rs->scene.m_accelerator.reset(harness_make_qbvh((unsigned)max_depth, (unsigned)max_leaf));
+    else
+        rs->scene.m_accelerator.reset(harness_make_obvh((unsigned)max_depth, (unsigned)max_leaf));
+    rs->scene.m_accelerator->Build(rs->scene);
+    return rs;
 }
 
 // Triangles followed by hair segments (10 floats each: p0, p1, v0, v1, w0, w1),

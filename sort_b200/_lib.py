@@ -69,6 +69,29 @@ class Transparency(ctypes.Structure):
     _fields_ = [("transparent", ctypes.c_int32), ("rgb", ctypes.c_float * 3)]
 
 
+class StreamInfo(ctypes.Structure):
+    _fields_ = [(n, ctypes.c_int32) for n in ("version", "threads", "spp", "image_width", "image_height")] + [
+        ("clamp", ctypes.c_float), ("integrator", ctypes.c_uint32), ("max_depth", ctypes.c_int32),
+        ("bssrdf_bounces", ctypes.c_int32), ("ao_max_distance", ctypes.c_float), ("mis", ctypes.c_int32),
+        ("ir_path_sets", ctypes.c_int32), ("ir_paths", ctypes.c_int32), ("ir_min_distance", ctypes.c_float),
+        ("triangles", ctypes.c_int64), ("lines", ctypes.c_int64)] + [
+        (n, ctypes.c_int32) for n in ("materials", "area_lights", "other_lights", "has_camera", "volumes")] + [
+        ("accelerator", ctypes.c_uint32), ("accel_max_depth", ctypes.c_int32), ("accel_max_leaf", ctypes.c_int32),
+        ("entity_offset", ctypes.c_int64)]
+
+
+class StreamCamera(ctypes.Structure):
+    _fields_ = [("eye", ctypes.c_float * 3), ("up", ctypes.c_float * 3), ("target", ctypes.c_float * 3),
+                ("image_width", ctypes.c_int32), ("image_height", ctypes.c_int32), ("lens_radius", ctypes.c_float),
+                ("sensor_w", ctypes.c_float), ("sensor_h", ctypes.c_float), ("aspect_fit", ctypes.c_int32),
+                ("aspect_ratio_w", ctypes.c_float), ("aspect_ratio_h", ctypes.c_float), ("fov", ctypes.c_float)]
+
+
+class StreamAreaLight(ctypes.Structure):
+    _fields_ = [("light2world", ctypes.c_float * 16), ("energy", ctypes.c_float), ("intensity", ctypes.c_float * 3),
+                ("shape", ctypes.c_uint32), ("size_x", ctypes.c_float), ("size_y", ctypes.c_float)]
+
+
 class Batch(ctypes.Structure):
     _fields_ = [("scene", ctypes.c_void_p), ("rays", ctypes.c_void_p), ("stride", ctypes.c_int64),
                 ("n", ctypes.c_int64), ("any", ctypes.c_int32), ("reserved", ctypes.c_int32), ("hits", Hits),
@@ -129,6 +152,15 @@ _SIGNATURES = {
     "sg_scene_topology": (ctypes.c_int, [_vp, _vp, _i64, ctypes.POINTER(_i64)]),
     "sg_build_topology_host": (ctypes.c_int, [_vp, _i64, ctypes.POINTER(BuildOpts), _vp, _i64,
                                               ctypes.POINTER(_i64), ctypes.POINTER(ctypes.c_int32)]),
+    "sg_stream_open": (ctypes.c_int, [ctypes.c_char_p, ctypes.POINTER(_vp)]),
+    "sg_stream_info_get": (ctypes.c_int, [_vp, ctypes.POINTER(StreamInfo)]),
+    "sg_stream_triangles": (ctypes.c_int, [_vp, _vp, _vp]),
+    "sg_stream_lines": (ctypes.c_int, [_vp, _vp, _vp]),
+    "sg_stream_camera_get": (ctypes.c_int, [_vp, ctypes.POINTER(StreamCamera)]),
+    "sg_stream_area_light_get": (ctypes.c_int, [_vp, ctypes.c_int32, ctypes.POINTER(StreamAreaLight)]),
+    "sg_stream_material": (ctypes.c_int, [_vp, ctypes.c_int32, ctypes.c_char_p, _i64, ctypes.POINTER(ctypes.c_int32)]),
+    "sg_stream_scene_create": (ctypes.c_int, [_vp, ctypes.POINTER(BuildOpts), ctypes.POINTER(_vp)]),
+    "sg_stream_close": (ctypes.c_int, [_vp]),
     "sg_build_topology_host_hair": (ctypes.c_int, [_vp, _i64, _vp, _i64, ctypes.POINTER(BuildOpts), _vp, _i64,
                                                    ctypes.POINTER(_i64), ctypes.POINTER(ctypes.c_int32)]),
     "sg_scene_set_tuning": (ctypes.c_int, [_vp, ctypes.POINTER(Tuning)]),

@@ -291,10 +291,11 @@ void sg_default_build_opts(sg_build_opts* o) {
 
 }  // extern "C"
 
-namespace {
+namespace sg {
 
-sg_status create_scene(const float* triangles, int64_t ntri, const float* lines, int64_t nlines,
-                       const sg_build_opts* opts, sg_scene** out) {
+sg_status scene_create_mixed(const float* triangles, int64_t ntri, const float* lines, int64_t nlines,
+                             const float* transforms, const int32_t* line_transform, const sg_build_opts* opts,
+                             sg_scene** out) {
     if (!out) return fail(SG_ERR_INVALID_ARGUMENT, "out is NULL");
     *out = nullptr;
     if (!opts) return fail(SG_ERR_INVALID_ARGUMENT, "opts is NULL");
@@ -332,7 +333,9 @@ sg_status create_scene(const float* triangles, int64_t ntri, const float* lines,
         delete s;
         return fail(SG_ERR_OUT_OF_MEMORY, "host allocation failed");
     }
-    for (int64_t k = 0; k < nlines; ++k) sg::line_setup(lines + k * 10, &line_recs[size_t(k) * 20], &line_boxes[size_t(k) * 6]);
+    for (int64_t k = 0; k < nlines; ++k)
+        sg::line_setup(lines + k * 10, &line_recs[size_t(k) * 20], &line_boxes[size_t(k) * 6],
+                       transforms ? transforms + size_t(line_transform[k]) * 16 : nullptr);
     bp.extra_boxes = line_boxes.data();
     bp.nextra = nlines;
     if (opts->builder != SG_BUILDER_HOST && opts->builder != SG_BUILDER_GPU && opts->builder != SG_BUILDER_LBVH) {
@@ -388,17 +391,17 @@ sg_status create_scene(const float* triangles, int64_t ntri, const float* lines,
     return SG_OK;
 }
 
-}  // namespace
+}  // namespace sg
 
 extern "C" {
 
 sg_status sg_scene_create(const float* triangles, int64_t ntri, const sg_build_opts* opts, sg_scene** out) {
-    return create_scene(triangles, ntri, nullptr, 0, opts, out);
+    return sg::scene_create_mixed(triangles, ntri, nullptr, 0, nullptr, nullptr, opts, out);
 }
 
 sg_status sg_scene_create_hair(const float* triangles, int64_t ntri, const float* lines, int64_t nlines,
                                const sg_build_opts* opts, sg_scene** out) {
-    return create_scene(triangles, ntri, lines, nlines, opts, out);
+    return sg::scene_create_mixed(triangles, ntri, lines, nlines, nullptr, nullptr, opts, out);
 }
 
 sg_status sg_scene_destroy(sg_scene* s) {

@@ -17,9 +17,13 @@ namespace sg {
 constexpr int kLineF4 = 5;
 constexpr int32_t kLineSlot = 1;
 
-// One segment in world space, 10 floats (p0 xyz, p1 xyz, v0, v1, w0, w1
-// half widths): its record (20 floats) and its box (min xyz, max xyz).
-void line_setup(const float* segment10, float* record20, float* box6);
+// One segment, 10 floats (p0 xyz, p1 xyz, v0, v1, w0, w1 half widths), in
+// the space `transform` (SORT's row-major 4x4 Matrix; NULL = the identity)
+// maps to world space: its record (20 floats) and its box (min xyz, max xyz).
+void line_setup(const float* segment10, float* record20, float* box6, const float* transform16 = nullptr);
+
+// Matrix::TransformPoint (math/matrix.cpp:70-82) of a row-major 4x4.
+void transform_point16(const float* m16, const float* p, float* out);
 
 struct TraceLaunch;
 // Closest-hit or any-hit (L.any) over a tree whose leaves hold triangles and

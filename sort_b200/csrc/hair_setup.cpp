@@ -5,9 +5,10 @@
 // are bit-identical to SORT's.
 //
 // SORT's HairVisual builds its lines in object space and applies the entity's
-// transform (entity/visual.cpp:41-102); the lines given here are already in
-// world space, so the transform is the identity, which SORT still applies
-// through Matrix::TransformPoint (a -0 coordinate becomes +0).
+// transform (entity/visual.cpp:41-102); lines given in world space take the
+// identity, which SORT would still apply through Matrix::TransformPoint (a -0
+// coordinate becomes +0), and lines read from a scene stream take their
+// entity's transform.
 #include "hair.h"
 
 #include <cmath>
@@ -19,20 +20,11 @@ struct V3 {
     float x, y, z;
 };
 
-// Matrix::TransformPoint (math/matrix.cpp:70-82) for a matrix whose last row is
-// (0, 0, 0, 1): w is 1 for finite input.
-V3 transform_point(const float (&m)[12], const V3& p) {
-    V3 r;
-    r.x = p.x * m[0] + p.y * m[1] + p.z * m[2] + m[3];
-    r.y = p.x * m[4] + p.y * m[5] + p.z * m[6] + m[7];
-    r.z = p.x * m[8] + p.y * m[9] + p.z * m[10] + m[11];
-    const float w = p.x * 0.0f + p.y * 0.0f + p.z * 0.0f + 1.0f;
-    if (w != 1.0f) {  // Point / w, only for non-finite input
-        r.x /= w;
-        r.y /= w;
-        r.z /= w;
-    }
-    return r;
+V3 transform_point(const float* m, const V3& p) {
+    const float in[3] = {p.x, p.y, p.z};
+    float out[3];
+    transform_point16(m, in, out);
+    return V3{out[0], out[1], out[2]};
 }
 
 // normalize (math/vector3.h:163-168).
@@ -44,11 +36,29 @@ V3 normalize(const V3& v) {
 
 }  // namespace
 
-void line_setup(const float* in, float* rec, float* box) {
+void transform_point16(const float* m, const float* p, float* out) {
+    const float x = p[0] * m[0] + p[1] * m[1] + p[2] * m[2] + m[3];
+    const float y = p[0] * m[4] + p[1] * m[5] + p[2] * m[6] + m[7];
+    const float z = p[0] * m[8] + p[1] * m[9] + p[2] * m[10] + m[11];
+    const float w = p[0] * m[12] + p[1] * m[13] + p[2] * m[14] + m[15];
+    if (w == 1.0f) {
+        out[0] = x;
+        out[1] = y;
+        out[2] = z;
+    } else {  // Point / w (math/vector3.h:218-220)
+        out[0] = x / w;
+        out[1] = y / w;
+        out[2] = z / w;
+    }
+}
+
+void line_setup(const float* in, float* rec, float* box, const float* transform16) {
     const V3 p0{in[0], in[1], in[2]}, p1{in[3], in[4], in[5]};
     const float v0 = in[6], v1 = in[7], w0 = in[8], w1 = in[9];
-    static const float identity[12] = {1.0f, 0.0f, 0.0f, 0.0f, 0.0f, 1.0f, 0.0f, 0.0f, 0.0f, 0.0f, 1.0f, 0.0f};
-    const V3 gp0 = transform_point(identity, p0), gp1 = transform_point(identity, p1);
+    static const float identity[16] = {1.0f, 0.0f, 0.0f, 0.0f, 0.0f, 1.0f, 0.0f, 0.0f,
+                                       0.0f, 0.0f, 1.0f, 0.0f, 0.0f, 0.0f, 0.0f, 1.0f};
+    const float* t16 = transform16 ? transform16 : identity;
+    const V3 gp0 = transform_point(t16, p0), gp1 = transform_point(t16, p1);
     const V3 y = normalize(V3{gp1.x - gp0.x, gp1.y - gp0.y, gp1.z - gp0.z});
     // coordinateSystem (math/vector3.h:171-180)
     V3 x;
@@ -60,9 +70,10 @@ void line_setup(const float* in, float* rec, float* box) {
         x = V3{0.0f, y.z * inv, -y.y * inv};
     }
     const V3 z{y.y * x.z - y.z * x.y, y.z * x.x - y.x * x.z, y.x * x.y - y.y * x.x};  // cross(y, x)
-    float m[12] = {x.x, x.y, x.z, -(x.x * gp0.x + x.y * gp0.y + x.z * gp0.z),
-                   y.x, y.y, y.z, -(y.x * gp0.x + y.y * gp0.y + y.z * gp0.z),
-                   z.x, z.y, z.z, -(z.x * gp0.x + z.y * gp0.y + z.z * gp0.z)};
+    const float m[16] = {x.x, x.y, x.z, -(x.x * gp0.x + x.y * gp0.y + x.z * gp0.z),
+                         y.x, y.y, y.z, -(y.x * gp0.x + y.y * gp0.y + y.z * gp0.z),
+                         z.x, z.y, z.z, -(z.x * gp0.x + z.y * gp0.y + z.z * gp0.z),
+                         0.0f, 0.0f, 0.0f, 1.0f};
     const V3 lp0 = transform_point(m, gp0), lp1 = transform_point(m, gp1);
     const float length = lp1.y - lp0.y;
     for (int k = 0; k < 12; ++k) rec[k] = m[k];

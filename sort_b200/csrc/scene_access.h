@@ -9,6 +9,13 @@
 
 namespace sg {
 
+// Scene creation with hair segments in object space: segment k is mapped to
+// world space by the row-major 4x4 transforms[16 * line_transform[k]] (both
+// NULL: the segments are in world space).
+sg_status scene_create_mixed(const float* triangles, int64_t ntri, const float* lines, int64_t nlines,
+                             const float* transforms, const int32_t* line_transform, const sg_build_opts* opts,
+                             sg_scene** out);
+
 // Records msg for sg_last_error() and returns s.
 sg_status set_error(sg_status s, const char* msg);
 

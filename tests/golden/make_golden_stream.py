@@ -1,0 +1,106 @@
+"""Generate tests/golden/scene.sort and tests/golden/stream.npz (oracle/_ref).
+
+Run from the repository root after ``make -C oracle ref``:
+
+    python tests/golden/make_golden_stream.py
+
+scene.sort is a SORT scene stream written by tests/sortstream_writer.py: a
+PathTracing configuration, a material section with a resource, a shader unit
+template, a shader group template and three materials, then a camera, two
+mesh entities (two transformed icospheres in one, a ground quad in the
+other), a hair entity with its own transform, an area light, a point light and
+a sky light, and an Obvh accelerator. stream.npz holds what SORT does with
+the entity section: its own MeshVisual / HairVisual Serialize and
+ApplyTransform, its tree (width 4 and 8), and its closest hits and any-hit
+answers for a ray set, plus the tree topologies.
+"""
+from __future__ import annotations
+
+import os
+import sys
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.dirname(os.path.dirname(os.path.abspath(__file__))))
+sys.path.insert(0, ROOT)
+sys.path.insert(0, os.path.join(ROOT, "tests"))
+
+from oracle.oracle import Reference  # noqa: E402
+from sort_b200 import scenes  # noqa: E402
+from sort_b200.stream import SortStream  # noqa: E402
+from sortstream_writer import write_stream  # noqa: E402
+
+OUT = os.path.dirname(os.path.abspath(__file__))
+
+
+def transform(angle, axis, scale, offset):
+    axis = np.asarray(axis, np.float64) / np.linalg.norm(axis)
+    c, s = np.cos(angle), np.sin(angle)
+    k = np.array([[0, -axis[2], axis[1]], [axis[2], 0, -axis[0]], [-axis[1], axis[0], 0]])
+    r = np.eye(3) * c + s * k + (1 - c) * np.outer(axis, axis)
+    m = np.eye(4)
+    m[:3, :3] = r * scale
+    m[:3, 3] = offset
+    return m.astype(np.float32)
+
+
+def scene_entities():
+    verts, faces = scenes.icosphere(3)
+    rng = np.random.default_rng(61)
+    mesh_a = (verts, faces, rng.integers(0, 3, len(faces)))
+    mesh_b = (verts * 0.5, faces, rng.integers(-1, 3, len(faces)))
+    ground = (np.array([[-20, -3, -20], [20, -3, -20], [20, -3, 20], [-20, -3, 20]], np.float32),
+              np.array([[0, 1, 2], [0, 2, 3]]), np.array([1, 1]))
+    strands = []
+    for _ in range(60):
+        root = rng.uniform(-1, 1, 3)
+        root /= np.linalg.norm(root)
+        pts = [root]
+        d = root.copy()
+        for _ in range(int(rng.integers(2, 8))):
+            d = d + rng.normal(scale=0.3, size=3)
+            d /= np.linalg.norm(d)
+            pts.append(pts[-1] + 0.25 * d)
+        strands.append(np.array(pts, np.float32))
+    return [
+        ("camera", (0.0, 1.0, 12.0), (0.0, 1.0, 0.0), (0.0, 0.0, 0.0)),
+        ("mesh", transform(0.4, (1, 2, 3), 2.0, (-3, 0, 0)), [mesh_a, mesh_b]),
+        ("mesh", np.eye(4, dtype=np.float32), [ground]),
+        ("hair", transform(-0.7, (0, 1, 1), 2.0, (3, 0.5, 0)), strands, 0.01, 0.04, 2),
+        ("area", transform(0.0, (1, 0, 0), 1.0, (0, 8, 0)), 20.0, (1.0, 0.95, 0.9), "RECTANGLE", (2.0, 1.5)),
+        ("point", transform(0.0, (1, 0, 0), 1.0, (5, 5, 5))),
+        ("sky", np.eye(4, dtype=np.float32)),
+    ]
+
+
+def main():
+    path = os.path.join(OUT, "scene.sort")
+    write_stream(path, materials=[("Wood", False, False), ("Glass", True, False), ("Skin", False, True)],
+                 entities=scene_entities(), accelerator=("Obvh", 16, 8))
+    s = SortStream(path)
+    ntri, nlines = s.info["triangles"], s.info["lines"]
+    rng = np.random.default_rng(62)
+    m = 3000  # rays aimed at the geometry: hair segment points and triangle centres
+    pick = rng.integers(0, nlines, m // 2)
+    f = rng.uniform(0.1, 0.9, (m // 2, 1))
+    tgt = np.concatenate([s.lines[pick, 0:3] * (1 - f) + s.lines[pick, 3:6] * f,
+                          s.triangles[rng.integers(0, ntri, m - m // 2)].reshape(-1, 3, 3).mean(1)])
+    o = tgt + rng.normal(size=(m, 3)) * 8.0
+    d = tgt - o
+    d /= np.linalg.norm(d, axis=1, keepdims=True)
+    aimed = np.concatenate([o.T, d.T, np.zeros((1, m)), np.full((1, m), 3.4e38)]).astype(np.float32)
+    rays = np.ascontiguousarray(np.concatenate([aimed, scenes.random_rays(2000, seed=63, box=6.0)], axis=1))
+    ref = Reference()
+    out = {"rays": rays, "entity_offset": s.info["entity_offset"], "triangles": ntri, "lines": nlines}
+    for w in (4, 8):
+        tree = ref.build_from_stream(path, s.info["entity_offset"], ntri + nlines, w)
+        prim, t, u, v = tree.closest(rays)
+        out.update({f"prim{w}": prim, f"t{w}": t, f"u{w}": u, f"v{w}": v, f"occ{w}": tree.any(rays),
+                    f"topology{w}": tree.topology(), f"depth{w}": tree.depth()})
+        print(f"width {w}: hits {np.mean(prim >= 0):.3f}, on hair {np.mean(prim >= ntri):.3f}")
+    np.savez_compressed(os.path.join(OUT, "stream.npz"), **out)
+    print(f"{ntri} triangles, {nlines} hair segments, {os.path.getsize(path)} bytes")
+
+
+if __name__ == "__main__":
+    main()
