@@ -345,6 +345,7 @@ def run_ours(args):
             traffic = tj.get("dram_bytes_per_launch")
 
     if rank == 0:
+        sorted_schedule = args.nodes == "fp32" and n >= (1 << 21)
         out = {
             "metric": METRIC if width == 8 else "Mrays/s primary closest-hit", "value": round(value, 3),
             "unit": UNIT, "n_gpus": world, "steps": args.steps,
@@ -355,7 +356,10 @@ def run_ours(args):
                 ({"tree": "LBVH (Morton-order wide BVH built on the GPU; algorithmic bytes counted on SORT's tree)"}
                  if args.builder == "lbvh" else {})) | (
                 {"parallelism": f"replicas x{world}", "build_seconds": round(info["build_seconds"], 2),
-                                       "tree_device_bytes": info["device_bytes"]}),
+                 "tree_device_bytes": info["device_bytes"],
+                 "schedule": "rays sorted by a 30-bit coherence key, then one per thread (default for "
+                             ">= 2^21 closest-hit rays; the sort is inside the timed step)"
+                             if sorted_schedule else "one ray per thread"}),
             "roofline": {"bound": bound, "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
                          "frac": round(achieved / peak, 4), "traffic": traffic,
                          "peak_source": peak_src,
@@ -370,7 +374,9 @@ def run_ours(args):
             "e2e": {"value": round(e2e_value, 3), "unit": UNIT, "h2d_bytes_per_step": int(n * 32),
                     "d2h_bytes_per_step": int(n * 16)},
             "clocks": clocks.summary(),
-            "gpu_launches": args.steps,
+            # the default schedule sorts closest-hit batches of >= 2^21 FP32 rays: a key kernel, CUB's
+            # radix sort (histogram, scan, four one-sweep passes), then the traversal kernel
+            "gpu_launches": args.steps * (8 if sorted_schedule else 1),
             **({"parity_vs_fp32_nodes": parity} if parity else {}),
         }
         if world == 1 and not args.no_cpu_baseline:

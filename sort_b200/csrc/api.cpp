@@ -787,7 +787,7 @@ sg_status sg_trace_any_host(const sg_scene* s, const float* rays8, int64_t n, ui
 
 sg_status sg_scene_set_tuning(sg_scene* s, const sg_trace_tuning* t) {
     if (!s || !t) return fail(SG_ERR_INVALID_ARGUMENT, "NULL argument");
-    if (t->schedule < SG_SCHEDULE_THREAD_PER_RAY || t->schedule > SG_SCHEDULE_SPECULATIVE)
+    if (t->schedule < SG_SCHEDULE_THREAD_PER_RAY || t->schedule > SG_SCHEDULE_AUTO)
         return fail(SG_ERR_INVALID_ARGUMENT, "unknown schedule");
     if (t->refill_threshold < 1 || t->refill_threshold > 32)
         return fail(SG_ERR_INVALID_ARGUMENT, "refill_threshold must be 1..32");

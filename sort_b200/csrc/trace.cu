@@ -20,10 +20,19 @@
 //     nearest) stays in registers and is descended into directly;
 //   * leaf triangles are fetched two at a time (the triangle array carries one
 //     padding slot), so the second's loads overlap the first's test;
-//   * two schedules: one ray per thread for the whole launch, or persistent
-//     warps in which a lane whose ray finished takes the next ray of the batch,
-//     so warps stay full instead of idling on their slowest ray.
+//   * schedules: one ray per thread for the whole launch; persistent warps in
+//     which a lane whose ray finished takes the next ray of the batch, so warps
+//     stay full instead of idling on their slowest ray; while-while and its
+//     speculative form; and one ray per thread with the rays taken in the order
+//     of a coherence key (direction octant, origin cell, coarse direction), so
+//     a warp's rays visit similar nodes (fewer idle lanes), which the automatic
+//     default uses for large closest-hit batches.
 #include <cuda_runtime.h>
+
+#include <cub/device/device_radix_sort.cuh>
+
+#include <mutex>
+#include <vector>
 
 #include "trace_kernels.h"
 #include "traversal.cuh"
@@ -109,15 +118,18 @@ __global__ void __launch_bounds__(128) k_trace_fp32_ww(DevTree tr, DevRays rays,
 // One ray per thread for the whole launch. With n_dev set, the batch size is
 // min(n, *n_dev), read on the device (queues whose length only the GPU knows).
 // Q8 reads 8-bit nodes.
+// With `order` set, thread k traces ray order[k] (the sorted schedule).
 template <int W, bool ANY, int STACK, bool STATS, bool Q8 = false>
 __global__ void __launch_bounds__(128) k_trace_fp32(DevTree tr, DevRays rays, int64_t n, int32_t* __restrict__ prim_out,
                                                     float* __restrict__ t_out, float* __restrict__ u_out,
                                                     float* __restrict__ v_out, uint8_t* __restrict__ occ_out,
                                                     int* __restrict__ err, unsigned long long* __restrict__ stats,
-                                                    const int* __restrict__ n_dev) {
-    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (n_dev && i >= (int64_t)*n_dev) return;
-    if (i >= n) return;
+                                                    const int* __restrict__ n_dev,
+                                                    const int32_t* __restrict__ order = nullptr) {
+    const int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (n_dev && k >= (int64_t)*n_dev) return;
+    if (k >= n) return;
+    const int64_t i = order ? (int64_t)__ldg(order + k) : k;
     Traversal<W, ANY, STACK, STATS, Q8> tv;
     if (tv.start(tr, rays, i))
         while (!tv.step(tr, err)) {
@@ -176,10 +188,113 @@ __global__ void __launch_bounds__(128) k_trace_fp32_persistent(DevTree tr, DevRa
     }
 }
 
+// Stream-ordered scratch for the sorted schedule: one pool per device that
+// keeps up to 1 GiB mapped between launches (NULL if it cannot be made).
+static cudaMemPool_t trace_scratch_pool(int device) {
+    static std::mutex lock;
+    static std::vector<cudaMemPool_t> pools;
+    std::lock_guard<std::mutex> g(lock);
+    if (device < 0) return nullptr;
+    if (pools.size() <= size_t(device)) pools.resize(size_t(device) + 1, nullptr);
+    if (!pools[size_t(device)]) {
+        cudaMemPoolProps props{};
+        props.allocType = cudaMemAllocationTypePinned;
+        props.location.type = cudaMemLocationTypeDevice;
+        props.location.id = device;
+        cudaMemPool_t pool = nullptr;
+        if (cudaMemPoolCreate(&pool, &props) != cudaSuccess) return nullptr;
+        uint64_t keep = uint64_t(1) << 30;
+        cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep);
+        pools[size_t(device)] = pool;
+    }
+    return pools[size_t(device)];
+}
+
+// Coherence key of a ray: direction octant (3 bits), origin cell in the scene
+// box (7 bits per axis, Morton order), coarse direction (2 bits per axis).
+__device__ __forceinline__ uint32_t spread7(uint32_t v) {  // 7 bits to every third bit
+    uint32_t r = 0;
+#pragma unroll
+    for (int b = 0; b < 7; ++b) r |= ((v >> b) & 1u) << (3 * b);
+    return r;
+}
+
+__global__ void k_ray_keys(DevRays rays, int64_t n, float3 lo, float3 inv_ext, uint32_t* __restrict__ keys,
+                           int32_t* __restrict__ index) {
+    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const float o[3] = {rays.ox[i], rays.oy[i], rays.oz[i]}, d[3] = {rays.dx[i], rays.dy[i], rays.dz[i]};
+    const float l[3] = {lo.x, lo.y, lo.z}, s[3] = {inv_ext.x, inv_ext.y, inv_ext.z};
+    uint32_t oct = 0, cell = 0, dir = 0;
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+        oct |= (d[a] < 0.0f ? 1u : 0u) << (2 - a);
+        const float q = fminf(fmaxf((o[a] - l[a]) * s[a], 0.0f), 127.0f);  // NaN -> 0
+        cell |= spread7((uint32_t)q) << (2 - a);
+        const float e = fminf(fmaxf((d[a] + 1.0f) * 2.0f, 0.0f), 3.0f);
+        dir |= ((uint32_t)e & 1u) << (2 - a) | (((uint32_t)e >> 1) & 1u) << (5 - a);
+    }
+    keys[i] = (oct << 27) | (cell << 6) | dir;
+    index[i] = (int32_t)i;
+}
+
+// The sorted schedule: keys, a 30-bit radix sort of (key, ray), then one ray
+// per thread in sorted order. Scratch comes from the library's stream-ordered
+// pool and is freed in stream order.
+template <int W, bool ANY, int STACK>
+static cudaError_t launch_sorted(const TraceLaunch& L, const DevTree& tr, const DevRays& rays, int64_t n,
+                                 cudaStream_t s) {
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return e;
+    cudaMemPool_t pool = trace_scratch_pool(dev);
+    if (!pool) return cudaErrorMemoryAllocation;
+    const int count = (int)n;
+    size_t temp = 0;
+    e = cub::DeviceRadixSort::SortPairs(nullptr, temp, (const uint32_t*)nullptr, (uint32_t*)nullptr,
+                                        (const int32_t*)nullptr, (int32_t*)nullptr, count, 0, 30, s);
+    if (e != cudaSuccess) return e;
+    const size_t al = 256, nb = ((size_t(n) * 4 + al - 1) / al) * al;
+    char* base = nullptr;
+    e = cudaMallocFromPoolAsync(reinterpret_cast<void**>(&base), 4 * nb + temp, pool, s);
+    if (e != cudaSuccess) return e;
+    uint32_t* keys = reinterpret_cast<uint32_t*>(base);
+    uint32_t* keys_sorted = reinterpret_cast<uint32_t*>(base + nb);
+    int32_t* index = reinterpret_cast<int32_t*>(base + 2 * nb);
+    int32_t* order = reinterpret_cast<int32_t*>(base + 3 * nb);
+    const float3 lo = make_float3(tr.box_lo[0], tr.box_lo[1], tr.box_lo[2]);
+    float inv[3];
+    for (int a = 0; a < 3; ++a) {
+        const float ext = tr.box_hi[a] - tr.box_lo[a];
+        inv[a] = ext > 0.0f ? 128.0f / ext : 0.0f;
+    }
+    const int threads = 128;
+    const unsigned blocks = (unsigned)((n + threads - 1) / threads);
+    k_ray_keys<<<blocks, threads, 0, s>>>(rays, n, lo, make_float3(inv[0], inv[1], inv[2]), keys, index);
+    e = cudaGetLastError();
+    if (e == cudaSuccess)
+        e = cub::DeviceRadixSort::SortPairs(base + 4 * nb, temp, keys, keys_sorted, index, order, count, 0, 30, s);
+    if (e == cudaSuccess) {
+        k_trace_fp32<W, ANY, STACK, false><<<blocks, threads, 0, s>>>(tr, rays, n, L.prim, L.t, L.u, L.v, L.occ,
+                                                                       L.err, nullptr, nullptr, order);
+        e = cudaGetLastError();
+    }
+    const cudaError_t f = cudaFreeAsync(base, s);
+    return e != cudaSuccess ? e : f;
+}
+
 template <int W, bool ANY, int STACK, bool STATS>
 static cudaError_t launch_stack(const TraceLaunch& L, const DevTree& tr, const DevRays& rays, int64_t n,
                                 cudaStream_t s) {
     const int threads = 128;
+    // Batches large enough for reordering to pay (and within a 32-bit sort);
+    // the automatic choice sorts large closest-hit batches only (any-hit rays
+    // end early, and measured no faster sorted).
+    const bool sorted = L.tuning.schedule == kScheduleSorted ? n >= (int64_t(1) << 16)
+                        : L.tuning.schedule == kScheduleAuto  ? !ANY && n >= (int64_t(1) << 21)
+                                                              : false;
+    if (!STATS && !L.q8 && !L.n_dev && sorted && n < (int64_t(1) << 31))
+        return launch_sorted<W, ANY, STACK>(L, tr, rays, n, s);
     // Counting launches keep the one-entry-per-step loop, whose interior-node
     // visits are exactly SORT's (speculation visits extra ones).
     // 8-bit nodes are read by the one-ray-per-thread kernel.

@@ -13,9 +13,11 @@ constexpr int kScheduleThreadPerRay = 0;  // one ray per thread for the whole la
 constexpr int kSchedulePersistent = 1;    // persistent warps refilling idle lanes
 constexpr int kScheduleWhileWhile = 2;    // warp alternates interior and leaf phases
 constexpr int kScheduleSpeculative = 3;   // while-while, lanes keep descending past their first leaf
+constexpr int kScheduleSorted = 4;        // one ray per thread, rays taken in the order of a coherence key
+constexpr int kScheduleAuto = 5;          // sorted for large closest-hit batches, else thread per ray
 
 struct TraceTuning {
-    int schedule = kScheduleThreadPerRay;
+    int schedule = kScheduleAuto;
     int refill_threshold = 8;  // idle lanes of a warp that trigger a refill (1..32)
 };
 

@@ -192,7 +192,8 @@ def test_gpu_trace_stats_match_oracle_counters(port, width):
 @pytest.mark.parametrize("width", [4, 8])
 def test_gpu_schedules_give_identical_results(port, width):
     """The launch schedule (thread per ray, persistent warps with any refill
-    threshold) never changes a result."""
+    threshold, while-while, speculative, rays sorted by a coherence key) never
+    changes a result; the sorted schedule twice in a row (its scratch reused)."""
     from sort_b200 import scenes
     tri = scenes.sphere_field(32, 3, seed=15)
     rays = np.concatenate([scenes.camera_rays(200, 200, seed=16), scenes.random_rays(60_000, seed=17)], axis=1)
@@ -201,7 +202,7 @@ def test_gpu_schedules_give_identical_results(port, width):
     ref = port.build(tri, width)
     rp, rt, ru, rv = ref.closest(rays)
     ro = ref.any(rays)
-    for schedule, refill in ((0, 1), (1, 1), (1, 8), (1, 16), (1, 32), (2, 8), (3, 8)):
+    for schedule, refill in ((0, 1), (1, 1), (1, 8), (1, 16), (1, 32), (2, 8), (3, 8), (4, 8), (4, 8), (5, 8)):
         acc.SetTuning(schedule, refill)
         assert acc.GetTuning() == {"schedule": schedule, "refill_threshold": refill}
         prim, t, u, v, occ = run_device(acc, rays)
