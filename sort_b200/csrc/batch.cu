@@ -73,7 +73,7 @@ __global__ void __launch_bounds__(BLOCK) k_trace_batches(BatchArgs a) {
     const int refill = a.header->refill;
     const long long budget = a.header->budget_ns;
     const BatchDesc* __restrict__ bt = a.batches + g.first;
-    Traversal<W, ANY, STACK, false, Q8> tv;
+    Traversal<W, ANY, STACK, false, Q8, true> tv;
     DevTree tr;
     tr.nodes = nullptr;
     tr.tris = nullptr;

@@ -134,7 +134,7 @@ __global__ void __launch_bounds__(128) k_srv_trace(const SrvScene* __restrict__ 
     const DevTree tr = scenes[scene_of[i]].tree;
     const DevRays rays{ray, ray + cap, ray + 2 * cap, ray + 3 * cap, ray + 4 * cap, ray + 5 * cap, ray + 6 * cap,
                        ray + 7 * cap};
-    Traversal<W, ANY, STACK, false, Q8> tv;
+    Traversal<W, ANY, STACK, false, Q8, true> tv;
     if (tv.start(tr, rays, i))
         while (!tv.step(tr, err)) {
         }

@@ -130,7 +130,7 @@ __global__ void __launch_bounds__(128) k_trace_fp32(DevTree tr, DevRays rays, in
     if (n_dev && k >= (int64_t)*n_dev) return;
     if (k >= n) return;
     const int64_t i = order ? (int64_t)__ldg(order + k) : k;
-    Traversal<W, ANY, STACK, STATS, Q8> tv;
+    Traversal<W, ANY, STACK, STATS, Q8, true> tv;
     if (tv.start(tr, rays, i))
         while (!tv.step(tr, err)) {
         }
@@ -150,7 +150,7 @@ __global__ void __launch_bounds__(128) k_trace_fp32_persistent(DevTree tr, DevRa
                                                                unsigned long long* __restrict__ stats) {
     const unsigned lane = threadIdx.x & 31u;
     const unsigned lt_mask = (1u << lane) - 1u;
-    Traversal<W, ANY, STACK, STATS> tv;
+    Traversal<W, ANY, STACK, STATS, false, true> tv;
     bool alive = false;
     bool drained = false;  // warp-uniform: the counter has passed n
     int64_t ray = -1;

@@ -208,3 +208,34 @@ def test_gpu_schedules_give_identical_results(port, width):
         prim, t, u, v, occ = run_device(acc, rays)
         assert np.array_equal(prim, rp) and same_bits(t, rt) and same_bits(u, ru) and same_bits(v, rv)
         assert np.array_equal(occ, ro)
+
+
+@pytest.mark.parametrize("width", [4, 8])
+def test_gpu_non_finite_rays_match_sort(port, width):
+    """Rays with a NaN or infinite origin, direction, tmin or tmax component give
+    SORT's answer (a miss, except an infinite tmax, which is an ordinary ray)
+    under every schedule. Such rays can reach empty child slots, which the
+    step-driven kernels pass over instead of testing each child for emptiness."""
+    from sort_b200 import scenes
+    tri = scenes.sphere_field(32, 3, seed=15)
+    rng = np.random.default_rng(19)
+    rays = scenes.random_rays(70_000, seed=18).copy()  # >= 2^16: the sorted schedule sorts
+    vals = np.array([np.nan, np.inf, -np.inf], np.float32)
+    k = 0
+    for comp in range(8):
+        for v in vals:
+            rays[comp, k:k + 16] = v
+            k += 16
+    for j in range(k, 1024):  # several bad components at once
+        comps = rng.choice(8, size=rng.integers(2, 5), replace=False)
+        rays[comps, j] = rng.choice(vals, size=comps.size)
+    acc = accel(width)
+    acc.Build(tri)
+    ref = port.build(tri, width)
+    rp, rt, ru, rv = ref.closest(rays)
+    ro = ref.any(rays)
+    for schedule, refill in ((0, 1), (1, 8), (2, 8), (3, 8), (4, 8), (5, 8)):
+        acc.SetTuning(schedule, refill)
+        prim, t, u, v, occ = run_device(acc, rays)
+        assert np.array_equal(prim, rp) and same_bits(t, rt)
+        assert np.array_equal(occ, ro)
