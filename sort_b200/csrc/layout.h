@@ -43,7 +43,8 @@ constexpr int kPadSlots = 8;
 //          float4 4..5: child[0:8].  96 B.
 //   W = 4: float4 1: lo_x[4] hi_x[4] lo_y[4] hi_y[4]; float4 2: lo_z[4] hi_z[4]
 //          and 8 B of padding; float4 3: child[0:4].  64 B.
-// A bound decodes to fl(origin + q * scale).
+// A bound decodes to fl(origin + q * scale). An empty slot has lower bytes 255
+// and upper bytes 0: an inverted box.
 constexpr int kQ8F4W8 = 6;
 constexpr int kQ8F4W4 = 4;
 

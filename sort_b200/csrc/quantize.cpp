@@ -38,8 +38,9 @@ bool quantize_axis(const float* lo, const float* hi, const int32_t* child, int W
                    uint8_t* qhi) {
     const float s = std::ldexp(1.0f, e);
     for (int j = 0; j < W; ++j) {
-        if (child[j] == kEmptyRef) {
-            qlo[j] = qhi[j] = 0;
+        if (child[j] == kEmptyRef) {  // inverted box: missed by every ray with finite origin and direction
+            qlo[j] = 255;
+            qhi[j] = 0;
             continue;
         }
         double fl = std::floor((double(lo[j]) - double(origin)) / double(s));

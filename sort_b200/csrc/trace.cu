@@ -241,7 +241,7 @@ __global__ void k_ray_keys(DevRays rays, int64_t n, float3 lo, float3 inv_ext, u
 // The sorted schedule: keys, a 30-bit radix sort of (key, ray), then one ray
 // per thread in sorted order. Scratch comes from the library's stream-ordered
 // pool and is freed in stream order.
-template <int W, bool ANY, int STACK>
+template <int W, bool ANY, int STACK, bool Q8>
 static cudaError_t launch_sorted(const TraceLaunch& L, const DevTree& tr, const DevRays& rays, int64_t n,
                                  cudaStream_t s) {
     int dev = 0;
@@ -275,8 +275,8 @@ static cudaError_t launch_sorted(const TraceLaunch& L, const DevTree& tr, const 
     if (e == cudaSuccess)
         e = cub::DeviceRadixSort::SortPairs(base + 4 * nb, temp, keys, keys_sorted, index, order, count, 0, 30, s);
     if (e == cudaSuccess) {
-        k_trace_fp32<W, ANY, STACK, false><<<blocks, threads, 0, s>>>(tr, rays, n, L.prim, L.t, L.u, L.v, L.occ,
-                                                                       L.err, nullptr, nullptr, order);
+        k_trace_fp32<W, ANY, STACK, false, Q8><<<blocks, threads, 0, s>>>(tr, rays, n, L.prim, L.t, L.u, L.v,
+                                                                           L.occ, L.err, nullptr, nullptr, order);
         e = cudaGetLastError();
     }
     const cudaError_t f = cudaFreeAsync(base, s);
@@ -293,8 +293,9 @@ static cudaError_t launch_stack(const TraceLaunch& L, const DevTree& tr, const D
     const bool sorted = L.tuning.schedule == kScheduleSorted ? n >= (int64_t(1) << 16)
                         : L.tuning.schedule == kScheduleAuto  ? !ANY && n >= (int64_t(1) << 21)
                                                               : false;
-    if (!STATS && !L.q8 && !L.n_dev && sorted && n < (int64_t(1) << 31))
-        return launch_sorted<W, ANY, STACK>(L, tr, rays, n, s);
+    if (!STATS && !L.n_dev && sorted && n < (int64_t(1) << 31))
+        return L.q8 ? launch_sorted<W, ANY, STACK, true>(L, tr, rays, n, s)
+                    : launch_sorted<W, ANY, STACK, false>(L, tr, rays, n, s);
     // Counting launches keep the one-entry-per-step loop, whose interior-node
     // visits are exactly SORT's (speculation visits extra ones).
     // 8-bit nodes are read by the one-ray-per-thread kernel.

@@ -126,12 +126,14 @@ __device__ __forceinline__ void load_node_q8(const float4* __restrict__ nodes, i
 // (+FLT_MAX .. -FLT_MAX), which a ray with finite origin and direction never
 // hits (per axis the entry distance is >= +FLT_MAX/|d| - |o/d| > 0 and the exit
 // distance the negative of that), so only a ray with a NaN or infinite
-// component can reach one. Dropping the per-child test saves two instructions
-// per child and six registers in the closest-hit kernel. 8-bit nodes keep the
-// test (their decoded empty boxes are not guaranteed to miss).
+// component can reach one. An empty 8-bit slot decodes to an inverted box
+// (lower bound 255 steps above the upper one), which such a ray misses too.
+// Dropping the per-child test saves two instructions per child and six
+// registers in the closest-hit kernel; skipping in step() keeps any empty
+// entry that is reached harmless.
 template <int W, bool ANY, int STACK, bool STATS, bool Q8 = false, bool STEP_SKIPS_EMPTY = false>
 struct Traversal {
-    static constexpr bool kTestEmpty = Q8 || !STEP_SKIPS_EMPTY;
+    static constexpr bool kTestEmpty = !STEP_SKIPS_EMPTY;
     RayState r;
     float best_t, best_u, best_v;
     int32_t best_prim;
