@@ -345,7 +345,7 @@ def run_ours(args):
             traffic = tj.get("dram_bytes_per_launch")
 
     if rank == 0:
-        sorted_schedule = args.nodes == "fp32" and n >= (1 << 21)
+        sorted_schedule = n >= (1 << 21)
         out = {
             "metric": METRIC if width == 8 else "Mrays/s primary closest-hit", "value": round(value, 3),
             "unit": UNIT, "n_gpus": world, "steps": args.steps,
@@ -365,8 +365,8 @@ def run_ours(args):
                          "peak_source": peak_src,
                          "algorithmic_bytes_per_ray": round(bytes_closest, 1),
                          "node_tests_per_ray": round(node_tests / n, 3), "prim_tests_per_ray": round(prim_tests / n, 3),
-                         "kernel": f"k_trace_fp32<{width},false,{64 if width == 4 else 128},false"
-                                   + (",true>" if args.nodes == "q8" else ">"),
+                         "kernel": ("k_trace_q8" if args.nodes == "q8" else "k_trace_fp32")
+                                   + f"<{width},false,{64 if width == 4 else 128},false>",
                          "launch_ms": round(launch_ms, 4)},
             "anyhit": {"mrays_s": round(n / (any_ms / 1e3) / 1e6, 3), "launch_ms": round(any_ms, 4),
                        "algorithmic_bytes_per_ray": round(bytes_any, 1),

@@ -119,13 +119,13 @@ __global__ void __launch_bounds__(128) k_trace_fp32_ww(DevTree tr, DevRays rays,
 // min(n, *n_dev), read on the device (queues whose length only the GPU knows).
 // Q8 reads 8-bit nodes.
 // With `order` set, thread k traces ray order[k] (the sorted schedule).
-template <int W, bool ANY, int STACK, bool STATS, bool Q8 = false>
-__global__ void __launch_bounds__(128) k_trace_fp32(DevTree tr, DevRays rays, int64_t n, int32_t* __restrict__ prim_out,
-                                                    float* __restrict__ t_out, float* __restrict__ u_out,
-                                                    float* __restrict__ v_out, uint8_t* __restrict__ occ_out,
-                                                    int* __restrict__ err, unsigned long long* __restrict__ stats,
-                                                    const int* __restrict__ n_dev,
-                                                    const int32_t* __restrict__ order = nullptr) {
+template <int W, bool ANY, int STACK, bool STATS, bool Q8>
+__device__ __forceinline__ void trace_one_ray(const DevTree& tr, const DevRays& rays, int64_t n,
+                                              int32_t* __restrict__ prim_out, float* __restrict__ t_out,
+                                              float* __restrict__ u_out, float* __restrict__ v_out,
+                                              uint8_t* __restrict__ occ_out, int* __restrict__ err,
+                                              unsigned long long* __restrict__ stats, const int* __restrict__ n_dev,
+                                              const int32_t* __restrict__ order) {
     const int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (n_dev && k >= (int64_t)*n_dev) return;
     if (k >= n) return;
@@ -135,6 +135,31 @@ __global__ void __launch_bounds__(128) k_trace_fp32(DevTree tr, DevRays rays, in
         while (!tv.step(tr, err)) {
         }
     tv.finish(i, prim_out, t_out, u_out, v_out, occ_out, stats);
+}
+
+template <int W, bool ANY, int STACK, bool STATS, bool Q8 = false>
+__global__ void __launch_bounds__(128) k_trace_fp32(DevTree tr, DevRays rays, int64_t n, int32_t* __restrict__ prim_out,
+                                                    float* __restrict__ t_out, float* __restrict__ u_out,
+                                                    float* __restrict__ v_out, uint8_t* __restrict__ occ_out,
+                                                    int* __restrict__ err, unsigned long long* __restrict__ stats,
+                                                    const int* __restrict__ n_dev,
+                                                    const int32_t* __restrict__ order = nullptr) {
+    trace_one_ray<W, ANY, STACK, STATS, Q8>(tr, rays, n, prim_out, t_out, u_out, v_out, occ_out, err, stats, n_dev,
+                                           order);
+}
+
+// The same for 8-bit nodes, held to 9 blocks of 128 per SM: the decode leaves
+// the compiler at 72-80 registers (7 blocks); at 56 it spills 64 bytes and is
+// still 4.6% faster on 4M incoherent rays (more warps hide the node loads).
+template <int W, bool ANY, int STACK, bool STATS>
+__global__ void __launch_bounds__(128, 9) k_trace_q8(DevTree tr, DevRays rays, int64_t n, int32_t* __restrict__ prim_out,
+                                                     float* __restrict__ t_out, float* __restrict__ u_out,
+                                                     float* __restrict__ v_out, uint8_t* __restrict__ occ_out,
+                                                     int* __restrict__ err, unsigned long long* __restrict__ stats,
+                                                     const int* __restrict__ n_dev,
+                                                     const int32_t* __restrict__ order = nullptr) {
+    trace_one_ray<W, ANY, STACK, STATS, true>(tr, rays, n, prim_out, t_out, u_out, v_out, occ_out, err, stats, n_dev,
+                                             order);
 }
 
 // Persistent warps: a lane whose ray finished takes the next ray in batch order
@@ -275,8 +300,12 @@ static cudaError_t launch_sorted(const TraceLaunch& L, const DevTree& tr, const 
     if (e == cudaSuccess)
         e = cub::DeviceRadixSort::SortPairs(base + 4 * nb, temp, keys, keys_sorted, index, order, count, 0, 30, s);
     if (e == cudaSuccess) {
-        k_trace_fp32<W, ANY, STACK, false, Q8><<<blocks, threads, 0, s>>>(tr, rays, n, L.prim, L.t, L.u, L.v,
-                                                                           L.occ, L.err, nullptr, nullptr, order);
+        if (Q8)
+            k_trace_q8<W, ANY, STACK, false><<<blocks, threads, 0, s>>>(tr, rays, n, L.prim, L.t, L.u, L.v, L.occ,
+                                                                        L.err, nullptr, nullptr, order);
+        else
+            k_trace_fp32<W, ANY, STACK, false><<<blocks, threads, 0, s>>>(tr, rays, n, L.prim, L.t, L.u, L.v, L.occ,
+                                                                          L.err, nullptr, nullptr, order);
         e = cudaGetLastError();
     }
     const cudaError_t f = cudaFreeAsync(base, s);
@@ -301,7 +330,7 @@ static cudaError_t launch_stack(const TraceLaunch& L, const DevTree& tr, const D
     // 8-bit nodes are read by the one-ray-per-thread kernel.
     if (L.q8) {
         const int64_t blocks = (n + threads - 1) / threads;
-        k_trace_fp32<W, ANY, STACK, STATS, true><<<(unsigned)blocks, threads, 0, s>>>(
+        k_trace_q8<W, ANY, STACK, STATS><<<(unsigned)blocks, threads, 0, s>>>(
             tr, rays, n, L.prim, L.t, L.u, L.v, L.occ, L.err, L.stats, L.n_dev);
         return cudaGetLastError();
     }
