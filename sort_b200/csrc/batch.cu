@@ -67,9 +67,9 @@ __device__ __forceinline__ void count_finished(bool fin, int b, const BatchArgs&
 
 // Held to 1,024 resident threads per SM (64 registers). Left alone the
 // compiler gives it 72-80 registers, and 6-7 blocks of 128 per SM; at 64 there
-// are no spills for closest hits (8 bytes for any-hit), and batched_31m runs 6%
-// faster (1,773 to 1,880 Mrays/s). Holding it to 1,152 threads (56 registers)
-// spills 80-106 bytes and gains less.
+// are no spills for closest hits (8 bytes for any-hit, 96-104 for 8-bit
+// nodes), and batched_31m runs 6% faster (1,773 to 1,880 Mrays/s). Holding it
+// to 1,152 threads (56 registers) spills 80-106 bytes and gains less.
 template <int W, bool ANY, int STACK, int BLOCK, bool Q8>
 __global__ void __launch_bounds__(BLOCK, 1024 / BLOCK) k_trace_batches(BatchArgs a) {
     const unsigned lane = threadIdx.x & 31u;

@@ -122,9 +122,12 @@ __global__ void k_srv_settle(SrvBuffers b) {
         b.counters->head = b.counters->tail;
 }
 
-// One ray per thread over a queue of rays from many scenes.
+// One ray per thread over a queue of rays from many scenes. Held to 9 blocks
+// of 128 per SM (56 registers; 12 bytes spilled for width-8 FP32 trees):
+// serve_27m's closed loop runs 3.6% faster than at the compiler's 60-80
+// registers.
 template <int W, bool ANY, int STACK, bool Q8>
-__global__ void __launch_bounds__(128) k_srv_trace(const SrvScene* __restrict__ scenes, const float* __restrict__ ray,
+__global__ void __launch_bounds__(128, 9) k_srv_trace(const SrvScene* __restrict__ scenes, const float* __restrict__ ray,
                                                    const int* __restrict__ scene_of, int cap,
                                                    const int* __restrict__ count, int32_t* __restrict__ prim,
                                                    float* __restrict__ t, uint8_t* __restrict__ occ,
