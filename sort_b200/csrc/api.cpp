@@ -18,6 +18,7 @@
 
 #include "builder.h"
 #include "hair.h"
+#include "staged_upload.h"
 #include "trace_kernels.h"
 
 namespace {
@@ -129,7 +130,8 @@ sg_status upload(sg_scene* s, const float* tri, int64_t ntri, const std::vector<
     if ((e = cudaMalloc(&s->d_err, sizeof(int))) != cudaSuccess) return cuda_fail(e, "cudaMalloc(status)");
     if ((e = cudaMalloc(&s->d_counters, sg_scene::kCounterSlots * sizeof(unsigned long long))) != cudaSuccess)
         return cuda_fail(e, "cudaMalloc(counters)");
-    if (!adopt && (e = cudaMemcpy(s->d_nodes, nodes.data(), nb, cudaMemcpyHostToDevice)) != cudaSuccess)
+    if (!adopt && ((e = sg::upload_host(s->d_nodes, nodes.data(), nb, nullptr)) != cudaSuccess ||
+                   (e = cudaStreamSynchronize(nullptr)) != cudaSuccess))
         return cuda_fail(e, "upload nodes");
     if ((e = cudaMemset(s->d_err, 0, sizeof(int))) != cudaSuccess) return cuda_fail(e, "clear status");
     if (s->tree.d_tris) {  // the GPU builder wrote the records on the device
@@ -176,7 +178,8 @@ sg_status upload(sg_scene* s, const float* tri, int64_t ntri, const std::vector<
         if (e != cudaSuccess)
             return e == cudaErrorMemoryAllocation ? fail(SG_ERR_OUT_OF_MEMORY, "cudaMalloc(triangles) failed")
                                                   : cuda_fail(e, "cudaMalloc(triangles)");
-        if ((e = cudaMemcpy(s->d_tris, tris.data(), tbytes, cudaMemcpyHostToDevice)) != cudaSuccess)
+        if ((e = sg::upload_host(s->d_tris, tris.data(), tbytes, nullptr)) != cudaSuccess ||
+            (e = cudaStreamSynchronize(nullptr)) != cudaSuccess)
             return cuda_fail(e, "upload triangles");
         if (nlines > 0) {
             if ((e = cudaMalloc(&s->d_lines, line_recs.size() * sizeof(float))) != cudaSuccess)

@@ -47,6 +47,7 @@
 
 #include "builder.h"
 #include "gpu_build_common.cuh"
+#include "staged_upload.h"
 #include "layout.h"
 
 namespace sg {
@@ -667,8 +668,7 @@ BuiltTree build_tree_gpu(const float* tri, int64_t ntri, const BuildParams& p, i
         empty_box(h_scene.p);
         if (n > 0) {
             if (nt > 0) {
-                check(cudaMemcpyAsync(d_tri.p, tri, size_t(nt) * 9 * sizeof(float), cudaMemcpyHostToDevice, st),
-                      "upload");
+                check(upload_host(d_tri.p, tri, size_t(nt) * 9 * sizeof(float), st), "upload");
                 k_prim_setup<<<grid(nt), 256, 0, st>>>(d_tri.p, nt, n, d_cx.p, d_cy.p, d_cz.p, d_idx.p, d_pb.p);
             }
             if (p.nextra > 0) {

@@ -40,6 +40,7 @@
 
 #include "builder.h"
 #include "gpu_build_common.cuh"
+#include "staged_upload.h"
 #include "layout.h"
 
 namespace sg {
@@ -341,7 +342,7 @@ BuiltTree build_tree_lbvh(const float* tri, int64_t ntri, const BuildParams& p, 
     empty_box(h_box.p);
     empty_box(h_box.p + 6);
     if (n > 0) {
-        check(cudaMemcpyAsync(d_tri.p, tri, size_t(n) * 9 * sizeof(float), cudaMemcpyHostToDevice, st), "upload");
+        check(upload_host(d_tri.p, tri, size_t(n) * 9 * sizeof(float), st), "upload");
         k_prim_setup<<<grid(n), 256, 0, st>>>(d_tri.p, n, n, d_cx.p, d_cy.p, d_cz.p, d_idx.p, d_pb.p);
         check(cudaMemcpyAsync(d_box.p, h_box.p, 12 * sizeof(int), cudaMemcpyHostToDevice, st), "boxes");
         const unsigned gb = std::min<unsigned>(grid(n), 148 * 8);
