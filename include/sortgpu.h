@@ -332,9 +332,14 @@ sg_status sg_trace_any_host(const sg_scene* scene, const float* rays8, int64_t n
  * take the allocator's locks or wait on an implicit synchronisation). Rays and hits are staged in a 24 MiB array compiled into
  * the library, held on every GPU that loads it until exit; at most 524,288 rays
  * per call (SG_ERR_LIMIT beyond). All calls share that array, so calls whose
- * work overlaps on the GPU race. The first call on a device looks up the
- * array's address; make it before capturing a stream on that device. Ordered
- * on `stream` (NULL = legacy default stream) and synchronises it. */
+ * work overlaps on the GPU race. Every batch runs one ray per thread, whatever
+ * schedule sg_scene_set_tuning chose (the sorted schedule would take scratch
+ * from a pool); results are the same under every schedule. Scenes with hair
+ * lines are rejected (SG_ERR_UNSUPPORTED). The first call on a device looks up
+ * the array's address (cudaGetSymbolAddress); make that first call before any
+ * stream capture begins on that device. Ordered on `stream` (NULL = legacy
+ * default stream); the call ends by synchronising `stream` to read the
+ * traversal status. */
 sg_status sg_trace_closest_host_static(const sg_scene* scene, const float* rays8, int64_t n, int32_t* prim, float* t,
                                        float* u, float* v, void* stream);
 

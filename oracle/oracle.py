@@ -122,6 +122,7 @@ class Port:
         L.orc_tri_test.argtypes = [_vp, _i64, _vp, _i64, _i64, ctypes.POINTER(ctypes.c_float)]
         L.orc_fp64_intersect.restype = ctypes.c_double
         L.orc_fp64_intersect.argtypes = [_vp, _i64, _vp, _i64, _i64]
+        L.orc_fp64_t_batch.argtypes = [_vp, _vp, _vp, _i64, _vp]
         self.L = L
         self._free, self._topo, self._depth, self._bbox = L.orc_free, L.orc_topology, L.orc_depth, L.orc_scene_bbox
         self._closest, self._any = L.orc_trace_closest, L.orc_trace_any
@@ -152,6 +153,21 @@ class Port:
         tri = np.ascontiguousarray(tri, np.float32)
         r = np.ascontiguousarray(rays, np.float32)
         return float(self.L.orc_fp64_intersect(tri.ctypes.data, prim, r.ctypes.data, r.shape[1], i))
+
+    def fp64_t_batch(self, tri: np.ndarray, prim: np.ndarray, rays: np.ndarray) -> np.ndarray:
+        """FP64 re-intersection of every ray with its hit triangle (-1 where prim < 0)."""
+        tri = np.ascontiguousarray(tri, np.float32)
+        r = np.ascontiguousarray(rays, np.float32)
+        p = np.ascontiguousarray(prim, np.int32)
+        out = np.empty(r.shape[1], np.float64)
+        self.L.orc_fp64_t_batch(tri.ctypes.data, p.ctypes.data, r.ctypes.data, r.shape[1], out.ctypes.data)
+        return out
+
+    def fp64_rel_err(self, tri: np.ndarray, prim: np.ndarray, t: np.ndarray, rays: np.ndarray) -> np.ndarray:
+        """|t - t_fp64| / t_fp64 per hit ray (hits whose FP64 test misses are left out)."""
+        t64 = self.fp64_t_batch(tri, prim, rays)
+        ok = (np.asarray(prim) >= 0) & (t64 > 0)
+        return np.abs(np.asarray(t, np.float64)[ok] - t64[ok]) / t64[ok]
 
 
 class Reference:

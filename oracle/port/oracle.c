@@ -710,3 +710,7 @@ double orc_fp64_intersect(const float* tri, int64_t prim, const float* rays, int
     if (det == 0.0) return -1.0;
     return (e0 * py[0] + e1 * py[1] + e2 * py[2]) / det;
 }
+
+void orc_fp64_t_batch(const float* tri, const int32_t* prim, const float* rays, int64_t n, double* t_out) {
+    for (int64_t i = 0; i < n; ++i) t_out[i] = prim[i] >= 0 ? orc_fp64_intersect(tri, prim[i], rays, n, i) : -1.0;
+}

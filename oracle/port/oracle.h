@@ -66,6 +66,9 @@ int orc_tri_test(const float* tri, int64_t prim, const float* rays, int64_t n, i
  * formulation in doubles); returns t, or -1 on a miss. */
 double orc_fp64_intersect(const float* tri, int64_t prim, const float* rays, int64_t n, int64_t i);
 
+/* orc_fp64_intersect of every ray i with triangle prim[i]; -1 where prim[i] < 0. */
+void orc_fp64_t_batch(const float* tri, const int32_t* prim, const float* rays, int64_t n, double* t_out);
+
 #ifdef __cplusplus
 }
 #endif

@@ -76,6 +76,12 @@ extern "C" sg_status sg_trace_closest_host_static(const sg_scene* scene, const f
     int device = 0;
     sg_status st = sg::scene_launch(scene, false, &L, &tree, &device);
     if (st != SG_OK) return st;
+    // The sorted schedule takes key and permutation scratch from a pool, and the
+    // automatic choice may pick it; this entry point runs every batch one ray per
+    // thread instead (same results: the schedule never changes a hit). The other
+    // schedules allocate nothing.
+    if (L.tuning.schedule == sg::kScheduleSorted || L.tuning.schedule == sg::kScheduleAuto)
+        L.tuning.schedule = sg::kScheduleThreadPerRay;
     int prev = -1;
     cudaError_t e = cudaGetDevice(&prev);
     if (e != cudaSuccess) return sg::set_error(SG_ERR_CUDA, cudaGetErrorString(e));

@@ -30,6 +30,7 @@ struct Stager {
     std::vector<char*> buf;            // workers * kSlots pinned buffers
     std::vector<cudaEvent_t> done;     // per buffer: its last copy finished
     std::vector<cudaStream_t> stream;  // per worker
+    cudaEvent_t entry = nullptr;       // the caller's stream at the start of a copy
 };
 
 // Per device; made on first use with that device current.
@@ -56,7 +57,10 @@ cudaError_t init(Stager& s) {
     }
     for (size_t k = 0; k < stream.size() && e == cudaSuccess; ++k)
         e = cudaStreamCreateWithFlags(&stream[k], cudaStreamNonBlocking);
+    cudaEvent_t entry = nullptr;
+    if (e == cudaSuccess) e = cudaEventCreateWithFlags(&entry, cudaEventDisableTiming);
     if (e != cudaSuccess) {
+        if (entry) cudaEventDestroy(entry);
         for (char* b : buf)
             if (b) cudaFreeHost(b);
         for (cudaEvent_t v : done)
@@ -68,6 +72,7 @@ cudaError_t init(Stager& s) {
     s.buf = std::move(buf);
     s.done = std::move(done);
     s.stream = std::move(stream);
+    s.entry = entry;
     s.workers = w;
     return cudaSuccess;
 }
@@ -92,12 +97,17 @@ cudaError_t upload_host(void* dst, const void* src, size_t bytes, cudaStream_t s
         return cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, stream);
     }
     const int w = s.workers;
+    // The destination may have just been taken from a stream-ordered pool on
+    // `stream`, or still be read by work queued there: the worker streams
+    // start their copies only after everything already on `stream`.
+    if ((e = cudaEventRecord(s.entry, stream)) != cudaSuccess) return e;
     // Shares in whole slots, so every copy but the last of a share is full.
     const size_t slots_total = (bytes + kSlotBytes - 1) / kSlotBytes;
     const size_t per = ((slots_total + size_t(w) - 1) / size_t(w)) * kSlotBytes;
     std::atomic<int> first_error{int(cudaSuccess)};
     auto work = [&](int k) {
         cudaError_t r = cudaSetDevice(device);
+        if (r == cudaSuccess) r = cudaStreamWaitEvent(s.stream[size_t(k)], s.entry, 0);
         const size_t a = size_t(k) * per, end = std::min(bytes, a + per);
         int slot = 0;
         for (size_t off = a; off < end && r == cudaSuccess; off += kSlotBytes) {

@@ -9,7 +9,9 @@
 namespace sg {
 
 // Copies `bytes` from host memory `src` to device memory `dst` of the current
-// device, ordered before later work on `stream`. When it returns, `src` has
+// device, ordered after earlier work and before later work on `stream` (the
+// worker streams wait for an event recorded on `stream` at entry, so `dst` may
+// come from a stream-ordered allocation on `stream`). When it returns, `src` has
 // been read and may be changed or freed. Buffers below 32 MB and pinned ones
 // go through one cudaMemcpyAsync. Larger pageable ones are split among up to
 // 8 host threads; each copies its share into two 4 MB pinned buffers in turn,

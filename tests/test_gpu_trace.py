@@ -4,8 +4,9 @@ Bar: primitive ids and hit distances bit-identical to SORT's (FP32 nodes use
 SORT's topology, visit order and rounding); u, v equal by value (SORT's own u, v
 pass through texture-coordinate interpolation, which maps -0 to +0); any-hit
 flags identical. Checked against the golden fixtures SORT produced, against the
-restated oracle at the 81,922-triangle ray-cast size, and at the 21M-triangle
-size on a ray sample plus size-independent properties on every ray.
+restated oracle at the 81,922-triangle ray-cast size and on random rays, and
+on the host-buffer forms. The 21M-triangle benchmark size is covered by
+test_gpu_incoherent_21m.py.
 """
 import numpy as np
 import pytest

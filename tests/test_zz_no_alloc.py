@@ -64,3 +64,44 @@ def test_static_entry_point_rejects_oversized_batch():
     out = np.empty(1, np.int32)
     assert lib.sg_trace_closest_host_static(acc._h, rays.ctypes.data, 0, out.ctypes.data, out.ctypes.data,
                                             None, None, ctypes.c_void_p()) == 0
+
+
+def test_static_entry_point_ignores_sorted_schedule():
+    """A scene tuned to the sorted schedule (which takes key and permutation
+    scratch from a pool) still runs allocation-free through this entry point:
+    the call runs one ray per thread, and device memory in use does not move."""
+    torch = pytest.importorskip("torch")
+    assert torch.cuda.is_available(), "GPU test needs a CUDA device"
+    from sort_b200 import Obvh, _lib, scenes
+
+    lib = _lib.load()
+    acc = Obvh()
+    acc.Build(scenes.sphere_field(32, 3, seed=36))
+    acc.SetTuning(schedule=4)  # SG_SCHEDULE_SORTED: sorts batches of 65,536 rays or more
+    rays = np.ascontiguousarray(scenes.random_rays(300_000, seed=37))
+    st, first = _call_static(lib, acc._h, rays)  # loads the kernel the call uses
+    assert st == 0, lib.sg_last_error()
+    torch.cuda.synchronize()
+    free_before = torch.cuda.mem_get_info()[0]
+    st, (prim, t, u, v) = _call_static(lib, acc._h, rays)
+    assert st == 0, lib.sg_last_error()
+    torch.cuda.synchronize()
+    assert torch.cuda.mem_get_info()[0] == free_before
+    ref = acc.GetIntersect(rays)  # sg_trace_closest_host, sorted schedule
+    assert np.array_equal(prim, ref.prim) and same_bits(t, ref.t)
+    assert same_bits(u, ref.u) and same_bits(v, ref.v)
+    assert all(np.array_equal(a.view(np.int32), b.view(np.int32)) for a, b in zip(first, (prim, t, u, v)))
+
+
+def test_static_entry_point_rejects_hair_scene():
+    torch = pytest.importorskip("torch")
+    assert torch.cuda.is_available(), "GPU test needs a CUDA device"
+    from conftest import golden
+    from sort_b200 import Obvh, Scene, _lib
+
+    lib = _lib.load()
+    z = golden("hair")
+    acc = Obvh()
+    acc.Build(Scene(z["triangles"], z["lines"]))
+    st, _ = _call_static(lib, acc._h, np.ascontiguousarray(z["rays"][:, :256]))
+    assert st == 4 and b"hair" in lib.sg_last_error()
