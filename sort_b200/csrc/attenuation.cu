@@ -39,6 +39,8 @@ __global__ void __launch_bounds__(128)
     const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
     Traversal<W, false, STACK, false, Q8> tv;
+    uint2 stk_mem[STACK];
+    tv.stk = stk_mem;
     float o[3] = {rays.ox[i], rays.oy[i], rays.oz[i]};
     const float d[3] = {rays.dx[i], rays.dy[i], rays.dz[i]};
     float tmin = rays.tmin[i], tmax = rays.tmax[i];

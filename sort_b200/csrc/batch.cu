@@ -78,7 +78,8 @@ __global__ void __launch_bounds__(BLOCK, 1024 / BLOCK) k_trace_batches(BatchArgs
     const int refill = a.header->refill;
     const long long budget = a.header->budget_ns;
     const BatchDesc* __restrict__ bt = a.batches + g.first;
-    Traversal<W, ANY, STACK, false, Q8, true> tv;
+    RayWalk<W, ANY, STACK, Q8> tv;
+    uint2 stk[STACK];
     DevTree tr;
     tr.nodes = nullptr;
     tr.tris = nullptr;
@@ -121,7 +122,7 @@ __global__ void __launch_bounds__(BLOCK, 1024 / BLOCK) k_trace_batches(BatchArgs
                     tr = a.trees[__ldg(&bt[b].tree)];
                     alive = tv.begin(tr);
                     if (!alive) {
-                        tv.finish(j, bt[b].prim, bt[b].t, bt[b].u, bt[b].v, bt[b].occ, nullptr);
+                        tv.finish(tr, j, bt[b].prim, bt[b].t, bt[b].u, bt[b].v, bt[b].occ);
                         fin = true;
                     }
                 }
@@ -136,8 +137,8 @@ __global__ void __launch_bounds__(BLOCK, 1024 / BLOCK) k_trace_batches(BatchArgs
         // Traverse until enough lanes are idle to be worth refilling.
         for (;;) {
             bool fin = false;
-            if (alive && tv.step(tr, &a.state->status)) {
-                tv.finish(j, bt[b].prim, bt[b].t, bt[b].u, bt[b].v, bt[b].occ, nullptr);
+            if (alive && tv.step(tr, stk, &a.state->status)) {
+                tv.finish(tr, j, bt[b].prim, bt[b].t, bt[b].u, bt[b].v, bt[b].occ);
                 alive = false;
                 fin = true;
             }

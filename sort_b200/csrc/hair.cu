@@ -70,6 +70,8 @@ __global__ void __launch_bounds__(128)
     const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
     Traversal<W, false, STACK, false, Q8> tv;
+    uint2 stk_mem[STACK];
+    tv.stk = stk_mem;
     bool hit_any = false;
     if (tv.start(tr, rays, i)) {
         for (;;) {

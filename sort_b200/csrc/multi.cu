@@ -77,6 +77,8 @@ __global__ void __launch_bounds__(128) k_trace_multi(DevTree tr, DevRays rays, i
     const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
     Traversal<W, false, STACK, false, Q8> tv;  // best_t plays SORT's intersect.maxt
+    uint2 stk_mem[STACK];
+    tv.stk = stk_mem;
     MultiHits h;
     if (tv.start(tr, rays, i)) {
         const int32_t mat = ray_mat[i];

@@ -137,11 +137,12 @@ __global__ void __launch_bounds__(128, 9) k_srv_trace(const SrvScene* __restrict
     const DevTree tr = scenes[scene_of[i]].tree;
     const DevRays rays{ray, ray + cap, ray + 2 * cap, ray + 3 * cap, ray + 4 * cap, ray + 5 * cap, ray + 6 * cap,
                        ray + 7 * cap};
-    Traversal<W, ANY, STACK, false, Q8, true> tv;
+    RayWalk<W, ANY, STACK, Q8> tv;
+    uint2 stk[STACK];
     if (tv.start(tr, rays, i))
-        while (!tv.step(tr, err)) {
+        while (!tv.step(tr, stk, err)) {
         }
-    tv.finish(i, prim, t, nullptr, nullptr, occ, nullptr);
+    tv.finish(tr, i, prim, t, nullptr, nullptr, occ);
 }
 
 __global__ void k_srv_shade(SrvBuffers b, const float* __restrict__ qray, const int* __restrict__ qslot,

@@ -64,6 +64,8 @@ __global__ void __launch_bounds__(128) k_trace_fp32_ww(DevTree tr, DevRays rays,
     const bool valid = i0 < n;
     const int64_t i = valid ? i0 : n - 1;  // lanes past the batch end idle through the loop
     Traversal<W, ANY, STACK, false> tv;
+    uint2 stk_mem[STACK];
+    tv.stk = stk_mem;
     const bool started = tv.start(tr, rays, i);
     bool have = valid && started;  // `cur` holds an entry still to process
     bool pend = false;             // a parked leaf is waiting for the leaf phase
@@ -131,6 +133,8 @@ __device__ __forceinline__ void trace_one_ray(const DevTree& tr, const DevRays& 
     if (k >= n) return;
     const int64_t i = order ? (int64_t)__ldg(order + k) : k;
     Traversal<W, ANY, STACK, STATS, Q8, true> tv;
+    uint2 stk_mem[STACK];
+    tv.stk = stk_mem;
     if (tv.start(tr, rays, i))
         while (!tv.step(tr, err)) {
         }
@@ -151,6 +155,30 @@ __global__ void __launch_bounds__(128, (W == 4 && ANY) ? 10 : 9) k_trace_fp32(De
                                                     const int32_t* __restrict__ order = nullptr) {
     trace_one_ray<W, ANY, STACK, STATS, Q8>(tr, rays, n, prim_out, t_out, u_out, v_out, occ_out, err, stats, n_dev,
                                            order);
+}
+
+// One ray per thread with RayWalk, the hot path for FP32 and 8-bit nodes. With
+// n_dev set the batch is min(n, *n_dev); with `order` set, thread k traces ray
+// order[k]. Held to 9 blocks of 128 per SM (56 registers): left alone the
+// compiler takes 94 registers (every node and triangle load in flight at
+// once); 8 blocks ran at 994 Mrays/s, 9 at 1,031, and 10 (48 registers)
+// spills inside the traversal loop and fell to 968 (one triangle per
+// iteration) or to about 240 (two).
+template <int W, bool ANY, int STACK, bool Q8>
+__global__ void __launch_bounds__(128, 9)
+    k_trace_walk(DevTree tr, DevRays rays, int64_t n, int32_t* __restrict__ prim_out, float* __restrict__ t_out,
+                 float* __restrict__ u_out, float* __restrict__ v_out, uint8_t* __restrict__ occ_out,
+                 int* __restrict__ err, const int* __restrict__ n_dev, const int32_t* __restrict__ order) {
+    const int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (n_dev && k >= (int64_t)*n_dev) return;
+    if (k >= n) return;
+    const int64_t i = order ? (int64_t)__ldg(order + k) : k;
+    uint2 stk[STACK];
+    RayWalk<W, ANY, STACK, Q8> w;
+    if (w.start(tr, rays, i))
+        while (!w.step(tr, stk, err)) {
+        }
+    w.finish(tr, i, prim_out, t_out, u_out, v_out, occ_out);
 }
 
 // The same for 8-bit nodes, held to 9 blocks of 128 per SM: the decode leaves
@@ -181,6 +209,8 @@ __global__ void __launch_bounds__(128) k_trace_fp32_persistent(DevTree tr, DevRa
     const unsigned lane = threadIdx.x & 31u;
     const unsigned lt_mask = (1u << lane) - 1u;
     Traversal<W, ANY, STACK, STATS, false, true> tv;
+    uint2 stk_mem[STACK];
+    tv.stk = stk_mem;
     bool alive = false;
     bool drained = false;  // warp-uniform: the counter has passed n
     int64_t ray = -1;
@@ -305,12 +335,8 @@ static cudaError_t launch_sorted(const TraceLaunch& L, const DevTree& tr, const 
     if (e == cudaSuccess)
         e = cub::DeviceRadixSort::SortPairs(base + 4 * nb, temp, keys, keys_sorted, index, order, count, 0, 30, s);
     if (e == cudaSuccess) {
-        if (Q8)
-            k_trace_q8<W, ANY, STACK, false><<<blocks, threads, 0, s>>>(tr, rays, n, L.prim, L.t, L.u, L.v, L.occ,
-                                                                        L.err, nullptr, nullptr, order);
-        else
-            k_trace_fp32<W, ANY, STACK, false><<<blocks, threads, 0, s>>>(tr, rays, n, L.prim, L.t, L.u, L.v, L.occ,
-                                                                          L.err, nullptr, nullptr, order);
+        k_trace_walk<W, ANY, STACK, Q8><<<blocks, threads, 0, s>>>(tr, rays, n, L.prim, L.t, L.u, L.v, L.occ, L.err,
+                                                                   nullptr, order);
         e = cudaGetLastError();
     }
     const cudaError_t f = cudaFreeAsync(base, s);
@@ -332,11 +358,15 @@ static cudaError_t launch_stack(const TraceLaunch& L, const DevTree& tr, const D
                     : launch_sorted<W, ANY, STACK, false>(L, tr, rays, n, s);
     // Counting launches keep the one-entry-per-step loop, whose interior-node
     // visits are exactly SORT's (speculation visits extra ones).
-    // 8-bit nodes are read by the one-ray-per-thread kernel.
+    // 8-bit nodes are read by the one-ray-per-thread kernels.
     if (L.q8) {
         const int64_t blocks = (n + threads - 1) / threads;
-        k_trace_q8<W, ANY, STACK, STATS><<<(unsigned)blocks, threads, 0, s>>>(
-            tr, rays, n, L.prim, L.t, L.u, L.v, L.occ, L.err, L.stats, L.n_dev);
+        if (STATS)
+            k_trace_q8<W, ANY, STACK, STATS><<<(unsigned)blocks, threads, 0, s>>>(
+                tr, rays, n, L.prim, L.t, L.u, L.v, L.occ, L.err, L.stats, L.n_dev);
+        else
+            k_trace_walk<W, ANY, STACK, true><<<(unsigned)blocks, threads, 0, s>>>(
+                tr, rays, n, L.prim, L.t, L.u, L.v, L.occ, L.err, L.n_dev, nullptr);
         return cudaGetLastError();
     }
     // A device-side batch size is only read by the one-ray-per-thread kernel.
@@ -367,10 +397,14 @@ static cudaError_t launch_stack(const TraceLaunch& L, const DevTree& tr, const D
         if (e != cudaSuccess) return e;
         k_trace_fp32_persistent<W, ANY, STACK, STATS><<<(unsigned)blocks, threads, 0, s>>>(
             tr, rays, n, L.counter, refill, L.prim, L.t, L.u, L.v, L.occ, L.err, L.stats);
-    } else {
+    } else if (STATS) {
         const int64_t blocks = (n + threads - 1) / threads;
         k_trace_fp32<W, ANY, STACK, STATS><<<(unsigned)blocks, threads, 0, s>>>(tr, rays, n, L.prim, L.t, L.u, L.v,
                                                                                 L.occ, L.err, L.stats, L.n_dev);
+    } else {
+        const int64_t blocks = (n + threads - 1) / threads;
+        k_trace_walk<W, ANY, STACK, false><<<(unsigned)blocks, threads, 0, s>>>(tr, rays, n, L.prim, L.t, L.u, L.v,
+                                                                               L.occ, L.err, L.n_dev, nullptr);
     }
     return cudaGetLastError();
 }
