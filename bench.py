@@ -357,8 +357,9 @@ def run_ours(args):
                  if args.builder == "lbvh" else {})) | (
                 {"parallelism": f"replicas x{world}", "build_seconds": round(info["build_seconds"], 2),
                  "tree_device_bytes": info["device_bytes"],
-                 "schedule": "rays sorted by a 30-bit coherence key, then one per thread (default for "
-                             ">= 2^21 closest-hit rays; the sort is inside the timed step)"
+                 "schedule": "rays in the order of a 30-bit coherence key (hand-written stable radix sort, "
+                             "3 passes of 10 bits), then one per thread (default for >= 2^21 closest-hit rays; the "
+                             "sort is inside the timed step)"
                              if sorted_schedule else "one ray per thread"}),
             "roofline": {"bound": bound, "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
                          "frac": round(achieved / peak, 4), "traffic": traffic,
@@ -374,9 +375,10 @@ def run_ours(args):
             "e2e": {"value": round(e2e_value, 3), "unit": UNIT, "h2d_bytes_per_step": int(n * 32),
                     "d2h_bytes_per_step": int(n * 16)},
             "clocks": clocks.summary(),
-            # the default schedule sorts closest-hit batches of >= 2^21 FP32 rays: a key kernel, CUB's
-            # radix sort (histogram, scan, four one-sweep passes), then the traversal kernel
-            "gpu_launches": args.steps * (8 if sorted_schedule else 1),
+            # the default schedule sorts closest-hit batches of >= 2^21 FP32 rays: the key kernel (which also
+            # counts the first digit), then per 10-bit digit a tile scan, a tile-sum scan and a scatter, the
+            # next digit's count between passes, then the traversal kernel: 13 launches for 4M rays
+            "gpu_launches": args.steps * (13 if sorted_schedule else 1),
             **({"parity_vs_fp32_nodes": parity} if parity else {}),
         }
         if world == 1 and not args.no_cpu_baseline:
