@@ -182,6 +182,46 @@ sg_status sg_scene_create(const float* triangles, int64_t ntri, const sg_build_o
 sg_status sg_scene_create_hair(const float* triangles, int64_t ntri, const float* lines, int64_t nlines,
                                const sg_build_opts* opts, sg_scene** out);
 
+/* ---- Area-light shapes in the accelerator --------------------------------
+ * SORT puts each area light's shape into the accelerator as a primitive
+ * (entity/light_entity.cpp:153-154); Fbvh keeps such primitives in a leaf's
+ * other_list and tests them after the leaf's triangle and line packs
+ * (accel/fast_bvh.hpp:244-247, 390-406) with the shape's own scalar test:
+ * Quad::GetIntersect (shape/quad.cpp:67-93) for SQUARE and RECTANGLE lights,
+ * Disk::GetIntersect (shape/disk.cpp) for DISK lights. That test takes a hit
+ * when t <= the current nearest t (not only when nearer), and a shape hit
+ * leaves u and v at the values of the hit it replaced (0 when none).
+ * sg_area_shape: the shape in its local frame (a sizeX x sizeY rectangle, or a
+ * disk of the given radius, in the x-z plane around the origin, normal +y)
+ * and Shape::m_transform (math/transform.h) as SORT holds it. */
+typedef enum { SG_SHAPE_QUAD = 0, SG_SHAPE_DISK = 1 } sg_shape_kind;
+typedef struct {
+    int32_t kind;       /* sg_shape_kind */
+    float size[2];      /* quad: sizeX, sizeY (shape/quad.h:107-108); disk: radius, unused */
+    float matrix[16];   /* local to world, row-major (Transform::matrix) */
+    float inverse[16];  /* world to local (Transform::invMatrix) */
+} sg_area_shape;
+
+/* Primitives of every kind, and the order SORT's builder sees them in.
+ * Primitive indices: triangles 0 .. ntri-1, then the hair segments (10 floats
+ * each, as sg_scene_create_hair takes them), then the area shapes. order:
+ * NULL (that order) or the ntri + nlines + nshapes indices in the order
+ * SORT's ScenePrimitiveIterator visits the primitives (entity by entity,
+ * core/scene.cpp:43-80), which decides the tree SORT builds. Hits report the
+ * indices above. Such a scene answers sg_trace_closest / sg_trace_any and
+ * their _host forms (the others: SG_ERR_UNSUPPORTED, as for hair), and is
+ * built by SG_BUILDER_HOST or SG_BUILDER_GPU. */
+typedef struct {
+    const float* triangles;
+    int64_t ntri;
+    const float* lines;
+    int64_t nlines;
+    const sg_area_shape* shapes;
+    int64_t nshapes;
+    const int32_t* order;
+} sg_shapes;
+sg_status sg_scene_create_shapes(const sg_shapes* shapes, const sg_build_opts* opts, sg_scene** out);
+
 /* SORT's binary scene stream (what the Blender exporter writes and
  * ImageEvaluation loads, work/image_evaluation/image_evaluation.cpp:62-108),
  * read for the GPU path: the configuration with the integrator's parameters
@@ -256,6 +296,10 @@ sg_status sg_build_topology_host(const float* triangles, int64_t ntri, const sg_
 sg_status sg_build_topology_host_hair(const float* triangles, int64_t ntri, const float* lines, int64_t nlines,
                                       const sg_build_opts* opts, int32_t* out, int64_t cap, int64_t* written,
                                       int32_t* depth);
+/* The same for primitives of every kind (as sg_scene_create_shapes takes
+ * them); a leaf lists its triangles, then its lines, then its area shapes. */
+sg_status sg_build_topology_host_shapes(const sg_shapes* shapes, const sg_build_opts* opts, int32_t* out,
+                                        int64_t cap, int64_t* written, int32_t* depth);
 
 sg_status sg_scene_set_tuning(sg_scene* scene, const sg_trace_tuning* tuning);
 sg_status sg_scene_get_tuning(const sg_scene* scene, sg_trace_tuning* tuning);

@@ -199,6 +199,9 @@ class Reference:
         L.sortref_trace_attenuation.argtypes = [_vp, _vp, _i64, _vp, ctypes.c_int]
         L.sortref_scene_from_stream.restype = _vp
         L.sortref_scene_from_stream.argtypes = [ctypes.c_char_p, _i64, ctypes.c_int, ctypes.c_int, ctypes.c_int]
+        L.sortref_scene_create_shapes.restype = _vp
+        L.sortref_scene_create_shapes.argtypes = [ctypes.c_int, _vp, ctypes.c_int, _vp, ctypes.c_int, _vp,
+                                                  ctypes.c_int, _vp, ctypes.c_int, ctypes.c_int]
         L.sortref_scene_create_hair.restype = _vp
         L.sortref_scene_create_hair.argtypes = [ctypes.c_int, _vp, ctypes.c_int, _vp, ctypes.c_int, ctypes.c_int,
                                                 ctypes.c_int]
@@ -252,6 +255,25 @@ class Reference:
         if not h:
             raise ValueError("reference build failed")
         return _Tree(self, h, width, tri.shape[0] + ln.shape[0])
+
+    def build_shapes(self, tri: np.ndarray, lines, shapes, order, width: int, max_depth: int = 16,
+                     max_leaf: int = 8) -> _Tree:
+        """Triangles, hair segments (m, 10) and area shapes (records of 35 words:
+        kind, size x, size y, matrix[16], inverse[16]; the layout of
+        sort_b200.SHAPE_DTYPE), ids in that order; `order` lists the ids in the
+        order SORT's scene presents them (None: increasing)."""
+        tri = np.ascontiguousarray(tri, np.float32).reshape(-1, 9)
+        ln = np.zeros((0, 10), np.float32) if lines is None else np.ascontiguousarray(lines, np.float32).reshape(-1, 10)
+        sh = np.zeros(0, np.dtype((np.void, 140))) if shapes is None else np.ascontiguousarray(shapes)
+        if sh.dtype.itemsize != 140:
+            raise ValueError("area shape records are 140 bytes")
+        od = None if order is None else np.ascontiguousarray(order, np.int32)
+        h = self.L.sortref_scene_create_shapes(width, tri.ctypes.data, tri.shape[0], ln.ctypes.data, ln.shape[0],
+                                               sh.ctypes.data, sh.shape[0], None if od is None else od.ctypes.data,
+                                               max_depth, max_leaf)
+        if not h:
+            raise ValueError("reference build failed")
+        return _Tree(self, h, width, tri.shape[0] + ln.shape[0] + sh.shape[0])
 
     def build(self, tri: np.ndarray, width: int, max_depth: int = 16, max_leaf: int = 8) -> _Tree:
         tri = np.ascontiguousarray(tri, np.float32).reshape(-1, 9)

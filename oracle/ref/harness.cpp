@@ -47,7 +47,9 @@
 #include "core/render_context.h"
 #include "math/interaction.h"
 #include "scatteringevent/bssrdf/bssrdf.h"
+#include "shape/disk.h"
 #include "shape/line.h"
+#include "shape/quad.h"
 #include "stream/fstream.h"
 #undef private
 #undef protected
@@ -159,6 +161,42 @@ private:
     std::vector<std::unique_ptr<Line>> m_lines;
 };
 
+// Area-light shapes as the accelerator sees them: one Quad or Disk with its
+// Transform per primitive (entity/light_entity.cpp:112-154 makes one per
+// light; the light itself plays no part in intersection).
+// Record per shape, 35 floats: kind (int bits; 0 quad, 1 disk), size x, size y
+// (a disk's radius in size x), matrix[16], inverse[16] (row-major).
+class HarnessShapes : public Visual {
+public:
+    void Fill(const float* rec, int n) {
+        for (int i = 0; i < n; ++i) {
+            const float* r = rec + (size_t)i * 35;
+            int32_t kind;
+            std::memcpy(&kind, r, 4);
+            const Transform xf(Matrix(r + 3), Matrix(r + 19));
+            std::unique_ptr<Shape> shape;
+            if (kind == 1) {
+                auto d = std::make_unique<Disk>();
+                d->SetRadius(r[1]);
+                shape = std::move(d);
+            } else {
+                auto q = std::make_unique<Quad>();
+                q->SetSizeX(r[1]);
+                q->SetSizeY(r[2]);
+                shape = std::move(q);
+            }
+            shape->SetTransform(xf);
+            m_primitives.push_back(std::make_unique<Primitive>(nullptr, &g_opaque, shape.get()));
+            m_shapes.push_back(std::move(shape));
+        }
+    }
+    void Serialize(IStreamBase&) override {}
+    void ApplyTransform(const Transform&) override {}
+
+private:
+    std::vector<std::unique_ptr<Shape>> m_shapes;
+};
+
 class HarnessEntity : public Entity {
 public:
     void Serialize(IStreamBase&) override {}
@@ -172,6 +210,12 @@ public:
     HarnessHair* AddHair() {
         auto v = std::make_unique<HarnessHair>();
         HarnessHair* raw = v.get();
+        m_visuals.push_back(std::move(v));
+        return raw;
+    }
+    HarnessShapes* AddShapes() {
+        auto v = std::make_unique<HarnessShapes>();
+        HarnessShapes* raw = v.get();
         m_visuals.push_back(std::move(v));
         return raw;
     }
@@ -306,6 +350,74 @@ static void* make_ref_scene(int width, const float* tri, int ntri, const float* 
     rs->scene.m_bbox.m_Min -= delta;
     rs->scene.m_bbox.m_Max += delta;
 
+    if (width == 4)
+        rs->scene.m_accelerator.reset(harness_make_qbvh((unsigned)max_depth, (unsigned)max_leaf));
+    else
+        rs->scene.m_accelerator.reset(harness_make_obvh((unsigned)max_depth, (unsigned)max_leaf));
+    const auto t0 = std::chrono::steady_clock::now();
+    rs->scene.m_accelerator->Build(rs->scene);
+    rs->build_seconds = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+    return rs;
+}
+
+// Triangles (9 floats each), hair segments (10 floats: p0, p1, v0, v1, w0, w1)
+// and area shapes (35-float records, see HarnessShapes): primitive ids in that
+// order. `order` (or NULL: increasing ids) lists the ids in the order the
+// scene presents them: each run of one kind is one entity, so SORT's
+// ScenePrimitiveIterator (core/scene.cpp:43-80) visits the primitives in that
+// order and Accelerator::Build sees them so. NULL on a bad argument.
+void* sortref_scene_create_shapes(int width, const float* tri, int ntri, const float* lines, int nlines,
+                                  const float* shapes, int nshapes, const int32_t* order, int max_depth,
+                                  int max_leaf) {
+    if ((width != 4 && width != 8) || ntri < 0 || nlines < 0 || nshapes < 0) return nullptr;
+    const int nall = ntri + nlines + nshapes;
+    std::vector<int32_t> ord((size_t)nall);
+    std::vector<uint8_t> seen((size_t)nall, 0);
+    for (int k = 0; k < nall; ++k) {
+        const int32_t id = order ? order[k] : k;
+        if (id < 0 || id >= nall || seen[(size_t)id]) return nullptr;
+        seen[(size_t)id] = 1;
+        ord[(size_t)k] = id;
+    }
+    auto kind_of = [&](int32_t id) { return id < ntri ? 0 : (id < ntri + nlines ? 1 : 2); };
+    auto* rs = new RefScene();
+    rs->width = width;
+    for (int k = 0; k < nall;) {
+        const int kind = kind_of(ord[(size_t)k]);
+        int e = k;
+        while (e < nall && kind_of(ord[(size_t)e]) == kind) ++e;
+        std::vector<float> buf;
+        const int per = kind == 0 ? 9 : (kind == 1 ? 10 : 35);
+        const float* src = kind == 0 ? tri : (kind == 1 ? lines : shapes);
+        const int first = kind == 0 ? 0 : (kind == 1 ? ntri : ntri + nlines);
+        for (int i = k; i < e; ++i) {
+            const float* x = src + (size_t)(ord[(size_t)i] - first) * per;
+            buf.insert(buf.end(), x, x + per);
+        }
+        auto entity = std::make_unique<HarnessEntity>();
+        if (kind == 0)
+            entity->AddVisual()->Fill(buf.data(), e - k);
+        else if (kind == 1)
+            entity->AddHair()->Fill(buf.data(), e - k);
+        else
+            entity->AddShapes()->Fill(buf.data(), e - k);
+        rs->scene.m_entities.push_back(std::move(entity));
+        k = e;
+    }
+    ScenePrimitiveIterator iter(rs->scene);
+    rs->prims.assign((size_t)nall, nullptr);
+    int32_t pos = 0;
+    while (auto p = iter.Next()) {
+        const int32_t id = ord[(size_t)pos++];
+        rs->index_of[p] = id;
+        rs->prims[(size_t)id] = p;
+        rs->scene.m_bbox.Union(p->GetBBox());
+    }
+    // core/scene.cpp:150-154
+    static const auto threshold = 0.001f;
+    auto delta = (rs->scene.m_bbox.m_Max - rs->scene.m_bbox.m_Min) * threshold;
+    rs->scene.m_bbox.m_Min -= delta;
+    rs->scene.m_bbox.m_Max += delta;
     if (width == 4)
         rs->scene.m_accelerator.reset(harness_make_qbvh((unsigned)max_depth, (unsigned)max_leaf));
     else

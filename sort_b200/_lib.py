@@ -125,6 +125,23 @@ class ServerStats(ctypes.Structure):
                                                     "graph_replays", "queued", "admitted")]
 
 
+SG_SHAPE_QUAD = 0
+SG_SHAPE_DISK = 1
+
+
+class AreaShape(ctypes.Structure):
+    """sg_area_shape: SORT's Quad (size = sizeX, sizeY) or Disk (size[0] = radius)
+    with its Transform (matrix and inverse, row-major)."""
+    _fields_ = [("kind", ctypes.c_int32), ("size", ctypes.c_float * 2), ("matrix", ctypes.c_float * 16),
+                ("inverse", ctypes.c_float * 16)]
+
+
+class Shapes(ctypes.Structure):
+    _fields_ = [("triangles", ctypes.c_void_p), ("ntri", ctypes.c_int64), ("lines", ctypes.c_void_p),
+                ("nlines", ctypes.c_int64), ("shapes", ctypes.c_void_p), ("nshapes", ctypes.c_int64),
+                ("order", ctypes.c_void_p)]
+
+
 _vp = ctypes.c_void_p
 _i64 = ctypes.c_int64
 _SIGNATURES = {
@@ -147,6 +164,9 @@ _SIGNATURES = {
     "sg_default_build_opts": (None, [ctypes.POINTER(BuildOpts)]),
     "sg_scene_create": (ctypes.c_int, [_vp, _i64, ctypes.POINTER(BuildOpts), ctypes.POINTER(_vp)]),
     "sg_scene_create_hair": (ctypes.c_int, [_vp, _i64, _vp, _i64, ctypes.POINTER(BuildOpts), ctypes.POINTER(_vp)]),
+    "sg_scene_create_shapes": (ctypes.c_int, [ctypes.POINTER(Shapes), ctypes.POINTER(BuildOpts), ctypes.POINTER(_vp)]),
+    "sg_build_topology_host_shapes": (ctypes.c_int, [ctypes.POINTER(Shapes), ctypes.POINTER(BuildOpts), _vp, _i64,
+                                                     ctypes.POINTER(_i64), ctypes.POINTER(ctypes.c_int32)]),
     "sg_scene_destroy": (ctypes.c_int, [_vp]),
     "sg_scene_info_get": (ctypes.c_int, [_vp, ctypes.POINTER(SceneInfo)]),
     "sg_scene_topology": (ctypes.c_int, [_vp, _vp, _i64, ctypes.POINTER(_i64)]),

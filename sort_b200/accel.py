@@ -41,20 +41,55 @@ class Hits:
     v: object     # barycentric weight of vertex 2
 
 
-class Scene:
-    """Triangle soup in primitive order (SORT's ScenePrimitiveIterator order),
-    optionally followed by hair line segments: (m, 10) float32 rows of p0 xyz,
-    p1 xyz, v0, v1, w0, w1 (half widths), in world space, primitive indices
-    after the triangles."""
+# sg_area_shape: SORT's Quad (size = sizeX, sizeY) or Disk (size[0] = radius)
+# in the x-z plane of its frame, and its Transform (local-to-world matrix and
+# its inverse, row-major).
+SHAPE_DTYPE = np.dtype([("kind", "<i4"), ("size", "<f4", (2,)), ("matrix", "<f4", (16,)),
+                        ("inverse", "<f4", (16,))])
 
-    def __init__(self, triangles, lines=None):
+
+def area_shapes(kind, size, matrix, inverse) -> np.ndarray:
+    """An array of area shapes: kind (n,) of SG_SHAPE_QUAD / SG_SHAPE_DISK,
+    size (n, 2), matrix and inverse (n, 16) or (n, 4, 4)."""
+    kind = np.atleast_1d(np.asarray(kind, np.int32))
+    out = np.zeros(kind.shape[0], SHAPE_DTYPE)
+    out["kind"] = kind
+    out["size"] = np.asarray(size, np.float32).reshape(-1, 2)
+    out["matrix"] = np.asarray(matrix, np.float32).reshape(-1, 16)
+    out["inverse"] = np.asarray(inverse, np.float32).reshape(-1, 16)
+    return out
+
+
+class Scene:
+    """Primitives in SORT's order: a triangle soup, optionally hair line segments
+    ((m, 10) float32 rows of p0 xyz, p1 xyz, v0, v1, w0, w1 half widths, world
+    space) and area-light shapes (an array of SHAPE_DTYPE). Primitive indices:
+    the triangles, then the lines, then the shapes. `order` (optional): every
+    primitive index in the order SORT's ScenePrimitiveIterator visits them,
+    which decides the tree SORT builds (default: indices in increasing order)."""
+
+    def __init__(self, triangles, lines=None, shapes=None, order=None):
         tri = np.ascontiguousarray(np.asarray(triangles, dtype=np.float32).reshape(-1, 9))
         self.triangles = tri
         self.lines = None if lines is None else np.ascontiguousarray(
             np.asarray(lines, dtype=np.float32).reshape(-1, 10))
+        self.shapes = None if shapes is None else np.ascontiguousarray(np.asarray(shapes, SHAPE_DTYPE).reshape(-1))
+        self.order = None if order is None else np.ascontiguousarray(np.asarray(order, np.int32).reshape(-1))
 
     def GetPrimitiveCount(self) -> int:
-        return int(self.triangles.shape[0]) + (0 if self.lines is None else int(self.lines.shape[0]))
+        return (int(self.triangles.shape[0]) + (0 if self.lines is None else int(self.lines.shape[0])) +
+                (0 if self.shapes is None else int(self.shapes.shape[0])))
+
+    def _shapes_struct(self) -> _lib.Shapes:
+        s = _lib.Shapes()
+        s.triangles, s.ntri = self.triangles.ctypes.data, self.triangles.shape[0]
+        if self.lines is not None:
+            s.lines, s.nlines = self.lines.ctypes.data, self.lines.shape[0]
+        if self.shapes is not None:
+            s.shapes, s.nshapes = self.shapes.ctypes.data, self.shapes.shape[0]
+        if self.order is not None:
+            s.order = self.order.ctypes.data
+        return s
 
 
 def _torch():
@@ -106,7 +141,10 @@ class Accelerator:
         self.Release()
         lib = _lib.load()
         h = ctypes.c_void_p()
-        if sc.lines is None:
+        if sc.shapes is not None or sc.order is not None:
+            _lib.check(lib.sg_scene_create_shapes(ctypes.byref(sc._shapes_struct()), ctypes.byref(self._opts()),
+                                                  ctypes.byref(h)))
+        elif sc.lines is None:
             _lib.check(lib.sg_scene_create(tri.ctypes.data, tri.shape[0], ctypes.byref(self._opts()),
                                            ctypes.byref(h)))
         else:
@@ -329,10 +367,12 @@ class Obvh(Accelerator):
 
 
 def build_topology_host(triangles, width: int, max_depth: int = 16, max_leaf: int = 8, threads: int = 0,
-                        lines=None):
+                        lines=None, shapes=None, order=None):
     """Build on the host only and return (topology stream, depth); needs no GPU.
-    With hair segments (lines, (m, 10)), they follow the triangles."""
+    With hair segments (lines, (m, 10)) and area shapes, they follow the
+    triangles, as in Scene; `order` as in Scene."""
     lib = _lib.load()
+    sc = Scene(triangles, lines, shapes, order) if (shapes is not None or order is not None) else None
     tri = np.ascontiguousarray(np.asarray(triangles, np.float32).reshape(-1, 9))
     ln = None if lines is None else np.ascontiguousarray(np.asarray(lines, np.float32).reshape(-1, 10))
     o = _lib.BuildOpts()
@@ -342,6 +382,9 @@ def build_topology_host(triangles, width: int, max_depth: int = 16, max_leaf: in
     depth = ctypes.c_int32(0)
 
     def call(out, cap):
+        if sc is not None:
+            return lib.sg_build_topology_host_shapes(ctypes.byref(sc._shapes_struct()), ctypes.byref(o), out, cap,
+                                                     ctypes.byref(need), ctypes.byref(depth))
         if ln is None:
             return lib.sg_build_topology_host(tri.ctypes.data, tri.shape[0], ctypes.byref(o), out, cap,
                                               ctypes.byref(need), ctypes.byref(depth))

@@ -18,6 +18,7 @@
 
 #include "builder.h"
 #include "hair.h"
+#include "scene_access.h"
 #include "staged_upload.h"
 #include "trace_kernels.h"
 
@@ -85,8 +86,8 @@ struct sg_scene {
     cudaEvent_t in_done[kMaxChunks] = {};
     cudaEvent_t trace_done[kMaxChunks] = {};
     int32_t* d_material = nullptr;  // per primitive, for sg_trace_multi_host (sg_scene_set_materials)
-    float4* d_lines = nullptr;      // hair line records (hair.h), primitives ntri .. ntri + n_lines - 1
-    int64_t n_lines = 0;
+    float4* d_lines = nullptr;      // line records, then area-shape records (hair.h): primitives ntri ..
+    int64_t n_lines = 0, n_shapes = 0;
 };
 
 namespace {
@@ -95,7 +96,7 @@ namespace {
 // each, primitives ntri ..), a leaf's triangles come before its lines, each in
 // leaf order, as SORT tests its triangle packs before its line packs.
 sg_status upload(sg_scene* s, const float* tri, int64_t ntri, const std::vector<float>& line_recs = {},
-                 int64_t nlines = 0) {
+                 int64_t nlines = 0, int64_t nshapes = 0) {
     const sg::BuiltTree& t = s->tree;
     const int W = t.width;
     const int f4 = W == 8 ? sg::NodeShape<8>::kF4 : sg::NodeShape<4>::kF4;
@@ -120,8 +121,8 @@ sg_status upload(sg_scene* s, const float* tri, int64_t ntri, const std::vector<
         for (int j = 0; j < W; ++j) ch[j] = t.child[size_t(k) * W + j];
     }
     const size_t nb = adopt ? size_t(nn) * f4 * sizeof(float4) : nodes.size() * sizeof(float4),
-                 tb = size_t(ntri + nlines + sg::kPadSlots) * 3 * sizeof(float4) +
-                      size_t(nlines) * sg::kLineF4 * sizeof(float4);
+                 tb = size_t(ntri + nlines + nshapes + sg::kPadSlots) * 3 * sizeof(float4) +
+                      size_t(nlines + nshapes) * sg::kLineF4 * sizeof(float4);
     cudaError_t e = cudaSuccess;
     if (adopt) {
         s->d_nodes = s->tree.d_nodes;
@@ -141,7 +142,7 @@ sg_status upload(sg_scene* s, const float* tri, int64_t ntri, const std::vector<
         s->d_tris = s->tree.d_tris;
         s->tree.d_tris = nullptr;
     } else {
-        const int64_t nall = ntri + nlines;
+        const int64_t nextra = nlines + nshapes, nall = ntri + nextra;
         std::vector<float4> tris(size_t(nall + sg::kPadSlots) * 3);
         std::memset(tris.data(), 0, tris.size() * sizeof(float4));
         auto put = [&](int64_t slot, int32_t p, int32_t last) {
@@ -151,25 +152,29 @@ sg_status upload(sg_scene* s, const float* tri, int64_t ntri, const std::vector<
                 dst[0] = make_float4(v[0], v[1], v[2], 0.0f);
                 dst[1] = make_float4(v[3], v[4], v[5], 0.0f);
                 dst[2] = make_float4(v[6], v[7], v[8], 0.0f);
-            } else {
-                const int32_t line = int32_t(p - ntri), kind = sg::kLineSlot;
-                std::memcpy(&dst[2].x, &line, 4);
+            } else {  // a line's or an area shape's record, lines first
+                const int32_t rec = int32_t(p - ntri), kind = rec < nlines ? sg::kLineSlot : sg::kShapeSlot;
+                std::memcpy(&dst[2].x, &rec, 4);
                 std::memcpy(&dst[2].w, &kind, 4);
             }
             std::memcpy(&dst[0].w, &p, 4);
             std::memcpy(&dst[1].w, &last, 4);
         };
-        if (nlines == 0) {
+        if (nextra == 0) {
             for (int64_t i = 0; i < ntri; ++i) put(i, t.order[size_t(i)], t.leaf_last[size_t(i)]);
         } else {
+            // A leaf's triangles, then its lines, then its area shapes, each in
+            // leaf order: SORT's leaf tests its triangle packs, its line packs,
+            // then its other_list (accel/fast_bvh.hpp:346-406).
+            auto kind = [&](int32_t p) { return p < ntri ? 0 : (p < ntri + nlines ? 1 : 2); };
             for (int64_t b = 0; b < nall;) {  // one leaf: slots b .. e
                 int64_t e = b;
                 while (!t.leaf_last[size_t(e)]) ++e;
                 int64_t k = b;
-                for (int pass = 0; pass < 2; ++pass)
+                for (int pass = 0; pass < 3; ++pass)
                     for (int64_t i = b; i <= e; ++i) {
                         const int32_t p = t.order[size_t(i)];
-                        if ((p >= ntri) != (pass == 1)) continue;
+                        if (kind(p) != pass) continue;
                         const int64_t slot = k++;
                         put(slot, p, slot == e ? 1 : 0);
                     }
@@ -184,13 +189,14 @@ sg_status upload(sg_scene* s, const float* tri, int64_t ntri, const std::vector<
         if ((e = sg::upload_host(s->d_tris, tris.data(), tbytes, nullptr)) != cudaSuccess ||
             (e = cudaStreamSynchronize(nullptr)) != cudaSuccess)
             return cuda_fail(e, "upload triangles");
-        if (nlines > 0) {
+        if (nextra > 0) {
             if ((e = cudaMalloc(&s->d_lines, line_recs.size() * sizeof(float))) != cudaSuccess)
                 return cuda_fail(e, "cudaMalloc(lines)");
             if ((e = cudaMemcpy(s->d_lines, line_recs.data(), line_recs.size() * sizeof(float),
                                 cudaMemcpyHostToDevice)) != cudaSuccess)
                 return cuda_fail(e, "upload lines");
             s->n_lines = nlines;
+            s->n_shapes = nshapes;
         }
     }
     s->device_bytes = int64_t(nb + tb);
@@ -265,7 +271,9 @@ const int32_t* scene_materials(const sg_scene* s) { return s ? s->d_material : n
 
 sg_status scene_launch(const sg_scene* s, bool any, TraceLaunch* L, DevTree* tree, int* device) {
     if (!s || !L || !tree || !device) return fail(SG_ERR_INVALID_ARGUMENT, "NULL argument");
-    if (s->d_lines) return fail(SG_ERR_UNSUPPORTED, "a scene with hair lines answers the closest-hit and any-hit queries only");
+    if (s->d_lines)
+        return fail(SG_ERR_UNSUPPORTED,
+                    "a scene with hair lines or area shapes answers the closest-hit and any-hit queries only");
     L->width = s->width;
     L->any = any;
     L->stack_need = s->stack_need;
@@ -299,22 +307,85 @@ void sg_default_build_opts(sg_build_opts* o) {
 
 namespace sg {
 
-sg_status scene_create_mixed(const float* triangles, int64_t ntri, const float* lines, int64_t nlines,
-                             const float* transforms, const int32_t* line_transform, const sg_build_opts* opts,
-                             sg_scene** out) {
+// The non-triangle primitives' records (20 floats each: the lines, then the
+// area shapes) and SORT's tree over every primitive, seen in `order` (NULL:
+// triangles, lines, shapes). Throws as build_tree does.
+BuiltTree build_mixed(const MixedInput& in, BuildParams bp, int builder, int device, std::vector<float>& recs) {
+    const int64_t nextra = in.nlines + in.nshapes, nall = in.ntri + nextra;
+    recs.assign(size_t(nextra) * 20, 0.0f);
+    std::vector<float> boxes(size_t(nextra) * 6);
+    for (int64_t k = 0; k < in.nlines; ++k)  // Line::SetTransform / GetBBox (hair_setup.cpp)
+        line_setup(in.lines + k * 10, &recs[size_t(k) * 20], &boxes[size_t(k) * 6],
+                   in.transforms ? in.transforms + size_t(in.line_transform[k]) * 16 : nullptr);
+    for (int64_t k = 0; k < in.nshapes; ++k)  // Quad / Disk: record and GetBBox
+        shape_setup(in.shapes[k], &recs[size_t(in.nlines + k) * 20], &boxes[size_t(in.nlines + k) * 6]);
+    auto run = [&](const float* tri, int64_t ntri) {
+        if (builder == SG_BUILDER_GPU) return build_tree_gpu(tri, ntri, bp, device);
+        if (builder == SG_BUILDER_LBVH) return build_tree_lbvh(tri, ntri, bp, device);
+        return build_tree(tri, ntri, bp);
+    };
+    BuiltTree t;
+    if (!in.order) {
+        bp.extra_boxes = boxes.data();
+        bp.nextra = nextra;
+        t = run(in.triangles, in.ntri);
+    } else {
+        // Every primitive's box in SORT's primitive order: the split rules see a
+        // primitive only as its box and box centre, so this builds SORT's tree.
+        std::vector<uint8_t> seen(size_t(nall), 0);
+        std::vector<float> all(size_t(std::max<int64_t>(nall, 1)) * 6);
+        for (int64_t k = 0; k < nall; ++k) {
+            const int32_t id = in.order[k];
+            if (id < 0 || id >= nall || seen[size_t(id)]) throw std::invalid_argument("order is not a permutation");
+            seen[size_t(id)] = 1;
+            float* b = &all[size_t(k) * 6];
+            if (id < in.ntri) {  // Triangle::GetBBox: BBox() then Union of the three vertices
+                for (int a = 0; a < 3; ++a) {
+                    b[a] = 3.402823466e+38f;
+                    b[3 + a] = -3.402823466e+38f;
+                }
+                for (int v = 0; v < 3; ++v)
+                    for (int a = 0; a < 3; ++a) {
+                        const float x = in.triangles[int64_t(id) * 9 + 3 * v + a];
+                        if (x < b[a]) b[a] = x;
+                        if (x > b[3 + a]) b[3 + a] = x;
+                    }
+            } else {
+                std::memcpy(b, &boxes[size_t(id - in.ntri) * 6], 6 * sizeof(float));
+            }
+        }
+        bp.extra_boxes = all.data();
+        bp.nextra = nall;
+        t = run(nullptr, 0);
+        for (int32_t& p : t.order) p = in.order[p];
+    }
+    t.first_extra = nextra > 0 ? in.ntri : -1;
+    t.first_shape = in.nshapes > 0 ? in.ntri + in.nlines : -1;
+    return t;
+}
+
+sg_status scene_create_mixed(const MixedInput& in, const sg_build_opts* opts, sg_scene** out) {
     if (!out) return fail(SG_ERR_INVALID_ARGUMENT, "out is NULL");
     *out = nullptr;
     if (!opts) return fail(SG_ERR_INVALID_ARGUMENT, "opts is NULL");
-    if (ntri < 0 || (ntri > 0 && !triangles)) return fail(SG_ERR_INVALID_ARGUMENT, "bad triangle buffer");
-    if (nlines < 0 || (nlines > 0 && !lines)) return fail(SG_ERR_INVALID_ARGUMENT, "bad line buffer");
-    if (nlines > 0 && opts->builder == SG_BUILDER_LBVH)
+    const int64_t ntri = in.ntri, nlines = in.nlines, nshapes = in.nshapes;
+    if (ntri < 0 || (ntri > 0 && !in.triangles)) return fail(SG_ERR_INVALID_ARGUMENT, "bad triangle buffer");
+    if (nlines < 0 || (nlines > 0 && !in.lines)) return fail(SG_ERR_INVALID_ARGUMENT, "bad line buffer");
+    if (nshapes < 0 || (nshapes > 0 && !in.shapes)) return fail(SG_ERR_INVALID_ARGUMENT, "bad area shape buffer");
+    for (int64_t k = 0; k < nshapes; ++k)
+        if (in.shapes[k].kind != SG_SHAPE_QUAD && in.shapes[k].kind != SG_SHAPE_DISK)
+            return fail(SG_ERR_INVALID_ARGUMENT, "unknown area shape kind");
+    if ((nlines > 0 || nshapes > 0 || in.order) && opts->builder == SG_BUILDER_LBVH)
         return fail(SG_ERR_UNSUPPORTED, "SG_BUILDER_LBVH builds triangle scenes only");
-    if (ntri + nlines >= int64_t(0x7fffffff)) return fail(SG_ERR_LIMIT, "more than 2^31-2 primitives");
+    if (ntri + nlines + nshapes >= int64_t(0x7fffffff)) return fail(SG_ERR_LIMIT, "more than 2^31-2 primitives");
     if (opts->width != 4 && opts->width != 8) return fail(SG_ERR_INVALID_ARGUMENT, "width must be 4 or 8");
     if (opts->max_leaf < 1 || opts->max_depth < 1) return fail(SG_ERR_INVALID_ARGUMENT, "max_leaf/max_depth < 1");
     if (opts->node_format != SG_NODES_FP32 && opts->node_format != SG_NODES_QUANT8)
         return fail(SG_ERR_UNSUPPORTED, "unknown node format");
-    if (ntri >= int64_t(0x7fffffff)) return fail(SG_ERR_LIMIT, "more than 2^31-2 triangles");
+    if (opts->builder != SG_BUILDER_HOST && opts->builder != SG_BUILDER_GPU && opts->builder != SG_BUILDER_LBVH)
+        return fail(SG_ERR_INVALID_ARGUMENT, "unknown builder");
+    if (opts->builder == SG_BUILDER_LBVH && opts->node_format != SG_NODES_FP32)
+        return fail(SG_ERR_UNSUPPORTED, "SG_BUILDER_LBVH writes FP32 nodes only");
     int ndev = 0;
     cudaError_t e = cudaGetDeviceCount(&ndev);
     if (e != cudaSuccess) return cuda_fail(e, "cudaGetDeviceCount");
@@ -330,36 +401,10 @@ sg_status scene_create_mixed(const float* triangles, int64_t ntri, const float* 
     bp.max_depth = opts->max_depth;
     bp.max_leaf = opts->max_leaf;
     bp.threads = opts->build_threads;
-    // Hair lines: SORT's per-line constants and boxes (hair_setup.cpp).
-    std::vector<float> line_recs, line_boxes;
-    try {
-        line_recs.resize(size_t(nlines) * 20);
-        line_boxes.resize(size_t(nlines) * 6);
-    } catch (const std::bad_alloc&) {
-        delete s;
-        return fail(SG_ERR_OUT_OF_MEMORY, "host allocation failed");
-    }
-    for (int64_t k = 0; k < nlines; ++k)
-        sg::line_setup(lines + k * 10, &line_recs[size_t(k) * 20], &line_boxes[size_t(k) * 6],
-                       transforms ? transforms + size_t(line_transform[k]) * 16 : nullptr);
-    bp.extra_boxes = line_boxes.data();
-    bp.nextra = nlines;
-    if (opts->builder != SG_BUILDER_HOST && opts->builder != SG_BUILDER_GPU && opts->builder != SG_BUILDER_LBVH) {
-        delete s;
-        return fail(SG_ERR_INVALID_ARGUMENT, "unknown builder");
-    }
-    if (opts->builder == SG_BUILDER_LBVH && opts->node_format != SG_NODES_FP32) {
-        delete s;
-        return fail(SG_ERR_UNSUPPORTED, "SG_BUILDER_LBVH writes FP32 nodes only");
-    }
+    std::vector<float> recs;
     const auto t0 = std::chrono::steady_clock::now();
     try {
-        if (opts->builder == SG_BUILDER_GPU)
-            s->tree = sg::build_tree_gpu(triangles, ntri, bp, opts->device);
-        else if (opts->builder == SG_BUILDER_LBVH)
-            s->tree = sg::build_tree_lbvh(triangles, ntri, bp, opts->device);
-        else
-            s->tree = sg::build_tree(triangles, ntri, bp);
+        s->tree = build_mixed(in, bp, opts->builder, opts->device, recs);
     } catch (const std::bad_alloc&) {
         delete s;
         return fail(SG_ERR_OUT_OF_MEMORY, "host memory exhausted during build");
@@ -383,7 +428,7 @@ sg_status scene_create_mixed(const float* triangles, int64_t ntri, const float* 
     }
     sg_status st;
     try {
-        st = upload(s, triangles, ntri, line_recs, nlines);
+        st = upload(s, in.triangles, ntri, recs, nlines, nshapes);
     } catch (const std::bad_alloc&) {
         st = fail(SG_ERR_OUT_OF_MEMORY, "host memory exhausted during upload");
     }
@@ -402,12 +447,33 @@ sg_status scene_create_mixed(const float* triangles, int64_t ntri, const float* 
 extern "C" {
 
 sg_status sg_scene_create(const float* triangles, int64_t ntri, const sg_build_opts* opts, sg_scene** out) {
-    return sg::scene_create_mixed(triangles, ntri, nullptr, 0, nullptr, nullptr, opts, out);
+    sg::MixedInput in;
+    in.triangles = triangles;
+    in.ntri = ntri;
+    return sg::scene_create_mixed(in, opts, out);
 }
 
 sg_status sg_scene_create_hair(const float* triangles, int64_t ntri, const float* lines, int64_t nlines,
                                const sg_build_opts* opts, sg_scene** out) {
-    return sg::scene_create_mixed(triangles, ntri, lines, nlines, nullptr, nullptr, opts, out);
+    sg::MixedInput in;
+    in.triangles = triangles;
+    in.ntri = ntri;
+    in.lines = lines;
+    in.nlines = nlines;
+    return sg::scene_create_mixed(in, opts, out);
+}
+
+sg_status sg_scene_create_shapes(const sg_shapes* shapes, const sg_build_opts* opts, sg_scene** out) {
+    if (!shapes) return fail(SG_ERR_INVALID_ARGUMENT, "shapes is NULL");
+    sg::MixedInput in;
+    in.triangles = shapes->triangles;
+    in.ntri = shapes->ntri;
+    in.lines = shapes->lines;
+    in.nlines = shapes->nlines;
+    in.shapes = shapes->shapes;
+    in.nshapes = shapes->nshapes;
+    in.order = shapes->order;
+    return sg::scene_create_mixed(in, opts, out);
 }
 
 sg_status sg_scene_destroy(sg_scene* s) {
@@ -455,21 +521,34 @@ sg_status sg_build_topology_host(const float* triangles, int64_t ntri, const sg_
 sg_status sg_build_topology_host_hair(const float* triangles, int64_t ntri, const float* lines, int64_t nlines,
                                       const sg_build_opts* opts, int32_t* out, int64_t cap, int64_t* written,
                                       int32_t* depth) {
-    if (!opts || !written) return fail(SG_ERR_INVALID_ARGUMENT, "NULL argument");
-    if (ntri < 0 || (ntri > 0 && !triangles)) return fail(SG_ERR_INVALID_ARGUMENT, "bad triangle buffer");
-    if (nlines < 0 || (nlines > 0 && !lines)) return fail(SG_ERR_INVALID_ARGUMENT, "bad line buffer");
+    sg_shapes sh{triangles, ntri, lines, nlines, nullptr, 0, nullptr};
+    return sg_build_topology_host_shapes(&sh, opts, out, cap, written, depth);
+}
+
+sg_status sg_build_topology_host_shapes(const sg_shapes* sh, const sg_build_opts* opts, int32_t* out, int64_t cap,
+                                        int64_t* written, int32_t* depth) {
+    if (!sh || !opts || !written) return fail(SG_ERR_INVALID_ARGUMENT, "NULL argument");
+    if (sh->ntri < 0 || (sh->ntri > 0 && !sh->triangles)) return fail(SG_ERR_INVALID_ARGUMENT, "bad triangle buffer");
+    if (sh->nlines < 0 || (sh->nlines > 0 && !sh->lines)) return fail(SG_ERR_INVALID_ARGUMENT, "bad line buffer");
+    if (sh->nshapes < 0 || (sh->nshapes > 0 && !sh->shapes))
+        return fail(SG_ERR_INVALID_ARGUMENT, "bad area shape buffer");
     sg::BuildParams bp;
     bp.width = opts->width;
     bp.max_depth = opts->max_depth;
     bp.max_leaf = opts->max_leaf;
     bp.threads = opts->build_threads;
+    sg::MixedInput in;
+    in.triangles = sh->triangles;
+    in.ntri = sh->ntri;
+    in.lines = sh->lines;
+    in.nlines = sh->nlines;
+    in.shapes = sh->shapes;
+    in.nshapes = sh->nshapes;
+    in.order = sh->order;
     std::vector<int32_t> v;
     try {
-        std::vector<float> rec(size_t(nlines) * 20), boxes(size_t(nlines) * 6);
-        for (int64_t k = 0; k < nlines; ++k) sg::line_setup(lines + k * 10, &rec[size_t(k) * 20], &boxes[size_t(k) * 6]);
-        bp.extra_boxes = boxes.data();
-        bp.nextra = nlines;
-        const sg::BuiltTree t = sg::build_tree(triangles, ntri, bp);
+        std::vector<float> recs;
+        const sg::BuiltTree t = sg::build_mixed(in, bp, SG_BUILDER_HOST, 0, recs);
         sg::tree_topology(t, v);
         if (depth) *depth = t.depth;
     } catch (const std::bad_alloc&) {

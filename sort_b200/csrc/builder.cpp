@@ -350,10 +350,13 @@ void topo_rec(const BuiltTree& t, int32_t ref, std::vector<int32_t>& out) {
         int64_t e = b;
         while (!t.leaf_last[size_t(e)]) ++e;
         int32_t n = 0;
-        for (int pass = 0; pass < (t.first_extra >= 0 ? 2 : 1); ++pass)  // triangles, then the others
+        auto kind = [&](int32_t p) {
+            if (t.first_extra < 0 || p < t.first_extra) return 0;
+            return (t.first_shape >= 0 && p >= t.first_shape) ? 2 : 1;
+        };
+        for (int pass = 0; pass < 3; ++pass)  // triangles, lines, area shapes
             for (int64_t i = b; i <= e; ++i) {
-                const bool extra = t.first_extra >= 0 && t.order[size_t(i)] >= t.first_extra;
-                if (extra != (pass == 1)) continue;
+                if (kind(t.order[size_t(i)]) != pass) continue;
                 out.push_back(t.order[size_t(i)]);
                 ++n;
             }

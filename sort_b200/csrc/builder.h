@@ -68,10 +68,12 @@ struct BuiltTree {
     // n_tri and n_interior give the sizes.
     float4* d_nodes = nullptr;
     int64_t n_interior = -1, n_tri = -1;
-    // Primitives from first_extra on are not triangles (hair lines); -1: none.
-    // A leaf tests its triangles before them, as SORT's leaf tests its triangle
-    // packs before its line packs.
+    // Primitives from first_extra on are not triangles (hair lines, then from
+    // first_shape on area shapes); -1: none. A leaf tests its triangles, then
+    // its lines, then its shapes, as SORT's leaf tests its triangle packs, its
+    // line packs, then its other_list.
     int64_t first_extra = -1;
+    int64_t first_shape = -1;
     int rounds = 0, launches = 0;  // GPU builders: rounds (levels) and their own kernel launches
     int64_t leaves = 0;
     int64_t interior() const { return n_interior >= 0 ? n_interior : (width ? int64_t(child.size()) / width : 0); }

@@ -1,4 +1,5 @@
-// Closest-hit and any-hit traversal for scenes with hair lines.
+// Closest-hit and any-hit traversal for scenes with hair lines and area-light
+// shapes.
 //
 // The tree and the box tests are the triangle path's (traversal.cuh); the leaf
 // loop also runs SORT's ray-line test. SORT's leaf tests all its triangle
@@ -13,6 +14,15 @@
 // an add): the ray in line space, the quadratic of the cone, the nearer root
 // whose line-space y lies strictly inside (0, length), else the farther one;
 // tmin < t < tmax; u = 1, v = lerp(v0, v1, y / length).
+//
+// Area shapes sit after a leaf's lines, as SORT's other_list follows its line
+// packs (accel/fast_bvh.hpp:390-406), and are tested with Quad::GetIntersect
+// (shape/quad.cpp:67-93) or Disk::GetIntersect (shape/disk.cpp): the ray taken
+// to the shape's frame by Matrix::TransformPoint / TransformVector
+// (math/matrix.cpp:70-92), t = -o.y / d.y with d.y != 0, kept when
+// tmin < t <= tmax and t <= the nearest t so far, then p = o + t d inside the
+// rectangle |x| <= sizeX/2, |z| <= sizeY/2, or the disk x^2 + z^2 <= r^2. A
+// shape hit leaves u, v as they were, as SORT's shape test does.
 #include <cuda_runtime.h>
 
 #include <cfloat>
@@ -62,6 +72,37 @@ __device__ __forceinline__ bool line_test(const RayState& r, const float4* __res
     return true;
 }
 
+// Returns true with t when the area shape is hit (t <= limit, the nearest t so far).
+__device__ __forceinline__ bool shape_test(const RayState& r, const float4* __restrict__ rec, float limit,
+                                           float& t_out) {
+    const float4 m0 = __ldg(rec), m1 = __ldg(rec + 1), m2 = __ldg(rec + 2), m3 = __ldg(rec + 3), g = __ldg(rec + 4);
+    float ox = f_add(f_add(f_add(f_mul(r.o[0], m0.x), f_mul(r.o[1], m0.y)), f_mul(r.o[2], m0.z)), m0.w);
+    float oy = f_add(f_add(f_add(f_mul(r.o[0], m1.x), f_mul(r.o[1], m1.y)), f_mul(r.o[2], m1.z)), m1.w);
+    float oz = f_add(f_add(f_add(f_mul(r.o[0], m2.x), f_mul(r.o[1], m2.y)), f_mul(r.o[2], m2.z)), m2.w);
+    const float ow = f_add(f_add(f_add(f_mul(r.o[0], m3.x), f_mul(r.o[1], m3.y)), f_mul(r.o[2], m3.z)), m3.w);
+    if (ow != 1.0f) {  // Point / w multiplies by the reciprocal (math/point.h:126-129)
+        const float inv = __fdiv_rn(1.0f, ow);
+        ox = f_mul(ox, inv);
+        oy = f_mul(oy, inv);
+        oz = f_mul(oz, inv);
+    }
+    const float dx = f_add(f_add(f_mul(r.d[0], m0.x), f_mul(r.d[1], m0.y)), f_mul(r.d[2], m0.z));
+    const float dy = f_add(f_add(f_mul(r.d[0], m1.x), f_mul(r.d[1], m1.y)), f_mul(r.d[2], m1.z));
+    const float dz = f_add(f_add(f_mul(r.d[0], m2.x), f_mul(r.d[1], m2.y)), f_mul(r.d[2], m2.z));
+    if (dy == 0.0f) return false;
+    const float t = __fdiv_rn(-oy, dy);
+    if (t > limit || t <= r.tmin || t > r.tmax) return false;
+    const float px = f_add(ox, f_mul(t, dx)), pz = f_add(oz, f_mul(t, dz));
+    if (__float_as_int(g.z) == SG_SHAPE_DISK) {
+        if (f_add(f_mul(px, px), f_mul(pz, pz)) > g.y) return false;
+    } else {
+        if (px > g.x || px < -g.x) return false;
+        if (pz > g.y || pz < -g.y) return false;
+    }
+    t_out = t;
+    return true;
+}
+
 template <int W, bool ANY, int STACK, bool Q8>
 __global__ void __launch_bounds__(128)
     k_trace_hair(DevTree tr, const float4* __restrict__ lines, DevRays rays, int64_t n, int32_t* __restrict__ prim_out,
@@ -82,15 +123,18 @@ __global__ void __launch_bounds__(128)
                     for (;; ++s) {
                         const float4* q = tr.tris + 3 * s;
                         const float4 a = __ldg(q), b = __ldg(q + 1), c = __ldg(q + 2);
-                        float t, u, v;
+                        float t, u = tv.best_u, v = tv.best_v;
                         bool hit;
-                        if (__float_as_int(c.w) == kLineSlot) {
+                        if (__float_as_int(c.w) == kShapeSlot) {
+                            hit = shape_test(tv.r, lines + int64_t(__float_as_int(c.x)) * kLineF4, tv.best_t, t);
+                        } else if (__float_as_int(c.w) == kLineSlot) {
                             u = 1.0f;
-                            hit = line_test(tv.r, lines + int64_t(__float_as_int(c.x)) * kLineF4, t, v);
+                            hit = line_test(tv.r, lines + int64_t(__float_as_int(c.x)) * kLineF4, t, v) &&
+                                  t < tv.best_t;
                         } else {
-                            hit = tri_test(tv.r, a, b, c, t, u, v);
+                            hit = tri_test(tv.r, a, b, c, t, u, v) && t < tv.best_t;
                         }
-                        if (hit && t < tv.best_t) {
+                        if (hit) {
                             tv.best_t = t;
                             tv.best_u = u;
                             tv.best_v = v;

@@ -1,4 +1,4 @@
-// Hair line set-up on the host: what SORT computes once per Line before any
+// Hair line and area-shape set-up on the host. Lines: what SORT computes once per Line before any
 // ray is traced (shape/line.cpp:117-135 Line::SetTransform, 98-106
 // Line::GetBBox), in SORT's operation order (this file is compiled without
 // floating-point contraction, as SORT is), so the per-line constants and boxes
@@ -12,6 +12,7 @@
 #include "hair.h"
 
 #include <cmath>
+#include <cstring>
 
 namespace sg {
 namespace {
@@ -45,10 +46,11 @@ void transform_point16(const float* m, const float* p, float* out) {
         out[0] = x;
         out[1] = y;
         out[2] = z;
-    } else {  // Point / w (math/vector3.h:218-220)
-        out[0] = x / w;
-        out[1] = y / w;
-        out[2] = z / w;
+    } else {  // Point / w multiplies by the reciprocal (math/point.h:126-129)
+        const float t = 1.0f / w;
+        out[0] = x * t;
+        out[1] = y * t;
+        out[2] = z * t;
     }
 }
 
@@ -99,6 +101,38 @@ void line_setup(const float* in, float* rec, float* box, const float* transform1
     for (int a = 0; a < 3; ++a) {
         box[a] = mn[a] - grow;
         box[3 + a] = mx[a] + grow;
+    }
+}
+
+void shape_setup(const sg_area_shape& shape, float* rec, float* box) {
+    const bool disk = shape.kind == SG_SHAPE_DISK;
+    // Quad: halfx = sizeX * 0.5f, halfy = sizeY * 0.5f (shape/quad.cpp:71-80, 86-89);
+    // Disk: the radius and its square as Disk::GetIntersect forms it.
+    const float a = disk ? shape.size[0] : shape.size[0] * 0.5f;
+    const float b = disk ? shape.size[0] * shape.size[0] : shape.size[1] * 0.5f;
+    for (int k = 0; k < 16; ++k) rec[k] = shape.inverse[k];
+    rec[16] = a;
+    rec[17] = b;
+    const int32_t kind = shape.kind;
+    std::memcpy(&rec[18], &kind, 4);
+    rec[19] = 0.0f;
+    // Quad::GetBBox / Disk::GetBBox: BBox() then Union of four corners of the
+    // shape in its plane through m_transform.TransformPoint.
+    const float ex = a, ez = disk ? a : b;
+    const float corners[4][3] = {{ex, 0.0f, ez}, {ex, 0.0f, -ez}, {-ex, 0.0f, ez}, {-ex, 0.0f, -ez}};
+    float mn[3] = {3.402823466e+38f, 3.402823466e+38f, 3.402823466e+38f};
+    float mx[3] = {-3.402823466e+38f, -3.402823466e+38f, -3.402823466e+38f};
+    for (const auto& c : corners) {
+        float w[3];
+        transform_point16(shape.matrix, c, w);
+        for (int k = 0; k < 3; ++k) {
+            if (w[k] < mn[k]) mn[k] = w[k];
+            if (w[k] > mx[k]) mx[k] = w[k];
+        }
+    }
+    for (int k = 0; k < 3; ++k) {
+        box[k] = mn[k];
+        box[3 + k] = mx[k];
     }
 }
 

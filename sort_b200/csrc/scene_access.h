@@ -4,17 +4,37 @@
 
 #include <cuda_runtime.h>
 
+#include <vector>
+
 #include "sortgpu.h"
 #include "trace_kernels.h"
 
 namespace sg {
 
-// Scene creation with hair segments in object space: segment k is mapped to
-// world space by the row-major 4x4 transforms[16 * line_transform[k]] (both
-// NULL: the segments are in world space).
-sg_status scene_create_mixed(const float* triangles, int64_t ntri, const float* lines, int64_t nlines,
-                             const float* transforms, const int32_t* line_transform, const sg_build_opts* opts,
-                             sg_scene** out);
+// Primitives of a scene: triangles (9 floats), hair segments (10 floats; with
+// transforms set, segment k is in the object space that the row-major 4x4
+// transforms[16 * line_transform[k]] maps to world space, else in world
+// space), area shapes, and optionally the order SORT's builder sees them in
+// (sg_shapes).
+struct MixedInput {
+    const float* triangles = nullptr;
+    int64_t ntri = 0;
+    const float* lines = nullptr;
+    int64_t nlines = 0;
+    const float* transforms = nullptr;
+    const int32_t* line_transform = nullptr;
+    const sg_area_shape* shapes = nullptr;
+    int64_t nshapes = 0;
+    const int32_t* order = nullptr;
+};
+
+struct BuiltTree;
+struct BuildParams;
+// SORT's tree over every primitive of `in` and the non-triangle primitives'
+// records (20 floats each, lines then shapes). Throws as build_tree does.
+BuiltTree build_mixed(const MixedInput& in, BuildParams bp, int builder, int device, std::vector<float>& recs);
+
+sg_status scene_create_mixed(const MixedInput& in, const sg_build_opts* opts, sg_scene** out);
 
 // Records msg for sg_last_error() and returns s.
 sg_status set_error(sg_status s, const char* msg);

@@ -462,9 +462,14 @@ sg_status sg_stream_scene_create(const sg_stream* s, const sg_build_opts* opts, 
             o.max_leaf = in.accel_max_leaf;
         }
     }
-    return sg::scene_create_mixed(s->triangles.data(), int64_t(s->tri_material.size()), s->lines.data(),
-                                  int64_t(s->line_material.size()), s->transforms.data(), s->line_transform.data(),
-                                  &o, out);
+    sg::MixedInput in;
+    in.triangles = s->triangles.data();
+    in.ntri = int64_t(s->tri_material.size());
+    in.lines = s->lines.data();
+    in.nlines = int64_t(s->line_material.size());
+    in.transforms = s->transforms.data();
+    in.line_transform = s->line_transform.data();
+    return sg::scene_create_mixed(in, &o, out);
 }
 
 }  // extern "C"

@@ -296,3 +296,42 @@ def hair_strands(strands: int, steps: int = 8, seed: int = 13, box: float = 10.0
         for j in range(steps):
             out[s * steps + j] = (*p[j], *p[j + 1], frac[j], frac[j + 1], w[j], w[j + 1])
     return out
+
+
+def quad_light_shape(light: np.ndarray) -> np.ndarray:
+    """The area light (centre xyz, size x, size z, ...) as SORT's Quad: sizeX x
+    sizeY in its frame, turned to face -y (the frame's +y axis maps to world
+    -y, its z axis to world -z), as the path-tracing harness places it."""
+    from .accel import area_shapes
+    cx, cy, cz, sx, sz = (float(v) for v in light[:5])
+    m = [1.0, 0.0, 0.0, cx, 0.0, -1.0, 0.0, cy, 0.0, 0.0, -1.0, cz, 0.0, 0.0, 0.0, 1.0]
+    inv = [1.0, 0.0, 0.0, -cx, 0.0, -1.0, 0.0, cy, 0.0, 0.0, -1.0, cz, 0.0, 0.0, 0.0, 1.0]
+    return area_shapes([0], [[sx, sz]], [m], [inv])
+
+
+def random_area_shapes(n: int, seed: int = 17, box: float = 10.0, size=(0.5, 4.0), disk_fraction: float = 0.4):
+    """n area-light shapes (SORT's Quad / Disk) with random sizes, orientations
+    (uniform random rotation, no scale, as SORT's light entity removes scale)
+    and positions in the box. Matrices are computed in double precision and
+    stored as float32; the inverse is the transposed rotation with the
+    translation taken back."""
+    from .accel import area_shapes
+    rng = np.random.default_rng(seed)
+    kinds = (rng.uniform(size=n) < disk_fraction).astype(np.int32)
+    sizes = rng.uniform(size[0], size[1], (n, 2))
+    mats, invs = [], []
+    for k in range(n):
+        q = rng.normal(size=4)
+        q /= np.linalg.norm(q)
+        w, x, y, z = q
+        r = np.array([[1 - 2 * (y * y + z * z), 2 * (x * y - w * z), 2 * (x * z + w * y)],
+                      [2 * (x * y + w * z), 1 - 2 * (x * x + z * z), 2 * (y * z - w * x)],
+                      [2 * (x * z - w * y), 2 * (y * z + w * x), 1 - 2 * (x * x + y * y)]])
+        t = rng.uniform(-box, box, 3)
+        m = np.eye(4)
+        m[:3, :3], m[:3, 3] = r, t
+        inv = np.eye(4)
+        inv[:3, :3], inv[:3, 3] = r.T, -r.T @ t
+        mats.append(m)
+        invs.append(inv)
+    return area_shapes(kinds, sizes, np.array(mats), np.array(invs))
