@@ -46,12 +46,18 @@
  *                     Scene::GetAttenuation (core/scene.cpp:192-208) with
  *                     Accelerator::GetAttenuation (accel/accelerator.cpp:26-69) on
  *                     scenes with transparent materials (ENABLE_TRANSPARENT_SHADOW).
+ *   sg_scene_create_hair / sg_scene_create_shapes
+ *                     Fbvh::Build over scenes whose primitives include hair
+ *                     Lines (Line4/8 packs) and area-light Quads and Disks (a
+ *                     leaf's other_list, accel/fast_bvh.hpp:221-264, 375-406).
  *
  * Semantics carried over from SORT:
  *   - hit identity is the primitive's index in input order (SORT returns a
  *     Primitive*, whose index in ScenePrimitiveIterator order this is);
- *   - a hit needs tmin < t <= tmax and is taken only if strictly nearer than
- *     the current one; a miss returns prim = -1 and t = FLT_MAX;
+ *   - a triangle hit needs tmin < t <= tmax and is taken only if strictly
+ *     nearer than the current one (a line hit: tmin < t < tmax, strictly
+ *     nearer; an area-shape hit: tmin < t <= tmax and t <= the current t, as
+ *     each SORT shape tests); a miss returns prim = -1 and t = FLT_MAX;
  *   - u, v are the barycentric weights of vertex 1 and vertex 2.
  *
  * Rays and hits are device pointers unless the function name ends in _host.
@@ -276,8 +282,20 @@ sg_status sg_stream_area_light_get(const sg_stream* stream, int32_t index, sg_st
 /* Name (NUL-terminated, cap bytes available) and flags (bit 0: a transparency
  * node, bit 1: an SSS node) of material `index` in the stream's order. */
 sg_status sg_stream_material(const sg_stream* stream, int32_t index, char* name, int64_t cap, int32_t* flags);
-/* The stream's scene as an sg_scene: its triangles, then its hair segments
- * (their entity's transform applied as SORT's Line::SetTransform applies it).
+/* The area lights' shapes (sg_stream_info.area_lights of them, in stream
+ * order) as SORT's scene holds them: a Quad for SQUARE / RECTANGLE lights, a
+ * Disk for DISK, with the transform AreaLightEntity::Serialize leaves the
+ * shape (entity/light_entity.cpp:97-150: the streamed matrix and its inverse
+ * by Matrix::Inverse, the scale taken out of both). */
+sg_status sg_stream_area_shapes(const sg_stream* stream, sg_area_shape* shapes);
+/* The scene's primitive indices (triangles, segments, shapes) in the order
+ * SORT's ScenePrimitiveIterator visits them (entity by entity): triangles +
+ * lines + area lights entries, the order sg_stream_scene_create builds in. */
+sg_status sg_stream_primitive_order(const sg_stream* stream, int32_t* order);
+/* The stream's scene as an sg_scene: its triangles, its hair segments (their
+ * entity's transform applied as SORT's Line::SetTransform applies it) and its
+ * area lights' shapes, built in the order SORT's scene presents them (entity
+ * by entity). Primitive indices: triangles, then segments, then shapes.
  * opts NULL: the stream's accelerator (Obvh: width 8, Qbvh: width 4, with
  * their depth and leaf size; any other class: SORT's fallback, a QBVH with
  * default parameters). */

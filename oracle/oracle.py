@@ -17,6 +17,8 @@ import numpy as np
 HERE = os.path.dirname(os.path.abspath(__file__))
 PORT_LIB = os.path.join(HERE, "_build", "liboracle.so")
 REF_LIB = os.path.join(HERE, "_ref", "libsortref.so")
+# The same harness with SORT's scenes built by the Gbvh adapter over the GPU engine.
+REF_GBVH_LIB = os.path.join(HERE, "_ref", "libsortref_gbvh.so")
 _vp = ctypes.c_void_p
 _i64 = ctypes.c_int64
 
@@ -170,13 +172,24 @@ class Port:
         return np.abs(np.asarray(t, np.float64)[ok] - t64[ok]) / t64[ok]
 
 
-class Reference:
-    """SORT's own QBVH/OBVH compiled from its sources (oracle/_ref/libsortref.so)."""
+def _load_reference(adapter: bool):
+    path = REF_GBVH_LIB if adapter else REF_LIB
+    if not os.path.exists(path):
+        raise FileNotFoundError(path)
+    L = ctypes.CDLL(path)
+    if adapter:
+        L.sortref_use_gbvh.argtypes = [ctypes.c_int]
+        L.sortref_use_gbvh(1)
+    return L
 
-    def __init__(self):
-        if not reference_available():
-            raise FileNotFoundError(REF_LIB)
-        L = ctypes.CDLL(REF_LIB)
+
+class Reference:
+    """SORT's own QBVH/OBVH compiled from its sources (oracle/_ref/libsortref.so).
+    adapter=True: the same SORT code with its scenes' accelerator being the
+    Gbvh adapter over the GPU engine (oracle/_ref/libsortref_gbvh.so)."""
+
+    def __init__(self, adapter: bool = False):
+        L = _load_reference(adapter)
         L.sortref_scene_create.restype = _vp
         L.sortref_scene_create.argtypes = [ctypes.c_int, _vp, ctypes.c_int, ctypes.c_int, ctypes.c_int]
         L.sortref_scene_destroy.argtypes = [_vp]
@@ -199,6 +212,7 @@ class Reference:
         L.sortref_trace_attenuation.argtypes = [_vp, _vp, _i64, _vp, ctypes.c_int]
         L.sortref_scene_from_stream.restype = _vp
         L.sortref_scene_from_stream.argtypes = [ctypes.c_char_p, _i64, ctypes.c_int, ctypes.c_int, ctypes.c_int]
+        L.sortref_light_shape.argtypes = [_vp, ctypes.c_int, ctypes.c_float, ctypes.c_float, _vp]
         L.sortref_scene_create_shapes.restype = _vp
         L.sortref_scene_create_shapes.argtypes = [ctypes.c_int, _vp, ctypes.c_int, _vp, ctypes.c_int, _vp,
                                                   ctypes.c_int, _vp, ctypes.c_int, ctypes.c_int]
@@ -256,6 +270,14 @@ class Reference:
             raise ValueError("reference build failed")
         return _Tree(self, h, width, tri.shape[0] + ln.shape[0])
 
+    def light_shape(self, light2world, shape: int, a: float, b: float = 0.0) -> np.ndarray:
+        """The 35-word shape record SORT makes for an area light (0 SQUARE,
+        1 RECTANGLE, 2 DISK) whose streamed transform is light2world (4x4)."""
+        m = np.ascontiguousarray(light2world, np.float32).reshape(16)
+        out = np.zeros(35, np.float32)
+        self.L.sortref_light_shape(m.ctypes.data, int(shape), float(a), float(b), out.ctypes.data)
+        return out
+
     def build_shapes(self, tri: np.ndarray, lines, shapes, order, width: int, max_depth: int = 16,
                      max_leaf: int = 8) -> _Tree:
         """Triangles, hair segments (m, 10) and area shapes (records of 35 words:
@@ -287,12 +309,11 @@ class Reference:
 
 
 class RefPathTracer:
-    """SORT's PathTracing::Li over a harness-built scene (oracle/ref/harness_pt.cpp)."""
+    """SORT's PathTracing::Li over a harness-built scene (oracle/ref/harness_pt.cpp);
+    adapter=True: its accelerator is the Gbvh adapter over the GPU engine."""
 
-    def __init__(self):
-        if not reference_available():
-            raise FileNotFoundError(REF_LIB)
-        L = ctypes.CDLL(REF_LIB)
+    def __init__(self, adapter: bool = False):
+        L = _load_reference(adapter)
         L.sortref_pt_scene_create.restype = _vp
         L.sortref_pt_scene_create.argtypes = [ctypes.c_int, _vp, ctypes.c_int, _vp, ctypes.c_int, _vp, _vp,
                                               ctypes.c_int, ctypes.c_int]

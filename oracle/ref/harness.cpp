@@ -190,6 +190,10 @@ public:
             m_shapes.push_back(std::move(shape));
         }
     }
+    void Add(std::unique_ptr<Shape> shape) {
+        m_primitives.push_back(std::make_unique<Primitive>(nullptr, &g_opaque, shape.get()));
+        m_shapes.push_back(std::move(shape));
+    }
     void Serialize(IStreamBase&) override {}
     void ApplyTransform(const Transform&) override {}
 
@@ -271,6 +275,13 @@ unsigned Scene::GetPrimitiveCount() const {
     return cnt;
 }
 
+HarnessAccelFactory g_harness_accel_factory = nullptr;
+
+Accelerator* harness_make_accel(int width, unsigned max_depth, unsigned max_leaf) {
+    if (g_harness_accel_factory) return g_harness_accel_factory(width, max_depth, max_leaf);
+    return width == 4 ? harness_make_qbvh(max_depth, max_leaf) : harness_make_obvh(max_depth, max_leaf);
+}
+
 // Symbols referenced from linked SORT objects on paths the harness never reaches.
 Spectrum EvaluateTransparency(Tsl_Namespace::ShaderInstance*, const SurfaceInteraction&) { return 0.0f; }
 
@@ -350,10 +361,7 @@ static void* make_ref_scene(int width, const float* tri, int ntri, const float* 
     rs->scene.m_bbox.m_Min -= delta;
     rs->scene.m_bbox.m_Max += delta;
 
-    if (width == 4)
-        rs->scene.m_accelerator.reset(harness_make_qbvh((unsigned)max_depth, (unsigned)max_leaf));
-    else
-        rs->scene.m_accelerator.reset(harness_make_obvh((unsigned)max_depth, (unsigned)max_leaf));
+    rs->scene.m_accelerator.reset(harness_make_accel(width, (unsigned)max_depth, (unsigned)max_leaf));
     const auto t0 = std::chrono::steady_clock::now();
     rs->scene.m_accelerator->Build(rs->scene);
     rs->build_seconds = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
@@ -418,14 +426,47 @@ void* sortref_scene_create_shapes(int width, const float* tri, int ntri, const f
     auto delta = (rs->scene.m_bbox.m_Max - rs->scene.m_bbox.m_Min) * threshold;
     rs->scene.m_bbox.m_Min -= delta;
     rs->scene.m_bbox.m_Max += delta;
-    if (width == 4)
-        rs->scene.m_accelerator.reset(harness_make_qbvh((unsigned)max_depth, (unsigned)max_leaf));
-    else
-        rs->scene.m_accelerator.reset(harness_make_obvh((unsigned)max_depth, (unsigned)max_leaf));
+    rs->scene.m_accelerator.reset(harness_make_accel(width, (unsigned)max_depth, (unsigned)max_leaf));
     const auto t0 = std::chrono::steady_clock::now();
     rs->scene.m_accelerator->Build(rs->scene);
     rs->build_seconds = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
     return rs;
+}
+
+// An area light's shape as AreaLightEntity::Serialize makes it
+// (entity/light_entity.cpp:97-150), with SORT's own arithmetic: the inverse
+// by Matrix::Inverse (what reading a Transform does), the scale taken out by
+// Matrix::operator* with Scale(). shape: 0 SQUARE (a), 1 RECTANGLE (a, b),
+// 2 DISK (radius a). out: the 35-word record of HarnessShapes (kind, sizes
+// as the shape holds them after SetSizeX / SetSizeY / SetRadius, matrix,
+// inverse).
+void sortref_light_shape(const float* m16, int shape, float a, float b, float* out) {
+    Transform xf;
+    xf.matrix = Matrix(m16);
+    xf.matrix.Inverse(xf.invMatrix);
+    const auto sx = Vector(xf.matrix.m[0], xf.matrix.m[4], xf.matrix.m[8]).Length();
+    const auto sy = Vector(xf.matrix.m[1], xf.matrix.m[5], xf.matrix.m[9]).Length();
+    const auto sz = Vector(xf.matrix.m[2], xf.matrix.m[6], xf.matrix.m[10]).Length();
+    const auto mat = xf.matrix * Scale(1 / sx, 1 / sy, 1 / sz).matrix;
+    const auto inv_mat = Scale(sx, sy, sz).matrix * xf.invMatrix;
+    int32_t kind = shape == 2 ? 1 : 0;
+    std::memcpy(out, &kind, 4);
+    if (shape == 2) {
+        Disk d;
+        d.SetRadius(a);
+        out[1] = a;
+        out[2] = 0.0f;
+    } else {
+        Quad q;
+        q.SetSizeX(a);
+        q.SetSizeY(shape == 0 ? a : b);
+        out[1] = q.sizeX;
+        out[2] = q.sizeY;
+    }
+    for (int k = 0; k < 16; ++k) {
+        out[3 + k] = mat.m[k];
+        out[19 + k] = inv_mat.m[k];
+    }
 }
 
 double sortref_build_seconds(void* h) { return ((RefScene*)h)->build_seconds; }
@@ -487,16 +528,45 @@ void* sortref_scene_from_stream(const char* path, int64_t offset, int width, int
             int fit;
             stream >> eye >> up >> target >> w >> h >> lens >> sw >> sh >> fit >> arw >> arh >> fov;
         } else if (cls == StringID("AreaLightEntity")) {
+            // AreaLightEntity::Serialize's steps (entity/light_entity.cpp:97-154)
+            // with SORT's own arithmetic: the Transform read (its inverse by
+            // Matrix::Inverse), the scale taken out by Matrix::operator* with
+            // Scale(), and the shape SORT makes, as one primitive.
             Transform xf;
             float energy;
             Spectrum in;
             StringID shape;
             stream >> xf >> energy >> in >> shape;
-            float a, b;
-            if (shape == StringID("RECTANGLE"))
+            const auto sx = Vector(xf.matrix.m[0], xf.matrix.m[4], xf.matrix.m[8]).Length();
+            const auto sy = Vector(xf.matrix.m[1], xf.matrix.m[5], xf.matrix.m[9]).Length();
+            const auto sz = Vector(xf.matrix.m[2], xf.matrix.m[6], xf.matrix.m[10]).Length();
+            const auto mat = xf.matrix * Scale(1 / sx, 1 / sy, 1 / sz).matrix;
+            const auto inv_mat = Scale(sx, sy, sz).matrix * xf.invMatrix;
+            const Transform l2w(mat, inv_mat);
+            std::unique_ptr<Shape> sh;
+            float a = 0.0f, b = 0.0f;
+            if (shape == StringID("RECTANGLE")) {
                 stream >> a >> b;
-            else
+                auto q = std::make_unique<Quad>();
+                q->SetSizeX(a);
+                q->SetSizeY(b);
+                sh = std::move(q);
+            } else if (shape == StringID("SQUARE")) {
                 stream >> a;
+                auto q = std::make_unique<Quad>();
+                q->SetSizeX(a);
+                q->SetSizeY(a);
+                sh = std::move(q);
+            } else {
+                stream >> a;
+                auto d = std::make_unique<Disk>();
+                d->SetRadius(a);
+                sh = std::move(d);
+            }
+            sh->SetTransform(l2w);
+            auto v = std::make_unique<HarnessShapes>();
+            v->Add(std::move(sh));
+            entity->Push(std::move(v));
         } else if (cls == StringID("PointLightEntity") || cls == StringID("DirLightEntity") ||
                    cls == StringID("SpotLightEntity")) {
             Transform xf;
@@ -530,10 +600,7 @@ void* sortref_scene_from_stream(const char* path, int64_t offset, int width, int
     auto delta = (rs->scene.m_bbox.m_Max - rs->scene.m_bbox.m_Min) * threshold;
     rs->scene.m_bbox.m_Min -= delta;
     rs->scene.m_bbox.m_Max += delta;
-    if (width == 4)
-        rs->scene.m_accelerator.reset(harness_make_qbvh((unsigned)max_depth, (unsigned)max_leaf));
-    else
-        rs->scene.m_accelerator.reset(harness_make_obvh((unsigned)max_depth, (unsigned)max_leaf));
+    rs->scene.m_accelerator.reset(harness_make_accel(width, (unsigned)max_depth, (unsigned)max_leaf));
     rs->scene.m_accelerator->Build(rs->scene);
     return rs;
 }
@@ -605,6 +672,7 @@ void sortref_scene_bbox(void* h, float* out6) {
 // Tree depth SORT recorded (Fbvh::m_depth).
 int sortref_depth(void* h) {
     RefScene* rs = (RefScene*)h;
+    if (g_harness_accel_factory) return -1;  // not SORT's Fbvh: no tree to walk
     if (rs->width == 4) return (int)harness_qbvh_depth(rs->scene.m_accelerator.get());
     return (int)harness_obvh_depth(rs->scene.m_accelerator.get());
 }
@@ -614,7 +682,7 @@ int sortref_depth(void* h) {
 int64_t sortref_topology(void* h, int32_t* out, int64_t cap) {
     RefScene* rs = (RefScene*)h;
     std::vector<int32_t> v;
-    if (!rs->scene.m_accelerator->GetIsValid()) return 0;
+    if (g_harness_accel_factory || !rs->scene.m_accelerator->GetIsValid()) return 0;
     if (rs->width == 4)
         harness_qbvh_topology(rs->scene.m_accelerator.get(), rs->index_of, v);
     else

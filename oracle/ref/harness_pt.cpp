@@ -276,10 +276,7 @@ void* sortref_pt_scene_create(int width, const float* tri, int ntri, const int32
     auto delta = (ps->scene.m_bbox.m_Max - ps->scene.m_bbox.m_Min) * threshold;
     ps->scene.m_bbox.m_Min -= delta;
     ps->scene.m_bbox.m_Max += delta;
-    if (width == 4)
-        ps->scene.m_accelerator.reset(harness_make_qbvh((unsigned)max_depth, (unsigned)max_leaf));
-    else
-        ps->scene.m_accelerator.reset(harness_make_obvh((unsigned)max_depth, (unsigned)max_leaf));
+    ps->scene.m_accelerator.reset(harness_make_accel(width, (unsigned)max_depth, (unsigned)max_leaf));
     ps->scene.m_accelerator->Build(ps->scene);
     return ps;
 }

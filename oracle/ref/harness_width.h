@@ -12,6 +12,13 @@ class Primitive;
 
 using HarnessIndexMap = std::unordered_map<const Primitive*, int32_t>;
 
+// The accelerator harness scenes are built with: SORT's Qbvh (width 4) or
+// Obvh (width 8), unless g_harness_accel_factory is set (harness_gbvh.cpp sets
+// it to the Gbvh adapter in the library that links the GPU engine).
+using HarnessAccelFactory = Accelerator* (*)(int width, unsigned max_depth, unsigned max_leaf);
+extern HarnessAccelFactory g_harness_accel_factory;
+Accelerator* harness_make_accel(int width, unsigned max_depth, unsigned max_leaf);
+
 Accelerator* harness_make_qbvh(unsigned max_depth, unsigned max_leaf);
 Accelerator* harness_make_obvh(unsigned max_depth, unsigned max_leaf);
 unsigned harness_qbvh_depth(const Accelerator* a);

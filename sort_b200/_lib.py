@@ -164,6 +164,8 @@ _SIGNATURES = {
     "sg_default_build_opts": (None, [ctypes.POINTER(BuildOpts)]),
     "sg_scene_create": (ctypes.c_int, [_vp, _i64, ctypes.POINTER(BuildOpts), ctypes.POINTER(_vp)]),
     "sg_scene_create_hair": (ctypes.c_int, [_vp, _i64, _vp, _i64, ctypes.POINTER(BuildOpts), ctypes.POINTER(_vp)]),
+    "sg_stream_area_shapes": (ctypes.c_int, [_vp, _vp]),
+    "sg_stream_primitive_order": (ctypes.c_int, [_vp, _vp]),
     "sg_scene_create_shapes": (ctypes.c_int, [ctypes.POINTER(Shapes), ctypes.POINTER(BuildOpts), ctypes.POINTER(_vp)]),
     "sg_build_topology_host_shapes": (ctypes.c_int, [ctypes.POINTER(Shapes), ctypes.POINTER(BuildOpts), _vp, _i64,
                                                      ctypes.POINTER(_i64), ctypes.POINTER(ctypes.c_int32)]),

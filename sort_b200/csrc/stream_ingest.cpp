@@ -18,8 +18,13 @@
 // transform, the camera, area lights, the integrator's parameters, material
 // names and flags, and the accelerator. Materials' TSL shader graphs, resource
 // files, volume data and the other light types are read past (their counts and
-// types are reported). Primitive order is SORT's ScenePrimitiveIterator order
-// within each kind: triangles in entity/visual order, then hair segments.
+// types are reported). Each area light's shape (a Quad for SQUARE and
+// RECTANGLE, a Disk for DISK) is a primitive of the scene, with the transform
+// AreaLightEntity::Serialize leaves it (entity/light_entity.cpp:97-154: the
+// streamed matrix, its inverse by Matrix::Inverse, the scale taken out of
+// both). The order of the primitives as SORT's ScenePrimitiveIterator visits
+// them (entity by entity) is recorded; the scene is built in that order.
+#include <algorithm>
 #include <cmath>
 #include <cstdint>
 #include <cstdio>
@@ -44,6 +49,8 @@ struct sg_stream {
     std::vector<float> transforms;        // 16 per hair entity
     sg_stream_camera camera{};
     std::vector<sg_stream_area_light> area_lights;
+    std::vector<sg_area_shape> shapes;  // one per area light, as the scene holds it
+    std::vector<std::pair<int, int64_t>> runs;  // (kind 0 triangle / 1 line / 2 shape, count) in entity order
     std::vector<std::string> material_names;
     std::vector<int32_t> material_flags;  // bit 0 transparency node, bit 1 SSS node
 };
@@ -58,6 +65,91 @@ constexpr uint32_t sid(const char* s) {
         for (int k = 0; k < 8; ++k) crc = (crc >> 1) ^ ((0u - (crc & 1u)) & 0xEDB88320u);
     }
     return ~crc;
+}
+
+// Matrix::Inverse (math/matrix.cpp:115-143, Cramer's rule, with the
+// determinant of 104-112), each entry in SORT's expression order so the
+// inverse is bit-identical; false (out untouched) when |det| < 1e-8.
+bool inverse16(const float* m, float* out) {
+    float d = (m[0] * m[5] - m[1] * m[4]) * (m[10] * m[15] - m[11] * m[14]) -
+              (m[0] * m[6] - m[2] * m[4]) * (m[9] * m[15] - m[11] * m[13]) +
+              (m[0] * m[7] - m[3] * m[4]) * (m[9] * m[14] - m[10] * m[13]) +
+              (m[1] * m[6] - m[2] * m[5]) * (m[8] * m[15] - m[11] * m[12]) -
+              (m[1] * m[7] - m[3] * m[5]) * (m[8] * m[14] - m[10] * m[12]) +
+              (m[2] * m[7] - m[3] * m[6]) * (m[8] * m[13] - m[9] * m[12]);
+    if (std::fabs(d) < 0.00000001f) return false;
+    d = 1.0f / d;
+    // Entry (r, c) is a cofactor written as a sum of three products; the table
+    // gives, per entry, the three (m[a], m[b] * m[c] - m[e] * m[f]) terms.
+    static const int8_t T[16][15] = {
+        {5, 10, 15, 11, 14, 6, 11, 13, 9, 15, 7, 9, 14, 10, 13},
+        {9, 2, 15, 3, 14, 10, 3, 13, 1, 15, 11, 1, 14, 2, 13},
+        {13, 2, 7, 3, 6, 14, 3, 5, 1, 7, 15, 1, 6, 2, 5},
+        {1, 7, 10, 6, 11, 2, 5, 11, 7, 9, 3, 6, 9, 5, 10},
+        {6, 8, 15, 11, 12, 7, 10, 12, 8, 14, 4, 11, 14, 10, 15},
+        {10, 0, 15, 3, 12, 11, 2, 12, 0, 14, 8, 3, 14, 2, 15},
+        {14, 0, 7, 3, 4, 15, 2, 4, 0, 6, 12, 3, 6, 2, 7},
+        {2, 7, 8, 4, 11, 3, 4, 10, 6, 8, 0, 6, 11, 7, 10},
+        {7, 8, 13, 9, 12, 4, 9, 15, 11, 13, 5, 11, 12, 8, 15},
+        {11, 0, 13, 1, 12, 8, 1, 15, 3, 13, 9, 3, 12, 0, 15},
+        {15, 0, 5, 1, 4, 12, 1, 7, 3, 5, 13, 3, 4, 0, 7},
+        {3, 5, 8, 4, 9, 0, 7, 9, 5, 11, 1, 4, 11, 7, 8},
+        {4, 10, 13, 9, 14, 5, 8, 14, 10, 12, 6, 9, 12, 8, 13},
+        {8, 2, 13, 1, 14, 9, 0, 14, 2, 12, 10, 1, 12, 0, 13},
+        {12, 2, 5, 1, 6, 13, 0, 6, 2, 4, 14, 1, 4, 0, 5},
+        {0, 5, 10, 6, 9, 1, 6, 8, 4, 10, 2, 4, 9, 5, 8}};
+    for (int k = 0; k < 16; ++k) {
+        const int8_t* t = T[k];
+        const float a = m[t[0]] * (m[t[1]] * m[t[2]] - m[t[3]] * m[t[4]]);
+        const float b = m[t[5]] * (m[t[6]] * m[t[7]] - m[t[8]] * m[t[9]]);
+        const float c = m[t[10]] * (m[t[11]] * m[t[12]] - m[t[13]] * m[t[14]]);
+        out[k] = d * (a + b + c);
+    }
+    return true;
+}
+
+// Matrix::operator* (math/matrix.cpp:51-67): each entry summed from 0 over k.
+void multiply16(const float* a, const float* b, float* out) {
+    for (int i = 0; i < 4; ++i)
+        for (int j = 0; j < 4; ++j) {
+            float v = 0.0f;
+            for (int k = 0; k < 4; ++k) v += a[i * 4 + k] * b[k * 4 + j];
+            out[i * 4 + j] = v;
+        }
+}
+
+// The shape of an area light as AreaLightEntity::Serialize leaves it
+// (entity/light_entity.cpp:97-150): the transform without its scale, a Quad
+// of size (SetSizeX / SetSizeY clamp to 0.0001) or a Disk of radius.
+sg_area_shape light_shape(const sg_stream_area_light& a) {
+    const float* m = a.light2world;
+    float inv[16] = {1, 0, 0, 0, 0, 1, 0, 0, 0, 0, 1, 0, 0, 0, 0, 1};  // Matrix() when not invertible
+    inverse16(m, inv);
+    auto length = [](float x, float y, float z) { return std::sqrt(x * x + y * y + z * z); };
+    const float sx = length(m[0], m[4], m[8]), sy = length(m[1], m[5], m[9]), sz = length(m[2], m[6], m[10]);
+    const float unscale[16] = {1 / sx, 0, 0, 0, 0, 1 / sy, 0, 0, 0, 0, 1 / sz, 0, 0, 0, 0, 1};
+    const float scale[16] = {sx, 0, 0, 0, 0, sy, 0, 0, 0, 0, sz, 0, 0, 0, 0, 1};
+    sg_area_shape out{};
+    multiply16(m, unscale, out.matrix);
+    multiply16(scale, inv, out.inverse);
+    if (a.shape == sid("DISK")) {
+        out.kind = SG_SHAPE_DISK;
+        out.size[0] = a.size_x;
+    } else {
+        out.kind = SG_SHAPE_QUAD;
+        const float y = a.shape == sid("SQUARE") ? a.size_x : a.size_y;
+        out.size[0] = std::max(0.0001f, a.size_x);
+        out.size[1] = std::max(0.0001f, y);
+    }
+    return out;
+}
+
+void add_run(sg_stream& s, int kind, int64_t count) {
+    if (count <= 0) return;
+    if (!s.runs.empty() && s.runs.back().first == kind)
+        s.runs.back().second += count;
+    else
+        s.runs.emplace_back(kind, count);
 }
 
 class Reader {
@@ -287,10 +379,14 @@ void read_entities(Reader& r, sg_stream& s) {
             for (uint32_t v = 0; v < visuals; ++v) {
                 const uint32_t vk = r.u32("visual class");
                 if (vk == sid("MeshVisual")) {
+                    const size_t before = s.tri_material.size();
                     read_mesh(r, xf, s);
+                    add_run(s, 0, int64_t(s.tri_material.size() - before));
                 } else if (vk == sid("HairVisual")) {
                     s.transforms.insert(s.transforms.end(), xf, xf + 16);
+                    const size_t before = s.line_material.size();
                     read_hair(r, int32_t(s.transforms.size() / 16 - 1), s);
+                    add_run(s, 1, int64_t(s.line_material.size() - before));
                 } else {
                     throw std::runtime_error("unknown visual class in the scene stream");
                 }
@@ -324,6 +420,8 @@ void read_entities(Reader& r, sg_stream& s) {
                 throw std::runtime_error("unknown area light shape");
             }
             s.area_lights.push_back(a);
+            s.shapes.push_back(light_shape(a));  // the light's Primitive (entity/light_entity.cpp:153-154)
+            add_run(s, 2, 1);
         } else if (kind == sid("PointLightEntity") || kind == sid("DirLightEntity") ||
                    kind == sid("SpotLightEntity")) {
             float m[16];
@@ -469,7 +567,44 @@ sg_status sg_stream_scene_create(const sg_stream* s, const sg_build_opts* opts, 
     in.nlines = int64_t(s->line_material.size());
     in.transforms = s->transforms.data();
     in.line_transform = s->line_transform.data();
+    in.shapes = s->shapes.data();
+    in.nshapes = int64_t(s->shapes.size());
+    // SORT's primitive order: the runs of each kind in entity order. Left out
+    // (NULL) when it is triangles, then lines, then shapes anyway.
+    std::vector<int32_t> order;
+    bool natural = true;
+    int last = 0;
+    for (const auto& run : s->runs) {
+        if (run.first < last) natural = false;
+        last = run.first;
+    }
+    if (!natural) {
+        int64_t next[3] = {0, in.ntri, in.ntri + in.nlines};
+        try {
+            order.reserve(size_t(in.ntri + in.nlines + in.nshapes));
+            for (const auto& run : s->runs)
+                for (int64_t k = 0; k < run.second; ++k) order.push_back(int32_t(next[run.first]++));
+        } catch (const std::bad_alloc&) {
+            return sg::set_error(SG_ERR_OUT_OF_MEMORY, "host allocation failed");
+        }
+        in.order = order.data();
+    }
     return sg::scene_create_mixed(in, &o, out);
+}
+
+sg_status sg_stream_primitive_order(const sg_stream* s, int32_t* order) {
+    if (!s || !order) return sg::set_error(SG_ERR_INVALID_ARGUMENT, "NULL argument");
+    const int64_t ntri = int64_t(s->tri_material.size()), nlines = int64_t(s->line_material.size());
+    int64_t next[3] = {0, ntri, ntri + nlines}, k = 0;
+    for (const auto& run : s->runs)
+        for (int64_t j = 0; j < run.second; ++j) order[k++] = int32_t(next[run.first]++);
+    return SG_OK;
+}
+
+sg_status sg_stream_area_shapes(const sg_stream* s, sg_area_shape* shapes) {
+    if (!s || (!shapes && !s->shapes.empty())) return sg::set_error(SG_ERR_INVALID_ARGUMENT, "NULL argument");
+    if (!s->shapes.empty()) std::memcpy(shapes, s->shapes.data(), s->shapes.size() * sizeof(sg_area_shape));
+    return SG_OK;
 }
 
 }  // extern "C"

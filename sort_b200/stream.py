@@ -52,6 +52,14 @@ class SortStream:
             self.area_lights.append({"light2world": np.array(a.light2world, np.float32).reshape(4, 4),
                                      "energy": a.energy, "intensity": list(a.intensity), "shape": a.shape,
                                      "size_x": a.size_x, "size_y": a.size_y})
+        from .accel import SHAPE_DTYPE
+        self.area_shapes = np.zeros(info.area_lights, SHAPE_DTYPE)
+        if info.area_lights:
+            _lib.check(lib.sg_stream_area_shapes(h, self.area_shapes.ctypes.data))
+        # primitive indices (triangles, segments, shapes) in the order SORT's scene visits them
+        self.order = np.empty(nt + nl + info.area_lights, np.int32)
+        if self.order.size:
+            _lib.check(lib.sg_stream_primitive_order(h, self.order.ctypes.data))
         self.materials = []
         for k in range(info.materials):
             buf = ctypes.create_string_buffer(4096)
@@ -60,9 +68,12 @@ class SortStream:
             self.materials.append((buf.value.decode(), flags.value))
 
     def scene(self):
-        """The geometry as an accel.Scene (triangles, then hair segments in world space)."""
+        """The geometry as an accel.Scene: triangles, hair segments in world space,
+        area lights' shapes (in that order; accelerator() builds in the order the
+        stream's entities present them)."""
         from .accel import Scene
-        return Scene(self.triangles, self.lines if len(self.lines) else None)
+        return Scene(self.triangles, self.lines if len(self.lines) else None,
+                     self.area_shapes if len(self.area_shapes) else None)
 
     def accelerator(self, builder: int = _lib.SG_BUILDER_HOST, device: int = 0, node_format: int = 0,
                     width: int | None = None):

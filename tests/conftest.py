@@ -42,3 +42,30 @@ def same_bits(a, b):
     a = np.asarray(a)
     b = np.asarray(b)
     return a.shape == b.shape and np.array_equal(a.view(np.int32), b.view(np.int32))
+
+
+def renumber_topology(topo, new_id):
+    """The pre-order topology stream (interior [cnt, children...], leaf
+    [0, cnt, ids...]) with every primitive id p replaced by new_id[p]."""
+    import numpy as np
+    topo = np.asarray(topo)
+    out = topo.copy()
+    new_id = np.asarray(new_id)
+    k = 0
+
+    def walk():
+        nonlocal k
+        cnt = int(topo[k])
+        k += 1
+        if cnt == 0:
+            n = int(topo[k])
+            k += 1
+            out[k:k + n] = new_id[topo[k:k + n]]
+            k += n
+            return
+        for _ in range(cnt):
+            walk()
+
+    if topo.size:
+        walk()
+    return out

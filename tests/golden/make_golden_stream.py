@@ -8,11 +8,14 @@ scene.sort is a SORT scene stream written by tests/sortstream_writer.py: a
 PathTracing configuration, a material section with a resource, a shader unit
 template, a shader group template and three materials, then a camera, two
 mesh entities (two transformed icospheres in one, a ground quad in the
-other), a hair entity with its own transform, an area light, a point light and
-a sky light, and an Obvh accelerator. stream.npz holds what SORT does with
-the entity section: its own MeshVisual / HairVisual Serialize and
-ApplyTransform, its tree (width 4 and 8), and its closest hits and any-hit
-answers for a ray set, plus the tree topologies.
+other) with a scaled, rotated RECTANGLE area light between them, a hair
+entity with its own transform, a DISK area light, a point light, a SQUARE
+area light and a sky light, and an Obvh accelerator. stream.npz holds what
+SORT does with the entity section: its own MeshVisual / HairVisual Serialize
+and ApplyTransform, each area light's shape as AreaLightEntity::Serialize
+makes it (entity/light_entity.cpp:97-154), its tree (width 4 and 8) over the
+primitives in entity order, and its closest hits and any-hit answers for a
+ray set, plus the tree topologies.
 """
 from __future__ import annotations
 
@@ -65,10 +68,12 @@ def scene_entities():
     return [
         ("camera", (0.0, 1.0, 12.0), (0.0, 1.0, 0.0), (0.0, 0.0, 0.0)),
         ("mesh", transform(0.4, (1, 2, 3), 2.0, (-3, 0, 0)), [mesh_a, mesh_b]),
+        ("area", transform(2.6, (1, 0.3, 0.2), 1.5, (0, 4, 1)), 20.0, (1.0, 0.95, 0.9), "RECTANGLE", (2.0, 1.5)),
         ("mesh", np.eye(4, dtype=np.float32), [ground]),
         ("hair", transform(-0.7, (0, 1, 1), 2.0, (3, 0.5, 0)), strands, 0.01, 0.04, 2),
-        ("area", transform(0.0, (1, 0, 0), 1.0, (0, 8, 0)), 20.0, (1.0, 0.95, 0.9), "RECTANGLE", (2.0, 1.5)),
+        ("area", transform(0.9, (0, 0.2, 1), 1.0, (4, -1, 2)), 10.0, (0.9, 0.9, 1.0), "DISK", (1.2,)),
         ("point", transform(0.0, (1, 0, 0), 1.0, (5, 5, 5))),
+        ("area", transform(3.1, (1, 0, 0.1), 0.8, (-4, 5, -2)), 5.0, (1.0, 1.0, 1.0), "SQUARE", (2.5,)),
         ("sky", np.eye(4, dtype=np.float32)),
     ]
 
@@ -78,7 +83,7 @@ def main():
     write_stream(path, materials=[("Wood", False, False), ("Glass", True, False), ("Skin", False, True)],
                  entities=scene_entities(), accelerator=("Obvh", 16, 8))
     s = SortStream(path)
-    ntri, nlines = s.info["triangles"], s.info["lines"]
+    ntri, nlines, nshapes = s.info["triangles"], s.info["lines"], s.info["area_lights"]
     rng = np.random.default_rng(62)
     m = 3000  # rays aimed at the geometry: hair segment points and triangle centres
     pick = rng.integers(0, nlines, m // 2)
@@ -89,15 +94,34 @@ def main():
     d = tgt - o
     d /= np.linalg.norm(d, axis=1, keepdims=True)
     aimed = np.concatenate([o.T, d.T, np.zeros((1, m)), np.full((1, m), 3.4e38)]).astype(np.float32)
-    rays = np.ascontiguousarray(np.concatenate([aimed, scenes.random_rays(2000, seed=63, box=6.0)], axis=1))
+    # rays aimed at points of the area lights' shapes (in their local frames)
+    ml = 1500
+    k = rng.integers(0, nshapes, ml)
+    sh = s.area_shapes
+    loc = np.stack([rng.uniform(-0.6, 0.6, ml) * sh["size"][k, 0], np.zeros(ml),
+                    rng.uniform(-0.6, 0.6, ml) * np.where(sh["kind"][k] == 1, sh["size"][k, 0], sh["size"][k, 1]),
+                    np.ones(ml)], 1)
+    tgt = np.einsum("nij,nj->ni", sh["matrix"][k].astype(np.float64).reshape(-1, 4, 4), loc)[:, :3]
+    o = tgt + rng.normal(size=(ml, 3)) * 8.0
+    d = tgt - o
+    d /= np.linalg.norm(d, axis=1, keepdims=True)
+    at_lights = np.concatenate([o.T, d.T, np.zeros((1, ml)), np.full((1, ml), 3.4e38)]).astype(np.float32)
+    rays = np.ascontiguousarray(np.concatenate([aimed, at_lights, scenes.random_rays(2000, seed=63, box=6.0)],
+                                               axis=1))
     ref = Reference()
-    out = {"rays": rays, "entity_offset": s.info["entity_offset"], "triangles": ntri, "lines": nlines}
+    from sort_b200.stream import sid
+    kinds = {sid("SQUARE"): 0, sid("RECTANGLE"): 1, sid("DISK"): 2}
+    light_shapes = np.stack([ref.light_shape(a["light2world"], kinds[a["shape"]], a["size_x"], a["size_y"])
+                             for a in s.area_lights])
+    out = {"rays": rays, "entity_offset": s.info["entity_offset"], "triangles": ntri, "lines": nlines,
+           "shapes": nshapes, "light_shapes": light_shapes}
     for w in (4, 8):
-        tree = ref.build_from_stream(path, s.info["entity_offset"], ntri + nlines, w)
+        tree = ref.build_from_stream(path, s.info["entity_offset"], ntri + nlines + nshapes, w)
         prim, t, u, v = tree.closest(rays)
         out.update({f"prim{w}": prim, f"t{w}": t, f"u{w}": u, f"v{w}": v, f"occ{w}": tree.any(rays),
                     f"topology{w}": tree.topology(), f"depth{w}": tree.depth()})
-        print(f"width {w}: hits {np.mean(prim >= 0):.3f}, on hair {np.mean(prim >= ntri):.3f}")
+        print(f"width {w}: hits {np.mean(prim >= 0):.3f}, on hair {np.mean((prim >= ntri) & (prim < ntri + nlines)):.3f}"
+              f", on lights {np.mean(prim >= ntri + nlines):.3f}")
     np.savez_compressed(os.path.join(OUT, "stream.npz"), **out)
     print(f"{ntri} triangles, {nlines} hair segments, {os.path.getsize(path)} bytes")
 

@@ -12,7 +12,7 @@ import os
 import numpy as np
 import pytest
 
-from conftest import ROOT, golden, same_bits
+from conftest import renumber_topology, ROOT, golden, same_bits
 
 GOLDEN = os.path.join(ROOT, "tests", "golden", "scene.sort")
 
@@ -36,7 +36,7 @@ def test_stream_fields_as_written():
     assert (i["spp"], i["image_width"], i["image_height"]) == (16, 64, 48)
     assert i["accelerator"] == sid("Obvh") and (i["accel_max_depth"], i["accel_max_leaf"]) == (16, 8)
     assert i["triangles"] == 2 * 1280 + 2 and i["lines"] > 0 and i["materials"] == 3
-    assert i["area_lights"] == 1 and i["other_lights"] == 2 and i["has_camera"] == 1 and i["volumes"] == 0
+    assert i["area_lights"] == 3 and i["other_lights"] == 2 and i["has_camera"] == 1 and i["volumes"] == 0
     assert s.materials == [("Wood", 0), ("Glass", 1), ("Skin", 2)]
     assert s.camera["eye"] == [0.0, 1.0, 12.0] and s.camera["image_width"] == 64
     a = s.area_lights[0]
@@ -62,9 +62,48 @@ def test_stream_geometry_is_sorts():
                 expect.append(w[np.asarray(tris)].reshape(-1, 9))
     assert same_bits(s.triangles, np.concatenate(expect))
     z = golden("stream")
+    n = s.triangles.shape[0] + s.lines.shape[0]
+    assert s.order.size == n + 3 and np.array_equal(np.sort(s.order), np.arange(n + 3))
+    assert list(s.order[1280 * 2: 1280 * 2 + 1]) == [n]  # the light between the two mesh entities
+    sort_index = np.argsort(s.order)  # primitive id -> its place in SORT's primitive order
     for w in (4, 8):
-        topo, depth = build_topology_host(s.triangles, w, lines=s.lines)
-        assert np.array_equal(topo, z[f"topology{w}"]) and depth == int(z[f"depth{w}"])
+        topo, depth = build_topology_host(s.triangles, w, lines=s.lines, shapes=s.area_shapes, order=s.order)
+        assert np.array_equal(renumber_topology(topo, sort_index), z[f"topology{w}"]) and depth == int(z[f"depth{w}"])
+
+
+def test_stream_light_shapes_are_sorts():
+    """Each area light's shape as AreaLightEntity::Serialize leaves it: the
+    streamed matrix's inverse (Matrix::Inverse), the scale taken out of both
+    (entity/light_entity.cpp:97-106), the shape's sizes; bit for bit against
+    the records SORT's own code made for the golden stream."""
+    from sort_b200.stream import SortStream
+    s = SortStream(GOLDEN)
+    assert np.array_equal(s.area_shapes.view(np.uint32).reshape(-1, 35), golden("stream")["light_shapes"].view(np.uint32))
+
+
+def test_stream_light_shapes_random_transforms(reference, tmp_path):
+    """Rotated, scaled and sheared light transforms, every shape kind: our
+    stream reader's shapes equal SORT's, computed by SORT's own matrix code."""
+    import sys
+    sys.path.insert(0, os.path.join(ROOT, "tests"))
+    from sortstream_writer import write_stream
+    from sort_b200.stream import SortStream
+    rng = np.random.default_rng(81)
+    names = ["SQUARE", "RECTANGLE", "DISK"]
+    ents = []
+    for k in range(24):
+        m = np.eye(4, dtype=np.float32)
+        m[:3, :3] = rng.normal(size=(3, 3)).astype(np.float32) * np.float32(rng.uniform(0.3, 3.0))
+        m[:3, 3] = rng.uniform(-10, 10, 3)
+        kind = names[k % 3]
+        sizes = (float(rng.uniform(0.00001, 3.0)),) if kind != "RECTANGLE" else tuple(rng.uniform(0.5, 3.0, 2))
+        ents.append(("area", m, 1.0, (1.0, 1.0, 1.0), kind, sizes))
+    path = tmp_path / "lights.sort"
+    write_stream(str(path), materials=[("M", False, False)], entities=ents, accelerator=("Obvh", 16, 8))
+    s = SortStream(path)
+    for k, a in enumerate(s.area_lights):
+        ref = reference.light_shape(a["light2world"], k % 3, a["size_x"], a["size_y"])
+        assert np.array_equal(s.area_shapes[k:k + 1].view(np.uint32), ref.view(np.uint32)), k
 
 
 def test_stream_hair_as_hairvisual_makes_it():
