@@ -144,7 +144,8 @@ def make_rays(acc, tri, rank: int, device):
 
 
 def reference_cpu(tri, rays, steps: int, warmup: int, threads: int, sample: int, width: int = WIDTH):
-    """SORT's OBVH on the host cores; returns (Mrays/s, description)."""
+    """SORT's OBVH on the host cores; returns (Mrays/s, kind, description, the
+    last timed block's first ray, SORT's (prim, t) for that block, the tree)."""
     from oracle.oracle import Reference, reference_available
     if not reference_available():
         from oracle.oracle import Port
@@ -154,16 +155,36 @@ def reference_cpu(tri, rays, steps: int, warmup: int, threads: int, sample: int,
     tree = impl.build(tri, width, DEPTH, LEAF)
     n = rays.shape[1]
     times = []
+    s, prim, t = 0, None, None
     for k in range(warmup + steps):
         s = (k * sample) % max(1, n - sample)
         block = np.ascontiguousarray(rays[:, s:s + sample])
         t0 = time.perf_counter()
-        tree.closest(block, threads)
+        prim, t, _, _ = tree.closest(block, threads)
         dt = time.perf_counter() - t0
         if k >= warmup:
             times.append(dt)
     rate = sample * len(times) / sum(times) / 1e6
-    return rate, kind, f"{sample} of the {n} diffuse rays per step, {len(times)} timed steps"
+    return rate, kind, f"{sample} of the {n} diffuse rays per step, {len(times)} timed steps", s, (prim, t)
+
+
+def parity_on_sample(tri, rays, first, sort_hits, gpu_prim, gpu_t):
+    """The GPU's hits on the CPU baseline's last block against SORT's, and both
+    hits' t error against an FP64 re-intersection of the hit triangle."""
+    from oracle.oracle import Port
+    sp, st = sort_hits
+    m = sp.shape[0]
+    gp, gt = gpu_prim[first:first + m], gpu_t[first:first + m]
+    block = np.ascontiguousarray(rays[:, first:first + m])
+    port = Port()
+    eg = port.fp64_rel_err(tri, gp, gt, block)
+    es = port.fp64_rel_err(tri, sp, st, block)
+
+    def summary(e):
+        return {"max": float(e.max()), "p99": float(np.percentile(e, 99)), "mean": float(e.mean())} if e.size else None
+    return {"rays": int(m), "prim_differs": int((gp != sp).sum()),
+            "t_bits_differ": int((gt.view(np.int32) != st.view(np.int32)).sum()),
+            "fp64_rel_err": {"gpu": summary(eg), "sort": summary(es), "hits": int(eg.size)}}
 
 
 def run_reference(args):
@@ -322,6 +343,10 @@ def run_ours(args):
     e2e_s = time.perf_counter() - t0
     e2e_value = world * n * args.steps / max_over_ranks(e2e_s, device) / 1e6
 
+    h_all = acc.GetIntersect(d_diff)  # the timed call's answers, for the parity check below (untimed)
+    torch.cuda.synchronize(device)
+    gpu_prim, gpu_t = h_all.prim.cpu().numpy(), h_all.t.cpu().numpy()
+
     peaks_path = os.path.join(ROOT, "MEASURED_PEAKS.json")
     if width == 4:
         # The 82k-triangle tree (~5 MB) stays in L2: its roofline is L2 bandwidth,
@@ -366,8 +391,8 @@ def run_ours(args):
                          "peak_source": peak_src,
                          "algorithmic_bytes_per_ray": round(bytes_closest, 1),
                          "node_tests_per_ray": round(node_tests / n, 3), "prim_tests_per_ray": round(prim_tests / n, 3),
-                         "kernel": ("k_trace_q8" if args.nodes == "q8" else "k_trace_fp32")
-                                   + f"<{width},false,{64 if width == 4 else 128},false>",
+                         "kernel": f"k_trace_walk<{width},false,{64 if width == 4 else 128},"
+                                   + ("true>" if args.nodes == "q8" else "false>"),
                          "launch_ms": round(launch_ms, 4)},
             "anyhit": {"mrays_s": round(n / (any_ms / 1e3) / 1e6, 3), "launch_ms": round(any_ms, 4),
                        "algorithmic_bytes_per_ray": round(bytes_any, 1),
@@ -383,10 +408,12 @@ def run_ours(args):
         }
         if world == 1 and not args.no_cpu_baseline:
             threads = os.cpu_count() or 1
-            rate, kind, desc = reference_cpu(tri, diffuse, steps=3, warmup=1, threads=threads, sample=args.sample,
-                                             width=width)
+            rate, kind, desc, first, sort_hits = reference_cpu(tri, diffuse, steps=3, warmup=1, threads=threads,
+                                                               sample=args.sample, width=width)
             out["cpu_baseline"] = {"value": round(rate, 3), "unit": UNIT, "cores": threads, "kind": kind,
                                    "sample": desc}
+            if args.nodes == "fp32" and args.builder != "lbvh":
+                out["parity"] = parity_on_sample(tri, diffuse, first, sort_hits, gpu_prim, gpu_t)
         print(json.dumps(out))
     acc.Release()
     if world > 1:
@@ -467,6 +494,22 @@ def run_pathtrace(args):
     host_img = img.cpu()
     e2e_s = time.perf_counter() - t0
     samples = PT_W * PT_H * args.steps
+    # Image error against SORT's converged render of a 192x108 window of this
+    # frame (tests/golden/pt21m.npz, made by SORT's PathTracing::Li at 1024 spp),
+    # at the workload's 16 spp, beside SORT's own 16-spp error (untimed).
+    rmse_info = None
+    gpath = os.path.join(ROOT, "tests", "golden", "pt21m.npz")
+    if os.path.exists(gpath):
+        z = np.load(gpath)
+        conv = z["converged"].astype(np.float64)
+        errs = []
+        for k in range(4):
+            win = pt.Render(z["camera"], int(z["width"]), int(z["height"]), 16, int(z["depth"]), seed=900 + k)
+            errs.append(float(np.sqrt(np.mean((win.cpu().numpy().astype(np.float64) - conv) ** 2))))
+        rmse_info = {"window": "192x108 of the 1920x1080 frame centred on pixel (600, 100)", "spp": 16,
+                     "rmse_vs_sort_converged": round(float(np.mean(errs)), 5),
+                     "sort_16spp_rmse": round(float(np.mean(z["rmse16"])), 5),
+                     "sort_converged_pair_rmse": round(float(z["rmse_converged_pair"]), 5)}
     out = {"metric": "path-traced Msamples/s", "value": round(samples / (ms / 1e3) / 1e6, 3), "unit": "Msamples/s",
            "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms / args.steps, 3),
            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
@@ -478,6 +521,7 @@ def run_pathtrace(args):
            "e2e": {"value": round(samples / e2e_s / 1e6, 3), "unit": "Msamples/s", "h2d_bytes_per_step": 0,
                    "d2h_bytes_per_step": int(host_img.numel() * 4 / args.steps)},
            "clocks": clocks.summary(), "image_mean": [round(float(v), 5) for v in host_img.mean(dim=(0, 1))],
+           **({"image_rmse": rmse_info} if rmse_info else {}),
            # per sample: generate, flush + per bounce (extend, shade, shadow, resolve, accumulate, count)
            "gpu_launches": args.steps * (2 + 6 * PT_DEPTH) + 2}
     if rank == 0:
