@@ -752,7 +752,7 @@ def run_serve(args):
         t.Render(scenes.CAMERA, 1920, 1080, 1, PT_DEPTH, seed=1)
     torch.cuda.synchronize(device)
     srv = RenderServer(device=local, path_slots=args.path_slots, pixel_budget=1 << 24, max_requests=1024,
-                       steps_per_poll=2)
+                       steps_per_poll=2, samples_per_claim=args.samples_per_claim)
     for t in tracers:
         srv.add_scene(t)
     srv.wait(srv.submit(0, scenes.CAMERA, 64, 64, 1))
@@ -832,7 +832,8 @@ def run_serve(args):
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
             "data": "synthetic (seeded procedural scenes and request stream)",
             "config": serve_config({"requests": len(reqs), "seed": args.batch_seed, "scene_triangles": tri_counts,
-                                    "path_slots": args.path_slots, "samples_per_run": int(work)}),
+                                    "path_slots": args.path_slots, "samples_per_claim": args.samples_per_claim,
+                                    "samples_per_run": int(work)}),
             "closed_loop": {"server": {"msamples_s": round(value, 2), "p50_ms": pct(srv_lat0, 50),
                                        "p99_ms": pct(srv_lat0, 99)},
                             "fifo": {"msamples_s": round(work / fifo_span0 / 1e6, 2), "p50_ms": pct(fifo_lat0, 50),
@@ -981,7 +982,9 @@ def main():
     p.add_argument("--workload", choices=["closest", "raycast", "pathtrace", "batched", "serve", "build"],
                    default="closest")
     p.add_argument("--requests", type=int, default=120, help="serve workload: requests per run")
-    p.add_argument("--path-slots", type=int, default=1 << 20, help="serve workload: server path pool")
+    p.add_argument("--path-slots", type=int, default=1 << 21, help="serve workload: server path pool")
+    p.add_argument("--samples-per-claim", type=int, default=64,
+                   help="serve workload: samples a pool slot renders of one pixel before handing it back")
     p.add_argument("--loads", type=float, nargs="*", default=[0.5, 0.8, 1.0],
                    help="serve workload: Poisson arrival rates as fractions of the FIFO arm's capacity")
     p.add_argument("--batches", type=int, default=64, help="batched workload: ray batches per step")

@@ -65,13 +65,11 @@ __device__ __forceinline__ void count_finished(bool fin, int b, const BatchArgs&
     }
 }
 
-// Held to 1,024 resident threads per SM (64 registers). Left alone the
-// compiler gives it 72-80 registers, and 6-7 blocks of 128 per SM; at 64 there
-// are no spills for closest hits (8 bytes for any-hit, 96-104 for 8-bit
-// nodes), and batched_31m runs 6% faster (1,773 to 1,880 Mrays/s). Holding it
-// to 1,152 threads (56 registers) spills 80-106 bytes and gains less.
+// Held to 1,152 resident threads per SM (56 registers, nine blocks of 128):
+// with the traversal in RayWalk, batched_31m runs at 1,903 Mrays/s there
+// against 1,868 at 1,024 threads (64 registers) and 1,873 at 896 (72).
 template <int W, bool ANY, int STACK, int BLOCK, bool Q8>
-__global__ void __launch_bounds__(BLOCK, 1024 / BLOCK) k_trace_batches(BatchArgs a) {
+__global__ void __launch_bounds__(BLOCK, 1152 / BLOCK) k_trace_batches(BatchArgs a) {
     const unsigned lane = threadIdx.x & 31u;
     const unsigned lt_mask = (1u << lane) - 1u;
     const GroupDesc g = a.header->groups[a.group];
