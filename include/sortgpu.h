@@ -146,7 +146,7 @@ typedef struct {
     int64_t device_bytes;    /* HBM held by the tree (nodes + triangles) */
     double build_seconds;    /* build time (host clock, whole build) */
     int32_t build_rounds;    /* GPU builders: split rounds (SG_BUILDER_GPU) or wide-tree levels (LBVH); 0 on the host */
-    int32_t build_launches;  /* GPU builders: their own kernels launched (CUB's scans and sorts not counted) */
+    int32_t build_launches;  /* GPU builders: their split / collapse kernels launched (prefix sums and sorts not counted) */
 } sg_scene_info;
 
 /* Traversal launch schedule (results never depend on it). */

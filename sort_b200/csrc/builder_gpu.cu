@@ -34,7 +34,6 @@
 // that is zero may carry the other sign, which no comparison sees.
 #include <cuda_runtime.h>
 
-#include <cub/device/device_scan.cuh>
 
 #include <algorithm>
 #include <cfloat>
@@ -49,6 +48,7 @@
 #include "gpu_build_common.cuh"
 #include "staged_upload.h"
 #include "layout.h"
+#include "prefix_sort.cuh"
 
 namespace sg {
 namespace gpub {
@@ -716,11 +716,15 @@ BuiltTree build_tree_gpu(const float* tri, int64_t ntri, const BuildParams& p, i
     check(cudaMemsetAsync(d_cnt_next.p, 0, size_t(cap) * sizeof(int), st), "clear counts");
     check(cudaMemsetAsync(d_cnt_shape.p, 0, size_t(cap) * sizeof(int), st), "clear counts");
 
-    size_t temp_bytes = 0, temp_nodes = 0;
-    check(cub::DeviceScan::ExclusiveSum(nullptr, temp_bytes, d_ml.p, d_sl.p, (int)n, st), "scan size");
-    check(cub::DeviceScan::ExclusiveSum(nullptr, temp_nodes, d_cnt_next.p, d_off_next.p, (int)cap, st), "scan size");
-    temp_bytes = std::max(temp_bytes, temp_nodes);
-    d_temp.alloc(temp_bytes);
+    // Scan scratch for the prefix sums over primitives and over nodes.
+    const size_t scan_words = std::max(psort::scan_scratch_words(size_t(n)), psort::scan_scratch_words(size_t(cap)));
+    d_temp.alloc(scan_words * sizeof(uint32_t));
+    uint32_t* scan_tmp = reinterpret_cast<uint32_t*>(d_temp.p);
+    auto scan = [&](const int* in, int* out, int64_t count) {
+        check(psort::scan_exclusive(reinterpret_cast<const uint32_t*>(in), reinterpret_cast<uint32_t*>(out),
+                                    size_t(count), scan_tmp, st),
+              "scan");
+    };
 
     // The root shape, and the root node unless splitNode returns at once.
     {
@@ -761,18 +765,16 @@ BuiltTree build_tree_gpu(const float* tri, int64_t ntri, const BuildParams& p, i
             k_count_left<<<grid(n), 256, 0, st>>>(n, d_rid.p, d_cx.p, d_cy.p, d_cz.p, d_pb.p, d_rt.p);
             k_misplaced<<<grid(n), 256, 0, st>>>(n, d_rid.p, d_cx.p, d_cy.p, d_cz.p, d_rt.p, d_ml.p, d_mr.p);
             check(cudaGetLastError(), "split kernels");
-            check(cub::DeviceScan::ExclusiveSum(d_temp.p, temp_bytes, d_ml.p, d_sl.p, (int)n, st), "scan");
-            check(cub::DeviceScan::ExclusiveSum(d_temp.p, temp_bytes, d_mr.p, d_sr.p, (int)n, st), "scan");
+            scan(d_ml.p, d_sl.p, n);
+            scan(d_mr.p, d_sr.p, n);
             k_pairs<<<grid(n), 256, 0, st>>>(n, d_rid.p, d_rt.p, d_ml.p, d_mr.p, d_sl.p, d_sr.p, d_pl.p, d_pr.p);
             k_swap<<<grid((n + 1) / 2), 256, 0, st>>>(n, d_sl.p, d_ml.p, d_pl.p, d_pr.p, d_cx.p, d_cy.p, d_cz.p,
                                                       d_pb.p, d_idx.p);
             k_node_apply<<<ng, 128, 0, st>>>(d_state.p, d_cur.p, d_rt.p, W, p.max_leaf, p.max_depth, d_cnt_next.p,
                                              d_cnt_shape.p);
             check(cudaGetLastError(), "partition kernels");
-            check(cub::DeviceScan::ExclusiveSum(d_temp.p, temp_bytes, d_cnt_next.p, d_off_next.p, (int)cap, st),
-                  "scan");
-            check(cub::DeviceScan::ExclusiveSum(d_temp.p, temp_bytes, d_cnt_shape.p, d_off_shape.p, (int)cap, st),
-                  "scan");
+            scan(d_cnt_next.p, d_off_next.p, cap);
+            scan(d_cnt_shape.p, d_off_shape.p, cap);
             k_summary<<<1, 1, 0, st>>>(d_state.p, d_cnt_next.p, d_off_next.p, d_cnt_shape.p, d_off_shape.p);
             k_node_commit<<<ng, 128, 0, st>>>(d_state.p, d_cur.p, d_off_next.p, d_off_shape.p, d_cnt_shape.p, W,
                                               p.max_leaf, p.max_depth, d_shapes.p, d_next.p);

@@ -30,7 +30,6 @@
 // to the host. max_depth does not apply (it is part of SORT's split rules).
 #include <cuda_runtime.h>
 
-#include <cub/device/device_radix_sort.cuh>
 
 #include <algorithm>
 #include <cfloat>
@@ -42,6 +41,7 @@
 #include "gpu_build_common.cuh"
 #include "staged_upload.h"
 #include "layout.h"
+#include "prefix_sort.cuh"
 
 namespace sg {
 namespace {
@@ -371,14 +371,22 @@ BuiltTree build_tree_lbvh(const float* tri, int64_t ntri, const BuildParams& p, 
     d_sorted.alloc(size_t(n));
     k_morton<<<grid(n), 256, 0, st>>>(n, d_cx.p, d_cy.p, d_cz.p, d_box.p + 6, d_keys.p, d_idx.p);
     check(cudaGetLastError(), "morton codes");
-    size_t temp_bytes = 0;
-    check(cub::DeviceRadixSort::SortPairs(nullptr, temp_bytes, d_keys.p, d_keys_sorted.p, d_idx.p, d_sorted.p, (int)n,
-                                          0, 3 * kMortonBits, st),
-          "sort size");
-    d_temp.alloc(temp_bytes);
-    check(cub::DeviceRadixSort::SortPairs(d_temp.p, temp_bytes, d_keys.p, d_keys_sorted.p, d_idx.p, d_sorted.p, (int)n,
-                                          0, 3 * kMortonBits, st),
-          "sort");
+    // Stable radix sort of (code, primitive) over the code's 63 bits
+    // (prefix_sort.cuh: seven passes of 10-bit digits).
+    const size_t count_words = psort::sort_count_words(n), scan_words = psort::sort_scan_words(n);
+    d_temp.alloc((count_words + scan_words) * sizeof(uint32_t));
+    {
+        uint64_t* keys[2] = {d_keys.p, d_keys_sorted.p};
+        int32_t* vals[2] = {d_idx.p, d_sorted.p};
+        uint32_t* cnt = reinterpret_cast<uint32_t*>(d_temp.p);
+        int in = 0;
+        check(psort::sort_pairs<uint64_t>(keys, vals, n, 0, 3 * kMortonBits, cnt, cnt + count_words, false, &in, st),
+              "sort");
+        if (in == 0) {  // an even pass count leaves the result where it started
+            check(cudaMemcpyAsync(d_keys_sorted.p, d_keys.p, size_t(n) * 8, cudaMemcpyDeviceToDevice, st), "sort");
+            check(cudaMemcpyAsync(d_sorted.p, d_idx.p, size_t(n) * 4, cudaMemcpyDeviceToDevice, st), "sort");
+        }
+    }
     int launches = 4;  // setup, scene box, centroid box, codes
 
     d_last.alloc(size_t(n));

@@ -32,6 +32,7 @@
 #include <mutex>
 #include <vector>
 
+#include "prefix_sort.cuh"
 #include "trace_kernels.h"
 #include "traversal.cuh"
 
@@ -345,15 +346,11 @@ static cudaMemPool_t trace_scratch_pool(int device) {
 // 902-954: the order inside a group matters.
 constexpr int kKeyBits = 30;
 constexpr int kSortBits = 30;  // top bits of the key that are sorted
-constexpr int kDigitBits = 10;
-constexpr int kDigits = 1 << kDigitBits;
-constexpr int kSortThreads = 256;
-constexpr int kSortWarps = kSortThreads / 32;
-constexpr int kSortItems = 16;                               // keys per thread
-constexpr int kSortTile = kSortThreads * kSortItems;        // 4,096 keys per block
-constexpr int kWarpChunk = kSortTile / kSortWarps;          // 512 keys per warp
-constexpr int kScanTile = 2048;
-static_assert(kSortBits % kDigitBits == 0 && kSortBits <= kKeyBits, "whole digits of the key");
+using psort::kDigits;
+using psort::kSortTile;
+using psort::kSortThreads;
+using psort::kSortItems;
+static_assert(kSortBits % psort::kDigitBits == 0 && kSortBits <= kKeyBits, "whole digits of the key");
 
 struct KeyGrid {
     float lo[3];
@@ -399,190 +396,6 @@ __global__ void __launch_bounds__(kSortThreads) k_sort_keys(DevRays rays, int64_
     for (int d = threadIdx.x; d < kDigits; d += kSortThreads) count[(size_t)d * tiles + blockIdx.x] = hist[d];
 }
 
-__global__ void __launch_bounds__(kSortThreads) k_digit_count(const uint32_t* __restrict__ keys, int64_t n, int shift,
-                                                              int tiles, uint32_t* __restrict__ count) {
-    __shared__ uint32_t hist[kDigits];
-    for (int d = threadIdx.x; d < kDigits; d += kSortThreads) hist[d] = 0;
-    __syncthreads();
-    const int64_t base = (int64_t)blockIdx.x * kSortTile;
-#pragma unroll 4
-    for (int j = 0; j < kSortItems; ++j) {
-        const int64_t p = base + j * kSortThreads + threadIdx.x;
-        if (p < n) atomicAdd(&hist[(__ldg(keys + p) >> shift) & (kDigits - 1)], 1u);
-    }
-    __syncthreads();
-    for (int d = threadIdx.x; d < kDigits; d += kSortThreads) count[(size_t)d * tiles + blockIdx.x] = hist[d];
-}
-
-__global__ void __launch_bounds__(kSortThreads) k_digit_scatter(const uint32_t* __restrict__ keys_in,
-                                                                const int32_t* __restrict__ idx_in, int64_t n,
-                                                                int shift, int tiles,
-                                                                const uint32_t* __restrict__ start,
-                                                                const uint32_t* __restrict__ start_tile,
-                                                                uint32_t* __restrict__ keys_out,
-                                                                int32_t* __restrict__ idx_out) {
-    __shared__ uint32_t wcount[kSortWarps][kDigits];  // per warp: keys of each digit, then its starting place
-    const unsigned lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
-    const unsigned lt = (1u << lane) - 1u;
-    for (int k = threadIdx.x; k < kSortWarps * kDigits; k += kSortThreads) (&wcount[0][0])[k] = 0;
-    __syncthreads();
-    const int64_t base = (int64_t)blockIdx.x * kSortTile + (int64_t)warp * kWarpChunk;
-    uint32_t key[kSortItems];
-    int32_t idx[kSortItems];
-#pragma unroll
-    for (int j = 0; j < kSortItems; ++j) {
-        const int64_t p = base + j * 32 + lane;
-        const bool ok = p < n;
-        key[j] = ok ? __ldg(keys_in + p) : 0xffffffffu;
-        idx[j] = ok ? __ldg(idx_in + p) : 0;
-        const uint32_t d = ok ? (key[j] >> shift) & (kDigits - 1) : 0xffffffffu;
-        const unsigned peers = __match_any_sync(0xffffffffu, d);
-        if (ok && (peers & lt) == 0) wcount[warp][d] += (uint32_t)__popc(peers);
-        __syncwarp();
-    }
-    __syncthreads();
-    // Starting place of each (warp, digit): the digit's run start for this tile
-    // plus the keys of that digit in the warps before.
-    for (int d = threadIdx.x; d < kDigits; d += kSortThreads) {
-        const size_t c = (size_t)d * tiles + blockIdx.x;
-        uint32_t run = __ldg(start + c) + (start_tile ? __ldg(start_tile + c / kScanTile) : 0u);
-#pragma unroll
-        for (int w = 0; w < kSortWarps; ++w) {
-            const uint32_t c = wcount[w][d];
-            wcount[w][d] = run;
-            run += c;
-        }
-    }
-    __syncthreads();
-#pragma unroll
-    for (int j = 0; j < kSortItems; ++j) {
-        const int64_t p = base + j * 32 + lane;
-        const bool ok = p < n;
-        const uint32_t d = ok ? (key[j] >> shift) & (kDigits - 1) : 0xffffffffu;
-        const unsigned peers = __match_any_sync(0xffffffffu, d);
-        uint32_t q = 0;
-        if (ok) q = wcount[warp][d] + (uint32_t)__popc(peers & lt);
-        __syncwarp();
-        if (ok && (peers & lt) == 0) wcount[warp][d] += (uint32_t)__popc(peers);
-        __syncwarp();
-        if (ok) {
-            keys_out[q] = key[j];
-            idx_out[q] = idx[j];
-        }
-    }
-}
-
-// Exclusive prefix sums inside each tile of kScanTile values (in place); the
-// tile's total goes to tile_sum[tile].
-__global__ void __launch_bounds__(1024) k_scan_tiles(uint32_t* __restrict__ v, uint32_t* __restrict__ tile_sum) {
-    __shared__ uint32_t warp_sum[32];
-    const size_t base = (size_t)blockIdx.x * kScanTile + 2 * threadIdx.x;
-    const uint32_t a = v[base], b = v[base + 1];
-    const uint32_t mine = a + b;
-    const unsigned lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
-    uint32_t x = mine;
-#pragma unroll
-    for (int o = 1; o < 32; o <<= 1) {
-        const uint32_t y = __shfl_up_sync(0xffffffffu, x, o);
-        if (lane >= (unsigned)o) x += y;
-    }
-    if (lane == 31) warp_sum[warp] = x;
-    __syncthreads();
-    if (warp == 0) {
-        uint32_t w = warp_sum[lane];
-#pragma unroll
-        for (int o = 1; o < 32; o <<= 1) {
-            const uint32_t y = __shfl_up_sync(0xffffffffu, w, o);
-            if (lane >= (unsigned)o) w += y;
-        }
-        warp_sum[lane] = w;  // inclusive over warps
-    }
-    __syncthreads();
-    const uint32_t before = (warp > 0 ? warp_sum[warp - 1] : 0u) + x - mine;
-    v[base] = before;
-    v[base + 1] = before + a;
-    if (threadIdx.x == 1023) tile_sum[blockIdx.x] = warp_sum[31];
-}
-
-// v[i] += tile_start[i / kScanTile].
-__global__ void __launch_bounds__(256) k_add_tile_start(uint32_t* __restrict__ v, size_t count,
-                                                        const uint32_t* __restrict__ tile_start) {
-    const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (i < count) v[i] += __ldg(tile_start + i / kScanTile);
-}
-
-// Exclusive prefix sums of the tile totals (one block; tiles <= 1024).
-__global__ void __launch_bounds__(1024) k_scan_tile_sums(uint32_t* __restrict__ tile_sum, int tiles) {
-    __shared__ uint32_t warp_sum[32];
-    const unsigned lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
-    const uint32_t mine = (int)threadIdx.x < tiles ? tile_sum[threadIdx.x] : 0u;
-    uint32_t x = mine;
-#pragma unroll
-    for (int o = 1; o < 32; o <<= 1) {
-        const uint32_t y = __shfl_up_sync(0xffffffffu, x, o);
-        if (lane >= (unsigned)o) x += y;
-    }
-    if (lane == 31) warp_sum[warp] = x;
-    __syncthreads();
-    if (warp == 0) {
-        uint32_t w = warp_sum[lane];
-#pragma unroll
-        for (int o = 1; o < 32; o <<= 1) {
-            const uint32_t y = __shfl_up_sync(0xffffffffu, w, o);
-            if (lane >= (unsigned)o) w += y;
-        }
-        warp_sum[lane] = w;
-    }
-    __syncthreads();
-    if ((int)threadIdx.x < tiles) tile_sum[threadIdx.x] = (warp > 0 ? warp_sum[warp - 1] : 0u) + x - mine;
-}
-
-// Words of scratch scan_exclusive needs for `count` values (which must be
-// padded with zeros to a multiple of kScanTile).
-static size_t scan_scratch_words(size_t count) {
-    size_t words = 0;
-    while (count > 1) {
-        const size_t tiles = (count + kScanTile - 1) / kScanTile;
-        const size_t padded = ((tiles + kScanTile - 1) / kScanTile) * kScanTile;
-        words += padded;
-        count = tiles;
-        if (tiles == 1) break;
-    }
-    return words;
-}
-
-// Exclusive prefix sums of v[0 .. count) in place (count a multiple of
-// kScanTile), level by level: tiles, then the tiles' totals, and so on.
-static cudaError_t scan_exclusive(uint32_t* v, size_t count, uint32_t* scratch, cudaStream_t s) {
-    const size_t tiles = count / kScanTile;
-    const size_t padded = ((tiles + kScanTile - 1) / kScanTile) * kScanTile;
-    cudaError_t e = cudaSuccess;
-    if (padded > tiles) e = cudaMemsetAsync(scratch + tiles, 0, (padded - tiles) * 4, s);
-    if (e != cudaSuccess) return e;
-    k_scan_tiles<<<(unsigned)tiles, 1024, 0, s>>>(v, scratch);
-    if (tiles == 1) return cudaGetLastError();
-    if ((e = scan_exclusive(scratch, padded, scratch + padded, s)) != cudaSuccess) return e;
-    k_add_tile_start<<<(unsigned)((count + 255) / 256), 256, 0, s>>>(v, count, scratch);
-    return cudaGetLastError();
-}
-
-// Prefix sums of the digit counts for k_digit_scatter. Up to 1,024 tiles of
-// kScanTile counts (2M counts: every batch up to 8M rays) the place of count
-// c is v[c] + tile_start[c / kScanTile], and *tile_start is set; beyond that
-// v is scanned in full and *tile_start is NULL.
-static cudaError_t scan_counts(uint32_t* v, size_t count, uint32_t* scratch, const uint32_t** tile_start,
-                               cudaStream_t s) {
-    const size_t tiles = count / kScanTile;
-    if (tiles <= 1024) {
-        k_scan_tiles<<<(unsigned)tiles, 1024, 0, s>>>(v, scratch);
-        k_scan_tile_sums<<<1, 1024, 0, s>>>(scratch, (int)tiles);
-        *tile_start = scratch;
-        return cudaGetLastError();
-    }
-    *tile_start = nullptr;
-    return scan_exclusive(v, count, scratch, s);
-}
-
 // The sorted schedule. Scratch (16 bytes per ray, 4 per (digit, tile) and the
 // scan's) comes from the library's stream-ordered pool and is freed in stream
 // order.
@@ -594,11 +407,11 @@ static cudaError_t launch_sorted(const TraceLaunch& L, const DevTree& tr, const 
     if (e != cudaSuccess) return e;
     cudaMemPool_t pool = trace_scratch_pool(dev);
     if (!pool) return cudaErrorMemoryAllocation;
-    const int tiles = (int)((n + kSortTile - 1) / kSortTile);
-    const size_t counts = ((size_t(kDigits) * tiles + kScanTile - 1) / kScanTile) * kScanTile;
+    const int tiles = psort::sort_tiles(n);
     const size_t al = 256;
     auto up = [al](size_t b) { return ((b + al - 1) / al) * al; };
-    const size_t b_ray = up(size_t(n) * 4), b_count = up(counts * 4), b_scan = up(scan_scratch_words(counts) * 4);
+    const size_t b_ray = up(size_t(n) * 4), b_count = up(psort::sort_count_words(n) * 4),
+                 b_scan = up(psort::sort_scan_words(n) * 4);
     char* base = nullptr;
     e = cudaMallocFromPoolAsync(reinterpret_cast<void**>(&base), 4 * b_ray + b_count + b_scan, pool, s);
     if (e != cudaSuccess) return e;
@@ -612,22 +425,11 @@ static cudaError_t launch_sorted(const TraceLaunch& L, const DevTree& tr, const 
         g.lo[a] = tr.box_lo[a];
         g.scale[a] = ext > 0.0f ? 128.0f / ext : 0.0f;
     }
+    const int first = kKeyBits - kSortBits;
+    k_sort_keys<<<tiles, kSortThreads, 0, s>>>(rays, n, g, first, tiles, keys[0], idx[0], count);
     int cur = 0;
-    if (counts > size_t(kDigits) * tiles)
-        e = cudaMemsetAsync(count + size_t(kDigits) * tiles, 0, (counts - size_t(kDigits) * tiles) * 4, s);
-    for (int shift = kKeyBits - kSortBits; shift < kKeyBits && e == cudaSuccess; shift += kDigitBits) {
-        if (shift == kKeyBits - kSortBits)
-            k_sort_keys<<<tiles, kSortThreads, 0, s>>>(rays, n, g, shift, tiles, keys[0], idx[0], count);
-        else
-            k_digit_count<<<tiles, kSortThreads, 0, s>>>(keys[cur], n, shift, tiles, count);
-        if ((e = cudaGetLastError()) != cudaSuccess) break;
-        const uint32_t* tile_start = nullptr;
-        if ((e = scan_counts(count, counts, scan, &tile_start, s)) != cudaSuccess) break;
-        k_digit_scatter<<<tiles, kSortThreads, 0, s>>>(keys[cur], idx[cur], n, shift, tiles, count, tile_start,
-                                                       keys[cur ^ 1], idx[cur ^ 1]);
-        e = cudaGetLastError();
-        cur ^= 1;
-    }
+    if ((e = cudaGetLastError()) == cudaSuccess)
+        e = psort::sort_pairs<uint32_t>(keys, idx, n, first, kKeyBits, count, scan, true, &cur, s);
     if (e == cudaSuccess) {
         k_trace_walk<W, ANY, STACK, Q8><<<(unsigned)((n + 127) / 128), 128, 0, s>>>(
             tr, rays, n, L.prim, L.t, L.u, L.v, L.occ, L.err, nullptr, idx[cur]);
