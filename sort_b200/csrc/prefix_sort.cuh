@@ -83,8 +83,116 @@ __global__ void __launch_bounds__(256) k_add_tile_start(uint32_t* __restrict__ v
     if (i < count) v[i] += __ldg(tile_start + i / kScanTile);
 }
 
+// Large arrays: reduce, then scan, over tiles of kBigTile values (8 per thread
+// of a 1,024-thread block, staged through shared memory so the global loads
+// and stores stay coalesced): the tiles' totals, their prefix sums, then each
+// tile scanned from its start. 1.5 passes of traffic and three launches.
+constexpr int kBigItems = 8;
+constexpr int kBigTile = 1024 * kBigItems;
+
+__device__ __forceinline__ uint32_t block_exclusive_1024(uint32_t mine, uint32_t* warp_sum, uint32_t* total) {
+    const unsigned lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
+    uint32_t x = mine;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const uint32_t y = __shfl_up_sync(0xffffffffu, x, o);
+        if (lane >= (unsigned)o) x += y;
+    }
+    if (lane == 31) warp_sum[warp] = x;
+    __syncthreads();
+    if (warp == 0) {
+        uint32_t w = warp_sum[lane];
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const uint32_t y = __shfl_up_sync(0xffffffffu, w, o);
+            if (lane >= (unsigned)o) w += y;
+        }
+        warp_sum[lane] = w;
+    }
+    __syncthreads();
+    *total = warp_sum[31];
+    return (warp > 0 ? warp_sum[warp - 1] : 0u) + x - mine;
+}
+
+// tile_sum[b] = sum of in[b * kBigTile ..) (values past count read as 0).
+__global__ void __launch_bounds__(1024) k_big_tile_sums(const uint32_t* __restrict__ in, size_t count,
+                                                        uint32_t* __restrict__ tile_sum) {
+    __shared__ uint32_t warp_sum[32];
+    const size_t base = (size_t)blockIdx.x * kBigTile;
+    uint32_t mine = 0;
+#pragma unroll
+    for (int j = 0; j < kBigItems; ++j) {
+        const size_t i = base + (size_t)j * 1024 + threadIdx.x;
+        if (i < count) mine += in[i];
+    }
+    uint32_t total;
+    block_exclusive_1024(mine, warp_sum, &total);
+    if (threadIdx.x == 0) tile_sum[blockIdx.x] = total;
+}
+
+// Exclusive prefix sums of up to kBigTile values in place, one block.
+__global__ void __launch_bounds__(1024) k_scan_one_block(uint32_t* __restrict__ v, int count) {
+    __shared__ uint32_t stage[kBigTile];
+    __shared__ uint32_t warp_sum[32];
+#pragma unroll
+    for (int j = 0; j < kBigItems; ++j) {
+        const int i = j * 1024 + threadIdx.x;
+        stage[i] = i < count ? v[i] : 0u;
+    }
+    __syncthreads();
+    uint32_t run = 0, own[kBigItems];
+#pragma unroll
+    for (int j = 0; j < kBigItems; ++j) {
+        own[j] = run;
+        run += stage[threadIdx.x * kBigItems + j];
+    }
+    uint32_t total;
+    const uint32_t before = block_exclusive_1024(run, warp_sum, &total);
+#pragma unroll
+    for (int j = 0; j < kBigItems; ++j) stage[threadIdx.x * kBigItems + j] = before + own[j];
+    __syncthreads();
+#pragma unroll
+    for (int j = 0; j < kBigItems; ++j) {
+        const int i = j * 1024 + threadIdx.x;
+        if (i < count) v[i] = stage[i];
+    }
+}
+
+// out = exclusive prefix sums inside each kBigTile tile of in, plus the
+// tile's start tile_start[b] (in may equal out).
+__global__ void __launch_bounds__(1024) k_big_scan(const uint32_t* in, uint32_t* out, size_t count,
+                                                   const uint32_t* __restrict__ tile_start) {
+    __shared__ uint32_t stage[kBigTile];
+    __shared__ uint32_t warp_sum[32];
+    const size_t base = (size_t)blockIdx.x * kBigTile;
+#pragma unroll
+    for (int j = 0; j < kBigItems; ++j) {
+        const size_t i = base + (size_t)j * 1024 + threadIdx.x;
+        stage[j * 1024 + threadIdx.x] = i < count ? in[i] : 0u;
+    }
+    __syncthreads();
+    uint32_t run = 0, own[kBigItems];
+#pragma unroll
+    for (int j = 0; j < kBigItems; ++j) {
+        own[j] = run;
+        run += stage[threadIdx.x * kBigItems + j];
+    }
+    uint32_t total;
+    const uint32_t before = block_exclusive_1024(run, warp_sum, &total) + __ldg(tile_start + blockIdx.x);
+#pragma unroll
+    for (int j = 0; j < kBigItems; ++j) stage[threadIdx.x * kBigItems + j] = before + own[j];
+    __syncthreads();
+#pragma unroll
+    for (int j = 0; j < kBigItems; ++j) {
+        const size_t i = base + (size_t)j * 1024 + threadIdx.x;
+        if (i < count) out[i] = stage[j * 1024 + threadIdx.x];
+    }
+}
+
 // Words of scratch scan_exclusive needs for `count` values.
 inline size_t scan_scratch_words(size_t count) {
+    const size_t big = (count + kBigTile - 1) / kBigTile;
+    if (big > 1 && big <= (size_t)kBigTile) return big;
     const size_t tiles = (count + kScanTile - 1) / kScanTile;
     return tiles <= 1 ? 1 : tiles + scan_scratch_words(tiles);
 }
@@ -93,6 +201,13 @@ inline size_t scan_scratch_words(size_t count) {
 inline cudaError_t scan_exclusive(const uint32_t* in, uint32_t* out, size_t count, uint32_t* scratch,
                                   cudaStream_t s) {
     if (count == 0) return cudaSuccess;
+    const size_t big = (count + kBigTile - 1) / kBigTile;
+    if (big > 1 && big <= (size_t)kBigTile) {  // up to 67M values: reduce, scan the totals, scan
+        k_big_tile_sums<<<(unsigned)big, 1024, 0, s>>>(in, count, scratch);
+        k_scan_one_block<<<1, 1024, 0, s>>>(scratch, (int)big);
+        k_big_scan<<<(unsigned)big, 1024, 0, s>>>(in, out, count, scratch);
+        return cudaGetLastError();
+    }
     const size_t tiles = (count + kScanTile - 1) / kScanTile;
     k_scan_tiles<<<(unsigned)tiles, 1024, 0, s>>>(in, out, count, scratch);
     cudaError_t e = cudaGetLastError();
