@@ -364,10 +364,11 @@ def run_ours(args):
     achieved = bytes_closest * n / (launch_ms / 1e3) / 1e9
     traffic = None
     tpath = os.path.join(ROOT, "profiles", "traffic.json")
-    if os.path.exists(tpath):
-        tj = json.load(open(tpath))
-        if tj.get("workload") == ("raycast_82k" if width == 4 else "incoherent_21m") and tj.get("nodes") == "fp32":
-            traffic = tj.get("dram_bytes_per_launch")
+    if os.path.exists(tpath):  # ncu DRAM bytes of this kernel, one launch of this workload
+        for tj in json.load(open(tpath)):
+            if (tj.get("workload") == ("raycast_82k" if width == 4 else "incoherent_21m")
+                    and tj.get("nodes") == args.nodes and args.builder != "lbvh"):
+                traffic = tj.get("dram_bytes_per_launch")
 
     if rank == 0:
         sorted_schedule = n >= (1 << 21)
