@@ -52,7 +52,9 @@ TRI_BYTES = 36                  # 9 floats per triangle test
 RAY_IN, HIT_OUT = 32, 16
 CPU_SAMPLE = 262_144            # rays per CPU-baseline step
 NODE_FORMATS = {"fp32": 0, "q8": 1}
-BUILDERS = {"host": 0, "gpu": 1, "lbvh": 2}  # host / gpu: SORT's tree; lbvh: Morton-order tree
+BUILDERS = {"host": 0, "gpu": 1, "lbvh": 2, "ploc": 3}  # host / gpu: SORT's tree; lbvh / ploc: built from Morton order
+MORTON_TREES = {"lbvh": "LBVH (radix tree over the Morton order, built on the GPU)",
+                "ploc": "PLOC (parallel locally-ordered clustering over the Morton order, built on the GPU)"}
 
 
 def workload_config(extra=None):
@@ -277,7 +279,7 @@ def run_ours(args):
     # SORT's traversal counters on these rays -> algorithmic bytes per ray. The
     # counts are SORT's (FP32 boxes), whatever node format is timed.
     parity = None
-    if args.nodes == "fp32" and args.builder != "lbvh":
+    if args.nodes == "fp32" and args.builder not in MORTON_TREES:
         node_tests, prim_tests = acc.TraceStats(d_diff, False)
         a_nodes, a_prims = acc.TraceStats(d_shad, True)
     else:
@@ -367,7 +369,7 @@ def run_ours(args):
     if os.path.exists(tpath):  # ncu DRAM bytes of this kernel, one launch of this workload
         for tj in json.load(open(tpath)):
             if (tj.get("workload") == ("raycast_82k" if width == 4 else "incoherent_21m")
-                    and tj.get("nodes") == args.nodes and args.builder != "lbvh"):
+                    and tj.get("nodes") == args.nodes and args.builder not in MORTON_TREES):
                 traffic = tj.get("dram_bytes_per_launch")
 
     if rank == 0:
@@ -379,8 +381,8 @@ def run_ours(args):
             "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded procedural scene)",
             "config": (raycast_config if width == 4 else workload_config)(
                 ({"nodes": args.nodes} if args.nodes != "fp32" else {}) |
-                ({"tree": "LBVH (Morton-order wide BVH built on the GPU; algorithmic bytes counted on SORT's tree)"}
-                 if args.builder == "lbvh" else {})) | (
+                ({"tree": MORTON_TREES[args.builder] + "; algorithmic bytes counted on SORT's tree"}
+                 if args.builder in MORTON_TREES else {})) | (
                 {"parallelism": f"replicas x{world}", "build_seconds": round(info["build_seconds"], 2),
                  "tree_device_bytes": info["device_bytes"],
                  "schedule": "rays in the order of a 30-bit coherence key (hand-written stable radix sort, "
@@ -413,7 +415,7 @@ def run_ours(args):
                                                                sample=args.sample, width=width)
             out["cpu_baseline"] = {"value": round(rate, 3), "unit": UNIT, "cores": threads, "kind": kind,
                                    "sample": desc}
-            if args.nodes == "fp32" and args.builder != "lbvh":
+            if args.nodes == "fp32" and args.builder not in MORTON_TREES:
                 out["parity"] = parity_on_sample(tri, diffuse, first, sort_hits, gpu_prim, gpu_t)
         print(json.dumps(out))
     acc.Release()
@@ -854,7 +856,8 @@ BUILD_SAMPLE = (64, LEVEL)  # SORT's single-threaded build, timed on 64 of the 1
 def build_config(extra=None, builder="gpu"):
     tree = {"gpu": "GPU builder (SG_BUILDER_GPU), the same tree as SORT's Fbvh::Build",
             "host": "this library's host builder, the same tree as SORT's Fbvh::Build",
-            "lbvh": "Morton-order wide BVH built on the GPU (SG_BUILDER_LBVH), not SORT's tree"}[builder]
+            "lbvh": "Morton-order wide BVH built on the GPU (SG_BUILDER_LBVH), not SORT's tree",
+            "ploc": "clustered wide BVH built on the GPU (SG_BUILDER_PLOC), not SORT's tree"}[builder]
     cfg = {
         "workload": "build_21m: BVH build of 1,024 level-5 icospheres + ground quad = 20,971,522 triangles, "
                     f"width 8, leaf 8, from host triangles; {tree}",
@@ -945,7 +948,7 @@ def run_build(args):
         return
     tris_bytes = (n + 8) * 48
     node_bytes = info["device_bytes"] - tris_bytes
-    lbvh = args.builder == "lbvh"
+    lbvh = args.builder in MORTON_TREES
     shapes = info["interior_nodes"] + info["leaves"]
     out = {
         "metric": "Mtriangles/s BVH build", "value": round(world * n / mean_build / 1e6, 3), "unit": "Mtriangles/s",
@@ -958,7 +961,7 @@ def run_build(args):
                 "d2h_bytes_per_step": int(16 * info["build_rounds"] if lbvh else n * 4 + shapes * 40)},
         "gpu_launches": info["build_launches"] * args.steps,
         "roofline": None,
-        **({"tree": "LBVH: Morton-order wide BVH built on the GPU, not SORT's tree (same hits except near-ties "
+        **({"tree": MORTON_TREES[args.builder] + ", not SORT's tree (same hits except near-ties "
                     "and box-grazing rays)"} if lbvh else {}),
         "clocks": clocks.summary(),
     }
@@ -993,8 +996,8 @@ def main():
     p.add_argument("--sample", type=int, default=CPU_SAMPLE)
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--builder", choices=sorted(BUILDERS), default=None,
-                   help="tree builder: host/gpu build SORT's tree (closest default host), lbvh the Morton-order "
-                        "tree (build workload default gpu)")
+                   help="tree builder: host/gpu build SORT's tree (closest default host), lbvh / ploc the trees built "
+                        "from the Morton order (build workload default gpu)")
     p.add_argument("--nodes", choices=sorted(NODE_FORMATS), default="fp32",
                    help="child-box format of the timed tree (q8: 8-bit, outward-rounded)")
     args = p.parse_args()

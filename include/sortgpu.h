@@ -108,11 +108,15 @@ typedef struct {
  * 1e-6 of each other and a rounded box entry distance decides which one is
  * kept, and rays whose slab test misses the hit triangle's own box by
  * rounding, so that finding it depends on the leaf boxes), FP32 nodes only,
- * max_depth ignored, no topology export. */
+ * max_depth ignored, no topology export. SG_BUILDER_PLOC builds a wide BVH
+ * by parallel locally-ordered clustering over the Morton order (Meister and
+ * Bittner 2018) on the device: tighter boxes than the LBVH, a few more passes,
+ * the same promises and limits. */
 typedef enum {
     SG_BUILDER_HOST = 0, /* host threads, one subtree per thread below the top */
     SG_BUILDER_GPU = 1,  /* data-parallel passes on the scene's device */
-    SG_BUILDER_LBVH = 2  /* Morton-order wide BVH on the scene's device */
+    SG_BUILDER_LBVH = 2, /* Morton-order wide BVH on the scene's device */
+    SG_BUILDER_PLOC = 3  /* clustered (PLOC) wide BVH on the scene's device */
 } sg_builder;
 
 /* Structure-of-arrays ray batch: n entries in each array. */
@@ -483,6 +487,15 @@ sg_status sg_pt_create(const sg_scene* scene, const float* triangles, int64_t nt
                        const float* materials, int32_t nmat, const float* light, sg_pt_scene** out);
 sg_status sg_pt_render(sg_pt_scene* pt, const float* camera, int32_t width, int32_t height, int32_t spp,
                        int32_t max_depth, uint64_t seed, float* image, void* stream);
+/* sg_pt_render_rows: rows [row_begin, row_end) of the same width x height
+ * frame into `image` (width*(row_end-row_begin)*3 floats): every pixel gets
+ * the random numbers of its place in the whole frame, so bands rendered
+ * separately (on one GPU or on several) put together are bit-identical to
+ * sg_pt_render of the frame. No SORT counterpart: SORT's render threads split
+ * a frame into tiles (work/image_evaluation/image_evaluation.cpp:153-279). */
+sg_status sg_pt_render_rows(sg_pt_scene* pt, const float* camera, int32_t width, int32_t height, int32_t row_begin,
+                            int32_t row_end, int32_t spp, int32_t max_depth, uint64_t seed, float* image,
+                            void* stream);
 sg_status sg_pt_destroy(sg_pt_scene* pt);
 /* Rays the last sg_pt_render traced: extension (closest-hit) and shadow
  * (any-hit) rays; synchronises `stream`. The counterpart of SORT's sRayCount /

@@ -38,6 +38,7 @@ class BuildOpts(ctypes.Structure):
 SG_BUILDER_HOST = 0
 SG_BUILDER_GPU = 1
 SG_BUILDER_LBVH = 2
+SG_BUILDER_PLOC = 3
 
 
 class Rays(ctypes.Structure):
@@ -197,6 +198,8 @@ _SIGNATURES = {
     "sg_pt_create": (ctypes.c_int, [_vp, _vp, _i64, _vp, _vp, ctypes.c_int32, _vp, ctypes.POINTER(_vp)]),
     "sg_pt_render": (ctypes.c_int, [_vp, _vp, ctypes.c_int32, ctypes.c_int32, ctypes.c_int32, ctypes.c_int32,
                                     ctypes.c_uint64, _vp, _vp]),
+    "sg_pt_render_rows": (ctypes.c_int, [_vp, _vp, ctypes.c_int32, ctypes.c_int32, ctypes.c_int32, ctypes.c_int32,
+                                         ctypes.c_int32, ctypes.c_int32, ctypes.c_uint64, _vp, _vp]),
     "sg_pt_destroy": (ctypes.c_int, [_vp]),
     "sg_pt_ray_counts": (ctypes.c_int, [_vp, ctypes.POINTER(_i64), ctypes.POINTER(_i64), _vp]),
     "sg_trace_multi": (ctypes.c_int, [_vp, ctypes.POINTER(Rays), _i64, _vp, _vp, ctypes.POINTER(MultiHits), _vp]),

@@ -102,7 +102,7 @@ sg_status upload(sg_scene* s, const float* tri, int64_t ntri, const std::vector<
     const int f4 = W == 8 ? sg::NodeShape<8>::kF4 : sg::NodeShape<4>::kF4;
     const int64_t nn = t.interior();
     std::vector<float4> nodes;
-    const bool adopt = t.d_nodes != nullptr;  // the LBVH builder wrote the nodes on the device
+    const bool adopt = t.d_nodes != nullptr;  // a Morton-order builder wrote the nodes on the device
     if (adopt) {
     } else if (s->node_format == SG_NODES_QUANT8) {
         sg::quantize_nodes(t, nodes);
@@ -322,6 +322,7 @@ BuiltTree build_mixed(const MixedInput& in, BuildParams bp, int builder, int dev
     auto run = [&](const float* tri, int64_t ntri) {
         if (builder == SG_BUILDER_GPU) return build_tree_gpu(tri, ntri, bp, device);
         if (builder == SG_BUILDER_LBVH) return build_tree_lbvh(tri, ntri, bp, device);
+        if (builder == SG_BUILDER_PLOC) return build_tree_ploc(tri, ntri, bp, device);
         return build_tree(tri, ntri, bp);
     };
     BuiltTree t;
@@ -375,17 +376,18 @@ sg_status scene_create_mixed(const MixedInput& in, const sg_build_opts* opts, sg
     for (int64_t k = 0; k < nshapes; ++k)
         if (in.shapes[k].kind != SG_SHAPE_QUAD && in.shapes[k].kind != SG_SHAPE_DISK)
             return fail(SG_ERR_INVALID_ARGUMENT, "unknown area shape kind");
-    if ((nlines > 0 || nshapes > 0 || in.order) && opts->builder == SG_BUILDER_LBVH)
-        return fail(SG_ERR_UNSUPPORTED, "SG_BUILDER_LBVH builds triangle scenes only");
+    const bool morton = opts->builder == SG_BUILDER_LBVH || opts->builder == SG_BUILDER_PLOC;
+    if ((nlines > 0 || nshapes > 0 || in.order) && morton)
+        return fail(SG_ERR_UNSUPPORTED, "SG_BUILDER_LBVH / SG_BUILDER_PLOC build triangle scenes only");
     if (ntri + nlines + nshapes >= int64_t(0x7fffffff)) return fail(SG_ERR_LIMIT, "more than 2^31-2 primitives");
     if (opts->width != 4 && opts->width != 8) return fail(SG_ERR_INVALID_ARGUMENT, "width must be 4 or 8");
     if (opts->max_leaf < 1 || opts->max_depth < 1) return fail(SG_ERR_INVALID_ARGUMENT, "max_leaf/max_depth < 1");
     if (opts->node_format != SG_NODES_FP32 && opts->node_format != SG_NODES_QUANT8)
         return fail(SG_ERR_UNSUPPORTED, "unknown node format");
-    if (opts->builder != SG_BUILDER_HOST && opts->builder != SG_BUILDER_GPU && opts->builder != SG_BUILDER_LBVH)
+    if (opts->builder != SG_BUILDER_HOST && opts->builder != SG_BUILDER_GPU && !morton)
         return fail(SG_ERR_INVALID_ARGUMENT, "unknown builder");
-    if (opts->builder == SG_BUILDER_LBVH && opts->node_format != SG_NODES_FP32)
-        return fail(SG_ERR_UNSUPPORTED, "SG_BUILDER_LBVH writes FP32 nodes only");
+    if (morton && opts->node_format != SG_NODES_FP32)
+        return fail(SG_ERR_UNSUPPORTED, "SG_BUILDER_LBVH / SG_BUILDER_PLOC write FP32 nodes only");
     int ndev = 0;
     cudaError_t e = cudaGetDeviceCount(&ndev);
     if (e != cudaSuccess) return cuda_fail(e, "cudaGetDeviceCount");
@@ -504,7 +506,7 @@ sg_status sg_scene_info_get(const sg_scene* s, sg_scene_info* info) {
 
 sg_status sg_scene_topology(const sg_scene* s, int32_t* out, int64_t cap, int64_t* written) {
     if (!s || !written) return fail(SG_ERR_INVALID_ARGUMENT, "NULL argument");
-    if (!s->tree.host_arrays()) return fail(SG_ERR_UNSUPPORTED, "an SG_BUILDER_LBVH tree has no topology export");
+    if (!s->tree.host_arrays()) return fail(SG_ERR_UNSUPPORTED, "an SG_BUILDER_LBVH / SG_BUILDER_PLOC tree has no topology export");
     std::vector<int32_t> v;
     sg::tree_topology(s->tree, v);
     *written = int64_t(v.size());

@@ -62,7 +62,7 @@ struct BuiltTree {
     // (layout.h), leaf order plus the zero pad slots, already on the build's
     // device. The receiver owns it (cudaFree).
     float4* d_tris = nullptr;
-    // Set by build_tree_lbvh only: the interior nodes already in the device
+    // Set by build_tree_lbvh and build_tree_ploc only: the interior nodes already in the device
     // layout (layout.h, FP32 boxes), n_interior of them, owned like d_tris. Its
     // host arrays (child, lo, hi, first_interior, order, leaf_last) stay empty;
     // n_tri and n_interior give the sizes.
@@ -95,6 +95,11 @@ BuiltTree build_tree_gpu(const float* tri, int64_t ntri, const BuildParams& p, i
 // triangle's own box by rounding), for fast scene admission.
 // max_depth does not apply. The result has no host arrays (host_arrays()).
 BuiltTree build_tree_lbvh(const float* tri, int64_t ntri, const BuildParams& p, int device);
+
+// A wide BVH by parallel locally-ordered clustering (PLOC) over the Morton
+// order, built entirely on the GPU (builder_ploc.cu): tighter boxes than the
+// LBVH, the same promises and limits.
+BuiltTree build_tree_ploc(const float* tri, int64_t ntri, const BuildParams& p, int device);
 
 // 8-bit node format (quantize.cpp): one record per interior node in the layout
 // layout.h describes; every decoded child box contains the FP32 box.

@@ -38,18 +38,19 @@
 namespace sg {
 namespace {
 
-__global__ void k_generate(Cam cam, int width, int height, uint2 key, uint32_t sample, Queue q, int cap,
-                           float* __restrict__ thr, int* __restrict__ count) {
+// Path p renders frame pixel p0 + p (a band of whole rows starts at p0).
+__global__ void k_generate(Cam cam, int width, int height, int p0, int n, uint2 key, uint32_t sample, Queue q,
+                           int cap, float* __restrict__ thr, int* __restrict__ count) {
     const int p = blockIdx.x * blockDim.x + threadIdx.x;
-    if (p >= width * height) return;
-    put_ray(q.ray, cap, p, cam.eye, camera_dir(cam, width, height, p, key, sample), 0.0f, FLT_MAX);
+    if (p >= n) return;
+    put_ray(q.ray, cap, p, cam.eye, camera_dir(cam, width, height, p0 + p, key, sample), 0.0f, FLT_MAX);
     q.slot[p] = p;
     thr[p] = thr[cap + p] = thr[2 * cap + p] = 1.0f;          // throughput
     thr[3 * cap + p] = thr[4 * cap + p] = thr[5 * cap + p] = 0.0f;  // radiance of this sample
-    if (p == 0) *count = width * height;
+    if (p == 0) *count = n;
 }
 
-__global__ void k_shade(PtDev sc, uint2 key, uint32_t sample, int bounce, int max_depth, Queue in, int cap,
+__global__ void k_shade(PtDev sc, uint2 key, int p0, uint32_t sample, int bounce, int max_depth, Queue in, int cap,
                         const int* __restrict__ in_count, const int32_t* __restrict__ hit_prim,
                         const float* __restrict__ hit_t, Queue next, int* __restrict__ next_count, Queue shadow,
                         int shadow_cap, int* __restrict__ shadow_count, float* __restrict__ thr,
@@ -64,7 +65,7 @@ __global__ void k_shade(PtDev sc, uint2 key, uint32_t sample, int bounce, int ma
     if (prim >= 0) {
         const float3 o = f3(in.ray[q], in.ray[cap + q], in.ray[2 * cap + q]);
         const float3 d = f3(in.ray[3 * cap + q], in.ray[4 * cap + q], in.ray[5 * cap + q]);
-        v = shade_vertex(sc, key, (uint32_t)p, sample, bounce, max_depth, o, d, prim, hit_t[q],
+        v = shade_vertex(sc, key, (uint32_t)(p0 + p), sample, bounce, max_depth, o, d, prim, hit_t[q],
                          f3(thr[p], thr[cap + p], thr[2 * cap + p]));
         if (v.emit) {
             thr[3 * cap + p] += v.Le.x;
@@ -309,10 +310,19 @@ extern "C" sg_status sg_pt_destroy(sg_pt_scene* ps) {
 
 extern "C" sg_status sg_pt_render(sg_pt_scene* ps, const float* camera, int32_t width, int32_t height, int32_t spp,
                                   int32_t max_depth, uint64_t seed, float* image, void* stream) {
+    return sg_pt_render_rows(ps, camera, width, height, 0, height, spp, max_depth, seed, image, stream);
+}
+
+extern "C" sg_status sg_pt_render_rows(sg_pt_scene* ps, const float* camera, int32_t width, int32_t height,
+                                       int32_t row_begin, int32_t row_end, int32_t spp, int32_t max_depth,
+                                       uint64_t seed, float* image, void* stream) {
     if (!ps || !camera || !image || width <= 0 || height <= 0 || spp <= 0 || max_depth <= 0)
         return sg::set_error(SG_ERR_INVALID_ARGUMENT, "bad render arguments");
     if ((int64_t)width * height > (int64_t)1 << 28) return sg::set_error(SG_ERR_LIMIT, "image too large");
-    const int P = width * height;
+    if (row_begin < 0 || row_end > height || row_begin >= row_end)
+        return sg::set_error(SG_ERR_INVALID_ARGUMENT, "bad row range");
+    const int P = width * (row_end - row_begin);  // pixels of the band
+    const int p0 = width * row_begin;
     sg::TraceLaunch base;
     sg::DevTree tree;
     int device = 0;
@@ -376,8 +386,8 @@ extern "C" sg_status sg_pt_render(sg_pt_scene* ps, const float* camera, int32_t 
     for (int sample = 0; sample < spp; ++sample) {
         sg::Queue* cur = &qa;
         sg::Queue* nxt = &qb;
-        sg::k_generate<<<blocks, threads, 0, s>>>(cam, width, height, key, (uint32_t)sample, *cur, (int)cap, thr,
-                                                  &counters[0]);
+        sg::k_generate<<<blocks, threads, 0, s>>>(cam, width, height, p0, P, key, (uint32_t)sample, *cur, (int)cap,
+                                                  thr, &counters[0]);
         for (int bounce = 0; bounce < max_depth; ++bounce) {
             sg::DevRays r{cur->ray,           cur->ray + cap,     cur->ray + 2 * cap, cur->ray + 3 * cap,
                           cur->ray + 4 * cap, cur->ray + 5 * cap, cur->ray + 6 * cap, cur->ray + 7 * cap};
@@ -388,7 +398,7 @@ extern "C" sg_status sg_pt_render(sg_pt_scene* ps, const float* camera, int32_t 
             Lc.n_dev = &counters[0];
             if ((e = sg::launch_trace_fp32(Lc, tree, r, (int64_t)cap, s)) != cudaSuccess) return pt_fail(e);
             if ((e = cudaMemsetAsync(&counters[1], 0, 2 * sizeof(int), s)) != cudaSuccess) return pt_fail(e);
-            sg::k_shade<<<blocks, threads, 0, s>>>(dev, key, (uint32_t)sample, bounce, max_depth, *cur, (int)cap,
+            sg::k_shade<<<blocks, threads, 0, s>>>(dev, key, p0, (uint32_t)sample, bounce, max_depth, *cur, (int)cap,
                                                    &counters[0], hit_prim, hit_t, *nxt, &counters[1], sq, (int)scap,
                                                    &counters[2], thr, vis);
             sg::DevRays sr{sq.ray,            sq.ray + scap,     sq.ray + 2 * scap, sq.ray + 3 * scap,

@@ -35,15 +35,23 @@ class PathTracer:
         self.device = device
 
     def Render(self, camera, width: int, height: int, spp: int, max_recursive_depth: int = 5, seed: int = 1,
-               out=None, stream=None):
-        """Mean radiance per pixel, a float32 CUDA tensor (height, width, 3)."""
+               out=None, stream=None, rows=None):
+        """Mean radiance per pixel, a float32 CUDA tensor (height, width, 3).
+        rows=(begin, end): only those rows of the frame, (end - begin, width, 3),
+        each pixel with its random numbers in the whole frame (sg_pt_render_rows)."""
         import torch
         cam = np.ascontiguousarray(np.asarray(camera, np.float32))
         dev = torch.device("cuda", self.device)
-        img = out if out is not None else torch.empty((height, width, 3), dtype=torch.float32, device=dev)
+        r0, r1 = (0, height) if rows is None else (int(rows[0]), int(rows[1]))
+        img = out if out is not None else torch.empty((r1 - r0, width, 3), dtype=torch.float32, device=dev)
         s = stream if stream is not None else torch.cuda.current_stream(dev).cuda_stream
-        _lib.check(_lib.load().sg_pt_render(self._h, cam.ctypes.data, width, height, spp, max_recursive_depth,
-                                            seed, img.data_ptr(), s))
+        lib = _lib.load()
+        if rows is None:
+            _lib.check(lib.sg_pt_render(self._h, cam.ctypes.data, width, height, spp, max_recursive_depth, seed,
+                                        img.data_ptr(), s))
+        else:
+            _lib.check(lib.sg_pt_render_rows(self._h, cam.ctypes.data, width, height, r0, r1, spp,
+                                             max_recursive_depth, seed, img.data_ptr(), s))
         return img
 
     def RayCounts(self, stream=None):

@@ -4,9 +4,11 @@ Rays, paths and render requests are independent, so every GPU holds a full
 replica of each scene's tree and takes a share of the work; no kernel reads
 another GPU's memory and nothing on the data path needs a collective. This
 module holds the host-side pieces: contiguous shares of a ray batch, tiles of
-an image dealt round-robin, a router that sends each render request to the
-replica with the least outstanding work, and the max-over-ranks reduction the
-timings use (torch.distributed, NCCL on GPUs, gloo on CPU).
+an image dealt round-robin, one frame rendered in bands of rows across the
+ranks and gathered (bit-identical to a one-GPU render), a router that sends
+each render request to the replica with the least outstanding work, and the
+max-over-ranks reduction the timings use (torch.distributed, NCCL on GPUs,
+gloo on CPU).
 
 SORT's counterpart is its thread pool splitting one image into 64x64 tiles
 (work/image_evaluation/image_evaluation.cpp:153-279); here the split is across
@@ -57,6 +59,50 @@ class ReplicaRouter:
         r, samples = self.where.pop(request_id)
         self.load[r] -= samples
         return r
+
+
+def _rank_world():
+    import torch.distributed as dist
+    if dist.is_available() and dist.is_initialized():
+        return dist.get_rank(), dist.get_world_size()
+    return 0, 1
+
+
+def gather_rows(band, height: int):
+    """The whole image, on every rank, from each rank's band of rows: rank r
+    holds rows shard_range(height, r, world) (possibly none). Bands are padded
+    to the largest band for one all_gather (NCCL on GPU tensors, gloo on CPU)."""
+    import torch
+    import torch.distributed as dist
+    rank, world = _rank_world()
+    if world == 1:
+        return band
+    rows_max = -(-height // world)
+    pad = torch.zeros((rows_max,) + tuple(band.shape[1:]), dtype=band.dtype, device=band.device)
+    pad[:band.shape[0]] = band
+    parts = [torch.empty_like(pad) for _ in range(world)]
+    dist.all_gather(parts, pad)
+    return torch.cat([parts[r][:shard_range(height, r, world)[1] - shard_range(height, r, world)[0]]
+                      for r in range(world)])
+
+
+def render_sharded(pathtracer, camera, width: int, height: int, spp: int, max_recursive_depth: int = 5,
+                   seed: int = 1):
+    """One frame split across the ranks by rows (one process per GPU, each with
+    its own replica of the scene): rank r renders its band with
+    PathTracer.Render(rows=...), and the bands are gathered on every rank. The
+    result is bit-identical to one GPU rendering the whole frame, because each
+    pixel draws the random numbers of its place in the frame."""
+    import torch
+    rank, world = _rank_world()
+    r0, r1 = shard_range(height, rank, world)
+    if r1 > r0:
+        band = pathtracer.Render(camera, width, height, spp, max_recursive_depth, seed, rows=(r0, r1))
+    else:
+        dev = pathtracer.device
+        band = torch.empty((0, width, 3), dtype=torch.float32,
+                           device=dev if isinstance(dev, torch.device) else torch.device("cuda", dev))
+    return gather_rows(band, height)
 
 
 def max_over_ranks(value: float, device=None) -> float:

@@ -1,6 +1,7 @@
-"""SG_BUILDER_LBVH: the Morton-order wide BVH built on the GPU.
+"""SG_BUILDER_LBVH and SG_BUILDER_PLOC: the wide BVHs built on the GPU from
+the Morton order (radix tree; parallel locally-ordered clustering).
 
-Its tree is not SORT's, so the bar is the one for a different tree over the
+Their trees are not SORT's, so the bar is the one for a different tree over the
 same triangles: every ray's closest distance equals the one through SORT's
 tree (the host builder's) bit for bit, the primitive is the same unless two
 triangles are hit at exactly that distance, and the any-hit answer is the
@@ -25,12 +26,20 @@ pytestmark = pytest.mark.gpu
 torch = pytest.importorskip("torch")
 
 
-def _pair(tri, width, **kw):
+BUILDERS = ["lbvh", "ploc"]
+
+
+def _code(builder):
+    from sort_b200 import _lib
+    return {"lbvh": _lib.SG_BUILDER_LBVH, "ploc": _lib.SG_BUILDER_PLOC}[builder]
+
+
+def _pair(tri, width, builder="lbvh", **kw):
     from sort_b200 import Obvh, Qbvh, _lib
     cls = Qbvh if width == 4 else Obvh
     ref = cls(builder=_lib.SG_BUILDER_HOST, **kw)
     ref.Build(tri)
-    lb = cls(builder=_lib.SG_BUILDER_LBVH, **kw)
+    lb = cls(builder=_code(builder), **kw)
     lb.Build(tri)
     return ref, lb
 
@@ -78,29 +87,32 @@ def _same_hits(tri, ref, lb, rays, check_ties=True):
     assert np.array_equal(oa[same_t], ob[same_t])
 
 
+@pytest.mark.parametrize("builder", BUILDERS)
 @pytest.mark.parametrize("width", [4, 8])
-def test_lbvh_sphere_fields(width):
+def test_lbvh_sphere_fields(width, builder):
     assert torch.cuda.is_available(), "GPU test needs a CUDA device"
     from sort_b200 import scenes
     for spheres, level, seed in ((64, 3, 1), (256, 4, 2)):
         tri = scenes.sphere_field(spheres, level, seed=seed)
         rays = np.concatenate([scenes.camera_rays(256, 256, seed=3), scenes.random_rays(50_000, seed=4)], axis=1)
-        ref, lb = _pair(tri, width)
+        ref, lb = _pair(tri, width, builder)
         _same_hits(tri, ref, lb, rays)
         info = lb.info()
         assert info["triangles"] == tri.shape[0] and info["leaves"] > 0 and info["interior_nodes"] > 0
         assert info["bbox"] == ref.info()["bbox"]
 
 
+@pytest.mark.parametrize("builder", BUILDERS)
 @pytest.mark.parametrize("width", [4, 8])
 @pytest.mark.parametrize("leaf", [1, 3, 8, 16])
-def test_lbvh_edge_scene(width, leaf):
+def test_lbvh_edge_scene(width, leaf, builder):
     z = golden("edges")
-    ref, lb = _pair(z["triangles"], width, max_pri_in_leaf=leaf)
+    ref, lb = _pair(z["triangles"], width, builder, max_pri_in_leaf=leaf)
     _same_hits(z["triangles"], ref, lb, z["rays"])
 
 
-def test_lbvh_random_soup_and_tiny_scenes():
+@pytest.mark.parametrize("builder", BUILDERS)
+def test_lbvh_random_soup_and_tiny_scenes(builder):
     from sort_b200 import scenes
     rng = np.random.default_rng(7)
     c = rng.uniform(-5, 5, (20000, 1, 3))
@@ -108,25 +120,44 @@ def test_lbvh_random_soup_and_tiny_scenes():
     tri[::5] = np.round(tri[::5])  # repeated coordinates: equal Morton codes
     rays = scenes.random_rays(20000, seed=8, box=8.0, axis_fraction=0.2)
     for width in (4, 8):
-        ref, lb = _pair(tri, width)
+        ref, lb = _pair(tri, width, builder)
         _same_hits(tri, ref, lb, rays)
         for k in (1, 2, 9, 17):
-            ref, lb = _pair(tri[:k], width)
+            ref, lb = _pair(tri[:k], width, builder)
             _same_hits(tri[:k], ref, lb, rays[:, :2000])
 
 
-def test_lbvh_limits_are_reported():
+@pytest.mark.parametrize("builder", BUILDERS)
+def test_lbvh_limits_are_reported(builder):
     from sort_b200 import Obvh, _lib, scenes
     tri = scenes.sphere_field(8, 2, seed=9)
-    acc = Obvh(builder=_lib.SG_BUILDER_LBVH)
+    acc = Obvh(builder=_code(builder))
     acc.Build(tri)
     with pytest.raises(_lib.SortGpuError) as ex:
         acc.topology()
     assert ex.value.status == 4  # SG_ERR_UNSUPPORTED
-    q8 = Obvh(builder=_lib.SG_BUILDER_LBVH, node_format=_lib.SG_NODES_QUANT8)
+    q8 = Obvh(builder=_code(builder), node_format=_lib.SG_NODES_QUANT8)
     with pytest.raises(_lib.SortGpuError) as ex:
         q8.Build(tri)
     assert ex.value.status == 4
-    empty = Obvh(builder=_lib.SG_BUILDER_LBVH)
+    empty = Obvh(builder=_code(builder))
     empty.Build(np.zeros((0, 9), np.float32))
     assert not empty.GetIsValid()
+
+
+@pytest.mark.parametrize("width", [4, 8])
+def test_ploc_tree_is_tighter_than_lbvh(width):
+    """The clustered tree's traversal does less work than the radix tree's on
+    the same rays (SORT's counters: interior nodes box-tested and primitives
+    tested per ray), and its build reports the clustering iterations."""
+    from sort_b200 import scenes
+    tri = scenes.sphere_field(256, 4, seed=2)
+    rays = torch.from_numpy(np.ascontiguousarray(scenes.random_rays(100_000, seed=5))).cuda()
+    work = {}
+    for builder in BUILDERS:
+        _, acc = _pair(tri, width, builder)
+        nodes, prims = acc.TraceStats(rays, False)
+        work[builder] = nodes * (width * 28) + prims * 36
+        info = acc.info()
+        assert info["build_rounds"] > 0 and info["build_launches"] > info["build_rounds"]
+    assert work["ploc"] < work["lbvh"], work

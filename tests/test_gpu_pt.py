@@ -60,6 +60,25 @@ def test_pt_same_seed_same_image(tracer):
     assert np.array_equal(a, b) and not np.array_equal(a, c)
 
 
+def test_pt_row_bands_put_together_are_the_frame(tracer):
+    """sg_pt_render_rows: bands of rows rendered separately (as the ranks of a
+    frame split across GPUs render them) give the whole frame's image bit for
+    bit, and render_sharded on one rank is the whole render."""
+    from sort_b200 import _lib
+    from sort_b200.replicas import render_sharded
+    pt, z = tracer
+    w, h = 61, 37
+    full = pt.Render(z["camera"], w, h, 8, 5, seed=21)
+    cuts = [0, 1, 13, 30, h]
+    bands = [pt.Render(z["camera"], w, h, 8, 5, seed=21, rows=(a, b)) for a, b in zip(cuts, cuts[1:])]
+    assert all(b.shape == (e - a, w, 3) for b, a, e in zip(bands, cuts, cuts[1:]))
+    assert torch.equal(torch.cat(bands), full)
+    assert torch.equal(render_sharded(pt, z["camera"], w, h, 8, 5, seed=21), full)
+    for rows in ((3, 3), (-1, 4), (0, h + 1)):
+        with pytest.raises(_lib.SortGpuError):
+            pt.Render(z["camera"], w, h, 8, 5, seed=21, rows=rows, out=full)
+
+
 def test_pt_quantized_nodes_match_sort(tracer):
     """8-bit child boxes: the same statistical bar against SORT's converged render;
     hits can differ from the FP32-node render only at near-ties, so the two

@@ -1,6 +1,8 @@
 """Multi-GPU work division, exercised as two gloo ranks on the CPU: shares of a
-ray batch and of an image's tiles cover the work exactly once, the timing
-reduction takes the slowest rank, and the request router balances load."""
+ray batch and of an image's tiles cover the work exactly once, a frame
+rendered in bands of rows comes back whole and in order on every rank (also
+when a rank has no rows), the timing reduction takes the slowest rank, and the
+request router balances load."""
 import os
 import socket
 
@@ -8,7 +10,22 @@ import pytest
 
 torch = pytest.importorskip("torch")
 
-from sort_b200.replicas import ReplicaRouter, max_over_ranks, rank_tiles, shard_range, tiles  # noqa: E402
+from sort_b200.replicas import (ReplicaRouter, gather_rows, max_over_ranks, rank_tiles, render_sharded,  # noqa: E402
+                                shard_range, tiles)
+
+
+class _RowImage:
+    """Stands in for PathTracer: a pixel's value is its index in the frame plus the seed."""
+    device = torch.device("cpu")
+
+    def Render(self, camera, width, height, spp, max_recursive_depth=5, seed=1, rows=None):
+        r0, r1 = rows
+        idx = torch.arange(r0 * width, r1 * width, dtype=torch.float32).reshape(r1 - r0, width, 1)
+        return idx.repeat(1, 1, 3) + seed
+
+
+def _frame(width, height, seed):
+    return torch.arange(width * height, dtype=torch.float32).reshape(height, width, 1).repeat(1, 1, 3) + seed
 
 
 def test_shard_range_partitions():
@@ -64,8 +81,13 @@ def _worker(rank, world, port, n, out):
         mine = rank_tiles(640, 360, rank, world)
         all_tiles = [None] * world
         dist.all_gather_object(all_tiles, mine)
+        frames = [bool(torch.equal(render_sharded(_RowImage(), None, w, h, 1, 5, seed=3), _frame(w, h, 3)))
+                  for w, h in ((7, 5), (4, 1), (3, 2), (640, 361))]
+        r0, r1 = shard_range(6, rank, world)
+        band = torch.arange(r0, r1, dtype=torch.int64).reshape(-1, 1)
+        frames.append(bool(torch.equal(gather_rows(band, 6), torch.arange(6).reshape(-1, 1))))
         if rank == 0:
-            out.put((spans, slowest, all_tiles))
+            out.put((spans, slowest, all_tiles, frames))
     finally:
         dist.destroy_process_group()
 
@@ -79,7 +101,7 @@ def test_two_gloo_ranks():
     procs = [ctx.Process(target=_worker, args=(r, 2, port, n, q)) for r in range(2)]
     for p in procs:
         p.start()
-    spans, slowest, all_tiles = q.get(timeout=120)
+    spans, slowest, all_tiles, frames = q.get(timeout=120)
     for p in procs:
         p.join(timeout=60)
         assert p.exitcode == 0
@@ -87,3 +109,8 @@ def test_two_gloo_ranks():
     assert slowest == 2.0
     flat = [t for ts in all_tiles for t in ts]
     assert len(flat) == len(set(flat)) == len(tiles(640, 360))
+    assert all(frames), frames
+
+
+def test_one_rank_renders_the_whole_frame():
+    assert torch.equal(render_sharded(_RowImage(), None, 9, 4, 1, seed=2), _frame(9, 4, 2))
