@@ -521,7 +521,12 @@ sg_status sg_pt_ray_counts(const sg_pt_scene* pt, int64_t* extension, int64_t* s
  *   at once; steps_per_poll = bounce steps per graph replay (even, >= 2);
  *   samples_per_claim = samples a pool slot renders of one pixel before the
  *   pixel goes back to the shared work queue (1 = strict turn-taking between
- *   requests; larger keeps neighbouring pixels together in the queues).
+ *   requests; larger keeps neighbouring pixels together in the queues);
+ *   solo_pixels = a request of at least this many pixels (and 2 or more
+ *   samples) that reaches an idle server renders as sg_pt_render renders,
+ *   one wave per sample on the idle pool's buffers, until another request
+ *   arrives; then its remaining samples join the pool like any admission
+ *   (the image is the same either way). 0 = path_slots / 4, < 0 = never.
  * sg_server_add_scene: all scenes of a server share one tree width and node
  *   format (SG_ERR_UNSUPPORTED otherwise); the sg_pt_scene and its sg_scene
  *   must outlive the server.
@@ -541,6 +546,7 @@ typedef struct {
     int64_t pixel_budget;
     int32_t steps_per_poll;
     int32_t samples_per_claim;
+    int64_t solo_pixels;
 } sg_server_opts;
 
 typedef struct {
@@ -572,6 +578,7 @@ typedef struct {
     int64_t graph_replays;
     int64_t queued;           /* submitted, not admitted */
     int64_t admitted;         /* admitted, not complete */
+    int64_t solo_waves;       /* samples rendered as whole-request waves (solo_pixels) */
 } sg_server_stats;
 
 typedef struct sg_server sg_server;

@@ -107,7 +107,7 @@ class BatchTuning(ctypes.Structure):
 class ServerOpts(ctypes.Structure):
     _fields_ = [("device", ctypes.c_int32), ("max_requests", ctypes.c_int32), ("path_slots", ctypes.c_int64),
                 ("pixel_budget", ctypes.c_int64), ("steps_per_poll", ctypes.c_int32),
-                ("samples_per_claim", ctypes.c_int32)]
+                ("samples_per_claim", ctypes.c_int32), ("solo_pixels", ctypes.c_int64)]
 
 
 class Request(ctypes.Structure):
@@ -123,7 +123,7 @@ class RequestResult(ctypes.Structure):
 
 class ServerStats(ctypes.Structure):
     _fields_ = [(name, ctypes.c_int64) for name in ("requests_done", "samples_done", "extension_rays", "shadow_rays",
-                                                    "graph_replays", "queued", "admitted")]
+                                                    "graph_replays", "queued", "admitted", "solo_waves")]
 
 
 SG_SHAPE_QUAD = 0

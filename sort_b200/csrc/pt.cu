@@ -32,6 +32,7 @@
 #include <vector>
 
 #include "pt_common.cuh"
+#include "pt_wave.h"
 #include "scene_access.h"
 #include "trace_kernels.h"
 
@@ -308,6 +309,62 @@ extern "C" sg_status sg_pt_destroy(sg_pt_scene* ps) {
     return SG_OK;
 }
 
+namespace sg {
+
+cudaError_t pt_wave(const PtDev& dev, const TraceLaunch& base_in, const DevTree& tree, const Cam& cam, int width,
+                    int height, int p0, int n, uint2 key, int sample, int max_depth, const PtWave& w, float* image,
+                    cudaStream_t s) {
+    const int cap = w.cap, scap = 2 * w.cap;
+    if (n <= 0 || n > cap) return cudaErrorInvalidValue;
+    TraceLaunch base = base_in;
+    base.tuning.schedule = kScheduleThreadPerRay;  // queue lengths live on the device
+    Queue qa{w.qa_ray, w.qa_slot, nullptr}, qb{w.qb_ray, w.qb_slot, nullptr};
+    const Queue sq{w.sq_ray, w.sq_slot, w.sq_contrib};
+    int* counters = w.counters;
+    const int threads = 256;
+    const int blocks = (n + threads - 1) / threads;
+    cudaError_t e = cudaSuccess;
+    Queue* cur = &qa;
+    Queue* nxt = &qb;
+    k_generate<<<blocks, threads, 0, s>>>(cam, width, height, p0, n, key, (uint32_t)sample, *cur, cap, w.thr,
+                                          &counters[0]);
+    for (int bounce = 0; bounce < max_depth; ++bounce) {
+        DevRays r{cur->ray,           cur->ray + cap,     cur->ray + 2 * cap, cur->ray + 3 * cap,
+                  cur->ray + 4 * cap, cur->ray + 5 * cap, cur->ray + 6 * cap, cur->ray + 7 * cap};
+        TraceLaunch Lc = base;
+        Lc.any = false;
+        Lc.prim = w.hit_prim;
+        Lc.t = w.hit_t;
+        Lc.n_dev = &counters[0];
+        if ((e = launch_trace_fp32(Lc, tree, r, (int64_t)cap, s)) != cudaSuccess) return e;
+        if ((e = cudaMemsetAsync(&counters[1], 0, 2 * sizeof(int), s)) != cudaSuccess) return e;
+        k_shade<<<blocks, threads, 0, s>>>(dev, key, p0, (uint32_t)sample, bounce, max_depth, *cur, cap,
+                                           &counters[0], w.hit_prim, w.hit_t, *nxt, &counters[1], sq, scap,
+                                           &counters[2], w.thr, w.vis);
+        DevRays sr{sq.ray,            sq.ray + scap,     sq.ray + 2 * scap, sq.ray + 3 * scap,
+                   sq.ray + 4 * scap, sq.ray + 5 * scap, sq.ray + 6 * scap, sq.ray + 7 * scap};
+        TraceLaunch La = base;
+        La.any = true;
+        La.occ = w.occ;
+        La.n_dev = &counters[2];
+        if ((e = launch_trace_fp32(La, tree, sr, (int64_t)scap, s)) != cudaSuccess) return e;
+        k_resolve<<<(scap + threads - 1) / threads, threads, 0, s>>>(sq, scap, &counters[2], w.occ, w.vis, cap);
+        k_accumulate<<<blocks, threads, 0, s>>>(*cur, &counters[0], w.vis, w.thr, cap);
+        k_count_rays<<<1, 32, 0, s>>>(counters, w.totals);
+        // the next queue becomes the current one
+        if ((e = cudaMemcpyAsync(&counters[0], &counters[1], sizeof(int), cudaMemcpyDeviceToDevice, s)) !=
+            cudaSuccess)
+            return e;
+        Queue* t = cur;
+        cur = nxt;
+        nxt = t;
+    }
+    k_flush<<<blocks, threads, 0, s>>>(w.thr, cap, n, image);
+    return cudaGetLastError();
+}
+
+}  // namespace sg
+
 extern "C" sg_status sg_pt_render(sg_pt_scene* ps, const float* camera, int32_t width, int32_t height, int32_t spp,
                                   int32_t max_depth, uint64_t seed, float* image, void* stream) {
     return sg_pt_render_rows(ps, camera, width, height, 0, height, spp, max_depth, seed, image, stream);
@@ -362,66 +419,36 @@ extern "C" sg_status sg_pt_render_rows(sg_pt_scene* ps, const float* camera, int
         b += align(bytes);
         return r;
     };
-    sg::Queue qa{(float*)take(cap * 32), (int*)take(cap * 4), nullptr};
-    sg::Queue qb{(float*)take(cap * 32), (int*)take(cap * 4), nullptr};
-    int32_t* hit_prim = (int32_t*)take(cap * 4);
-    float* hit_t = (float*)take(cap * 4);
-    sg::Queue sq{(float*)take(scap * 32), (int*)take(scap * 4), (float*)take(scap * 12)};
-    uint8_t* occ = (uint8_t*)take(scap);
-    float* thr = (float*)take(cap * 24);  // throughput and radiance per path
-    float* vis = (float*)take(cap * 24);  // two shadow results per path
-    int* counters = (int*)take(16);  // [0] current queue, [1] next queue, [2] shadow queue
-    unsigned long long* totals = (unsigned long long*)take(16);  // rays traced: extension, shadow
+    sg::PtWave w{};
+    w.qa_ray = (float*)take(cap * 32);
+    w.qa_slot = (int*)take(cap * 4);
+    w.qb_ray = (float*)take(cap * 32);
+    w.qb_slot = (int*)take(cap * 4);
+    w.hit_prim = (int32_t*)take(cap * 4);
+    w.hit_t = (float*)take(cap * 4);
+    w.sq_ray = (float*)take(scap * 32);
+    w.sq_slot = (int*)take(scap * 4);
+    w.sq_contrib = (float*)take(scap * 12);
+    w.occ = (uint8_t*)take(scap);
+    w.thr = (float*)take(cap * 24);  // throughput and radiance per path
+    w.vis = (float*)take(cap * 24);  // two shadow results per path
+    w.counters = (int*)take(16);  // [0] current queue, [1] next queue, [2] shadow queue
+    w.totals = (unsigned long long*)take(16);  // rays traced: extension, shadow
+    w.cap = (int)cap;
     if ((size_t)(b - (char*)ps->d_buf) > need) return sg::set_error(SG_ERR_INTERNAL, "render buffer layout overflow");
-    ps->d_totals = totals;
-    if ((e = cudaMemsetAsync(totals, 0, 16, s)) != cudaSuccess) return pt_fail(e);
+    ps->d_totals = w.totals;
+    if ((e = cudaMemsetAsync(w.totals, 0, 16, s)) != cudaSuccess) return pt_fail(e);
 
     const sg::Cam cam = sg::make_camera(camera, width, height);
     const uint2 key = make_uint2((uint32_t)seed, (uint32_t)(seed >> 32));
     sg::PtDev dev{ps->d_prim, ps->d_mats, ps->light};
     const int threads = 256;
-    const int blocks = (P + threads - 1) / threads;
     const int img_n = 3 * P;
     sg::k_zero<<<(img_n + threads - 1) / threads, threads, 0, s>>>(image, img_n);
-    for (int sample = 0; sample < spp; ++sample) {
-        sg::Queue* cur = &qa;
-        sg::Queue* nxt = &qb;
-        sg::k_generate<<<blocks, threads, 0, s>>>(cam, width, height, p0, P, key, (uint32_t)sample, *cur, (int)cap,
-                                                  thr, &counters[0]);
-        for (int bounce = 0; bounce < max_depth; ++bounce) {
-            sg::DevRays r{cur->ray,           cur->ray + cap,     cur->ray + 2 * cap, cur->ray + 3 * cap,
-                          cur->ray + 4 * cap, cur->ray + 5 * cap, cur->ray + 6 * cap, cur->ray + 7 * cap};
-            sg::TraceLaunch Lc = base;
-            Lc.any = false;
-            Lc.prim = hit_prim;
-            Lc.t = hit_t;
-            Lc.n_dev = &counters[0];
-            if ((e = sg::launch_trace_fp32(Lc, tree, r, (int64_t)cap, s)) != cudaSuccess) return pt_fail(e);
-            if ((e = cudaMemsetAsync(&counters[1], 0, 2 * sizeof(int), s)) != cudaSuccess) return pt_fail(e);
-            sg::k_shade<<<blocks, threads, 0, s>>>(dev, key, p0, (uint32_t)sample, bounce, max_depth, *cur, (int)cap,
-                                                   &counters[0], hit_prim, hit_t, *nxt, &counters[1], sq, (int)scap,
-                                                   &counters[2], thr, vis);
-            sg::DevRays sr{sq.ray,            sq.ray + scap,     sq.ray + 2 * scap, sq.ray + 3 * scap,
-                           sq.ray + 4 * scap, sq.ray + 5 * scap, sq.ray + 6 * scap, sq.ray + 7 * scap};
-            sg::TraceLaunch La = base;
-            La.any = true;
-            La.occ = occ;
-            La.n_dev = &counters[2];
-            if ((e = sg::launch_trace_fp32(La, tree, sr, (int64_t)scap, s)) != cudaSuccess) return pt_fail(e);
-            sg::k_resolve<<<(int)((scap + threads - 1) / threads), threads, 0, s>>>(sq, (int)scap, &counters[2], occ,
-                                                                                   vis, (int)cap);
-            sg::k_accumulate<<<blocks, threads, 0, s>>>(*cur, &counters[0], vis, thr, (int)cap);
-            sg::k_count_rays<<<1, 32, 0, s>>>(counters, totals);
-            // the next queue becomes the current one
-            if ((e = cudaMemcpyAsync(&counters[0], &counters[1], sizeof(int), cudaMemcpyDeviceToDevice, s)) !=
-                cudaSuccess)
-                return pt_fail(e);
-            sg::Queue* t = cur;
-            cur = nxt;
-            nxt = t;
-        }
-        sg::k_flush<<<blocks, threads, 0, s>>>(thr, (int)cap, P, image);
-    }
+    for (int sample = 0; sample < spp; ++sample)
+        if ((e = sg::pt_wave(dev, base, tree, cam, width, height, p0, P, key, sample, max_depth, w, image, s)) !=
+            cudaSuccess)
+            return pt_fail(e);
     sg::k_scale<<<(img_n + threads - 1) / threads, threads, 0, s>>>(image, img_n, 1.0f / (float)spp);
     if ((e = cudaGetLastError()) != cudaSuccess) return pt_fail(e);
     return SG_OK;

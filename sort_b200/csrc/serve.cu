@@ -51,7 +51,7 @@ __device__ __forceinline__ void pixel_finished(const SrvBuffers& b, int r) {
     if (atomicSub(&b.units_left[r], 1u) == 1u) b.done[r] = 1;
 }
 
-// This replay's admissions: sample 0 of every pixel, appended after the ring's end.
+// This replay's admissions: the first sample to render of every pixel, appended after the ring's end.
 __global__ void k_srv_admit(SrvBuffers b) {
     const SrvControl* c = b.control;
     const int64_t total = c->admit_total;
@@ -67,7 +67,7 @@ __global__ void k_srv_admit(SrvBuffers b) {
         }
         const SrvAdmit ad = c->admit[lo];
         b.ring[(tail + (unsigned long long)i) % (unsigned long long)b.ring_cap] =
-            srv_unit(ad.request, 0, (int)(i - ad.first));
+            srv_unit(ad.request, ad.sample0, (int)(i - ad.first));
     }
 }
 

@@ -7,6 +7,16 @@
 // while the next one runs (two replays in flight). A completed request's
 // image is copied to its host buffer on a second stream, then its slot and
 // image range are released and its waiters are woken.
+//
+// Solo phase: a large request that finds the server idle (nothing admitted,
+// no replay in flight) is rendered the way sg_pt_render renders a frame, one
+// wave per sample (pt_wave, on the idle pool's queues), with two waves queued
+// ahead, until another request arrives or one sample is left. Its remaining
+// samples then enter the pool like an admission that starts at that sample.
+// The pool's waves for a lone frame drain slowly (each pixel's samples run
+// one after another in one slot); the solo waves have no such tail. Each
+// pixel's samples are still added in sample order, so the image does not
+// depend on where the switch happens.
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -22,6 +32,7 @@
 #include <unordered_map>
 #include <vector>
 
+#include "pt_wave.h"
 #include "scene_access.h"
 #include "serve_kernels.h"
 #include "sortgpu.h"
@@ -109,6 +120,10 @@ struct sg_server {
     Arena arena{0};
     int64_t admitted = 0;
     std::vector<sg::SrvScene> scenes;
+    std::vector<sg::TraceLaunch> launches;  // per scene, for the solo waves
+    int64_t solo_pixels = 0;                // 0: no solo phase
+    int64_t handoff = -1;                   // ticket whose solo phase ended, to admit next
+    int handoff_sample = 0;                 // its first sample for the pool
     sg_server_stats stats{};
     // device
     char* d_mem = nullptr;
@@ -125,7 +140,7 @@ struct sg_server {
     int* h_done[2] = {};
     sg::SrvCounters* h_counters[2] = {};
     cudaStream_t stream = nullptr, copy_stream = nullptr;
-    cudaEvent_t replay_done[2] = {}, copy_done = nullptr;
+    cudaEvent_t replay_done[2] = {}, copy_done = nullptr, solo_done[2] = {};
     cudaGraphExec_t graph = nullptr;
     int graph_stack = 0;
 };
@@ -142,6 +157,7 @@ void free_server(sg_server* S) {
         if (S->h_done[k]) cudaFreeHost(S->h_done[k]);
         if (S->h_counters[k]) cudaFreeHost(S->h_counters[k]);
         if (S->replay_done[k]) cudaEventDestroy(S->replay_done[k]);
+        if (S->solo_done[k]) cudaEventDestroy(S->solo_done[k]);
     }
     if (S->copy_done) cudaEventDestroy(S->copy_done);
     if (S->h_requests) cudaFreeHost(S->h_requests);
@@ -184,47 +200,70 @@ sg_status capture(sg_server* S) {
     return SG_OK;
 }
 
-// Admits queued requests into the control block of the next replay (S->mu held).
+// Gives ticket id a request-table slot and an image range, stages its table
+// entry and zeroes its image (S->mu held). False when either is not free.
+bool reserve(sg_server* S, int64_t id) {
+    if (S->free_slots.empty()) return false;
+    Ticket& t = S->tickets[id];
+    const int64_t P = int64_t(t.req.width) * t.req.height;
+    const int64_t off = S->arena.alloc(P);
+    if (off < 0) return false;  // FIFO: wait for image memory
+    const int r = S->free_slots.back();
+    S->free_slots.pop_back();
+    sg::SrvRequest& q = S->h_requests[r];
+    q = sg::SrvRequest{};
+    q.cam = sg::make_camera(t.req.camera, t.req.width, t.req.height);
+    q.key = make_uint2((uint32_t)t.req.seed, (uint32_t)(t.req.seed >> 32));
+    q.image = S->d_images + 3 * off;
+    q.scene = t.req.scene;
+    q.width = t.req.width;
+    q.height = t.req.height;
+    q.spp = t.req.spp;
+    q.max_depth = t.req.max_depth;
+    q.inv_spp = 1.0f / (float)t.req.spp;
+    q.cancelled = 0;
+    S->h_units[r] = (unsigned)P;
+    cudaMemcpyAsync(S->d_requests + r, &q, sizeof(q), cudaMemcpyHostToDevice, S->stream);
+    cudaMemsetAsync(q.image, 0, size_t(P) * 3 * sizeof(float), S->stream);
+    cudaMemcpyAsync(S->b.units_left + r, &S->h_units[r], sizeof(unsigned), cudaMemcpyHostToDevice, S->stream);
+    cudaMemsetAsync(S->b.done + r, 0, sizeof(int), S->stream);
+    t.slot = r;
+    t.arena = off;
+    t.admit_ns = now_ns();
+    S->slot_ticket[size_t(r)] = id;
+    return true;
+}
+
+// Enters a reserved ticket's pixels, from sample0 on, into the next replay's
+// admissions (S->mu held).
+void enter_pool(sg_server* S, sg::SrvControl& ctl, int64_t id, int sample0, int64_t replay) {
+    Ticket& t = S->tickets[id];
+    const int64_t P = int64_t(t.req.width) * t.req.height;
+    ctl.admit[ctl.nadmit].request = t.slot;
+    ctl.admit[ctl.nadmit].pixels = (int32_t)P;
+    ctl.admit[ctl.nadmit].first = ctl.admit_total;
+    ctl.admit[ctl.nadmit].sample0 = sample0;
+    ctl.admit[ctl.nadmit].pad = 0;
+    ctl.nadmit++;
+    ctl.admit_total += P;
+    t.replay = replay;
+    S->admitted++;
+}
+
+// Admits queued requests into the control block of the next replay (S->mu
+// held), after the request whose solo phase just ended.
 void admit(sg_server* S, sg::SrvControl& ctl, int64_t replay) {
     ctl.nadmit = 0;
     ctl.admit_total = 0;
-    while (!S->pending.empty() && ctl.nadmit < sg::kSrvMaxAdmit && !S->free_slots.empty()) {
+    if (S->handoff >= 0) {
+        enter_pool(S, ctl, S->handoff, S->handoff_sample, replay);
+        S->handoff = -1;
+    }
+    while (!S->pending.empty() && ctl.nadmit < sg::kSrvMaxAdmit) {
         const int64_t id = S->pending.front();
-        Ticket& t = S->tickets[id];
-        const int64_t P = int64_t(t.req.width) * t.req.height;
-        const int64_t off = S->arena.alloc(P);
-        if (off < 0) break;  // FIFO: wait for image memory
+        if (!reserve(S, id)) break;
         S->pending.pop_front();
-        const int r = S->free_slots.back();
-        S->free_slots.pop_back();
-        sg::SrvRequest& q = S->h_requests[r];
-        q = sg::SrvRequest{};
-        q.cam = sg::make_camera(t.req.camera, t.req.width, t.req.height);
-        q.key = make_uint2((uint32_t)t.req.seed, (uint32_t)(t.req.seed >> 32));
-        q.image = S->d_images + 3 * off;
-        q.scene = t.req.scene;
-        q.width = t.req.width;
-        q.height = t.req.height;
-        q.spp = t.req.spp;
-        q.max_depth = t.req.max_depth;
-        q.inv_spp = 1.0f / (float)t.req.spp;
-        q.cancelled = 0;
-        S->h_units[r] = (unsigned)P;
-        cudaMemcpyAsync(S->d_requests + r, &q, sizeof(q), cudaMemcpyHostToDevice, S->stream);
-        cudaMemsetAsync(q.image, 0, size_t(P) * 3 * sizeof(float), S->stream);
-        cudaMemcpyAsync(S->b.units_left + r, &S->h_units[r], sizeof(unsigned), cudaMemcpyHostToDevice, S->stream);
-        cudaMemsetAsync(S->b.done + r, 0, sizeof(int), S->stream);
-        ctl.admit[ctl.nadmit].request = r;
-        ctl.admit[ctl.nadmit].pixels = (int32_t)P;
-        ctl.admit[ctl.nadmit].first = ctl.admit_total;
-        ctl.nadmit++;
-        ctl.admit_total += P;
-        t.slot = r;
-        t.arena = off;
-        t.replay = replay;
-        t.admit_ns = now_ns();
-        S->slot_ticket[size_t(r)] = id;
-        S->admitted++;
+        enter_pool(S, ctl, id, 0, replay);
     }
     for (int r : S->to_cancel) {
         S->h_requests[r].cancelled = 1;
@@ -232,6 +271,78 @@ void admit(sg_server* S, sg::SrvControl& ctl, int64_t replay) {
                         cudaMemcpyHostToDevice, S->stream);
     }
     S->to_cancel.clear();
+}
+
+// The queue head, reserved, if it starts a solo phase: the server is idle (no
+// admitted request, no replay in flight) and the request is large with at
+// least two samples (S->mu held); else -1.
+int64_t take_solo(sg_server* S, bool inflight) {
+    if (inflight || S->admitted > 0 || S->handoff >= 0 || S->solo_pixels <= 0 || S->pending.empty()) return -1;
+    const int64_t id = S->pending.front();
+    const Ticket& t = S->tickets[id];
+    if (int64_t(t.req.width) * t.req.height < S->solo_pixels || t.req.spp < 2) return -1;
+    if (!reserve(S, id)) return -1;
+    S->pending.pop_front();
+    return id;
+}
+
+// Renders ticket id's samples one wave each on the idle pool's buffers until
+// another request is queued (or the ticket is cancelled, or the server
+// stops), leaving the last sample to the pool; then hands the ticket over.
+sg_status run_solo(sg_server* S, int64_t id) {
+    sg::SrvRequest q;
+    int spp = 0;
+    const Ticket* t = nullptr;
+    {
+        std::lock_guard<std::mutex> lk(S->mu);
+        t = &S->tickets[id];
+        q = S->h_requests[t->slot];
+        spp = t->req.spp;
+    }
+    const sg::SrvScene& sc = S->scenes[size_t(q.scene)];
+    const sg::TraceLaunch& base = S->launches[size_t(q.scene)];
+    sg::PtWave w{};
+    w.qa_ray = S->b.qa_ray;
+    w.qa_slot = S->b.qa_slot;
+    w.qb_ray = S->b.qb_ray;
+    w.qb_slot = S->b.qb_slot;
+    w.sq_ray = S->b.sq_ray;
+    w.sq_slot = S->b.sq_slot;
+    w.sq_contrib = S->b.sq_contrib;
+    w.hit_prim = S->b.hit_prim;
+    w.hit_t = S->b.hit_t;
+    w.occ = S->b.occ;
+    w.thr = S->b.thr;
+    w.vis = S->b.vis;
+    w.counters = S->d_counters->queue;
+    w.totals = &S->d_counters->ext_rays;
+    w.cap = (int)S->b.slots;
+    const int rows = std::max(1, w.cap / q.width);  // rows per band: a band fits the pool
+    int k = 0;
+    cudaError_t e = cudaSuccess;
+    for (; k < spp - 1; ++k) {
+        {
+            std::lock_guard<std::mutex> lk(S->mu);
+            if (S->stop || t->cancel || !S->pending.empty()) break;
+        }
+        for (int y = 0; y < q.height && e == cudaSuccess; y += rows) {
+            const int y1 = std::min(q.height, y + rows);
+            const int p0 = y * q.width;
+            e = sg::pt_wave(sc.pt, base, sc.tree, q.cam, q.width, q.height, p0, (y1 - y) * q.width, q.key, k,
+                            q.max_depth, w, q.image + 3 * int64_t(p0), S->stream);
+        }
+        if (e == cudaSuccess) e = cudaEventRecord(S->solo_done[k % 2], S->stream);
+        if (e == cudaSuccess && k >= 1) e = cudaEventSynchronize(S->solo_done[(k - 1) % 2]);
+        if (e != cudaSuccess) return fail(SG_ERR_CUDA, std::string("solo wave: ") + cudaGetErrorString(e));
+    }
+    // The pool's first step starts from empty queues.
+    if ((e = cudaMemsetAsync(S->d_counters->queue, 0, sizeof(S->d_counters->queue), S->stream)) != cudaSuccess)
+        return fail(SG_ERR_CUDA, std::string("solo handoff: ") + cudaGetErrorString(e));
+    std::lock_guard<std::mutex> lk(S->mu);
+    S->handoff = id;
+    S->handoff_sample = k;
+    S->stats.solo_waves += k;
+    return SG_OK;
 }
 
 // Reads the completion flags of replay k and hands out finished requests.
@@ -293,13 +404,23 @@ void serve_loop(sg_server* S) {
     sg_status st = SG_OK;
     for (;;) {
         bool launch = false;
+        int64_t solo = -1;
         {
             std::unique_lock<std::mutex> lk(S->mu);
             if (!inflight)
-                S->cv_work.wait(lk, [&] { return S->stop || !S->pending.empty() || S->admitted > 0; });
+                S->cv_work.wait(lk, [&] {
+                    return S->stop || !S->pending.empty() || S->admitted > 0 || S->handoff >= 0;
+                });
             if (S->stop) break;
-            admit(S, *S->h_control[j % 2], j);
-            launch = S->admitted > 0;
+            solo = take_solo(S, inflight);
+            if (solo < 0) {
+                admit(S, *S->h_control[j % 2], j);
+                launch = S->admitted > 0;
+            }
+        }
+        if (solo >= 0) {  // no replay is in flight: the pool is idle
+            if ((st = run_solo(S, solo)) != SG_OK) break;
+            continue;
         }
         if (launch) {
             cudaError_t e = cudaSuccess;
@@ -350,6 +471,7 @@ void sg_default_server_opts(sg_server_opts* o) {
     o->pixel_budget = int64_t(1) << 24;
     o->steps_per_poll = 4;
     o->samples_per_claim = 1;
+    o->solo_pixels = 0;
 }
 
 sg_status sg_server_create(const sg_server_opts* opts, sg_server** out) {
@@ -374,6 +496,7 @@ sg_status sg_server_create(const sg_server_opts* opts, sg_server** out) {
     sg_server* S = new (std::nothrow) sg_server;
     if (!S) return fail(SG_ERR_OUT_OF_MEMORY, "host allocation failed");
     S->opts = o;
+    S->solo_pixels = o.solo_pixels < 0 ? 0 : o.solo_pixels > 0 ? o.solo_pixels : std::max<int64_t>(1, o.path_slots / 4);
     S->arena = Arena(o.pixel_budget);
     S->slot_ticket.assign(size_t(o.max_requests), -1);
     for (int r = o.max_requests - 1; r >= 0; --r) S->free_slots.push_back(r);
@@ -474,6 +597,7 @@ sg_status sg_server_create(const sg_server_opts* opts, sg_server** out) {
         if (e == cudaSuccess) e = cudaMallocHost(&S->h_done[k], R * sizeof(int));
         if (e == cudaSuccess) e = cudaMallocHost(&S->h_counters[k], sizeof(sg::SrvCounters));
         if (e == cudaSuccess) e = cudaEventCreateWithFlags(&S->replay_done[k], cudaEventDisableTiming);
+        if (e == cudaSuccess) e = cudaEventCreateWithFlags(&S->solo_done[k], cudaEventDisableTiming);
     }
     if (e == cudaSuccess) e = cudaEventCreateWithFlags(&S->copy_done, cudaEventDisableTiming);
     if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&S->stream, cudaStreamNonBlocking);
@@ -512,6 +636,7 @@ sg_status sg_server_add_scene(sg_server* S, const sg_pt_scene* pt, int32_t* scen
     if (prev >= 0) cudaSetDevice(prev);
     if (e != cudaSuccess) return fail(SG_ERR_CUDA, std::string("scene table: ") + cudaGetErrorString(e));
     S->scenes.push_back(sc);
+    S->launches.push_back(L);
     S->width = L.width;
     S->node_format = fmt;
     S->stack_need = std::max(S->stack_need, L.stack_need);

@@ -27,12 +27,14 @@ def _pinned(shape):
 
 class RenderServer:
     def __init__(self, device: int = 0, path_slots: int = 1 << 20, pixel_budget: int = 1 << 24,
-                 max_requests: int = 1024, steps_per_poll: int = 4, samples_per_claim: int = 1):
+                 max_requests: int = 1024, steps_per_poll: int = 4, samples_per_claim: int = 1,
+                 solo_pixels: int = 0):
         o = _lib.ServerOpts()
         _lib.load().sg_default_server_opts(ctypes.byref(o))
         o.device, o.path_slots, o.pixel_budget = int(device), int(path_slots), int(pixel_budget)
         o.max_requests, o.steps_per_poll = int(max_requests), int(steps_per_poll)
         o.samples_per_claim = int(samples_per_claim)
+        o.solo_pixels = int(solo_pixels)
         h = ctypes.c_void_p()
         _lib.check(_lib.load().sg_server_create(ctypes.byref(o), ctypes.byref(h)))
         self._h = h

@@ -1,6 +1,8 @@
 """Render server (sg_server): every request's image is bit-identical to
 sg_pt_render of the same request, rendered alone or in a mix of requests that
-share the path pool and wavefront queues; admission, cancellation and limits.
+share the path pool and wavefront queues, and whether or not it started in a
+solo phase (whole-request waves while the server is idle) and joined the pool
+part-way; admission, cancellation and limits.
 
 The pools here are small (a few thousand path slots, a pixel budget below the
 mix's total) so that slots are reused many times, requests wait for admission
@@ -68,6 +70,35 @@ def test_each_request_matches_single_render_alone_and_mixed(tracers, per_claim):
     assert st["samples_done"] == 2 * sum(w * h * spp for _, _, w, h, spp, _, _ in reqs)
     assert st["queued"] == 0 and st["admitted"] == 0
     srv.close()
+
+
+def test_solo_phase_and_handoff_give_the_same_image(tracers):
+    """A large request on an idle server renders its samples as waves and
+    leaves the last one to the pool; requests arriving meanwhile end the solo
+    phase early and the rest of its samples join the pool. Images equal
+    sg_pt_render's in every case, and with the solo phase turned off."""
+    import time
+
+    from sort_b200 import scenes
+    big = (1, scenes.CAMERA, 400, 300, 48, 5, 21)
+    small = [(0, scenes.CAMERA, 64, 48, 4, 5, 22), (2, scenes.CAMERA, 33, 17, 7, 4, 23),
+             (1, scenes.CAMERA, 200, 10, 2, 6, 24)]
+    refs = [reference(tracers, r) for r in [big] + small]
+    for solo in (1000, -1):
+        srv = server(tracers, path_slots=50_000, pixel_budget=400_000, max_requests=8, samples_per_claim=8,
+                     solo_pixels=solo)
+        img, res = srv.wait(srv.submit(*big[:2], *big[2:6], seed=big[6]))  # alone: 47 waves, then the pool
+        assert res["status"] == 0 and np.array_equal(img.view(np.uint32), refs[0].view(np.uint32))
+        waves = srv.stats()["solo_waves"]
+        assert waves == (big[4] - 1 if solo > 0 else 0)
+        t_big = srv.submit(*big[:2], *big[2:6], seed=big[6])
+        time.sleep(0.02)  # arrivals during the solo phase
+        tickets = [srv.submit(*r[:2], *r[2:6], seed=r[6]) for r in small]
+        for t, ref in zip([t_big] + tickets, refs):
+            img, res = srv.wait(t)
+            assert res["status"] == 0 and np.array_equal(img.view(np.uint32), ref.view(np.uint32))
+        assert 0 <= srv.stats()["solo_waves"] - waves <= big[4] - 1
+        srv.close()
 
 
 def test_cancel_leaves_others_unchanged(tracers):
