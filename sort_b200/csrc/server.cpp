@@ -8,20 +8,21 @@
 // image is copied to its host buffer on a second stream, then its slot and
 // image range are released and its waiters are woken.
 //
-// Solo phase: a large request that finds the server idle (nothing admitted,
-// no replay in flight) is rendered the way sg_pt_render renders a frame, one
-// wave per sample (pt_wave, on the idle pool's queues), with two waves queued
-// ahead, until another request arrives or one sample is left. Its remaining
-// samples then enter the pool like an admission that starts at that sample.
-// The pool's waves for a lone frame drain slowly (each pixel's samples run
-// one after another in one slot); the solo waves have no such tail. Each
-// pixel's samples are still added in sample order, so the image does not
-// depend on where the switch happens.
+// Solo phase: a large request at the head of the queue (one at a time) is
+// rendered the way sg_pt_render renders a frame, one wave per sample
+// (pt_wave, on its own buffers), with two waves queued ahead on a second
+// stream, so that the pool keeps serving the other requests meanwhile. When all but its last sample are queued (or it is
+// cancelled) its remaining samples enter the pool like an admission that
+// starts at that sample. A large request in the pool finishes with its
+// slowest pixel (each pixel's samples run one after another in one slot); the
+// waves have no such tail. Each pixel's samples are still added in sample
+// order, so the image does not depend on where the switch happens.
 #include <cuda_runtime.h>
 
 #include <algorithm>
 #include <chrono>
 #include <condition_variable>
+#include <cstdint>
 #include <cstring>
 #include <deque>
 #include <map>
@@ -122,8 +123,17 @@ struct sg_server {
     std::vector<sg::SrvScene> scenes;
     std::vector<sg::TraceLaunch> launches;  // per scene, for the solo waves
     int64_t solo_pixels = 0;                // 0: no solo phase
-    int64_t handoff = -1;                   // ticket whose solo phase ended, to admit next
-    int handoff_sample = 0;                 // its first sample for the pool
+    struct {
+        int64_t id = -1;  // ticket in its solo phase
+        int next = 0;     // next sample to queue a wave for
+        int done = 0;     // waves finished
+        int last = 0;     // waves the phase may run (spp - 1)
+    } solo;
+    int64_t handoff = -1;  // ticket whose solo phase ended, to admit next
+    int handoff_sample = 0;  // its first sample for the pool
+    sg::PtWave solo_w{};     // the solo waves' own buffers (in d_solo)
+    char* d_solo = nullptr;
+    cudaStream_t solo_stream = nullptr;  // the solo waves, beside the pool's `stream`
     sg_server_stats stats{};
     // device
     char* d_mem = nullptr;
@@ -140,7 +150,7 @@ struct sg_server {
     int* h_done[2] = {};
     sg::SrvCounters* h_counters[2] = {};
     cudaStream_t stream = nullptr, copy_stream = nullptr;
-    cudaEvent_t replay_done[2] = {}, copy_done = nullptr, solo_done[2] = {};
+    cudaEvent_t replay_done[2] = {}, copy_done = nullptr, solo_done[2] = {}, solo_ready = nullptr, solo_end = nullptr;
     cudaGraphExec_t graph = nullptr;
     int graph_stack = 0;
 };
@@ -160,6 +170,11 @@ void free_server(sg_server* S) {
         if (S->solo_done[k]) cudaEventDestroy(S->solo_done[k]);
     }
     if (S->copy_done) cudaEventDestroy(S->copy_done);
+    if (S->solo_ready) cudaEventDestroy(S->solo_ready);
+    if (S->solo_end) cudaEventDestroy(S->solo_end);
+    if (S->solo_stream) cudaStreamSynchronize(S->solo_stream);
+    if (S->solo_stream) cudaStreamDestroy(S->solo_stream);
+    if (S->d_solo) cudaFree(S->d_solo);
     if (S->h_requests) cudaFreeHost(S->h_requests);
     if (S->h_units) cudaFreeHost(S->h_units);
     if (S->stream) cudaStreamDestroy(S->stream);
@@ -255,7 +270,8 @@ void enter_pool(sg_server* S, sg::SrvControl& ctl, int64_t id, int sample0, int6
 void admit(sg_server* S, sg::SrvControl& ctl, int64_t replay) {
     ctl.nadmit = 0;
     ctl.admit_total = 0;
-    if (S->handoff >= 0) {
+    if (S->handoff >= 0) {  // after its last solo wave
+        cudaStreamWaitEvent(S->stream, S->solo_end, 0);
         enter_pool(S, ctl, S->handoff, S->handoff_sample, replay);
         S->handoff = -1;
     }
@@ -273,75 +289,88 @@ void admit(sg_server* S, sg::SrvControl& ctl, int64_t replay) {
     S->to_cancel.clear();
 }
 
-// The queue head, reserved, if it starts a solo phase: the server is idle (no
-// admitted request, no replay in flight) and the request is large with at
-// least two samples (S->mu held); else -1.
-int64_t take_solo(sg_server* S, bool inflight) {
-    if (inflight || S->admitted > 0 || S->handoff >= 0 || S->solo_pixels <= 0 || S->pending.empty()) return -1;
+// Starts a solo phase for the queue head (S->mu held) when none is running
+// and the head is large with at least two samples: reserves it and makes the
+// solo stream wait for its zeroed image.
+void start_solo(sg_server* S) {
+    if (S->solo.id >= 0 || S->handoff >= 0 || S->solo_pixels <= 0 || S->pending.empty()) return;
     const int64_t id = S->pending.front();
     const Ticket& t = S->tickets[id];
-    if (int64_t(t.req.width) * t.req.height < S->solo_pixels || t.req.spp < 2) return -1;
-    if (!reserve(S, id)) return -1;
+    if (int64_t(t.req.width) * t.req.height < S->solo_pixels || t.req.spp < 2) return;
+    if (!reserve(S, id)) return;
     S->pending.pop_front();
-    return id;
+    // Not in any replay until the hand-off: a completion flag read back for
+    // its table slot before then belongs to the slot's previous request.
+    S->tickets[id].replay = INT64_MAX;
+    cudaEventRecord(S->solo_ready, S->stream);
+    cudaStreamWaitEvent(S->solo_stream, S->solo_ready, 0);
+    S->solo.id = id;
+    S->solo.next = S->solo.done = 0;
+    S->solo.last = t.req.spp - 1;
 }
 
-// Renders ticket id's samples one wave each on the idle pool's buffers until
-// another request is queued (or the ticket is cancelled, or the server
-// stops), leaving the last sample to the pool; then hands the ticket over.
-sg_status run_solo(sg_server* S, int64_t id) {
-    sg::SrvRequest q;
-    int spp = 0;
-    const Ticket* t = nullptr;
-    {
-        std::lock_guard<std::mutex> lk(S->mu);
-        t = &S->tickets[id];
-        q = S->h_requests[t->slot];
-        spp = t->req.spp;
-    }
-    const sg::SrvScene& sc = S->scenes[size_t(q.scene)];
-    const sg::TraceLaunch& base = S->launches[size_t(q.scene)];
-    sg::PtWave w{};
-    w.qa_ray = S->b.qa_ray;
-    w.qa_slot = S->b.qa_slot;
-    w.qb_ray = S->b.qb_ray;
-    w.qb_slot = S->b.qb_slot;
-    w.sq_ray = S->b.sq_ray;
-    w.sq_slot = S->b.sq_slot;
-    w.sq_contrib = S->b.sq_contrib;
-    w.hit_prim = S->b.hit_prim;
-    w.hit_t = S->b.hit_t;
-    w.occ = S->b.occ;
-    w.thr = S->b.thr;
-    w.vis = S->b.vis;
-    w.counters = S->d_counters->queue;
-    w.totals = &S->d_counters->ext_rays;
-    w.cap = (int)S->b.slots;
-    const int rows = std::max(1, w.cap / q.width);  // rows per band: a band fits the pool
-    int k = 0;
+// Keeps two waves of the solo request queued on the solo stream; when its
+// waves up to the last sample are queued (or it is cancelled, or the server
+// stops) hands it to the pool from the next sample on.
+sg_status pump_solo(sg_server* S) {
+    if (S->solo.id < 0) return SG_OK;
     cudaError_t e = cudaSuccess;
-    for (; k < spp - 1; ++k) {
-        {
-            std::lock_guard<std::mutex> lk(S->mu);
-            if (S->stop || t->cancel || !S->pending.empty()) break;
+    while (S->solo.done < S->solo.next) {  // retire finished waves
+        e = cudaEventQuery(S->solo_done[S->solo.done % 2]);
+        if (e == cudaErrorNotReady) {
+            // Not an error, but the runtime keeps it as the last error, which
+            // the next launch check (cudaGetLastError) would report.
+            cudaGetLastError();
+            e = cudaSuccess;
+            break;
         }
+        if (e != cudaSuccess) return fail(SG_ERR_CUDA, std::string("solo wave: ") + cudaGetErrorString(e));
+        S->solo.done++;
+    }
+    sg::SrvRequest q;
+    sg::SrvScene sc;
+    sg::TraceLaunch base;
+    bool end = false;
+    {
+        std::lock_guard<std::mutex> lk(S->mu);  // add_scene may grow the scene tables meanwhile
+        const Ticket& t = S->tickets[S->solo.id];
+        q = S->h_requests[t.slot];
+        sc = S->scenes[size_t(q.scene)];
+        base = S->launches[size_t(q.scene)];
+        end = S->stop || t.cancel;
+    }
+    const int rows = std::max(1, S->solo_w.cap / q.width);  // rows per band: a band fits the wave buffers
+    while (!end && S->solo.next < S->solo.last && S->solo.next - S->solo.done < 2) {
+        const int k = S->solo.next;
         for (int y = 0; y < q.height && e == cudaSuccess; y += rows) {
             const int y1 = std::min(q.height, y + rows);
             const int p0 = y * q.width;
             e = sg::pt_wave(sc.pt, base, sc.tree, q.cam, q.width, q.height, p0, (y1 - y) * q.width, q.key, k,
-                            q.max_depth, w, q.image + 3 * int64_t(p0), S->stream);
+                            q.max_depth, S->solo_w, q.image + 3 * int64_t(p0), S->solo_stream);
         }
-        if (e == cudaSuccess) e = cudaEventRecord(S->solo_done[k % 2], S->stream);
-        if (e == cudaSuccess && k >= 1) e = cudaEventSynchronize(S->solo_done[(k - 1) % 2]);
+        if (e == cudaSuccess) e = cudaEventRecord(S->solo_done[k % 2], S->solo_stream);
         if (e != cudaSuccess) return fail(SG_ERR_CUDA, std::string("solo wave: ") + cudaGetErrorString(e));
+        S->solo.next++;
+        std::lock_guard<std::mutex> lk(S->mu);
+        S->stats.solo_waves++;
     }
-    // The pool's first step starts from empty queues.
-    if ((e = cudaMemsetAsync(S->d_counters->queue, 0, sizeof(S->d_counters->queue), S->stream)) != cudaSuccess)
-        return fail(SG_ERR_CUDA, std::string("solo handoff: ") + cudaGetErrorString(e));
-    std::lock_guard<std::mutex> lk(S->mu);
-    S->handoff = id;
-    S->handoff_sample = k;
-    S->stats.solo_waves += k;
+    if (end || S->solo.next == S->solo.last) {
+        if ((e = cudaEventRecord(S->solo_end, S->solo_stream)) != cudaSuccess)
+            return fail(SG_ERR_CUDA, std::string("solo handoff: ") + cudaGetErrorString(e));
+        std::lock_guard<std::mutex> lk(S->mu);
+        S->handoff = S->solo.id;
+        S->handoff_sample = S->solo.next;
+        S->solo.id = -1;
+    }
+    return SG_OK;
+}
+
+// Blocks until the oldest queued solo wave has finished.
+sg_status wait_solo(sg_server* S) {
+    if (S->solo.id < 0 || S->solo.done >= S->solo.next) return SG_OK;
+    const cudaError_t e = cudaEventSynchronize(S->solo_done[S->solo.done % 2]);
+    if (e != cudaSuccess) return fail(SG_ERR_CUDA, std::string("solo wave: ") + cudaGetErrorString(e));
+    S->solo.done++;
     return SG_OK;
 }
 
@@ -404,24 +433,18 @@ void serve_loop(sg_server* S) {
     sg_status st = SG_OK;
     for (;;) {
         bool launch = false;
-        int64_t solo = -1;
         {
             std::unique_lock<std::mutex> lk(S->mu);
-            if (!inflight)
+            if (!inflight && S->solo.id < 0)
                 S->cv_work.wait(lk, [&] {
                     return S->stop || !S->pending.empty() || S->admitted > 0 || S->handoff >= 0;
                 });
             if (S->stop) break;
-            solo = take_solo(S, inflight);
-            if (solo < 0) {
-                admit(S, *S->h_control[j % 2], j);
-                launch = S->admitted > 0;
-            }
+            start_solo(S);
+            admit(S, *S->h_control[j % 2], j);
+            launch = S->admitted > 0;
         }
-        if (solo >= 0) {  // no replay is in flight: the pool is idle
-            if ((st = run_solo(S, solo)) != SG_OK) break;
-            continue;
-        }
+        if ((st = pump_solo(S)) != SG_OK) break;
         if (launch) {
             cudaError_t e = cudaSuccess;
             if ((st = capture(S)) != SG_OK) break;
@@ -443,10 +466,12 @@ void serve_loop(sg_server* S) {
             S->stats.graph_replays++;
         }
         if (inflight && (st = collect(S, int((j - 1) % 2), j - 1)) != SG_OK) break;
+        if (!inflight && !launch && (st = wait_solo(S)) != SG_OK) break;  // only the solo waves run
         inflight = launch;
         if (launch) ++j;
     }
     if (st == SG_OK && inflight) st = collect(S, int((j - 1) % 2), j - 1);
+    cudaStreamSynchronize(S->solo_stream);
     cudaStreamSynchronize(S->stream);
     std::lock_guard<std::mutex> lk(S->mu);
     if (st != SG_OK) {
@@ -600,8 +625,49 @@ sg_status sg_server_create(const sg_server_opts* opts, sg_server** out) {
         if (e == cudaSuccess) e = cudaEventCreateWithFlags(&S->solo_done[k], cudaEventDisableTiming);
     }
     if (e == cudaSuccess) e = cudaEventCreateWithFlags(&S->copy_done, cudaEventDisableTiming);
+    if (e == cudaSuccess) e = cudaEventCreateWithFlags(&S->solo_ready, cudaEventDisableTiming);
+    if (e == cudaSuccess) e = cudaEventCreateWithFlags(&S->solo_end, cudaEventDisableTiming);
+    // The pool's steps and the solo waves share the GPU at equal priority
+    // (giving the pool's stream the higher one measured a little worse p99).
     if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&S->stream, cudaStreamNonBlocking);
+    if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&S->solo_stream, cudaStreamNonBlocking);
     if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&S->copy_stream, cudaStreamNonBlocking);
+    if (e == cudaSuccess && S->solo_pixels > 0) {
+        // The solo waves' buffers (pt_wave.h), path_slots paths: extension
+        // queues, hits, the shadow queue (2 per path), flags, path state,
+        // counters and ray totals.
+        const size_t cap = C, scap = 2 * C;
+        const size_t parts[] = {cap * 32, cap * 4, cap * 32, cap * 4, cap * 4, cap * 4, scap * 32, scap * 4,
+                                scap * 12, scap, cap * 24, cap * 24, 16, 16};
+        size_t bytes = 0;
+        for (size_t x : parts) bytes += align_up(x);
+        e = cudaMalloc(&S->d_solo, bytes);
+        if (e == cudaSuccess) e = cudaMemset(S->d_solo, 0, bytes);
+        if (e == cudaSuccess) {
+            char* q = S->d_solo;
+            char* at[14];
+            for (int k = 0; k < 14; ++k) {
+                at[k] = q;
+                q += align_up(parts[k]);
+            }
+            sg::PtWave& w = S->solo_w;
+            w.qa_ray = reinterpret_cast<float*>(at[0]);
+            w.qa_slot = reinterpret_cast<int*>(at[1]);
+            w.qb_ray = reinterpret_cast<float*>(at[2]);
+            w.qb_slot = reinterpret_cast<int*>(at[3]);
+            w.hit_prim = reinterpret_cast<int32_t*>(at[4]);
+            w.hit_t = reinterpret_cast<float*>(at[5]);
+            w.sq_ray = reinterpret_cast<float*>(at[6]);
+            w.sq_slot = reinterpret_cast<int*>(at[7]);
+            w.sq_contrib = reinterpret_cast<float*>(at[8]);
+            w.occ = reinterpret_cast<uint8_t*>(at[9]);
+            w.thr = reinterpret_cast<float*>(at[10]);
+            w.vis = reinterpret_cast<float*>(at[11]);
+            w.counters = reinterpret_cast<int*>(at[12]);
+            w.totals = reinterpret_cast<unsigned long long*>(at[13]);
+            w.cap = int(cap);
+        }
+    }
     if (prev >= 0) cudaSetDevice(prev);
     if (e != cudaSuccess) {
         free_server(S);
@@ -713,7 +779,18 @@ sg_status sg_server_stats_get(sg_server* S, sg_server_stats* out) {
     std::lock_guard<std::mutex> lk(S->mu);
     *out = S->stats;
     out->queued = int64_t(S->pending.size());
-    out->admitted = S->admitted;
+    out->admitted = S->admitted + (S->solo.id >= 0 ? 1 : 0);
+    if (S->solo_w.totals) {  // rays of the solo waves (a snapshot while they run)
+        unsigned long long h[2] = {0, 0};
+        int prev = -1;
+        cudaGetDevice(&prev);
+        cudaSetDevice(S->opts.device);
+        if (cudaMemcpy(h, S->solo_w.totals, sizeof(h), cudaMemcpyDeviceToHost) == cudaSuccess) {
+            out->extension_rays += int64_t(h[0]);
+            out->shadow_rays += int64_t(h[1]);
+        }
+        if (prev >= 0) cudaSetDevice(prev);
+    }
     return SG_OK;
 }
 

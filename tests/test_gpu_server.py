@@ -43,6 +43,16 @@ def reference(tracers, req):
     return img.cpu().numpy()
 
 
+def loop_error(srv):
+    """The error that stopped the server's loop (a submit after it reports it)."""
+    from sort_b200 import scenes
+    try:
+        srv.submit(0, scenes.CAMERA, 1, 1, 1)
+    except Exception as ex:  # noqa: BLE001 - the message is the point
+        return str(ex)
+    return "loop still running"
+
+
 def server(tracers, **kw):
     from sort_b200.server import RenderServer
     srv = RenderServer(**kw)
@@ -58,7 +68,7 @@ def test_each_request_matches_single_render_alone_and_mixed(tracers, per_claim):
     srv = server(tracers, path_slots=3000, pixel_budget=20_000, max_requests=4, samples_per_claim=per_claim)
     for r, ref in zip(reqs, refs):  # alone
         img, res = srv.wait(srv.submit(*r[:2], *r[2:6], seed=r[6]))
-        assert res["status"] == 0
+        assert res["status"] == 0, loop_error(srv)
         assert np.array_equal(img.view(np.uint32), ref.view(np.uint32))
     tickets = [srv.submit(*r[:2], *r[2:6], seed=r[6]) for r in reqs[::-1]]  # mixed, reverse order
     for t, ref in zip(tickets, refs[::-1]):
@@ -88,7 +98,8 @@ def test_solo_phase_and_handoff_give_the_same_image(tracers):
         srv = server(tracers, path_slots=50_000, pixel_budget=400_000, max_requests=8, samples_per_claim=8,
                      solo_pixels=solo)
         img, res = srv.wait(srv.submit(*big[:2], *big[2:6], seed=big[6]))  # alone: 47 waves, then the pool
-        assert res["status"] == 0 and np.array_equal(img.view(np.uint32), refs[0].view(np.uint32))
+        assert res["status"] == 0, loop_error(srv)
+        assert np.array_equal(img.view(np.uint32), refs[0].view(np.uint32))
         waves = srv.stats()["solo_waves"]
         assert waves == (big[4] - 1 if solo > 0 else 0)
         t_big = srv.submit(*big[:2], *big[2:6], seed=big[6])
