@@ -148,10 +148,11 @@ __global__ void k_zero(float* __restrict__ image, int n) {
 }
 
 // Adds this bounce's queue lengths (extension rays, shadow rays) to the totals.
-__global__ void k_count_rays(const int* __restrict__ counters, unsigned long long* __restrict__ totals) {
+__global__ void k_count_rays(const int* __restrict__ extension, const int* __restrict__ shadow,
+                             unsigned long long* __restrict__ totals) {
     if (threadIdx.x == 0) {
-        totals[0] += (unsigned long long)counters[0];
-        totals[1] += (unsigned long long)counters[2];
+        totals[0] += (unsigned long long)*extension;
+        totals[1] += (unsigned long long)*shadow;
     }
 }
 
@@ -169,6 +170,9 @@ struct sg_pt_scene {
     void* d_buf = nullptr;
     size_t buf_bytes = 0;
     unsigned long long* d_totals = nullptr;  // rays traced by the last render: extension, shadow
+    // The shadow rays' stream and its two events (pt_wave.h), made by the first render.
+    cudaStream_t side = nullptr;
+    cudaEvent_t shaded = nullptr, shadowed = nullptr;
 };
 
 extern "C" sg_status sg_pt_ray_counts(const sg_pt_scene* ps, int64_t* extension, int64_t* shadow, void* stream) {
@@ -304,6 +308,12 @@ extern "C" sg_status sg_pt_destroy(sg_pt_scene* ps) {
     if (ps->d_prim) cudaFree(ps->d_prim);
     if (ps->d_mats) cudaFree(ps->d_mats);
     if (ps->d_buf) cudaFree(ps->d_buf);
+    if (ps->side) {
+        cudaStreamSynchronize(ps->side);
+        cudaStreamDestroy(ps->side);
+    }
+    if (ps->shaded) cudaEventDestroy(ps->shaded);
+    if (ps->shadowed) cudaEventDestroy(ps->shadowed);
     if (prev >= 0) cudaSetDevice(prev);
     delete ps;
     return SG_OK;
@@ -326,31 +336,56 @@ cudaError_t pt_wave(const PtDev& dev, const TraceLaunch& base_in, const DevTree&
     cudaError_t e = cudaSuccess;
     Queue* cur = &qa;
     Queue* nxt = &qb;
-    k_generate<<<blocks, threads, 0, s>>>(cam, width, height, p0, n, key, (uint32_t)sample, *cur, cap, w.thr,
-                                          &counters[0]);
-    for (int bounce = 0; bounce < max_depth; ++bounce) {
-        DevRays r{cur->ray,           cur->ray + cap,     cur->ray + 2 * cap, cur->ray + 3 * cap,
-                  cur->ray + 4 * cap, cur->ray + 5 * cap, cur->ray + 6 * cap, cur->ray + 7 * cap};
+    auto closest = [&](const Queue* q) {
+        DevRays r{q->ray,           q->ray + cap,     q->ray + 2 * cap, q->ray + 3 * cap,
+                  q->ray + 4 * cap, q->ray + 5 * cap, q->ray + 6 * cap, q->ray + 7 * cap};
         TraceLaunch Lc = base;
         Lc.any = false;
         Lc.prim = w.hit_prim;
         Lc.t = w.hit_t;
         Lc.n_dev = &counters[0];
-        if ((e = launch_trace_fp32(Lc, tree, r, (int64_t)cap, s)) != cudaSuccess) return e;
-        if ((e = cudaMemsetAsync(&counters[1], 0, 2 * sizeof(int), s)) != cudaSuccess) return e;
-        k_shade<<<blocks, threads, 0, s>>>(dev, key, p0, (uint32_t)sample, bounce, max_depth, *cur, cap,
-                                           &counters[0], w.hit_prim, w.hit_t, *nxt, &counters[1], sq, scap,
-                                           &counters[2], w.thr, w.vis);
+        return launch_trace_fp32(Lc, tree, r, (int64_t)cap, s);
+    };
+    // Shadow rays, their results and the path radiance of bounce `cur` on
+    // stream t; `shaded` is the length of the bounce's extension queue.
+    auto shadows = [&](const Queue* q, const int* shaded, cudaStream_t t) {
         DevRays sr{sq.ray,            sq.ray + scap,     sq.ray + 2 * scap, sq.ray + 3 * scap,
                    sq.ray + 4 * scap, sq.ray + 5 * scap, sq.ray + 6 * scap, sq.ray + 7 * scap};
         TraceLaunch La = base;
         La.any = true;
         La.occ = w.occ;
         La.n_dev = &counters[2];
-        if ((e = launch_trace_fp32(La, tree, sr, (int64_t)scap, s)) != cudaSuccess) return e;
-        k_resolve<<<(scap + threads - 1) / threads, threads, 0, s>>>(sq, scap, &counters[2], w.occ, w.vis, cap);
-        k_accumulate<<<blocks, threads, 0, s>>>(*cur, &counters[0], w.vis, w.thr, cap);
-        k_count_rays<<<1, 32, 0, s>>>(counters, w.totals);
+        cudaError_t r = launch_trace_fp32(La, tree, sr, (int64_t)scap, t);
+        if (r != cudaSuccess) return r;
+        k_resolve<<<(scap + threads - 1) / threads, threads, 0, t>>>(sq, scap, &counters[2], w.occ, w.vis, cap);
+        k_accumulate<<<blocks, threads, 0, t>>>(*q, shaded, w.vis, w.thr, cap);
+        k_count_rays<<<1, 32, 0, t>>>(shaded, &counters[2], w.totals);
+        return cudaGetLastError();
+    };
+    k_generate<<<blocks, threads, 0, s>>>(cam, width, height, p0, n, key, (uint32_t)sample, *cur, cap, w.thr,
+                                          &counters[0]);
+    if ((e = closest(cur)) != cudaSuccess) return e;
+    for (int bounce = 0; bounce < max_depth; ++bounce) {
+        if ((e = cudaMemsetAsync(&counters[1], 0, 2 * sizeof(int), s)) != cudaSuccess) return e;
+        k_shade<<<blocks, threads, 0, s>>>(dev, key, p0, (uint32_t)sample, bounce, max_depth, *cur, cap,
+                                           &counters[0], w.hit_prim, w.hit_t, *nxt, &counters[1], sq, scap,
+                                           &counters[2], w.thr, w.vis);
+        const bool more = bounce + 1 < max_depth;
+        if (!w.side) {
+            if ((e = shadows(cur, &counters[0], s)) != cudaSuccess) return e;
+        } else {
+            // The shadow rays of this bounce go to the side stream and run
+            // beside the next bounce's extension rays; the next shading (which
+            // reuses the shadow queue, the path state and the counters) waits
+            // for them.
+            if ((e = cudaMemcpyAsync(&counters[3], &counters[0], sizeof(int), cudaMemcpyDeviceToDevice, s)) !=
+                    cudaSuccess ||
+                (e = cudaEventRecord(w.shaded, s)) != cudaSuccess ||
+                (e = cudaStreamWaitEvent(w.side, w.shaded, 0)) != cudaSuccess ||
+                (e = shadows(cur, &counters[3], w.side)) != cudaSuccess ||
+                (e = cudaEventRecord(w.shadowed, w.side)) != cudaSuccess)
+                return e;
+        }
         // the next queue becomes the current one
         if ((e = cudaMemcpyAsync(&counters[0], &counters[1], sizeof(int), cudaMemcpyDeviceToDevice, s)) !=
             cudaSuccess)
@@ -358,6 +393,8 @@ cudaError_t pt_wave(const PtDev& dev, const TraceLaunch& base_in, const DevTree&
         Queue* t = cur;
         cur = nxt;
         nxt = t;
+        if (more && (e = closest(cur)) != cudaSuccess) return e;
+        if (w.side && (e = cudaStreamWaitEvent(s, w.shadowed, 0)) != cudaSuccess) return e;
     }
     k_flush<<<blocks, threads, 0, s>>>(w.thr, cap, n, image);
     return cudaGetLastError();
@@ -437,6 +474,13 @@ extern "C" sg_status sg_pt_render_rows(sg_pt_scene* ps, const float* camera, int
     w.cap = (int)cap;
     if ((size_t)(b - (char*)ps->d_buf) > need) return sg::set_error(SG_ERR_INTERNAL, "render buffer layout overflow");
     ps->d_totals = w.totals;
+    if ((!ps->side && (e = cudaStreamCreateWithFlags(&ps->side, cudaStreamNonBlocking)) != cudaSuccess) ||
+        (!ps->shaded && (e = cudaEventCreateWithFlags(&ps->shaded, cudaEventDisableTiming)) != cudaSuccess) ||
+        (!ps->shadowed && (e = cudaEventCreateWithFlags(&ps->shadowed, cudaEventDisableTiming)) != cudaSuccess))
+        return pt_fail(e);
+    w.side = ps->side;
+    w.shaded = ps->shaded;
+    w.shadowed = ps->shadowed;
     if ((e = cudaMemsetAsync(w.totals, 0, 16, s)) != cudaSuccess) return pt_fail(e);
 
     const sg::Cam cam = sg::make_camera(camera, width, height);

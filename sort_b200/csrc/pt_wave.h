@@ -17,8 +17,9 @@ namespace sg {
 // extension queues (8 floats per ray with stride cap, a path index per
 // entry), the hits (cap each), the shadow queue (stride 2 * cap, three
 // contribution planes) and its occlusion flags, per-path throughput and
-// radiance (6 * cap floats) and shadow results (6 * cap), three queue
-// counters (current, next, shadow) and two ray totals (extension, shadow).
+// radiance (6 * cap floats) and shadow results (6 * cap), four queue
+// counters (current, next, shadow, and the shaded queue's length for the side
+// stream) and two ray totals (extension, shadow).
 struct PtWave {
     float* qa_ray;
     int* qa_slot;
@@ -32,9 +33,13 @@ struct PtWave {
     uint8_t* occ;
     float* thr;
     float* vis;
-    int* counters;
+    int* counters;  // 4: current, next and shadow queue lengths, the shaded queue's length
     unsigned long long* totals;
     int cap;
+    // Optional: a second stream on which each bounce's shadow rays run beside
+    // the next bounce's extension rays, with two events for the hand-offs.
+    cudaStream_t side;
+    cudaEvent_t shaded, shadowed;
 };
 
 // Sample `sample` of pixels p0 .. p0 + n - 1 (n <= w.cap) of a width x height

@@ -134,6 +134,7 @@ struct sg_server {
     sg::PtWave solo_w{};     // the solo waves' own buffers (in d_solo)
     char* d_solo = nullptr;
     cudaStream_t solo_stream = nullptr;  // the solo waves, beside the pool's `stream`
+    cudaStream_t solo_side = nullptr;    // the solo waves' shadow rays (pt_wave.h)
     sg_server_stats stats{};
     // device
     char* d_mem = nullptr;
@@ -174,6 +175,10 @@ void free_server(sg_server* S) {
     if (S->solo_end) cudaEventDestroy(S->solo_end);
     if (S->solo_stream) cudaStreamSynchronize(S->solo_stream);
     if (S->solo_stream) cudaStreamDestroy(S->solo_stream);
+    if (S->solo_side) cudaStreamSynchronize(S->solo_side);
+    if (S->solo_side) cudaStreamDestroy(S->solo_side);
+    if (S->solo_w.shaded) cudaEventDestroy(S->solo_w.shaded);
+    if (S->solo_w.shadowed) cudaEventDestroy(S->solo_w.shadowed);
     if (S->d_solo) cudaFree(S->d_solo);
     if (S->h_requests) cudaFreeHost(S->h_requests);
     if (S->h_units) cudaFreeHost(S->h_units);
@@ -666,6 +671,10 @@ sg_status sg_server_create(const sg_server_opts* opts, sg_server** out) {
             w.counters = reinterpret_cast<int*>(at[12]);
             w.totals = reinterpret_cast<unsigned long long*>(at[13]);
             w.cap = int(cap);
+            e = cudaStreamCreateWithFlags(&S->solo_side, cudaStreamNonBlocking);
+            if (e == cudaSuccess) e = cudaEventCreateWithFlags(&w.shaded, cudaEventDisableTiming);
+            if (e == cudaSuccess) e = cudaEventCreateWithFlags(&w.shadowed, cudaEventDisableTiming);
+            w.side = S->solo_side;
         }
     }
     if (prev >= 0) cudaSetDevice(prev);
