@@ -38,3 +38,15 @@ def test_version_and_errors():
     assert st == 1
     assert lib.sg_trace_closest(None, None, 0, None, None) == 1
     assert lib.sg_scene_destroy(None) == 0
+
+
+def test_server_option_layout():
+    """sg_server_opts / sg_server_stats as the Python mirror lays them out:
+    the defaults the library writes land in the right fields."""
+    lib = _lib.load()
+    o = _lib.ServerOpts()
+    o.solo_pixels = -7
+    lib.sg_default_server_opts(ctypes.byref(o))
+    assert (o.device, o.max_requests, o.path_slots, o.pixel_budget) == (0, 1024, 1 << 20, 1 << 24)
+    assert (o.steps_per_poll, o.samples_per_claim, o.solo_pixels) == (4, 1, 0)
+    assert ctypes.sizeof(_lib.ServerOpts) == 40 and ctypes.sizeof(_lib.ServerStats) == 8 * 8
