@@ -755,7 +755,8 @@ def run_serve(args):
         t.Render(scenes.CAMERA, 1920, 1080, 1, PT_DEPTH, seed=1)
     torch.cuda.synchronize(device)
     srv = RenderServer(device=local, path_slots=args.path_slots, pixel_budget=1 << 24, max_requests=1024,
-                       steps_per_poll=2, samples_per_claim=args.samples_per_claim, solo_pixels=args.solo_pixels)
+                       steps_per_poll=args.steps_per_poll, samples_per_claim=args.samples_per_claim,
+                       solo_pixels=args.solo_pixels)
     for t in tracers:
         srv.add_scene(t)
     srv.wait(srv.submit(0, scenes.CAMERA, 64, 64, 1))
@@ -814,9 +815,11 @@ def run_serve(args):
         st0 = srv.stats()
         srv_lat0, srv_span0 = server_run(zero)
         st1 = srv.stats()
-        # the server's own kernels in the closed-loop run: per graph replay the admission pair and
-        # 8 per bounce step; per solo wave a generate and a flush, 6 per bounce
-        launches0 = ((st1["graph_replays"] - st0["graph_replays"]) * (2 + 8 * 2)
+        # the server's own kernels in the closed-loop run: per graph replay the admission pair, 8 per
+        # bounce step and a continuation trace on the side stream for every step but the last; per
+        # solo wave a generate and a flush, 6 per bounce
+        spp_ = args.steps_per_poll
+        launches0 = ((st1["graph_replays"] - st0["graph_replays"]) * (2 + 8 * spp_ + spp_ - 1)
                      + (st1["solo_waves"] - st0["solo_waves"]) * (2 + 6 * PT_DEPTH))
         fifo_rate = len(reqs) / fifo_span0
         rows = []
@@ -842,7 +845,8 @@ def run_serve(args):
             "data": "synthetic (seeded procedural scenes and request stream)",
             "config": serve_config({"requests": len(reqs), "seed": args.batch_seed, "scene_triangles": tri_counts,
                                     "path_slots": args.path_slots, "samples_per_claim": args.samples_per_claim,
-                                    "solo_pixels": (args.solo_pixels or args.path_slots // 4) if args.solo_pixels >= 0 else None,
+                                    "steps_per_poll": args.steps_per_poll,
+                                    "solo_pixels": (args.solo_pixels or args.path_slots // 16) if args.solo_pixels >= 0 else None,
                                     "samples_per_run": int(work)}),
             "closed_loop": {"server": {"msamples_s": round(value, 2), "p50_ms": pct(srv_lat0, 50),
                                        "p99_ms": pct(srv_lat0, 99)},
@@ -997,9 +1001,11 @@ def main():
     p.add_argument("--path-slots", type=int, default=1 << 21, help="serve workload: server path pool")
     p.add_argument("--samples-per-claim", type=int, default=64,
                    help="serve workload: samples a pool slot renders of one pixel before handing it back")
+    p.add_argument("--steps-per-poll", type=int, default=2,
+                   help="serve workload: bounce steps per graph replay (even)")
     p.add_argument("--solo-pixels", type=int, default=0,
-                   help="serve workload: requests this large render as whole waves while the server is idle "
-                        "(0: path slots / 4, -1: never)")
+                   help="serve workload: requests this large render as whole-frame waves beside the pool "
+                        "(0: path slots / 16, -1: never)")
     p.add_argument("--loads", type=float, nargs="*", default=[0.5, 0.8, 1.0],
                    help="serve workload: Poisson arrival rates as fractions of the FIFO arm's capacity")
     p.add_argument("--batches", type=int, default=64, help="batched workload: ray batches per step")

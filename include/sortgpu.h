@@ -522,11 +522,11 @@ sg_status sg_pt_ray_counts(const sg_pt_scene* pt, int64_t* extension, int64_t* s
  *   samples_per_claim = samples a pool slot renders of one pixel before the
  *   pixel goes back to the shared work queue (1 = strict turn-taking between
  *   requests; larger keeps neighbouring pixels together in the queues);
- *   solo_pixels = a request of at least this many pixels (and 2 or more
- *   samples) that reaches an idle server renders as sg_pt_render renders,
- *   one wave per sample on the idle pool's buffers, until another request
- *   arrives; then its remaining samples join the pool like any admission
- *   (the image is the same either way). 0 = path_slots / 4, < 0 = never.
+ *   solo_pixels = the oldest queued request of at least this many pixels
+ *   (and 2 or more samples), one at a time, renders as sg_pt_render renders,
+ *   one wave per sample on the server's own wave buffers, beside the pool;
+ *   its last sample joins the pool like an admission that starts there (the
+ *   image is the same either way). 0 = path_slots / 16, < 0 = never.
  * sg_server_add_scene: all scenes of a server share one tree width and node
  *   format (SG_ERR_UNSUPPORTED otherwise); the sg_pt_scene and its sg_scene
  *   must outlive the server.

@@ -11,7 +11,9 @@
 //   settle      the claim counter is pulled back to the ring's end if warps
 //               over-claimed;
 //   extend      closest-hit traversal of the extension queue, each ray in its
-//               own scene's tree;
+//               own scene's tree (after a replay's first step only the camera
+//               rays: the continuations were traced on the side stream during
+//               the previous step's shadow rays);
 //   shade       shade_vertex per hit; shadow rays and continuations appended
 //               with their scene;
 //   shadow      any-hit traversal of the shadow queue;
@@ -126,14 +128,15 @@ __global__ void k_srv_settle(SrvBuffers b) {
 // of 128 per SM (56 registers; 12 bytes spilled for width-8 FP32 trees):
 // serve_27m's closed loop runs 3.6% faster than at the compiler's 60-80
 // registers.
+// Rays begin (null: 0) .. count - 1 of the queue.
 template <int W, bool ANY, int STACK, bool Q8>
 __global__ void __launch_bounds__(128, 9) k_srv_trace(const SrvScene* __restrict__ scenes, const float* __restrict__ ray,
                                                    const int* __restrict__ scene_of, int cap,
-                                                   const int* __restrict__ count, int32_t* __restrict__ prim,
-                                                   float* __restrict__ t, uint8_t* __restrict__ occ,
-                                                   int* __restrict__ err) {
+                                                   const int* __restrict__ begin, const int* __restrict__ count,
+                                                   int32_t* __restrict__ prim, float* __restrict__ t,
+                                                   uint8_t* __restrict__ occ, int* __restrict__ err) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= *count) return;
+    if (i >= *count || (begin && i < *begin)) return;
     const DevTree tr = scenes[scene_of[i]].tree;
     const DevRays rays{ray, ray + cap, ray + 2 * cap, ray + 3 * cap, ray + 4 * cap, ray + 5 * cap, ray + 6 * cap,
                        ray + 7 * cap};
@@ -276,11 +279,13 @@ __global__ void k_srv_advance(SrvBuffers b) {
 }
 
 template <int W, bool Q8, int STACK>
-cudaError_t enqueue_stack(const SrvBuffers& b, int iterations, cudaStream_t s) {
+cudaError_t enqueue_stack(const SrvBuffers& b, int iterations, const SrvStreams& st) {
+    const cudaStream_t s = st.main;
     const int C = (int)b.slots;
     const int pool_blocks = (C + kThreads - 1) / kThreads;
     const int trace_blocks = (C + 127) / 128;
     const int shadow_blocks = (2 * C + 127) / 128;
+    cudaError_t e = cudaSuccess;
     for (int it = 0; it < iterations; ++it) {
         const bool a_cur = (it % 2) == 0;  // even steps read queue A and write queue B
         float* cray = a_cur ? b.qa_ray : b.qb_ray;
@@ -289,6 +294,8 @@ cudaError_t enqueue_stack(const SrvBuffers& b, int iterations, cudaStream_t s) {
         float* nray = a_cur ? b.qb_ray : b.qa_ray;
         int* nslot = a_cur ? b.qb_slot : b.qa_slot;
         int* nscene = a_cur ? b.qb_scene : b.qa_scene;
+        // Continuations of this queue traced by the previous step on the side stream.
+        const bool traced = st.side && it > 0;
         if (it == 0) {
             k_srv_admit<<<1184, kThreads, 0, s>>>(b);
             k_srv_admit_commit<<<1, 32, 0, s>>>(b);
@@ -296,10 +303,24 @@ cudaError_t enqueue_stack(const SrvBuffers& b, int iterations, cudaStream_t s) {
         k_srv_regen<<<pool_blocks, kThreads, 0, s>>>(b, cray, cslot, cscene);
         k_srv_settle<<<1, 32, 0, s>>>(b);
         k_srv_trace<W, false, STACK, Q8><<<trace_blocks, 128, 0, s>>>(
-            b.scenes, cray, cscene, C, &b.counters->queue[0], b.hit_prim, b.hit_t, nullptr, b.err);
+            b.scenes, cray, cscene, C, traced ? &b.counters->queue[3] : nullptr, &b.counters->queue[0], b.hit_prim,
+            b.hit_t, nullptr, b.err);
+        if (traced && (e = cudaStreamWaitEvent(s, st.joined, 0)) != cudaSuccess) return e;
         k_srv_shade<<<pool_blocks, kThreads, 0, s>>>(b, cray, cslot, cscene, nray, nslot, nscene);
+        if (st.side && it + 1 < iterations) {
+            // The next queue's continuation rays are complete: trace them on the
+            // side stream (their count fixed in queue[3]; advance resets queue[1]).
+            if ((e = cudaMemcpyAsync(&b.counters->queue[3], &b.counters->queue[1], sizeof(int),
+                                     cudaMemcpyDeviceToDevice, s)) != cudaSuccess ||
+                (e = cudaEventRecord(st.forked, s)) != cudaSuccess ||
+                (e = cudaStreamWaitEvent(st.side, st.forked, 0)) != cudaSuccess)
+                return e;
+            k_srv_trace<W, false, STACK, Q8><<<trace_blocks, 128, 0, st.side>>>(
+                b.scenes, nray, nscene, C, nullptr, &b.counters->queue[3], b.hit_prim, b.hit_t, nullptr, b.err);
+            if ((e = cudaEventRecord(st.joined, st.side)) != cudaSuccess) return e;
+        }
         k_srv_trace<W, true, STACK, Q8><<<shadow_blocks, 128, 0, s>>>(
-            b.scenes, b.sq_ray, b.sq_scene, 2 * C, &b.counters->queue[2], nullptr, nullptr, b.occ, b.err);
+            b.scenes, b.sq_ray, b.sq_scene, 2 * C, nullptr, &b.counters->queue[2], nullptr, nullptr, b.occ, b.err);
         k_srv_resolve<<<(2 * C + kThreads - 1) / kThreads, kThreads, 0, s>>>(b);
         k_srv_accumulate<<<pool_blocks, kThreads, 0, s>>>(b, cslot);
         k_srv_advance<<<1, 32, 0, s>>>(b);
@@ -308,19 +329,22 @@ cudaError_t enqueue_stack(const SrvBuffers& b, int iterations, cudaStream_t s) {
 }
 
 template <int W, bool Q8>
-cudaError_t enqueue_w(const SrvBuffers& b, int iterations, int stack, cudaStream_t s) {
-    if (stack <= 64) return enqueue_stack<W, Q8, 64>(b, iterations, s);
-    if (stack <= 128) return enqueue_stack<W, Q8, 128>(b, iterations, s);
-    if (stack <= 256) return enqueue_stack<W, Q8, 256>(b, iterations, s);
+cudaError_t enqueue_w(const SrvBuffers& b, int iterations, int stack, const SrvStreams& st) {
+    if (stack <= 64) return enqueue_stack<W, Q8, 64>(b, iterations, st);
+    if (stack <= 128) return enqueue_stack<W, Q8, 128>(b, iterations, st);
+    if (stack <= 256) return enqueue_stack<W, Q8, 256>(b, iterations, st);
     return cudaErrorInvalidValue;
 }
 
 }  // namespace
 
-cudaError_t srv_enqueue_steps(const SrvBuffers& b, int iterations, int width, int stack, bool q8, cudaStream_t s) {
+cudaError_t srv_enqueue_steps(const SrvBuffers& b, int iterations, int width, int stack, bool q8,
+                              const SrvStreams& st) {
     if (iterations < 2 || iterations % 2 != 0) return cudaErrorInvalidValue;
-    if (width == 8) return q8 ? enqueue_w<8, true>(b, iterations, stack, s) : enqueue_w<8, false>(b, iterations, stack, s);
-    if (width == 4) return q8 ? enqueue_w<4, true>(b, iterations, stack, s) : enqueue_w<4, false>(b, iterations, stack, s);
+    if (width == 8)
+        return q8 ? enqueue_w<8, true>(b, iterations, stack, st) : enqueue_w<8, false>(b, iterations, stack, st);
+    if (width == 4)
+        return q8 ? enqueue_w<4, true>(b, iterations, stack, st) : enqueue_w<4, false>(b, iterations, stack, st);
     return cudaErrorInvalidValue;
 }
 

@@ -59,7 +59,8 @@ struct SrvControl {
 };
 
 struct SrvCounters {
-    int queue[4];               // [0] current extension queue, [1] next, [2] shadow queue
+    int queue[4];               // [0] current extension queue, [1] next, [2] shadow queue,
+                                // [3] continuation rays of the current queue already traced
     unsigned long long head;    // ring entries claimed
     unsigned long long tail;    // ring entries appended
     unsigned long long ext_rays, shadow_rays;
@@ -113,8 +114,19 @@ struct SrvBuffers {
 // Bytes of path state per pool slot (the buffers above, per slot).
 constexpr int64_t kSrvBytesPerSlot = 5 * 4 + 6 * 4 * 2 + 2 * (8 * 4 + 4 + 4) + 4 + 4 + 2 * (8 * 4 + 4 + 4 + 3 * 4 + 1);
 
-// Enqueues `iterations` bounce steps on s; the first takes this replay's
+// Stream pair of the bounce steps: with a side stream, a step's continuation
+// rays are traced on it beside the step's shadow rays (the next step then
+// traces only the camera rays its regeneration adds); `forked` and `joined`
+// are the hand-off events.
+struct SrvStreams {
+    cudaStream_t main;
+    cudaStream_t side;  // may be null: everything on `main`
+    cudaEvent_t forked, joined;
+};
+
+// Enqueues `iterations` bounce steps; the first takes this replay's
 // admissions. Tree width / stack / node format are those of every scene.
-cudaError_t srv_enqueue_steps(const SrvBuffers& b, int iterations, int width, int stack, bool q8, cudaStream_t s);
+cudaError_t srv_enqueue_steps(const SrvBuffers& b, int iterations, int width, int stack, bool q8,
+                              const SrvStreams& st);
 
 }  // namespace sg

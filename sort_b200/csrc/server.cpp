@@ -135,6 +135,10 @@ struct sg_server {
     char* d_solo = nullptr;
     cudaStream_t solo_stream = nullptr;  // the solo waves, beside the pool's `stream`
     cudaStream_t solo_side = nullptr;    // the solo waves' shadow rays (pt_wave.h)
+    // The bounce steps' side stream (continuation rays beside shadow rays,
+    // serve_kernels.h) and its events; captured into the graph.
+    cudaStream_t pool_side = nullptr;
+    cudaEvent_t pool_forked = nullptr, pool_joined = nullptr;
     sg_server_stats stats{};
     // device
     char* d_mem = nullptr;
@@ -177,6 +181,9 @@ void free_server(sg_server* S) {
     if (S->solo_stream) cudaStreamDestroy(S->solo_stream);
     if (S->solo_side) cudaStreamSynchronize(S->solo_side);
     if (S->solo_side) cudaStreamDestroy(S->solo_side);
+    if (S->pool_side) cudaStreamDestroy(S->pool_side);
+    if (S->pool_forked) cudaEventDestroy(S->pool_forked);
+    if (S->pool_joined) cudaEventDestroy(S->pool_joined);
     if (S->solo_w.shaded) cudaEventDestroy(S->solo_w.shaded);
     if (S->solo_w.shadowed) cudaEventDestroy(S->solo_w.shadowed);
     if (S->d_solo) cudaFree(S->d_solo);
@@ -205,8 +212,9 @@ sg_status capture(sg_server* S) {
     }
     cudaError_t e = cudaStreamBeginCapture(S->stream, cudaStreamCaptureModeThreadLocal);
     if (e != cudaSuccess) return fail(SG_ERR_CUDA, std::string("begin capture: ") + cudaGetErrorString(e));
+    const sg::SrvStreams streams{S->stream, S->pool_side, S->pool_forked, S->pool_joined};
     cudaError_t le = sg::srv_enqueue_steps(S->b, S->opts.steps_per_poll, S->width, stack,
-                                           S->node_format == SG_NODES_QUANT8, S->stream);
+                                           S->node_format == SG_NODES_QUANT8, streams);
     cudaGraph_t g = nullptr;
     e = cudaStreamEndCapture(S->stream, &g);
     if (le != cudaSuccess || e != cudaSuccess) {
@@ -526,7 +534,7 @@ sg_status sg_server_create(const sg_server_opts* opts, sg_server** out) {
     sg_server* S = new (std::nothrow) sg_server;
     if (!S) return fail(SG_ERR_OUT_OF_MEMORY, "host allocation failed");
     S->opts = o;
-    S->solo_pixels = o.solo_pixels < 0 ? 0 : o.solo_pixels > 0 ? o.solo_pixels : std::max<int64_t>(1, o.path_slots / 4);
+    S->solo_pixels = o.solo_pixels < 0 ? 0 : o.solo_pixels > 0 ? o.solo_pixels : std::max<int64_t>(1, o.path_slots / 16);
     S->arena = Arena(o.pixel_budget);
     S->slot_ticket.assign(size_t(o.max_requests), -1);
     for (int r = o.max_requests - 1; r >= 0; --r) S->free_slots.push_back(r);
@@ -636,6 +644,9 @@ sg_status sg_server_create(const sg_server_opts* opts, sg_server** out) {
     // (giving the pool's stream the higher one measured a little worse p99).
     if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&S->stream, cudaStreamNonBlocking);
     if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&S->solo_stream, cudaStreamNonBlocking);
+    if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&S->pool_side, cudaStreamNonBlocking);
+    if (e == cudaSuccess) e = cudaEventCreateWithFlags(&S->pool_forked, cudaEventDisableTiming);
+    if (e == cudaSuccess) e = cudaEventCreateWithFlags(&S->pool_joined, cudaEventDisableTiming);
     if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&S->copy_stream, cudaStreamNonBlocking);
     if (e == cudaSuccess && S->solo_pixels > 0) {
         // The solo waves' buffers (pt_wave.h), path_slots paths: extension
