@@ -150,9 +150,9 @@ __global__ void k_zero(float* __restrict__ image, int n) {
 // Adds this bounce's queue lengths (extension rays, shadow rays) to the totals.
 __global__ void k_count_rays(const int* __restrict__ extension, const int* __restrict__ shadow,
                              unsigned long long* __restrict__ totals) {
-    if (threadIdx.x == 0) {
-        totals[0] += (unsigned long long)*extension;
-        totals[1] += (unsigned long long)*shadow;
+    if (threadIdx.x == 0) {  // waves of two samples may count at once
+        atomicAdd(&totals[0], (unsigned long long)*extension);
+        atomicAdd(&totals[1], (unsigned long long)*shadow);
     }
 }
 
@@ -170,9 +170,13 @@ struct sg_pt_scene {
     void* d_buf = nullptr;
     size_t buf_bytes = 0;
     unsigned long long* d_totals = nullptr;  // rays traced by the last render: extension, shadow
-    // The shadow rays' stream and its two events (pt_wave.h), made by the first render.
-    cudaStream_t side = nullptr;
-    cudaEvent_t shaded = nullptr, shadowed = nullptr;
+    // Two samples are in flight at once, each with its own buffers: sample k
+    // runs on the caller's stream (k even) or on `second` (k odd), its shadow
+    // rays on side[k % 2] (pt_wave.h); the events order the hand-offs and the
+    // image additions. Made by the first render.
+    cudaStream_t second = nullptr;
+    cudaStream_t side[2] = {};
+    cudaEvent_t shaded[2] = {}, shadowed[2] = {}, flushed[2] = {}, begun = nullptr;
 };
 
 extern "C" sg_status sg_pt_ray_counts(const sg_pt_scene* ps, int64_t* extension, int64_t* shadow, void* stream) {
@@ -308,12 +312,15 @@ extern "C" sg_status sg_pt_destroy(sg_pt_scene* ps) {
     if (ps->d_prim) cudaFree(ps->d_prim);
     if (ps->d_mats) cudaFree(ps->d_mats);
     if (ps->d_buf) cudaFree(ps->d_buf);
-    if (ps->side) {
-        cudaStreamSynchronize(ps->side);
-        cudaStreamDestroy(ps->side);
-    }
-    if (ps->shaded) cudaEventDestroy(ps->shaded);
-    if (ps->shadowed) cudaEventDestroy(ps->shadowed);
+    for (cudaStream_t t : {ps->second, ps->side[0], ps->side[1]})
+        if (t) {
+            cudaStreamSynchronize(t);
+            cudaStreamDestroy(t);
+        }
+    for (int k = 0; k < 2; ++k)
+        for (cudaEvent_t ev : {ps->shaded[k], ps->shadowed[k], ps->flushed[k]})
+            if (ev) cudaEventDestroy(ev);
+    if (ps->begun) cudaEventDestroy(ps->begun);
     if (prev >= 0) cudaSetDevice(prev);
     delete ps;
     return SG_OK;
@@ -396,7 +403,9 @@ cudaError_t pt_wave(const PtDev& dev, const TraceLaunch& base_in, const DevTree&
         if (more && (e = closest(cur)) != cudaSuccess) return e;
         if (w.side && (e = cudaStreamWaitEvent(s, w.shadowed, 0)) != cudaSuccess) return e;
     }
+    if (w.flush_after && (e = cudaStreamWaitEvent(s, w.flush_after, 0)) != cudaSuccess) return e;
     k_flush<<<blocks, threads, 0, s>>>(w.thr, cap, n, image);
+    if (w.flush_done && (e = cudaEventRecord(w.flush_done, s)) != cudaSuccess) return e;
     return cudaGetLastError();
 }
 
@@ -435,14 +444,16 @@ extern "C" sg_status sg_pt_render_rows(sg_pt_scene* ps, const float* camera, int
     } restore{prev};
     cudaStream_t s = (cudaStream_t)stream;
 
-    // Buffers: two extension queues (rays + slots), hits, one shadow queue of
-    // 2 entries per path (rays + slots + contributions), occlusion flags,
-    // throughput, 3 counters.
+    // Buffers, twice (two samples in flight): two extension queues (rays +
+    // slots), hits, one shadow queue of 2 entries per path (rays + slots +
+    // contributions), occlusion flags, throughput, shadow results, 4
+    // counters; then the shared ray totals.
     const size_t cap = (size_t)P, scap = 2 * (size_t)P;
     auto align = [](size_t x) { return (x + 255) & ~size_t(255); };
     const size_t qbytes = align(cap * 8 * 4) + align(cap * 4);
-    const size_t need = 2 * qbytes + align(cap * 4) * 2 + align(scap * 8 * 4) + align(scap * 4) +
-                        align(scap * 3 * 4) + align(scap) + align(cap * 6 * 4) + align(cap * 6 * 4) + align(16) + align(16);
+    const size_t set = 2 * qbytes + align(cap * 4) * 2 + align(scap * 8 * 4) + align(scap * 4) +
+                       align(scap * 3 * 4) + align(scap) + align(cap * 6 * 4) + align(cap * 6 * 4) + align(16);
+    const size_t need = 2 * set + align(16);
     if (ps->buf_bytes < need) {
         if (ps->d_buf) cudaFree(ps->d_buf);
         ps->d_buf = nullptr;
@@ -456,32 +467,40 @@ extern "C" sg_status sg_pt_render_rows(sg_pt_scene* ps, const float* camera, int
         b += align(bytes);
         return r;
     };
-    sg::PtWave w{};
-    w.qa_ray = (float*)take(cap * 32);
-    w.qa_slot = (int*)take(cap * 4);
-    w.qb_ray = (float*)take(cap * 32);
-    w.qb_slot = (int*)take(cap * 4);
-    w.hit_prim = (int32_t*)take(cap * 4);
-    w.hit_t = (float*)take(cap * 4);
-    w.sq_ray = (float*)take(scap * 32);
-    w.sq_slot = (int*)take(scap * 4);
-    w.sq_contrib = (float*)take(scap * 12);
-    w.occ = (uint8_t*)take(scap);
-    w.thr = (float*)take(cap * 24);  // throughput and radiance per path
-    w.vis = (float*)take(cap * 24);  // two shadow results per path
-    w.counters = (int*)take(16);  // [0] current queue, [1] next queue, [2] shadow queue
-    w.totals = (unsigned long long*)take(16);  // rays traced: extension, shadow
-    w.cap = (int)cap;
+    bool made = true;
+    for (cudaStream_t* t : {&ps->second, &ps->side[0], &ps->side[1]})
+        made = made && (*t || cudaStreamCreateWithFlags(t, cudaStreamNonBlocking) == cudaSuccess);
+    for (int k = 0; k < 2; ++k)
+        for (cudaEvent_t* ev : {&ps->shaded[k], &ps->shadowed[k], &ps->flushed[k]})
+            made = made && (*ev || cudaEventCreateWithFlags(ev, cudaEventDisableTiming) == cudaSuccess);
+    made = made && (ps->begun || cudaEventCreateWithFlags(&ps->begun, cudaEventDisableTiming) == cudaSuccess);
+    if (!made) return sg::set_error(SG_ERR_CUDA, "render streams and events");
+    sg::PtWave w[2] = {};
+    for (int k = 0; k < 2; ++k) {
+        w[k].qa_ray = (float*)take(cap * 32);
+        w[k].qa_slot = (int*)take(cap * 4);
+        w[k].qb_ray = (float*)take(cap * 32);
+        w[k].qb_slot = (int*)take(cap * 4);
+        w[k].hit_prim = (int32_t*)take(cap * 4);
+        w[k].hit_t = (float*)take(cap * 4);
+        w[k].sq_ray = (float*)take(scap * 32);
+        w[k].sq_slot = (int*)take(scap * 4);
+        w[k].sq_contrib = (float*)take(scap * 12);
+        w[k].occ = (uint8_t*)take(scap);
+        w[k].thr = (float*)take(cap * 24);  // throughput and radiance per path
+        w[k].vis = (float*)take(cap * 24);  // two shadow results per path
+        w[k].counters = (int*)take(16);     // current, next, shadow queue; the shaded queue's length
+        w[k].cap = (int)cap;
+        w[k].side = ps->side[k];
+        w[k].shaded = ps->shaded[k];
+        w[k].shadowed = ps->shadowed[k];
+        w[k].flush_done = ps->flushed[k];
+    }
+    unsigned long long* totals = (unsigned long long*)take(16);  // rays traced: extension, shadow
     if ((size_t)(b - (char*)ps->d_buf) > need) return sg::set_error(SG_ERR_INTERNAL, "render buffer layout overflow");
-    ps->d_totals = w.totals;
-    if ((!ps->side && (e = cudaStreamCreateWithFlags(&ps->side, cudaStreamNonBlocking)) != cudaSuccess) ||
-        (!ps->shaded && (e = cudaEventCreateWithFlags(&ps->shaded, cudaEventDisableTiming)) != cudaSuccess) ||
-        (!ps->shadowed && (e = cudaEventCreateWithFlags(&ps->shadowed, cudaEventDisableTiming)) != cudaSuccess))
-        return pt_fail(e);
-    w.side = ps->side;
-    w.shaded = ps->shaded;
-    w.shadowed = ps->shadowed;
-    if ((e = cudaMemsetAsync(w.totals, 0, 16, s)) != cudaSuccess) return pt_fail(e);
+    w[0].totals = w[1].totals = totals;
+    ps->d_totals = totals;
+    if ((e = cudaMemsetAsync(totals, 0, 16, s)) != cudaSuccess) return pt_fail(e);
 
     const sg::Cam cam = sg::make_camera(camera, width, height);
     const uint2 key = make_uint2((uint32_t)seed, (uint32_t)(seed >> 32));
@@ -489,10 +508,21 @@ extern "C" sg_status sg_pt_render_rows(sg_pt_scene* ps, const float* camera, int
     const int threads = 256;
     const int img_n = 3 * P;
     sg::k_zero<<<(img_n + threads - 1) / threads, threads, 0, s>>>(image, img_n);
-    for (int sample = 0; sample < spp; ++sample)
-        if ((e = sg::pt_wave(dev, base, tree, cam, width, height, p0, P, key, sample, max_depth, w, image, s)) !=
+    // The second stream starts after everything the caller put on `stream`.
+    if ((e = cudaEventRecord(ps->begun, s)) != cudaSuccess ||
+        (e = cudaStreamWaitEvent(ps->second, ps->begun, 0)) != cudaSuccess)
+        return pt_fail(e);
+    for (int sample = 0; sample < spp; ++sample) {
+        sg::PtWave& ws = w[sample % 2];
+        ws.flush_after = sample > 0 ? ps->flushed[(sample - 1) % 2] : nullptr;  // image sums in sample order
+        const cudaStream_t on = sample % 2 ? ps->second : s;
+        if ((e = sg::pt_wave(dev, base, tree, cam, width, height, p0, P, key, sample, max_depth, ws, image, on)) !=
             cudaSuccess)
             return pt_fail(e);
+    }
+    // Both streams' work is done before the scale: the last addition closes
+    // the chain, and the other stream's last sample precedes it.
+    if ((e = cudaStreamWaitEvent(s, ps->flushed[(spp - 1) % 2], 0)) != cudaSuccess) return pt_fail(e);
     sg::k_scale<<<(img_n + threads - 1) / threads, threads, 0, s>>>(image, img_n, 1.0f / (float)spp);
     if ((e = cudaGetLastError()) != cudaSuccess) return pt_fail(e);
     return SG_OK;

@@ -40,6 +40,10 @@ struct PtWave {
     // the next bounce's extension rays, with two events for the hand-offs.
     cudaStream_t side;
     cudaEvent_t shaded, shadowed;
+    // Optional: the radiance is added to the image only after `flush_after`
+    // (the previous sample's addition, when samples run on several streams),
+    // and `flush_done` is recorded after it.
+    cudaEvent_t flush_after, flush_done;
 };
 
 // Sample `sample` of pixels p0 .. p0 + n - 1 (n <= w.cap) of a width x height
