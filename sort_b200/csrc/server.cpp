@@ -42,6 +42,7 @@
 namespace {
 
 constexpr int kMaxScenes = 64;
+constexpr int kSoloLanes = 2;  // large requests rendered as whole-frame waves at once
 
 int64_t now_ns() {
     return std::chrono::duration_cast<std::chrono::nanoseconds>(std::chrono::steady_clock::now().time_since_epoch())
@@ -123,18 +124,30 @@ struct sg_server {
     std::vector<sg::SrvScene> scenes;
     std::vector<sg::TraceLaunch> launches;  // per scene, for the solo waves
     int64_t solo_pixels = 0;                // 0: no solo phase
-    struct {
+    // Solo lanes: each renders one large request as whole-frame waves
+    // (pt_wave), two samples in flight on its own buffer sets and stream
+    // pairs (sample k on [k % 2]), beside the pool's `stream`.
+    struct Lane {
         int64_t id = -1;  // ticket in its solo phase
         int next = 0;     // next sample to queue a wave for
         int done = 0;     // waves finished
         int last = 0;     // waves the phase may run (spp - 1)
-    } solo;
-    int64_t handoff = -1;  // ticket whose solo phase ended, to admit next
-    int handoff_sample = 0;  // its first sample for the pool
-    sg::PtWave solo_w{};     // the solo waves' own buffers (in d_solo)
+        sg::PtWave w[2] = {};
+        cudaStream_t stream[2] = {};   // the waves
+        cudaStream_t side[2] = {};     // their shadow rays (pt_wave.h)
+        cudaEvent_t flushed[2] = {};   // image additions, chained in sample order
+        cudaEvent_t wave_done[2] = {};
+        cudaEvent_t ready = nullptr;   // the ticket's image is zeroed
+        cudaEvent_t end = nullptr;     // its last wave is done
+    };
+    std::vector<Lane> lanes;
+    struct Handoff {
+        int64_t id;
+        int sample0;  // its first sample for the pool
+        int lane;     // whose `end` the pool waits for
+    };
+    std::vector<Handoff> handoffs;  // solo phases that ended, to admit next
     char* d_solo = nullptr;
-    cudaStream_t solo_stream = nullptr;  // the solo waves, beside the pool's `stream`
-    cudaStream_t solo_side = nullptr;    // the solo waves' shadow rays (pt_wave.h)
     // The bounce steps' side stream (continuation rays beside shadow rays,
     // serve_kernels.h) and its events; captured into the graph.
     cudaStream_t pool_side = nullptr;
@@ -155,7 +168,7 @@ struct sg_server {
     int* h_done[2] = {};
     sg::SrvCounters* h_counters[2] = {};
     cudaStream_t stream = nullptr, copy_stream = nullptr;
-    cudaEvent_t replay_done[2] = {}, copy_done = nullptr, solo_done[2] = {}, solo_ready = nullptr, solo_end = nullptr;
+    cudaEvent_t replay_done[2] = {}, copy_done = nullptr;
     cudaGraphExec_t graph = nullptr;
     int graph_stack = 0;
 };
@@ -172,20 +185,25 @@ void free_server(sg_server* S) {
         if (S->h_done[k]) cudaFreeHost(S->h_done[k]);
         if (S->h_counters[k]) cudaFreeHost(S->h_counters[k]);
         if (S->replay_done[k]) cudaEventDestroy(S->replay_done[k]);
-        if (S->solo_done[k]) cudaEventDestroy(S->solo_done[k]);
     }
     if (S->copy_done) cudaEventDestroy(S->copy_done);
-    if (S->solo_ready) cudaEventDestroy(S->solo_ready);
-    if (S->solo_end) cudaEventDestroy(S->solo_end);
-    if (S->solo_stream) cudaStreamSynchronize(S->solo_stream);
-    if (S->solo_stream) cudaStreamDestroy(S->solo_stream);
-    if (S->solo_side) cudaStreamSynchronize(S->solo_side);
-    if (S->solo_side) cudaStreamDestroy(S->solo_side);
+    for (sg_server::Lane& L : S->lanes) {
+        for (int k = 0; k < 2; ++k) {
+            for (cudaStream_t t : {L.stream[k], L.side[k]})
+                if (t) {
+                    cudaStreamSynchronize(t);
+                    cudaStreamDestroy(t);
+                }
+            for (cudaEvent_t ev : {L.w[k].shaded, L.w[k].shadowed, L.flushed[k], L.wave_done[k]})
+                if (ev) cudaEventDestroy(ev);
+        }
+        for (cudaEvent_t ev : {L.ready, L.end})
+            if (ev) cudaEventDestroy(ev);
+    }
     if (S->pool_side) cudaStreamDestroy(S->pool_side);
     if (S->pool_forked) cudaEventDestroy(S->pool_forked);
     if (S->pool_joined) cudaEventDestroy(S->pool_joined);
-    if (S->solo_w.shaded) cudaEventDestroy(S->solo_w.shaded);
-    if (S->solo_w.shadowed) cudaEventDestroy(S->solo_w.shadowed);
+
     if (S->d_solo) cudaFree(S->d_solo);
     if (S->h_requests) cudaFreeHost(S->h_requests);
     if (S->h_units) cudaFreeHost(S->h_units);
@@ -278,20 +296,31 @@ void enter_pool(sg_server* S, sg::SrvControl& ctl, int64_t id, int sample0, int6
     S->admitted++;
 }
 
-// Admits queued requests into the control block of the next replay (S->mu
-// held), after the request whose solo phase just ended.
+// A request the solo lanes take (large, two or more samples); it waits in the
+// queue for a free lane rather than entering the pool.
+bool solo_kind(const sg_server* S, const Ticket& t) {
+    return S->solo_pixels > 0 && int64_t(t.req.width) * t.req.height >= S->solo_pixels && t.req.spp >= 2;
+}
+
+// Admits into the control block of the next replay (S->mu held): first the
+// requests whose solo phase ended, then the queued requests the lanes do not
+// take, in queue order.
 void admit(sg_server* S, sg::SrvControl& ctl, int64_t replay) {
     ctl.nadmit = 0;
     ctl.admit_total = 0;
-    if (S->handoff >= 0) {  // after its last solo wave
-        cudaStreamWaitEvent(S->stream, S->solo_end, 0);
-        enter_pool(S, ctl, S->handoff, S->handoff_sample, replay);
-        S->handoff = -1;
+    for (const sg_server::Handoff& h : S->handoffs) {  // after each one's last solo wave
+        cudaStreamWaitEvent(S->stream, S->lanes[size_t(h.lane)].end, 0);
+        enter_pool(S, ctl, h.id, h.sample0, replay);
     }
-    while (!S->pending.empty() && ctl.nadmit < sg::kSrvMaxAdmit) {
-        const int64_t id = S->pending.front();
-        if (!reserve(S, id)) break;
-        S->pending.pop_front();
+    S->handoffs.clear();
+    for (auto it = S->pending.begin(); it != S->pending.end() && ctl.nadmit < sg::kSrvMaxAdmit;) {
+        const int64_t id = *it;
+        if (solo_kind(S, S->tickets[id])) {
+            ++it;
+            continue;
+        }
+        if (!reserve(S, id)) break;  // FIFO: wait for image memory
+        it = S->pending.erase(it);
         enter_pool(S, ctl, id, 0, replay);
     }
     for (int r : S->to_cancel) {
@@ -302,34 +331,46 @@ void admit(sg_server* S, sg::SrvControl& ctl, int64_t replay) {
     S->to_cancel.clear();
 }
 
-// Starts a solo phase for the queue head (S->mu held) when none is running
-// and the head is large with at least two samples: reserves it and makes the
-// solo stream wait for its zeroed image.
+// Gives each free lane the oldest queued request it takes (S->mu held):
+// reserves it and makes the lane's streams wait for its zeroed image.
 void start_solo(sg_server* S) {
-    if (S->solo.id >= 0 || S->handoff >= 0 || S->solo_pixels <= 0 || S->pending.empty()) return;
-    const int64_t id = S->pending.front();
-    const Ticket& t = S->tickets[id];
-    if (int64_t(t.req.width) * t.req.height < S->solo_pixels || t.req.spp < 2) return;
-    if (!reserve(S, id)) return;
-    S->pending.pop_front();
-    // Not in any replay until the hand-off: a completion flag read back for
-    // its table slot before then belongs to the slot's previous request.
-    S->tickets[id].replay = INT64_MAX;
-    cudaEventRecord(S->solo_ready, S->stream);
-    cudaStreamWaitEvent(S->solo_stream, S->solo_ready, 0);
-    S->solo.id = id;
-    S->solo.next = S->solo.done = 0;
-    S->solo.last = t.req.spp - 1;
+    for (size_t l = 0; l < S->lanes.size(); ++l) {
+        sg_server::Lane& L = S->lanes[l];
+        if (L.id >= 0) continue;
+        auto it = std::find_if(S->pending.begin(), S->pending.end(),
+                               [&](int64_t id) { return solo_kind(S, S->tickets[id]); });
+        if (it == S->pending.end()) return;
+        const int64_t id = *it;
+        if (!reserve(S, id)) return;
+        S->pending.erase(it);
+        Ticket& t = S->tickets[id];
+        // Not in any replay until the hand-off: a completion flag read back for
+        // its table slot before then belongs to the slot's previous request.
+        t.replay = INT64_MAX;
+        cudaEventRecord(L.ready, S->stream);
+        cudaStreamWaitEvent(L.stream[0], L.ready, 0);
+        cudaStreamWaitEvent(L.stream[1], L.ready, 0);
+        L.id = id;
+        L.next = L.done = 0;
+        L.last = t.req.spp - 1;
+    }
 }
 
-// Keeps two waves of the solo request queued on the solo stream; when its
-// waves up to the last sample are queued (or it is cancelled, or the server
-// stops) hands it to the pool from the next sample on.
-sg_status pump_solo(sg_server* S) {
-    if (S->solo.id < 0) return SG_OK;
+bool lanes_busy(const sg_server* S) {
+    for (const sg_server::Lane& L : S->lanes)
+        if (L.id >= 0) return true;
+    return false;
+}
+
+// Keeps two waves of a lane's request queued; when its waves up to the last
+// sample are queued (or it is cancelled, or the server stops) hands it to the
+// pool from the next sample on.
+sg_status pump_lane(sg_server* S, int l) {
+    sg_server::Lane& L = S->lanes[size_t(l)];
+    if (L.id < 0) return SG_OK;
     cudaError_t e = cudaSuccess;
-    while (S->solo.done < S->solo.next) {  // retire finished waves
-        e = cudaEventQuery(S->solo_done[S->solo.done % 2]);
+    while (L.done < L.next) {  // retire finished waves
+        e = cudaEventQuery(L.wave_done[L.done % 2]);
         if (e == cudaErrorNotReady) {
             // Not an error, but the runtime keeps it as the last error, which
             // the next launch check (cudaGetLastError) would report.
@@ -338,7 +379,7 @@ sg_status pump_solo(sg_server* S) {
             break;
         }
         if (e != cudaSuccess) return fail(SG_ERR_CUDA, std::string("solo wave: ") + cudaGetErrorString(e));
-        S->solo.done++;
+        L.done++;
     }
     sg::SrvRequest q;
     sg::SrvScene sc;
@@ -346,44 +387,54 @@ sg_status pump_solo(sg_server* S) {
     bool end = false;
     {
         std::lock_guard<std::mutex> lk(S->mu);  // add_scene may grow the scene tables meanwhile
-        const Ticket& t = S->tickets[S->solo.id];
+        const Ticket& t = S->tickets[L.id];
         q = S->h_requests[t.slot];
         sc = S->scenes[size_t(q.scene)];
         base = S->launches[size_t(q.scene)];
         end = S->stop || t.cancel;
     }
-    const int rows = std::max(1, S->solo_w.cap / q.width);  // rows per band: a band fits the wave buffers
-    while (!end && S->solo.next < S->solo.last && S->solo.next - S->solo.done < 2) {
-        const int k = S->solo.next;
+    const int rows = std::max(1, L.w[0].cap / q.width);  // rows per band: a band fits the wave buffers
+    while (!end && L.next < L.last && L.next - L.done < 2) {
+        // Sample k on buffer set and stream pair k % 2; its image additions
+        // wait for sample k - 1's.
+        const int k = L.next;
+        sg::PtWave w = L.w[k % 2];
+        w.flush_after = k > 0 ? L.flushed[(k - 1) % 2] : nullptr;
+        w.flush_done = L.flushed[k % 2];
+        const cudaStream_t on = L.stream[k % 2];
         for (int y = 0; y < q.height && e == cudaSuccess; y += rows) {
             const int y1 = std::min(q.height, y + rows);
             const int p0 = y * q.width;
             e = sg::pt_wave(sc.pt, base, sc.tree, q.cam, q.width, q.height, p0, (y1 - y) * q.width, q.key, k,
-                            q.max_depth, S->solo_w, q.image + 3 * int64_t(p0), S->solo_stream);
+                            q.max_depth, w, q.image + 3 * int64_t(p0), on);
         }
-        if (e == cudaSuccess) e = cudaEventRecord(S->solo_done[k % 2], S->solo_stream);
+        if (e == cudaSuccess) e = cudaEventRecord(L.wave_done[k % 2], on);
         if (e != cudaSuccess) return fail(SG_ERR_CUDA, std::string("solo wave: ") + cudaGetErrorString(e));
-        S->solo.next++;
+        L.next++;
         std::lock_guard<std::mutex> lk(S->mu);
         S->stats.solo_waves++;
     }
-    if (end || S->solo.next == S->solo.last) {
-        if ((e = cudaEventRecord(S->solo_end, S->solo_stream)) != cudaSuccess)
+    if (end || L.next == L.last) {
+        // after the last wave, whose additions came after every earlier one's
+        const cudaStream_t last = L.stream[L.next > 0 ? (L.next - 1) % 2 : 0];
+        if ((e = cudaEventRecord(L.end, last)) != cudaSuccess)
             return fail(SG_ERR_CUDA, std::string("solo handoff: ") + cudaGetErrorString(e));
         std::lock_guard<std::mutex> lk(S->mu);
-        S->handoff = S->solo.id;
-        S->handoff_sample = S->solo.next;
-        S->solo.id = -1;
+        S->handoffs.push_back({L.id, L.next, l});
+        L.id = -1;
     }
     return SG_OK;
 }
 
-// Blocks until the oldest queued solo wave has finished.
+// Blocks until the oldest queued wave of a busy lane has finished.
 sg_status wait_solo(sg_server* S) {
-    if (S->solo.id < 0 || S->solo.done >= S->solo.next) return SG_OK;
-    const cudaError_t e = cudaEventSynchronize(S->solo_done[S->solo.done % 2]);
-    if (e != cudaSuccess) return fail(SG_ERR_CUDA, std::string("solo wave: ") + cudaGetErrorString(e));
-    S->solo.done++;
+    for (sg_server::Lane& L : S->lanes) {
+        if (L.id < 0 || L.done >= L.next) continue;
+        const cudaError_t e = cudaEventSynchronize(L.wave_done[L.done % 2]);
+        if (e != cudaSuccess) return fail(SG_ERR_CUDA, std::string("solo wave: ") + cudaGetErrorString(e));
+        L.done++;
+        return SG_OK;
+    }
     return SG_OK;
 }
 
@@ -448,16 +499,17 @@ void serve_loop(sg_server* S) {
         bool launch = false;
         {
             std::unique_lock<std::mutex> lk(S->mu);
-            if (!inflight && S->solo.id < 0)
+            if (!inflight && !lanes_busy(S))
                 S->cv_work.wait(lk, [&] {
-                    return S->stop || !S->pending.empty() || S->admitted > 0 || S->handoff >= 0;
+                    return S->stop || !S->pending.empty() || S->admitted > 0 || !S->handoffs.empty();
                 });
             if (S->stop) break;
+            admit(S, *S->h_control[j % 2], j);  // hand-offs first: a lane may be reused next
             start_solo(S);
-            admit(S, *S->h_control[j % 2], j);
             launch = S->admitted > 0;
         }
-        if ((st = pump_solo(S)) != SG_OK) break;
+        for (int l = 0; l < int(S->lanes.size()) && st == SG_OK; ++l) st = pump_lane(S, l);
+        if (st != SG_OK) break;
         if (launch) {
             cudaError_t e = cudaSuccess;
             if ((st = capture(S)) != SG_OK) break;
@@ -484,7 +536,8 @@ void serve_loop(sg_server* S) {
         if (launch) ++j;
     }
     if (st == SG_OK && inflight) st = collect(S, int((j - 1) % 2), j - 1);
-    cudaStreamSynchronize(S->solo_stream);
+    for (const sg_server::Lane& L : S->lanes)
+        for (cudaStream_t t : L.stream) cudaStreamSynchronize(t);
     cudaStreamSynchronize(S->stream);
     std::lock_guard<std::mutex> lk(S->mu);
     if (st != SG_OK) {
@@ -635,58 +688,65 @@ sg_status sg_server_create(const sg_server_opts* opts, sg_server** out) {
         if (e == cudaSuccess) e = cudaMallocHost(&S->h_done[k], R * sizeof(int));
         if (e == cudaSuccess) e = cudaMallocHost(&S->h_counters[k], sizeof(sg::SrvCounters));
         if (e == cudaSuccess) e = cudaEventCreateWithFlags(&S->replay_done[k], cudaEventDisableTiming);
-        if (e == cudaSuccess) e = cudaEventCreateWithFlags(&S->solo_done[k], cudaEventDisableTiming);
     }
     if (e == cudaSuccess) e = cudaEventCreateWithFlags(&S->copy_done, cudaEventDisableTiming);
-    if (e == cudaSuccess) e = cudaEventCreateWithFlags(&S->solo_ready, cudaEventDisableTiming);
-    if (e == cudaSuccess) e = cudaEventCreateWithFlags(&S->solo_end, cudaEventDisableTiming);
     // The pool's steps and the solo waves share the GPU at equal priority
     // (giving the pool's stream the higher one measured a little worse p99).
     if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&S->stream, cudaStreamNonBlocking);
-    if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&S->solo_stream, cudaStreamNonBlocking);
     if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&S->pool_side, cudaStreamNonBlocking);
     if (e == cudaSuccess) e = cudaEventCreateWithFlags(&S->pool_forked, cudaEventDisableTiming);
     if (e == cudaSuccess) e = cudaEventCreateWithFlags(&S->pool_joined, cudaEventDisableTiming);
     if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&S->copy_stream, cudaStreamNonBlocking);
     if (e == cudaSuccess && S->solo_pixels > 0) {
-        // The solo waves' buffers (pt_wave.h), path_slots paths: extension
-        // queues, hits, the shadow queue (2 per path), flags, path state,
-        // counters and ray totals.
+        // Each lane's wave buffers (pt_wave.h), two sets of path_slots paths:
+        // extension queues, hits, the shadow queue (2 per path), flags, path
+        // state, counters; then the ray totals every set adds to.
+        S->lanes.resize(kSoloLanes);
         const size_t cap = C, scap = 2 * C;
         const size_t parts[] = {cap * 32, cap * 4, cap * 32, cap * 4, cap * 4, cap * 4, scap * 32, scap * 4,
-                                scap * 12, scap, cap * 24, cap * 24, 16, 16};
-        size_t bytes = 0;
-        for (size_t x : parts) bytes += align_up(x);
+                                scap * 12, scap, cap * 24, cap * 24, 16};
+        constexpr int kParts = int(sizeof(parts) / sizeof(parts[0]));
+        size_t set = 0;
+        for (size_t x : parts) set += align_up(x);
+        const size_t bytes = 2 * kSoloLanes * set + align_up(16);
         e = cudaMalloc(&S->d_solo, bytes);
         if (e == cudaSuccess) e = cudaMemset(S->d_solo, 0, bytes);
-        if (e == cudaSuccess) {
-            char* q = S->d_solo;
-            char* at[14];
-            for (int k = 0; k < 14; ++k) {
-                at[k] = q;
-                q += align_up(parts[k]);
+        char* q = S->d_solo;
+        for (sg_server::Lane& L : S->lanes) {
+            for (int k = 0; k < 2 && e == cudaSuccess; ++k) {
+                char* at[kParts];
+                for (int x = 0; x < kParts; ++x) {
+                    at[x] = q;
+                    q += align_up(parts[x]);
+                }
+                sg::PtWave& w = L.w[k];
+                w.qa_ray = reinterpret_cast<float*>(at[0]);
+                w.qa_slot = reinterpret_cast<int*>(at[1]);
+                w.qb_ray = reinterpret_cast<float*>(at[2]);
+                w.qb_slot = reinterpret_cast<int*>(at[3]);
+                w.hit_prim = reinterpret_cast<int32_t*>(at[4]);
+                w.hit_t = reinterpret_cast<float*>(at[5]);
+                w.sq_ray = reinterpret_cast<float*>(at[6]);
+                w.sq_slot = reinterpret_cast<int*>(at[7]);
+                w.sq_contrib = reinterpret_cast<float*>(at[8]);
+                w.occ = reinterpret_cast<uint8_t*>(at[9]);
+                w.thr = reinterpret_cast<float*>(at[10]);
+                w.vis = reinterpret_cast<float*>(at[11]);
+                w.counters = reinterpret_cast<int*>(at[12]);
+                w.cap = int(cap);
+                e = cudaStreamCreateWithFlags(&L.stream[k], cudaStreamNonBlocking);
+                if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&L.side[k], cudaStreamNonBlocking);
+                if (e == cudaSuccess) e = cudaEventCreateWithFlags(&w.shaded, cudaEventDisableTiming);
+                if (e == cudaSuccess) e = cudaEventCreateWithFlags(&w.shadowed, cudaEventDisableTiming);
+                if (e == cudaSuccess) e = cudaEventCreateWithFlags(&L.flushed[k], cudaEventDisableTiming);
+                if (e == cudaSuccess) e = cudaEventCreateWithFlags(&L.wave_done[k], cudaEventDisableTiming);
+                w.side = L.side[k];
             }
-            sg::PtWave& w = S->solo_w;
-            w.qa_ray = reinterpret_cast<float*>(at[0]);
-            w.qa_slot = reinterpret_cast<int*>(at[1]);
-            w.qb_ray = reinterpret_cast<float*>(at[2]);
-            w.qb_slot = reinterpret_cast<int*>(at[3]);
-            w.hit_prim = reinterpret_cast<int32_t*>(at[4]);
-            w.hit_t = reinterpret_cast<float*>(at[5]);
-            w.sq_ray = reinterpret_cast<float*>(at[6]);
-            w.sq_slot = reinterpret_cast<int*>(at[7]);
-            w.sq_contrib = reinterpret_cast<float*>(at[8]);
-            w.occ = reinterpret_cast<uint8_t*>(at[9]);
-            w.thr = reinterpret_cast<float*>(at[10]);
-            w.vis = reinterpret_cast<float*>(at[11]);
-            w.counters = reinterpret_cast<int*>(at[12]);
-            w.totals = reinterpret_cast<unsigned long long*>(at[13]);
-            w.cap = int(cap);
-            e = cudaStreamCreateWithFlags(&S->solo_side, cudaStreamNonBlocking);
-            if (e == cudaSuccess) e = cudaEventCreateWithFlags(&w.shaded, cudaEventDisableTiming);
-            if (e == cudaSuccess) e = cudaEventCreateWithFlags(&w.shadowed, cudaEventDisableTiming);
-            w.side = S->solo_side;
+            if (e == cudaSuccess) e = cudaEventCreateWithFlags(&L.ready, cudaEventDisableTiming);
+            if (e == cudaSuccess) e = cudaEventCreateWithFlags(&L.end, cudaEventDisableTiming);
         }
+        if (e == cudaSuccess)
+            for (sg_server::Lane& L : S->lanes) L.w[0].totals = L.w[1].totals = reinterpret_cast<unsigned long long*>(q);
     }
     if (prev >= 0) cudaSetDevice(prev);
     if (e != cudaSuccess) {
@@ -799,13 +859,13 @@ sg_status sg_server_stats_get(sg_server* S, sg_server_stats* out) {
     std::lock_guard<std::mutex> lk(S->mu);
     *out = S->stats;
     out->queued = int64_t(S->pending.size());
-    out->admitted = S->admitted + (S->solo.id >= 0 ? 1 : 0);
-    if (S->solo_w.totals) {  // rays of the solo waves (a snapshot while they run)
+    for (const sg_server::Lane& L : S->lanes) out->admitted += L.id >= 0 ? 1 : 0;
+    if (!S->lanes.empty() && S->lanes[0].w[0].totals) {  // rays of the solo waves (a snapshot while they run)
         unsigned long long h[2] = {0, 0};
         int prev = -1;
         cudaGetDevice(&prev);
         cudaSetDevice(S->opts.device);
-        if (cudaMemcpy(h, S->solo_w.totals, sizeof(h), cudaMemcpyDeviceToHost) == cudaSuccess) {
+        if (cudaMemcpy(h, S->lanes[0].w[0].totals, sizeof(h), cudaMemcpyDeviceToHost) == cudaSuccess) {
             out->extension_rays += int64_t(h[0]);
             out->shadow_rays += int64_t(h[1]);
         }
