@@ -846,7 +846,7 @@ def run_serve(args):
             "config": serve_config({"requests": len(reqs), "seed": args.batch_seed, "scene_triangles": tri_counts,
                                     "path_slots": args.path_slots, "samples_per_claim": args.samples_per_claim,
                                     "steps_per_poll": args.steps_per_poll,
-                                    "solo_pixels": (args.solo_pixels or args.path_slots // 16) if args.solo_pixels >= 0 else None,
+                                    "solo_pixels": (args.solo_pixels or 1) if args.solo_pixels >= 0 else None,
                                     "samples_per_run": int(work)}),
             "closed_loop": {"server": {"msamples_s": round(value, 2), "p50_ms": pct(srv_lat0, 50),
                                        "p99_ms": pct(srv_lat0, 99)},
@@ -1004,8 +1004,8 @@ def main():
     p.add_argument("--steps-per-poll", type=int, default=2,
                    help="serve workload: bounce steps per graph replay (even)")
     p.add_argument("--solo-pixels", type=int, default=0,
-                   help="serve workload: requests this large render as whole-frame waves beside the pool "
-                        "(0: path slots / 16, -1: never)")
+                   help="serve workload: multi-sample requests this large render in the solo lanes as "
+                        "whole-frame waves (0: every one, -1: never)")
     p.add_argument("--loads", type=float, nargs="*", default=[0.5, 0.8, 1.0],
                    help="serve workload: Poisson arrival rates as fractions of the FIFO arm's capacity")
     p.add_argument("--batches", type=int, default=64, help="batched workload: ray batches per step")

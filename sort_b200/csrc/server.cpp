@@ -133,8 +133,12 @@ struct sg_server {
         int done = 0;     // waves finished
         int last = 0;     // waves the phase may run (spp - 1)
         sg::PtWave w[2] = {};
-        cudaStream_t stream[2] = {};   // the waves
-        cudaStream_t side[2] = {};     // their shadow rays (pt_wave.h)
+        // The waves and their shadow rays (pt_wave.h), [priority][sample % 2]:
+        // the lane holding the oldest request queues its waves on the
+        // high-priority streams, the others (and the pool) on normal ones.
+        cudaStream_t stream[2][2] = {};
+        cudaStream_t side[2][2] = {};
+        cudaStream_t last_on = nullptr;  // the stream of the newest wave
         cudaEvent_t flushed[2] = {};   // image additions, chained in sample order
         cudaEvent_t wave_done[2] = {};
         cudaEvent_t ready = nullptr;   // the ticket's image is zeroed
@@ -189,7 +193,7 @@ void free_server(sg_server* S) {
     if (S->copy_done) cudaEventDestroy(S->copy_done);
     for (sg_server::Lane& L : S->lanes) {
         for (int k = 0; k < 2; ++k) {
-            for (cudaStream_t t : {L.stream[k], L.side[k]})
+            for (cudaStream_t t : {L.stream[0][k], L.stream[1][k], L.side[0][k], L.side[1][k]})
                 if (t) {
                     cudaStreamSynchronize(t);
                     cudaStreamDestroy(t);
@@ -348,8 +352,8 @@ void start_solo(sg_server* S) {
         // its table slot before then belongs to the slot's previous request.
         t.replay = INT64_MAX;
         cudaEventRecord(L.ready, S->stream);
-        cudaStreamWaitEvent(L.stream[0], L.ready, 0);
-        cudaStreamWaitEvent(L.stream[1], L.ready, 0);
+        for (auto& pair : L.stream)
+            for (cudaStream_t t : pair) cudaStreamWaitEvent(t, L.ready, 0);
         L.id = id;
         L.next = L.done = 0;
         L.last = t.req.spp - 1;
@@ -384,7 +388,7 @@ sg_status pump_lane(sg_server* S, int l) {
     sg::SrvRequest q;
     sg::SrvScene sc;
     sg::TraceLaunch base;
-    bool end = false;
+    bool end = false, oldest = true;
     {
         std::lock_guard<std::mutex> lk(S->mu);  // add_scene may grow the scene tables meanwhile
         const Ticket& t = S->tickets[L.id];
@@ -392,6 +396,11 @@ sg_status pump_lane(sg_server* S, int l) {
         sc = S->scenes[size_t(q.scene)];
         base = S->launches[size_t(q.scene)];
         end = S->stop || t.cancel;
+        for (const sg_server::Lane& o : S->lanes)  // an older request in another lane
+            if (o.id >= 0 && o.id != L.id) {
+                const Ticket& u = S->tickets[o.id];
+                if (u.submit_ns < t.submit_ns || (u.submit_ns == t.submit_ns && o.id < L.id)) oldest = false;
+            }
     }
     const int rows = std::max(1, L.w[0].cap / q.width);  // rows per band: a band fits the wave buffers
     while (!end && L.next < L.last && L.next - L.done < 2) {
@@ -401,7 +410,9 @@ sg_status pump_lane(sg_server* S, int l) {
         sg::PtWave w = L.w[k % 2];
         w.flush_after = k > 0 ? L.flushed[(k - 1) % 2] : nullptr;
         w.flush_done = L.flushed[k % 2];
-        const cudaStream_t on = L.stream[k % 2];
+        const int prio = oldest ? 0 : 1;
+        const cudaStream_t on = L.stream[prio][k % 2];
+        w.side = L.side[prio][k % 2];
         for (int y = 0; y < q.height && e == cudaSuccess; y += rows) {
             const int y1 = std::min(q.height, y + rows);
             const int p0 = y * q.width;
@@ -410,13 +421,14 @@ sg_status pump_lane(sg_server* S, int l) {
         }
         if (e == cudaSuccess) e = cudaEventRecord(L.wave_done[k % 2], on);
         if (e != cudaSuccess) return fail(SG_ERR_CUDA, std::string("solo wave: ") + cudaGetErrorString(e));
+        L.last_on = on;
         L.next++;
         std::lock_guard<std::mutex> lk(S->mu);
         S->stats.solo_waves++;
     }
     if (end || L.next == L.last) {
         // after the last wave, whose additions came after every earlier one's
-        const cudaStream_t last = L.stream[L.next > 0 ? (L.next - 1) % 2 : 0];
+        const cudaStream_t last = L.next > 0 ? L.last_on : L.stream[1][0];
         if ((e = cudaEventRecord(L.end, last)) != cudaSuccess)
             return fail(SG_ERR_CUDA, std::string("solo handoff: ") + cudaGetErrorString(e));
         std::lock_guard<std::mutex> lk(S->mu);
@@ -537,7 +549,8 @@ void serve_loop(sg_server* S) {
     }
     if (st == SG_OK && inflight) st = collect(S, int((j - 1) % 2), j - 1);
     for (const sg_server::Lane& L : S->lanes)
-        for (cudaStream_t t : L.stream) cudaStreamSynchronize(t);
+        for (const auto& pair : L.stream)
+            for (cudaStream_t t : pair) cudaStreamSynchronize(t);
     cudaStreamSynchronize(S->stream);
     std::lock_guard<std::mutex> lk(S->mu);
     if (st != SG_OK) {
@@ -587,7 +600,7 @@ sg_status sg_server_create(const sg_server_opts* opts, sg_server** out) {
     sg_server* S = new (std::nothrow) sg_server;
     if (!S) return fail(SG_ERR_OUT_OF_MEMORY, "host allocation failed");
     S->opts = o;
-    S->solo_pixels = o.solo_pixels < 0 ? 0 : o.solo_pixels > 0 ? o.solo_pixels : std::max<int64_t>(1, o.path_slots / 16);
+    S->solo_pixels = o.solo_pixels < 0 ? 0 : o.solo_pixels > 0 ? o.solo_pixels : int64_t(1);
     S->arena = Arena(o.pixel_budget);
     S->slot_ticket.assign(size_t(o.max_requests), -1);
     for (int r = o.max_requests - 1; r >= 0; --r) S->free_slots.push_back(r);
@@ -690,8 +703,9 @@ sg_status sg_server_create(const sg_server_opts* opts, sg_server** out) {
         if (e == cudaSuccess) e = cudaEventCreateWithFlags(&S->replay_done[k], cudaEventDisableTiming);
     }
     if (e == cudaSuccess) e = cudaEventCreateWithFlags(&S->copy_done, cudaEventDisableTiming);
-    // The pool's steps and the solo waves share the GPU at equal priority
-    // (giving the pool's stream the higher one measured a little worse p99).
+    // Stream priorities: the oldest lane's waves above everything else.
+    int least = 0, greatest = 0;
+    if (e == cudaSuccess) e = cudaDeviceGetStreamPriorityRange(&least, &greatest);
     if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&S->stream, cudaStreamNonBlocking);
     if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&S->pool_side, cudaStreamNonBlocking);
     if (e == cudaSuccess) e = cudaEventCreateWithFlags(&S->pool_forked, cudaEventDisableTiming);
@@ -734,13 +748,16 @@ sg_status sg_server_create(const sg_server_opts* opts, sg_server** out) {
                 w.vis = reinterpret_cast<float*>(at[11]);
                 w.counters = reinterpret_cast<int*>(at[12]);
                 w.cap = int(cap);
-                e = cudaStreamCreateWithFlags(&L.stream[k], cudaStreamNonBlocking);
-                if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&L.side[k], cudaStreamNonBlocking);
+                for (int pr = 0; pr < 2 && e == cudaSuccess; ++pr) {
+                    const int level = pr == 0 ? greatest : least;
+                    e = cudaStreamCreateWithPriority(&L.stream[pr][k], cudaStreamNonBlocking, level);
+                    if (e == cudaSuccess) e = cudaStreamCreateWithPriority(&L.side[pr][k], cudaStreamNonBlocking, level);
+                }
                 if (e == cudaSuccess) e = cudaEventCreateWithFlags(&w.shaded, cudaEventDisableTiming);
                 if (e == cudaSuccess) e = cudaEventCreateWithFlags(&w.shadowed, cudaEventDisableTiming);
                 if (e == cudaSuccess) e = cudaEventCreateWithFlags(&L.flushed[k], cudaEventDisableTiming);
                 if (e == cudaSuccess) e = cudaEventCreateWithFlags(&L.wave_done[k], cudaEventDisableTiming);
-                w.side = L.side[k];
+                w.side = L.side[1][k];
             }
             if (e == cudaSuccess) e = cudaEventCreateWithFlags(&L.ready, cudaEventDisableTiming);
             if (e == cudaSuccess) e = cudaEventCreateWithFlags(&L.end, cudaEventDisableTiming);

@@ -29,8 +29,9 @@ class RenderServer:
     def __init__(self, device: int = 0, path_slots: int = 1 << 20, pixel_budget: int = 1 << 24,
                  max_requests: int = 1024, steps_per_poll: int = 4, samples_per_claim: int = 1,
                  solo_pixels: int = 0):
-        """solo_pixels: requests of at least this many pixels render as
-        whole-frame waves beside the pool (0: path_slots / 16, < 0: never)."""
+        """solo_pixels: multi-sample requests of at least this many pixels
+        render in the solo lanes as whole-frame waves (0: every one, < 0:
+        never); the pool renders the rest."""
         o = _lib.ServerOpts()
         _lib.load().sg_default_server_opts(ctypes.byref(o))
         o.device, o.path_slots, o.pixel_budget = int(device), int(path_slots), int(pixel_budget)
