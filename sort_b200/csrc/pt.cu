@@ -170,13 +170,15 @@ struct sg_pt_scene {
     void* d_buf = nullptr;
     size_t buf_bytes = 0;
     unsigned long long* d_totals = nullptr;  // rays traced by the last render: extension, shadow
-    // Two samples are in flight at once, each with its own buffers: sample k
-    // runs on the caller's stream (k even) or on `second` (k odd), its shadow
-    // rays on side[k % 2] (pt_wave.h); the events order the hand-offs and the
-    // image additions. Made by the first render.
-    cudaStream_t second = nullptr;
-    cudaStream_t side[2] = {};
-    cudaEvent_t shaded[2] = {}, shadowed[2] = {}, flushed[2] = {}, begun = nullptr;
+    // kInFlight samples are in flight at once, each with its own buffers:
+    // sample k runs on the caller's stream (k % kInFlight == 0) or on
+    // extra[k % kInFlight], its shadow rays on side[k % kInFlight]
+    // (pt_wave.h); the events order the hand-offs and the image additions.
+    // Made by the first render.
+    cudaStream_t extra[sg::kInFlight] = {};  // [0] unused: the caller's stream
+    cudaStream_t side[sg::kInFlight] = {};
+    cudaEvent_t shaded[sg::kInFlight] = {}, shadowed[sg::kInFlight] = {}, flushed[sg::kInFlight] = {};
+    cudaEvent_t begun = nullptr;
 };
 
 extern "C" sg_status sg_pt_ray_counts(const sg_pt_scene* ps, int64_t* extension, int64_t* shadow, void* stream) {
@@ -312,14 +314,15 @@ extern "C" sg_status sg_pt_destroy(sg_pt_scene* ps) {
     if (ps->d_prim) cudaFree(ps->d_prim);
     if (ps->d_mats) cudaFree(ps->d_mats);
     if (ps->d_buf) cudaFree(ps->d_buf);
-    for (cudaStream_t t : {ps->second, ps->side[0], ps->side[1]})
-        if (t) {
-            cudaStreamSynchronize(t);
-            cudaStreamDestroy(t);
-        }
-    for (int k = 0; k < 2; ++k)
+    for (int k = 0; k < sg::kInFlight; ++k) {
+        for (cudaStream_t t : {ps->extra[k], ps->side[k]})
+            if (t) {
+                cudaStreamSynchronize(t);
+                cudaStreamDestroy(t);
+            }
         for (cudaEvent_t ev : {ps->shaded[k], ps->shadowed[k], ps->flushed[k]})
             if (ev) cudaEventDestroy(ev);
+    }
     if (ps->begun) cudaEventDestroy(ps->begun);
     if (prev >= 0) cudaSetDevice(prev);
     delete ps;
@@ -444,7 +447,7 @@ extern "C" sg_status sg_pt_render_rows(sg_pt_scene* ps, const float* camera, int
     } restore{prev};
     cudaStream_t s = (cudaStream_t)stream;
 
-    // Buffers, twice (two samples in flight): two extension queues (rays +
+    // Buffers, kInFlight times (samples in flight): two extension queues (rays +
     // slots), hits, one shadow queue of 2 entries per path (rays + slots +
     // contributions), occlusion flags, throughput, shadow results, 4
     // counters; then the shared ray totals.
@@ -453,7 +456,7 @@ extern "C" sg_status sg_pt_render_rows(sg_pt_scene* ps, const float* camera, int
     const size_t qbytes = align(cap * 8 * 4) + align(cap * 4);
     const size_t set = 2 * qbytes + align(cap * 4) * 2 + align(scap * 8 * 4) + align(scap * 4) +
                        align(scap * 3 * 4) + align(scap) + align(cap * 6 * 4) + align(cap * 6 * 4) + align(16);
-    const size_t need = 2 * set + align(16);
+    const size_t need = sg::kInFlight * set + align(16);
     if (ps->buf_bytes < need) {
         if (ps->d_buf) cudaFree(ps->d_buf);
         ps->d_buf = nullptr;
@@ -468,15 +471,17 @@ extern "C" sg_status sg_pt_render_rows(sg_pt_scene* ps, const float* camera, int
         return r;
     };
     bool made = true;
-    for (cudaStream_t* t : {&ps->second, &ps->side[0], &ps->side[1]})
-        made = made && (*t || cudaStreamCreateWithFlags(t, cudaStreamNonBlocking) == cudaSuccess);
-    for (int k = 0; k < 2; ++k)
+    for (int k = 0; k < sg::kInFlight; ++k) {
+        for (cudaStream_t* t : {&ps->extra[k], &ps->side[k]})
+            if (t != &ps->extra[0])
+                made = made && (*t || cudaStreamCreateWithFlags(t, cudaStreamNonBlocking) == cudaSuccess);
         for (cudaEvent_t* ev : {&ps->shaded[k], &ps->shadowed[k], &ps->flushed[k]})
             made = made && (*ev || cudaEventCreateWithFlags(ev, cudaEventDisableTiming) == cudaSuccess);
+    }
     made = made && (ps->begun || cudaEventCreateWithFlags(&ps->begun, cudaEventDisableTiming) == cudaSuccess);
     if (!made) return sg::set_error(SG_ERR_CUDA, "render streams and events");
-    sg::PtWave w[2] = {};
-    for (int k = 0; k < 2; ++k) {
+    sg::PtWave w[sg::kInFlight] = {};
+    for (int k = 0; k < sg::kInFlight; ++k) {
         w[k].qa_ray = (float*)take(cap * 32);
         w[k].qa_slot = (int*)take(cap * 4);
         w[k].qb_ray = (float*)take(cap * 32);
@@ -498,7 +503,7 @@ extern "C" sg_status sg_pt_render_rows(sg_pt_scene* ps, const float* camera, int
     }
     unsigned long long* totals = (unsigned long long*)take(16);  // rays traced: extension, shadow
     if ((size_t)(b - (char*)ps->d_buf) > need) return sg::set_error(SG_ERR_INTERNAL, "render buffer layout overflow");
-    w[0].totals = w[1].totals = totals;
+    for (sg::PtWave& x : w) x.totals = totals;
     ps->d_totals = totals;
     if ((e = cudaMemsetAsync(totals, 0, 16, s)) != cudaSuccess) return pt_fail(e);
 
@@ -508,21 +513,22 @@ extern "C" sg_status sg_pt_render_rows(sg_pt_scene* ps, const float* camera, int
     const int threads = 256;
     const int img_n = 3 * P;
     sg::k_zero<<<(img_n + threads - 1) / threads, threads, 0, s>>>(image, img_n);
-    // The second stream starts after everything the caller put on `stream`.
-    if ((e = cudaEventRecord(ps->begun, s)) != cudaSuccess ||
-        (e = cudaStreamWaitEvent(ps->second, ps->begun, 0)) != cudaSuccess)
-        return pt_fail(e);
+    // The other streams start after everything the caller put on `stream`.
+    if ((e = cudaEventRecord(ps->begun, s)) != cudaSuccess) return pt_fail(e);
+    for (int k = 1; k < sg::kInFlight; ++k)
+        if ((e = cudaStreamWaitEvent(ps->extra[k], ps->begun, 0)) != cudaSuccess) return pt_fail(e);
     for (int sample = 0; sample < spp; ++sample) {
-        sg::PtWave& ws = w[sample % 2];
-        ws.flush_after = sample > 0 ? ps->flushed[(sample - 1) % 2] : nullptr;  // image sums in sample order
-        const cudaStream_t on = sample % 2 ? ps->second : s;
+        const int set = sample % sg::kInFlight;
+        sg::PtWave& ws = w[set];
+        ws.flush_after = sample > 0 ? ps->flushed[(sample - 1) % sg::kInFlight] : nullptr;  // image sums in order
+        const cudaStream_t on = set ? ps->extra[set] : s;
         if ((e = sg::pt_wave(dev, base, tree, cam, width, height, p0, P, key, sample, max_depth, ws, image, on)) !=
             cudaSuccess)
             return pt_fail(e);
     }
-    // Both streams' work is done before the scale: the last addition closes
-    // the chain, and the other stream's last sample precedes it.
-    if ((e = cudaStreamWaitEvent(s, ps->flushed[(spp - 1) % 2], 0)) != cudaSuccess) return pt_fail(e);
+    // Every stream's work is done before the scale: the last addition closes
+    // the chain, and every other stream's last sample precedes it.
+    if ((e = cudaStreamWaitEvent(s, ps->flushed[(spp - 1) % sg::kInFlight], 0)) != cudaSuccess) return pt_fail(e);
     sg::k_scale<<<(img_n + threads - 1) / threads, threads, 0, s>>>(image, img_n, 1.0f / (float)spp);
     if ((e = cudaGetLastError()) != cudaSuccess) return pt_fail(e);
     return SG_OK;

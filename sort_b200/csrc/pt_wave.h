@@ -13,6 +13,9 @@
 
 namespace sg {
 
+// Samples sg_pt_render keeps in flight, each on its own buffers and streams.
+constexpr int kInFlight = 2;
+
 // Device buffers of a wave, with the layouts the server's pool uses: two
 // extension queues (8 floats per ray with stride cap, a path index per
 // entry), the hits (cap each), the shadow queue (stride 2 * cap, three
