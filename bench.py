@@ -969,7 +969,9 @@ def run_build(args):
         "config": build_config({"depth": info["depth"], "interior_nodes": info["interior_nodes"],
                                 "leaves": info["leaves"], "rounds": info["build_rounds"]}, args.builder or "gpu"),
         "e2e": {"value": round(world * n / mean_create / 1e6, 3), "unit": "Mtriangles/s",
-                "h2d_bytes_per_step": int(n * 36 + (0 if lbvh else node_bytes)),
+                # the triangles; the host builder's nodes, or the GPU builder's node map (8 B per node)
+                "h2d_bytes_per_step": int(n * 36 + (0 if lbvh else node_bytes if (args.builder or "gpu") == "host"
+                                                    else 8 * info["interior_nodes"])),
                 "d2h_bytes_per_step": int(16 * info["build_rounds"] if lbvh else n * 4 + shapes * 40)},
         "gpu_launches": info["build_launches"] * args.steps,
         "roofline": None,

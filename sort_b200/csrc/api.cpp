@@ -102,7 +102,11 @@ sg_status upload(sg_scene* s, const float* tri, int64_t ntri, const std::vector<
     const int f4 = W == 8 ? sg::NodeShape<8>::kF4 : sg::NodeShape<4>::kF4;
     const int64_t nn = t.interior();
     std::vector<float4> nodes;
-    const bool adopt = t.d_nodes != nullptr;  // a Morton-order builder wrote the nodes on the device
+    if (t.d_nodes && s->node_format != SG_NODES_FP32 && t.host_arrays()) {  // 8-bit nodes come from the host arrays
+        cudaFree(t.d_nodes);
+        s->tree.d_nodes = nullptr;
+    }
+    const bool adopt = t.d_nodes != nullptr;  // a GPU builder wrote the nodes on the device
     if (adopt) {
     } else if (s->node_format == SG_NODES_QUANT8) {
         sg::quantize_nodes(t, nodes);
@@ -403,6 +407,7 @@ sg_status scene_create_mixed(const MixedInput& in, const sg_build_opts* opts, sg
     bp.max_depth = opts->max_depth;
     bp.max_leaf = opts->max_leaf;
     bp.threads = opts->build_threads;
+    bp.host_boxes = opts->node_format != SG_NODES_FP32;
     std::vector<float> recs;
     const auto t0 = std::chrono::steady_clock::now();
     try {

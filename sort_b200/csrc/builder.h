@@ -41,6 +41,9 @@ struct BuildParams {
     // split rules see every primitive as its box and the box centre.
     const float* extra_boxes = nullptr;
     int64_t nextra = 0;
+    // build_tree_gpu: also fill the host arrays lo / hi (the FP32 nodes are
+    // written on the device either way; 8-bit nodes are made from lo / hi).
+    bool host_boxes = true;
 };
 
 // Flat tree. Interior node k owns child[k*W + j] and, for child j on axis a,
@@ -62,10 +65,11 @@ struct BuiltTree {
     // (layout.h), leaf order plus the zero pad slots, already on the build's
     // device. The receiver owns it (cudaFree).
     float4* d_tris = nullptr;
-    // Set by build_tree_lbvh and build_tree_ploc only: the interior nodes already in the device
-    // layout (layout.h, FP32 boxes), n_interior of them, owned like d_tris. Its
-    // host arrays (child, lo, hi, first_interior, order, leaf_last) stay empty;
-    // n_tri and n_interior give the sizes.
+    // The interior nodes already in the device layout (layout.h, FP32 boxes),
+    // owned like d_tris. Set by build_tree_lbvh and build_tree_ploc, whose host
+    // arrays (child, lo, hi, first_interior, order, leaf_last) stay empty
+    // (n_tri and n_interior give the sizes), and by build_tree_gpu beside its
+    // host arrays (a scene with 8-bit nodes converts those instead).
     float4* d_nodes = nullptr;
     int64_t n_interior = -1, n_tri = -1;
     // Primitives from first_extra on are not triangles (hair lines, then from

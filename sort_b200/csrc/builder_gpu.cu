@@ -39,6 +39,7 @@
 #include <cfloat>
 #include <cstdint>
 #include <cstring>
+#include <memory>
 #include <mutex>
 #include <stdexcept>
 #include <string>
@@ -78,6 +79,28 @@ cudaMemPool_t scratch_pool(int device) {
 }
 
 thread_local Scratch scratch;
+
+namespace {
+
+// Pinned host memory the GPU builds of a device read their results into,
+// kept between builds (pinning 130 MB anew costs about 200 ms); one build at
+// a time per device holds it.
+struct Staging {
+    std::mutex lock;
+    void* p = nullptr;
+    size_t bytes = 0;
+};
+
+Staging& staging(int device) {
+    static std::mutex lock;
+    static std::vector<std::unique_ptr<Staging>> all;
+    std::lock_guard<std::mutex> g(lock);
+    if (all.size() <= size_t(device)) all.resize(size_t(device) + 1);
+    if (!all[size_t(device)]) all[size_t(device)] = std::make_unique<Staging>();
+    return *all[size_t(device)];
+}
+
+}  // namespace
 
 }  // namespace gpub
 namespace {
@@ -597,6 +620,41 @@ __global__ void k_node_commit(const BuildState* __restrict__ bs, const DNode* __
     }
 }
 
+// Interior node k of the flattened tree in the device layout (layout.h, FP32
+// boxes), from its shape: children in shape order, a leaf child as its first
+// leaf slot, an interior child as base[k] plus its rank among the interior
+// children (the host's numbering), empty slots with SORT's empty box.
+template <int W>
+__global__ void k_write_nodes(int64_t nodes, const DShape* __restrict__ shapes, const int32_t* __restrict__ shape_of,
+                              const int32_t* __restrict__ base, float4* __restrict__ out) {
+    const int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= nodes) return;
+    constexpr int Q = W / 4;
+    constexpr int F4 = W == 8 ? NodeShape<8>::kF4 : NodeShape<4>::kF4;
+    const DShape sn = shapes[shape_of[k]];
+    float* node = reinterpret_cast<float*>(out + k * F4);
+    int32_t* ch = reinterpret_cast<int32_t*>(node + 6 * Q * 4);
+    int inner = 0;
+    for (int j = 0; j < W; ++j) {
+        if (j >= sn.nkids) {
+            for (int a = 0; a < 3; ++a) {
+                node[(2 * a) * Q * 4 + j] = FLT_MAX;
+                node[(2 * a + 1) * Q * 4 + j] = -FLT_MAX;
+            }
+            ch[j] = kEmptyRef;
+            continue;
+        }
+        const DShape kid = shapes[sn.first_kid + j];
+        for (int a = 0; a < 3; ++a) {
+            node[(2 * a) * Q * 4 + j] = kid.mn[a];
+            node[(2 * a + 1) * Q * 4 + j] = kid.mx[a];
+        }
+        ch[j] = kid.nkids == 0 ? int32_t(uint32_t(kid.off) | 0x80000000u) : base[k] + inner++;
+    }
+    if (W == 4)  // the layout's padding
+        for (int x = 28; x < 32; ++x) node[x] = 0.0f;
+}
+
 __global__ void k_advance(BuildState* __restrict__ bs) {
     if (bs->na > 0) ++bs->rounds;
     bs->shapes += bs->new_shapes;
@@ -792,57 +850,71 @@ BuiltTree build_tree_gpu(const float* tri, int64_t ntri, const BuildParams& p, i
     const int shape_count = fin.shapes;
     t.depth = fin.depth_max;
 
-    // Shapes and the final permutation (leaf order) to the host.
-    std::vector<DShape> shape(static_cast<size_t>(shape_count));
-    std::vector<int32_t> order(static_cast<size_t>(n));
-    check(cudaMemcpyAsync(shape.data(), d_shapes.p, shape.size() * sizeof(DShape), cudaMemcpyDeviceToHost, st),
+    // Shapes and the final permutation (leaf order) to the host, through the
+    // device's pinned staging memory (pageable copies of these 130 MB cost
+    // about 100 ms).
+    Staging& stage = staging(device);
+    std::lock_guard<std::mutex> stage_lock(stage.lock);
+    const size_t shape_bytes = (size_t(shape_count) * sizeof(DShape) + 255) & ~size_t(255);
+    const size_t stage_bytes = shape_bytes + size_t(n) * 4;
+    if (stage.bytes < stage_bytes) {
+        if (stage.p) cudaFreeHost(stage.p);
+        stage.p = nullptr;
+        stage.bytes = 0;
+        check(cudaMallocHost(&stage.p, stage_bytes), "cudaMallocHost(staging)");
+        stage.bytes = stage_bytes;
+    }
+    const DShape* shape = static_cast<const DShape*>(stage.p);
+    const int32_t* h_order = reinterpret_cast<const int32_t*>(static_cast<const char*>(stage.p) + shape_bytes);
+    check(cudaMemcpyAsync(stage.p, d_shapes.p, size_t(shape_count) * sizeof(DShape), cudaMemcpyDeviceToHost, st),
           "shapes");
-    check(cudaMemcpyAsync(order.data(), d_idx.p, size_t(n) * 4, cudaMemcpyDeviceToHost, st), "order");
+    check(cudaMemcpyAsync(const_cast<int32_t*>(h_order), d_idx.p, size_t(n) * 4, cudaMemcpyDeviceToHost, st),
+          "order");
     check(cudaStreamSynchronize(st), "download");
+    t.order.assign(h_order, h_order + n);
     t.leaf_last.assign(size_t(n), 0);
-    t.order.swap(order);
     // Flatten exactly as build_tree numbers nodes: a node allocates its interior
-    // children consecutively when it is filled, then fills them in order.
+    // children consecutively when it is filled, then fills them in order. The
+    // arrays are sized once (the interior count is known), then filled.
     size_t interior_total = 0;
-    for (const DShape& sn : shape) interior_total += sn.nkids ? 1 : 0;
-    t.first_interior.reserve(interior_total);
-    t.child.reserve(interior_total * W);
-    t.lo.reserve(interior_total * 3 * W);
-    t.hi.reserve(interior_total * 3 * W);
-    auto alloc = [&](int cnt) {
-        const int32_t base = int32_t(t.first_interior.size());
-        t.first_interior.resize(t.first_interior.size() + size_t(cnt), -1);
-        t.child.resize(t.child.size() + size_t(cnt) * W, kEmptyRef);
-        t.lo.resize(t.lo.size() + size_t(cnt) * 3 * W, FLT_MAX);
-        t.hi.resize(t.hi.size() + size_t(cnt) * 3 * W, -FLT_MAX);
-        return base;
-    };
+    for (int s_ = 0; s_ < shape_count; ++s_) interior_total += shape[s_].nkids ? 1 : 0;
+    t.first_interior.assign(interior_total, -1);
+    t.child.assign(interior_total * W, kEmptyRef);
+    if (p.host_boxes) {  // only a scene with 8-bit nodes reads the boxes on the host
+        t.lo.assign(interior_total * 3 * W, FLT_MAX);
+        t.hi.assign(interior_total * 3 * W, -FLT_MAX);
+    }
+    std::vector<int32_t> shape_of(interior_total);  // the shape each interior node came from
+    int32_t allocated = 0;
     auto leaf = [&](const DShape& sn) {
         t.leaves++;
         t.leaf_last[size_t(sn.off + sn.cnt - 1)] = 1;
     };
     std::vector<std::pair<int, int32_t>> stack;  // (shape id, node index), filled depth-first in order
+    stack.reserve(64 * 8);
     if (shape[0].nkids == 0) {
         t.root = leaf_ref(0);
         leaf(shape[0]);
     } else {
-        t.root = alloc(1);
+        t.root = allocated++;
         stack.push_back({0, t.root});
     }
     while (!stack.empty()) {
         const auto [sid, idx] = stack.back();
         stack.pop_back();
-        const DShape sn = shape[size_t(sid)];
+        const DShape& sn = shape[sid];
+        shape_of[size_t(idx)] = sid;
         int interior = 0;
-        for (int j = 0; j < sn.nkids; ++j) interior += shape[size_t(sn.first_kid + j)].nkids ? 1 : 0;
-        const int32_t base = interior ? alloc(interior) : -1;
+        for (int j = 0; j < sn.nkids; ++j) interior += shape[sn.first_kid + j].nkids ? 1 : 0;
+        const int32_t base = interior ? allocated : -1;
+        allocated += interior;
         t.first_interior[size_t(idx)] = base;
         int k = 0;
         std::pair<int, int32_t> sub[8];
         int nsub = 0;
         for (int j = 0; j < sn.nkids; ++j) {
             const int kid_id = sn.first_kid + j;
-            const DShape& kid = shape[size_t(kid_id)];
+            const DShape& kid = shape[kid_id];
             int32_t ref;
             if (kid.nkids == 0) {
                 ref = leaf_ref(kid.off);
@@ -852,19 +924,50 @@ BuiltTree build_tree_gpu(const float* tri, int64_t ntri, const BuildParams& p, i
                 sub[nsub++] = {kid_id, ref};
             }
             t.child[size_t(idx) * W + j] = ref;
-            for (int a = 0; a < 3; ++a) {
-                t.lo[(size_t(idx) * 3 + a) * W + j] = kid.mn[a];
-                t.hi[(size_t(idx) * 3 + a) * W + j] = kid.mx[a];
-            }
+            if (p.host_boxes)
+                for (int a = 0; a < 3; ++a) {
+                    t.lo[(size_t(idx) * 3 + a) * W + j] = kid.mn[a];
+                    t.hi[(size_t(idx) * 3 + a) * W + j] = kid.mx[a];
+                }
         }
         for (int q = nsub - 1; q >= 0; --q) stack.push_back(sub[q]);  // first child filled next
     }
 
-    // This file's kernels: setup and scene box, 13 per queued round, the triangle
-    // records (the prefix sums are CUB's, four per round, not counted).
+    // The interior nodes in the device layout, written where the shapes are
+    // (FP32 boxes; a scene with 8-bit nodes converts the host arrays instead).
+    // Owned here until the tree is returned.
+    struct Owned {
+        float4* p = nullptr;
+        ~Owned() {
+            if (p) cudaFree(p);
+        }
+    } nodes_owned;
+    if (interior_total > 0) {
+        DevBuf<int32_t> d_map;
+        d_map.alloc(2 * interior_total);
+        check(upload_host(d_map.p, shape_of.data(), interior_total * 4, st), "node map");
+        check(upload_host(d_map.p + interior_total, t.first_interior.data(), interior_total * 4, st), "node map");
+        const int F4 = W == 8 ? NodeShape<8>::kF4 : NodeShape<4>::kF4;
+        check(cudaMalloc(&nodes_owned.p, interior_total * F4 * sizeof(float4)), "cudaMalloc(nodes)");
+        if (W == 8)
+            k_write_nodes<8><<<grid(int64_t(interior_total)), 256, 0, st>>>(
+                int64_t(interior_total), d_shapes.p, d_map.p, d_map.p + interior_total, nodes_owned.p);
+        else
+            k_write_nodes<4><<<grid(int64_t(interior_total)), 256, 0, st>>>(
+                int64_t(interior_total), d_shapes.p, d_map.p, d_map.p + interior_total, nodes_owned.p);
+        check(cudaGetLastError(), "write nodes");
+        check(cudaStreamSynchronize(st), "write nodes");
+    }
+
+    // This file's kernels: setup and scene box, 13 per queued round, the node
+    // writer, the triangle records (the prefix sums are counted apart, four per round).
     t.rounds = int(fin.rounds);
-    t.launches = int(3 + 13 * queued);
-    if (p.nextra > 0) return t;  // mixed primitives: the scene writes its slot records on the host
+    t.launches = int(4 + 13 * queued);
+    if (p.nextra > 0) {  // mixed primitives: the scene writes its slot records on the host
+        t.d_nodes = nodes_owned.p;
+        nodes_owned.p = nullptr;
+        return t;
+    }
     // The triangle records in leaf order, built where the triangles already are.
     uint8_t* d_last = reinterpret_cast<uint8_t*>(d_rid.p);  // n bytes fit in the n-int buffer
     check(cudaMemcpyAsync(d_last, t.leaf_last.data(), size_t(n), cudaMemcpyHostToDevice, st), "leaf flags");
@@ -882,6 +985,8 @@ BuiltTree build_tree_gpu(const float* tri, int64_t ntri, const BuildParams& p, i
         check(e, "triangle records");
     }
     t.d_tris = d_tris;
+    t.d_nodes = nodes_owned.p;
+    nodes_owned.p = nullptr;
     return t;
 }
 

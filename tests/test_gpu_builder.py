@@ -69,3 +69,13 @@ def test_gpu_builder_random_soup_and_tiny_scenes():
         same_tree(*both(tri, width), rays)
         for k in (1, 2, 9, 17):
             same_tree(*both(tri[:k], width), rays[:, :2000])
+
+
+def test_gpu_builder_quantized_nodes_from_host_arrays():
+    """8-bit nodes of a GPU-built tree come from its host arrays, as the host
+    builder's do (the builder's device-written FP32 nodes are not used)."""
+    from sort_b200 import _lib, scenes
+    tri = scenes.sphere_field(64, 3, seed=5)
+    rays = np.concatenate([scenes.camera_rays(128, 128, seed=6), scenes.random_rays(20_000, seed=7)], axis=1)
+    for width in (4, 8):
+        same_tree(*both(tri, width, node_format=_lib.SG_NODES_QUANT8), rays)
