@@ -108,7 +108,7 @@ typedef struct {
  * 1e-6 of each other and a rounded box entry distance decides which one is
  * kept, and rays whose slab test misses the hit triangle's own box by
  * rounding, so that finding it depends on the leaf boxes), FP32 nodes only,
- * max_depth ignored, no topology export. SG_BUILDER_PLOC builds a wide BVH
+ * max_depth ignored. SG_BUILDER_PLOC builds a wide BVH
  * by parallel locally-ordered clustering over the Morton order (Meister and
  * Bittner 2018) on the device: tighter boxes than the LBVH, a few more passes,
  * the same promises and limits. */

@@ -451,6 +451,47 @@ sg_status scene_create_mixed(const MixedInput& in, const sg_build_opts* opts, sg
 
 }  // namespace sg
 
+namespace {
+
+// The child references, leaf order and leaf flags of a tree that has no host
+// arrays (built on the device), read back from its FP32 nodes and slot
+// records (layout.h): enough for tree_topology.
+sg_status device_topology_tree(const sg_scene* s, sg::BuiltTree& h) {
+    const sg::BuiltTree& t = s->tree;
+    if (s->node_format != SG_NODES_FP32) return fail(SG_ERR_UNSUPPORTED, "topology of a device-built 8-bit tree");
+    h.width = t.width;
+    h.root = t.root;
+    h.depth = t.depth;
+    h.first_extra = t.first_extra;
+    h.first_shape = t.first_shape;
+    const int W = t.width;
+    const int f4 = W == 8 ? sg::NodeShape<8>::kF4 : sg::NodeShape<4>::kF4;
+    const int64_t nn = t.interior(), nall = t.triangles() + s->n_lines + s->n_shapes;
+    std::vector<float4> nodes(size_t(std::max<int64_t>(nn, 0)) * f4), tris(size_t(nall) * 3);
+    DeviceGuard g(s->device);
+    if (!g.ok) return fail(SG_ERR_CUDA, "cudaSetDevice failed");
+    cudaError_t e = cudaSuccess;
+    if (nn > 0) e = cudaMemcpy(nodes.data(), s->d_nodes, nodes.size() * sizeof(float4), cudaMemcpyDeviceToHost);
+    if (e == cudaSuccess && nall > 0)
+        e = cudaMemcpy(tris.data(), s->d_tris, tris.size() * sizeof(float4), cudaMemcpyDeviceToHost);
+    if (e != cudaSuccess) return cuda_fail(e, "read the tree back");
+    h.child.resize(size_t(nn) * W);
+    for (int64_t k = 0; k < nn; ++k)  // the child references follow the 6 planes of W boxes
+        std::memcpy(&h.child[size_t(k) * W], reinterpret_cast<const float*>(&nodes[size_t(k) * f4]) + 6 * W,
+                    size_t(W) * sizeof(int32_t));
+    h.order.resize(size_t(nall));
+    h.leaf_last.resize(size_t(nall));
+    for (int64_t i = 0; i < nall; ++i) {
+        int32_t last = 0;
+        std::memcpy(&h.order[size_t(i)], &tris[size_t(i) * 3].w, 4);
+        std::memcpy(&last, &tris[size_t(i) * 3 + 1].w, 4);
+        h.leaf_last[size_t(i)] = last ? 1 : 0;
+    }
+    return SG_OK;
+}
+
+}  // namespace
+
 extern "C" {
 
 sg_status sg_scene_create(const float* triangles, int64_t ntri, const sg_build_opts* opts, sg_scene** out) {
@@ -511,9 +552,15 @@ sg_status sg_scene_info_get(const sg_scene* s, sg_scene_info* info) {
 
 sg_status sg_scene_topology(const sg_scene* s, int32_t* out, int64_t cap, int64_t* written) {
     if (!s || !written) return fail(SG_ERR_INVALID_ARGUMENT, "NULL argument");
-    if (!s->tree.host_arrays()) return fail(SG_ERR_UNSUPPORTED, "an SG_BUILDER_LBVH / SG_BUILDER_PLOC tree has no topology export");
     std::vector<int32_t> v;
-    sg::tree_topology(s->tree, v);
+    if (s->tree.host_arrays()) {
+        sg::tree_topology(s->tree, v);
+    } else {  // built on the device: read the topology back from the device layout
+        sg::BuiltTree h;
+        const sg_status st = device_topology_tree(s, h);
+        if (st != SG_OK) return st;
+        sg::tree_topology(h, v);
+    }
     *written = int64_t(v.size());
     if (int64_t(v.size()) > cap || (!out && !v.empty())) return fail(SG_ERR_LIMIT, "topology buffer too small");
     if (!v.empty()) std::memcpy(out, v.data(), v.size() * sizeof(int32_t));

@@ -655,6 +655,14 @@ __global__ void k_write_nodes(int64_t nodes, const DShape* __restrict__ shapes, 
         for (int x = 28; x < 32; ++x) node[x] = 0.0f;
 }
 
+// The last-in-leaf flag of every leaf shape's last slot (flags zeroed first).
+__global__ void k_leaf_flags(int shapes, const DShape* __restrict__ shape, uint8_t* __restrict__ last) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= shapes) return;
+    const DShape sn = shape[i];
+    if (sn.nkids == 0) last[sn.off + sn.cnt - 1] = 1;
+}
+
 __global__ void k_advance(BuildState* __restrict__ bs) {
     if (bs->na > 0) ++bs->rounds;
     bs->shapes += bs->new_shapes;
@@ -855,8 +863,13 @@ BuiltTree build_tree_gpu(const float* tri, int64_t ntri, const BuildParams& p, i
     // about 100 ms).
     Staging& stage = staging(device);
     std::lock_guard<std::mutex> stage_lock(stage.lock);
+    // Host arrays (child references, leaf order and flags) only where the scene
+    // reads them: 8-bit nodes and mixed primitives. A triangle scene with FP32
+    // nodes takes its nodes and records from the device (its topology export
+    // reads them back from there).
+    const bool host = p.host_boxes || p.nextra > 0;
     const size_t shape_bytes = (size_t(shape_count) * sizeof(DShape) + 255) & ~size_t(255);
-    const size_t stage_bytes = shape_bytes + size_t(n) * 4;
+    const size_t stage_bytes = shape_bytes + (host ? size_t(n) * 4 : 0);
     if (stage.bytes < stage_bytes) {
         if (stage.p) cudaFreeHost(stage.p);
         stage.p = nullptr;
@@ -868,27 +881,36 @@ BuiltTree build_tree_gpu(const float* tri, int64_t ntri, const BuildParams& p, i
     const int32_t* h_order = reinterpret_cast<const int32_t*>(static_cast<const char*>(stage.p) + shape_bytes);
     check(cudaMemcpyAsync(stage.p, d_shapes.p, size_t(shape_count) * sizeof(DShape), cudaMemcpyDeviceToHost, st),
           "shapes");
-    check(cudaMemcpyAsync(const_cast<int32_t*>(h_order), d_idx.p, size_t(n) * 4, cudaMemcpyDeviceToHost, st),
-          "order");
+    if (host)
+        check(cudaMemcpyAsync(const_cast<int32_t*>(h_order), d_idx.p, size_t(n) * 4, cudaMemcpyDeviceToHost, st),
+              "order");
     check(cudaStreamSynchronize(st), "download");
-    t.order.assign(h_order, h_order + n);
-    t.leaf_last.assign(size_t(n), 0);
+    if (host) {
+        t.order.assign(h_order, h_order + n);
+        t.leaf_last.assign(size_t(n), 0);
+    }
     // Flatten exactly as build_tree numbers nodes: a node allocates its interior
     // children consecutively when it is filled, then fills them in order. The
     // arrays are sized once (the interior count is known), then filled.
     size_t interior_total = 0;
     for (int s_ = 0; s_ < shape_count; ++s_) interior_total += shape[s_].nkids ? 1 : 0;
-    t.first_interior.assign(interior_total, -1);
-    t.child.assign(interior_total * W, kEmptyRef);
+    if (host) {
+        t.first_interior.assign(interior_total, -1);
+        t.child.assign(interior_total * W, kEmptyRef);
+    } else {
+        t.n_interior = int64_t(interior_total);
+        t.n_tri = n;
+    }
     if (p.host_boxes) {  // only a scene with 8-bit nodes reads the boxes on the host
         t.lo.assign(interior_total * 3 * W, FLT_MAX);
         t.hi.assign(interior_total * 3 * W, -FLT_MAX);
     }
     std::vector<int32_t> shape_of(interior_total);  // the shape each interior node came from
+    std::vector<int32_t> base_of(interior_total);   // and its first interior child
     int32_t allocated = 0;
     auto leaf = [&](const DShape& sn) {
         t.leaves++;
-        t.leaf_last[size_t(sn.off + sn.cnt - 1)] = 1;
+        if (host) t.leaf_last[size_t(sn.off + sn.cnt - 1)] = 1;
     };
     std::vector<std::pair<int, int32_t>> stack;  // (shape id, node index), filled depth-first in order
     stack.reserve(64 * 8);
@@ -908,7 +930,8 @@ BuiltTree build_tree_gpu(const float* tri, int64_t ntri, const BuildParams& p, i
         for (int j = 0; j < sn.nkids; ++j) interior += shape[sn.first_kid + j].nkids ? 1 : 0;
         const int32_t base = interior ? allocated : -1;
         allocated += interior;
-        t.first_interior[size_t(idx)] = base;
+        base_of[size_t(idx)] = base;
+        if (host) t.first_interior[size_t(idx)] = base;
         int k = 0;
         std::pair<int, int32_t> sub[8];
         int nsub = 0;
@@ -923,7 +946,7 @@ BuiltTree build_tree_gpu(const float* tri, int64_t ntri, const BuildParams& p, i
                 ref = base + k++;
                 sub[nsub++] = {kid_id, ref};
             }
-            t.child[size_t(idx) * W + j] = ref;
+            if (host) t.child[size_t(idx) * W + j] = ref;
             if (p.host_boxes)
                 for (int a = 0; a < 3; ++a) {
                     t.lo[(size_t(idx) * 3 + a) * W + j] = kid.mn[a];
@@ -946,7 +969,7 @@ BuiltTree build_tree_gpu(const float* tri, int64_t ntri, const BuildParams& p, i
         DevBuf<int32_t> d_map;
         d_map.alloc(2 * interior_total);
         check(upload_host(d_map.p, shape_of.data(), interior_total * 4, st), "node map");
-        check(upload_host(d_map.p + interior_total, t.first_interior.data(), interior_total * 4, st), "node map");
+        check(upload_host(d_map.p + interior_total, base_of.data(), interior_total * 4, st), "node map");
         const int F4 = W == 8 ? NodeShape<8>::kF4 : NodeShape<4>::kF4;
         check(cudaMalloc(&nodes_owned.p, interior_total * F4 * sizeof(float4)), "cudaMalloc(nodes)");
         if (W == 8)
@@ -962,7 +985,7 @@ BuiltTree build_tree_gpu(const float* tri, int64_t ntri, const BuildParams& p, i
     // This file's kernels: setup and scene box, 13 per queued round, the node
     // writer, the triangle records (the prefix sums are counted apart, four per round).
     t.rounds = int(fin.rounds);
-    t.launches = int(4 + 13 * queued);
+    t.launches = int(4 + 13 * queued + (host ? 0 : 1));
     if (p.nextra > 0) {  // mixed primitives: the scene writes its slot records on the host
         t.d_nodes = nodes_owned.p;
         nodes_owned.p = nullptr;
@@ -970,7 +993,13 @@ BuiltTree build_tree_gpu(const float* tri, int64_t ntri, const BuildParams& p, i
     }
     // The triangle records in leaf order, built where the triangles already are.
     uint8_t* d_last = reinterpret_cast<uint8_t*>(d_rid.p);  // n bytes fit in the n-int buffer
-    check(cudaMemcpyAsync(d_last, t.leaf_last.data(), size_t(n), cudaMemcpyHostToDevice, st), "leaf flags");
+    if (host) {
+        check(cudaMemcpyAsync(d_last, t.leaf_last.data(), size_t(n), cudaMemcpyHostToDevice, st), "leaf flags");
+    } else {
+        check(cudaMemsetAsync(d_last, 0, size_t(n), st), "leaf flags");
+        k_leaf_flags<<<grid(shape_count), 256, 0, st>>>(shape_count, d_shapes.p, d_last);
+        check(cudaGetLastError(), "leaf flags");
+    }
     const size_t tris_bytes = size_t(n + kPadSlots) * 3 * sizeof(float4);
     float4* d_tris = nullptr;
     check(cudaMalloc(&d_tris, tris_bytes), "cudaMalloc(triangles)");

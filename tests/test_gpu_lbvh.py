@@ -127,15 +127,41 @@ def test_lbvh_random_soup_and_tiny_scenes(builder):
             _same_hits(tri[:k], ref, lb, rays[:, :2000])
 
 
+def _leaf_prims(topo, width, max_leaf=8):
+    """Primitive ids in leaf order from a pre-order topology (interior: child
+    count then the children; leaf: 0, its count, its ids); checks the child
+    counts and leaf sizes on the way."""
+    out, pos = [], 0
+
+    def walk():
+        nonlocal pos
+        c = int(topo[pos])
+        pos += 1
+        if c == 0:
+            n = int(topo[pos])
+            assert 0 < n <= max_leaf
+            out.extend(int(x) for x in topo[pos + 1:pos + 1 + n])
+            pos += 1 + n
+            return 1
+        assert 0 < c <= width
+        return 1 + sum(walk() for _ in range(c))
+    walk()
+    assert pos == len(topo)
+    return out
+
+
 @pytest.mark.parametrize("builder", BUILDERS)
 def test_lbvh_limits_are_reported(builder):
+    """The topology export reads a device-built tree back from the device:
+    every primitive in exactly one leaf, leaves of at most max_leaf, at most
+    W children per node. 8-bit nodes are refused, an empty scene is invalid."""
     from sort_b200 import Obvh, _lib, scenes
     tri = scenes.sphere_field(8, 2, seed=9)
     acc = Obvh(builder=_code(builder))
     acc.Build(tri)
-    with pytest.raises(_lib.SortGpuError) as ex:
-        acc.topology()
-    assert ex.value.status == 4  # SG_ERR_UNSUPPORTED
+    topo = acc.topology()
+    prims = _leaf_prims(topo, 8)
+    assert sorted(prims) == list(range(tri.shape[0]))
     q8 = Obvh(builder=_code(builder), node_format=_lib.SG_NODES_QUANT8)
     with pytest.raises(_lib.SortGpuError) as ex:
         q8.Build(tri)
