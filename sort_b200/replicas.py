@@ -6,9 +6,10 @@ another GPU's memory and nothing on the data path needs a collective. This
 module holds the host-side pieces: contiguous shares of a ray batch, tiles of
 an image dealt round-robin, one frame rendered in bands of rows across the
 ranks and gathered (bit-identical to a one-GPU render), a router that sends
-each render request to the replica with the least outstanding work, and the
-max-over-ranks reduction the timings use (torch.distributed, NCCL on GPUs,
-gloo on CPU).
+each render request to the replica with the least outstanding work and a
+server front that routes one request stream over one render server per GPU
+with it, and the max-over-ranks reduction the timings use (torch.distributed,
+NCCL on GPUs, gloo on CPU).
 
 SORT's counterpart is its thread pool splitting one image into 64x64 tiles
 (work/image_evaluation/image_evaluation.cpp:153-279); here the split is across
@@ -115,3 +116,57 @@ def max_over_ranks(value: float, device=None) -> float:
     t = torch.tensor([float(value)], dtype=torch.float64, device=device)
     dist.all_reduce(t, op=dist.ReduceOp.MAX)
     return float(t.item())
+
+
+class ReplicatedServer:
+    """Render servers on several GPUs of one node behind one request stream:
+    each GPU runs its own sg_server (its own host loop, path pool and solo
+    lanes) over its own replica of every scene, and each request goes to the
+    replica with the least outstanding samples (ReplicaRouter). Tickets are
+    the server's own; wait and cancel go to the replica that took the request.
+
+    servers: one RenderServer-like object per GPU (add_scene, submit, wait,
+    cancel, stats, close), already holding the same scenes in the same order.
+    """
+
+    def __init__(self, servers):
+        if not servers:
+            raise ValueError("at least one server")
+        self.servers = list(servers)
+        self.router = ReplicaRouter(len(self.servers))
+        self._where = {}  # ticket -> (replica, the replica's ticket)
+        self._next = 1
+
+    def submit(self, scene: int, camera, width: int, height: int, spp: int, max_depth: int = 5, seed: int = 1,
+               image=None) -> int:
+        ticket = self._next
+        self._next += 1
+        r = self.router.route(ticket, int(width) * int(height) * int(spp))
+        try:
+            inner = self.servers[r].submit(scene, camera, width, height, spp, max_depth, seed=seed, image=image)
+        except Exception:
+            self.router.done(ticket)
+            raise
+        self._where[ticket] = (r, inner)
+        return ticket
+
+    def wait(self, ticket: int, timeout: float | None = None):
+        r, inner = self._where[ticket]
+        img, res = self.servers[r].wait(inner, timeout)
+        del self._where[ticket]
+        self.router.done(ticket)
+        return img, dict(res, ticket=ticket, replica=r)
+
+    def cancel(self, ticket: int) -> None:
+        r, inner = self._where[ticket]
+        self.servers[r].cancel(inner)
+
+    def stats(self) -> dict:
+        per = [s.stats() for s in self.servers]
+        total = {k: sum(p[k] for p in per) for k in per[0]}
+        total["replicas"] = per
+        return total
+
+    def close(self) -> None:
+        for s in self.servers:
+            s.close()

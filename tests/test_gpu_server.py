@@ -163,3 +163,20 @@ def test_quantized_nodes_server(tracers):
     assert res["status"] == 0
     assert np.array_equal(img.view(np.uint32), reference([pt], req).view(np.uint32))
     srv.close()
+
+
+def test_replicated_server_front(tracers):
+    """ReplicatedServer over one server per GPU (the scenes here live on GPU 0,
+    so one replica): the same images as sg_pt_render, tickets and results of
+    its own."""
+    from sort_b200.replicas import ReplicatedServer
+    front = ReplicatedServer([server(tracers, device=0, path_slots=4096, pixel_budget=40_000, max_requests=8)])
+    reqs = requests()[:5]
+    refs = [reference(tracers, r) for r in reqs]
+    tickets = [front.submit(*r[:2], *r[2:6], seed=r[6]) for r in reqs]
+    for t, ref in zip(tickets, refs):
+        img, res = front.wait(t)
+        assert res["status"] == 0 and res["ticket"] == t and res["replica"] == 0
+        assert np.array_equal(img.view(np.uint32), ref.view(np.uint32))
+    assert front.stats()["requests_done"] == len(reqs)
+    front.close()

@@ -114,3 +114,51 @@ def test_two_gloo_ranks():
 
 def test_one_rank_renders_the_whole_frame():
     assert torch.equal(render_sharded(_RowImage(), None, 9, 4, 1, seed=2), _frame(9, 4, 2))
+
+
+class _FakeServer:
+    """Stands in for RenderServer: remembers what it was given."""
+
+    def __init__(self):
+        self.submitted, self.cancelled, self.closed, self.next = [], [], False, 100
+
+    def submit(self, scene, camera, width, height, spp, max_depth=5, seed=1, image=None):
+        self.next += 1
+        self.submitted.append((self.next, scene, width, height, spp, seed))
+        return self.next
+
+    def wait(self, ticket, timeout=None):
+        return "image-%d" % ticket, {"ticket": ticket, "status": 0}
+
+    def cancel(self, ticket):
+        self.cancelled.append(ticket)
+
+    def stats(self):
+        return {"requests_done": len(self.submitted), "samples_done": 7}
+
+    def close(self):
+        self.closed = True
+
+
+def test_replicated_server_routes_by_outstanding_samples():
+    from sort_b200.replicas import ReplicatedServer
+    a, b = _FakeServer(), _FakeServer()
+    srv = ReplicatedServer([a, b])
+    t1 = srv.submit(0, None, 100, 100, 16)  # 160k samples -> a
+    t2 = srv.submit(1, None, 10, 10, 4)     # -> b
+    t3 = srv.submit(0, None, 20, 20, 4, seed=9)  # b still has less -> b
+    assert [x[1:] for x in a.submitted] == [(0, 100, 100, 16, 1)]
+    assert [x[1:] for x in b.submitted] == [(1, 10, 10, 4, 1), (0, 20, 20, 4, 9)]
+    img, res = srv.wait(t1)  # a's load released: the next request goes to a
+    assert img == "image-101" and res["ticket"] == t1 and res["replica"] == 0
+    t4 = srv.submit(2, None, 8, 8, 1)
+    assert a.submitted[-1][1:4] == (2, 8, 8)
+    srv.cancel(t3)
+    assert b.cancelled == [b.submitted[1][0]]
+    st = srv.stats()
+    assert st["requests_done"] == 4 and st["samples_done"] == 14 and len(st["replicas"]) == 2
+    for t in (t2, t3, t4):
+        srv.wait(t)
+    assert srv.router.load == [0, 0]
+    srv.close()
+    assert a.closed and b.closed
