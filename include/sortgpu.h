@@ -526,9 +526,9 @@ sg_status sg_pt_ray_counts(const sg_pt_scene* pt, int64_t* extension, int64_t* s
  *   samples take one of the server's solo lanes, in queue order: rendered as
  *   sg_pt_render renders, one wave per sample (two in flight) on the lane's
  *   own buffers, beside the pool, the oldest lane's waves at the highest
- *   stream priority; the last sample joins the pool like an admission that
- *   starts there (the image is the same either way). The pool renders the
- *   other requests. 0 = 1 (every multi-sample request), < 0 = never.
+ *   stream priority; the lane scales and completes the request (the image
+ *   is the same either way). The pool renders the other requests.
+ *   0 = 1 (every multi-sample request), < 0 = never.
  * sg_server_add_scene: all scenes of a server share one tree width and node
  *   format (SG_ERR_UNSUPPORTED otherwise); the sg_pt_scene and its sg_scene
  *   must outlive the server.

@@ -331,6 +331,13 @@ extern "C" sg_status sg_pt_destroy(sg_pt_scene* ps) {
 
 namespace sg {
 
+cudaError_t pt_scale(float* image, int64_t n, float s, cudaStream_t st) {
+    if (n <= 0) return cudaSuccess;
+    if (n > int64_t(1) << 30) return cudaErrorInvalidValue;
+    k_scale<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(image, (int)n, s);
+    return cudaGetLastError();
+}
+
 cudaError_t pt_wave(const PtDev& dev, const TraceLaunch& base_in, const DevTree& tree, const Cam& cam, int width,
                     int height, int p0, int n, uint2 key, int sample, int max_depth, const PtWave& w, float* image,
                     cudaStream_t s) {

@@ -54,6 +54,9 @@ struct PtWave {
 // zeroed or scaled. Every pixel draws the random numbers of its place in the
 // frame, so waves over bands and over whole frames give the same sums.
 // `base` is the scene's launch (scene_launch), `tree` its tree.
+// image[i] *= s for i < n (the 1/spp of a finished render), on stream st.
+cudaError_t pt_scale(float* image, int64_t n, float s, cudaStream_t st);
+
 cudaError_t pt_wave(const PtDev& dev, const TraceLaunch& base, const DevTree& tree, const Cam& cam, int width,
                     int height, int p0, int n, uint2 key, int sample, int max_depth, const PtWave& w, float* image,
                     cudaStream_t s);

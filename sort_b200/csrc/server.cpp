@@ -131,7 +131,8 @@ struct sg_server {
         int64_t id = -1;  // ticket in its solo phase
         int next = 0;     // next sample to queue a wave for
         int done = 0;     // waves finished
-        int last = 0;     // waves the phase may run (spp - 1)
+        int last = 0;     // waves to run (spp)
+        bool finishing = false;  // every wave queued (and the scale), or cancelled: waiting for `end`
         sg::PtWave w[2] = {};
         // The waves and their shadow rays (pt_wave.h), [priority][sample % 2]:
         // the lane holding the oldest request queues its waves on the
@@ -142,15 +143,9 @@ struct sg_server {
         cudaEvent_t flushed[2] = {};   // image additions, chained in sample order
         cudaEvent_t wave_done[2] = {};
         cudaEvent_t ready = nullptr;   // the ticket's image is zeroed
-        cudaEvent_t end = nullptr;     // its last wave is done
+        cudaEvent_t end = nullptr;     // its last wave (and the scale) is done
     };
     std::vector<Lane> lanes;
-    struct Handoff {
-        int64_t id;
-        int sample0;  // its first sample for the pool
-        int lane;     // whose `end` the pool waits for
-    };
-    std::vector<Handoff> handoffs;  // solo phases that ended, to admit next
     char* d_solo = nullptr;
     // The bounce steps' side stream (continuation rays beside shadow rays,
     // serve_kernels.h) and its events; captured into the graph.
@@ -312,11 +307,6 @@ bool solo_kind(const sg_server* S, const Ticket& t) {
 void admit(sg_server* S, sg::SrvControl& ctl, int64_t replay) {
     ctl.nadmit = 0;
     ctl.admit_total = 0;
-    for (const sg_server::Handoff& h : S->handoffs) {  // after each one's last solo wave
-        cudaStreamWaitEvent(S->stream, S->lanes[size_t(h.lane)].end, 0);
-        enter_pool(S, ctl, h.id, h.sample0, replay);
-    }
-    S->handoffs.clear();
     for (auto it = S->pending.begin(); it != S->pending.end() && ctl.nadmit < sg::kSrvMaxAdmit;) {
         const int64_t id = *it;
         if (solo_kind(S, S->tickets[id])) {
@@ -356,7 +346,8 @@ void start_solo(sg_server* S) {
             for (cudaStream_t t : pair) cudaStreamWaitEvent(t, L.ready, 0);
         L.id = id;
         L.next = L.done = 0;
-        L.last = t.req.spp - 1;
+        L.last = t.req.spp;
+        L.finishing = false;
     }
 }
 
@@ -366,13 +357,62 @@ bool lanes_busy(const sg_server* S) {
     return false;
 }
 
-// Keeps two waves of a lane's request queued; when its waves up to the last
-// sample are queued (or it is cancelled, or the server stops) hands it to the
-// pool from the next sample on.
+// Completes a lane's request once its last wave (and the scale) is done:
+// copies the image out (unless cancelled), frees its table slot and image
+// range, wakes its waiters, frees the lane.
+sg_status finish_lane(sg_server* S, sg_server::Lane& L) {
+    cudaError_t e = cudaSuccess;
+    int64_t id;
+    bool cancelled;
+    void* dst;
+    const float* src;
+    size_t bytes;
+    {
+        std::lock_guard<std::mutex> lk(S->mu);
+        id = L.id;
+        Ticket& t = S->tickets[id];
+        cancelled = t.cancel;
+        dst = t.req.image;
+        src = S->d_images + 3 * t.arena;
+        bytes = size_t(t.req.width) * t.req.height * 3 * sizeof(float);
+    }
+    if (!cancelled) {
+        if ((e = cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDeviceToHost, S->copy_stream)) != cudaSuccess ||
+            (e = cudaStreamSynchronize(S->copy_stream)) != cudaSuccess)
+            return fail(SG_ERR_CUDA, std::string("copy image: ") + cudaGetErrorString(e));
+    }
+    std::lock_guard<std::mutex> lk(S->mu);
+    Ticket& t = S->tickets[id];
+    const int64_t P = int64_t(t.req.width) * t.req.height;
+    S->arena.release(t.arena, P);
+    S->slot_ticket[size_t(t.slot)] = -1;
+    S->free_slots.push_back(t.slot);
+    t.slot = -1;
+    S->stats.requests_done++;
+    if (!cancelled) S->stats.samples_done += P * t.req.spp;
+    complete(S, t, cancelled ? SG_ERR_CANCELLED : SG_OK);
+    L.id = -1;
+    L.finishing = false;
+    S->cv_work.notify_all();
+    return SG_OK;
+}
+
+// Keeps two waves of a lane's request queued; after the last one (or a
+// cancellation, or the server's stop) scales the image and, once that is
+// done, completes the request.
 sg_status pump_lane(sg_server* S, int l) {
     sg_server::Lane& L = S->lanes[size_t(l)];
     if (L.id < 0) return SG_OK;
     cudaError_t e = cudaSuccess;
+    if (L.finishing) {
+        e = cudaEventQuery(L.end);
+        if (e == cudaErrorNotReady) {
+            cudaGetLastError();  // not an error (see below)
+            return SG_OK;
+        }
+        if (e != cudaSuccess) return fail(SG_ERR_CUDA, std::string("solo wave: ") + cudaGetErrorString(e));
+        return finish_lane(S, L);
+    }
     while (L.done < L.next) {  // retire finished waves
         e = cudaEventQuery(L.wave_done[L.done % 2]);
         if (e == cudaErrorNotReady) {
@@ -427,21 +467,29 @@ sg_status pump_lane(sg_server* S, int l) {
         S->stats.solo_waves++;
     }
     if (end || L.next == L.last) {
-        // after the last wave, whose additions came after every earlier one's
+        // After the last wave, whose additions came after every earlier one's:
+        // the 1/spp scale (as sg_pt_render's), then `end`.
         const cudaStream_t last = L.next > 0 ? L.last_on : L.stream[1][0];
+        if (!end && (e = sg::pt_scale(q.image, 3 * int64_t(q.width) * q.height, q.inv_spp, last)) != cudaSuccess)
+            return fail(SG_ERR_CUDA, std::string("solo scale: ") + cudaGetErrorString(e));
         if ((e = cudaEventRecord(L.end, last)) != cudaSuccess)
-            return fail(SG_ERR_CUDA, std::string("solo handoff: ") + cudaGetErrorString(e));
-        std::lock_guard<std::mutex> lk(S->mu);
-        S->handoffs.push_back({L.id, L.next, l});
-        L.id = -1;
+            return fail(SG_ERR_CUDA, std::string("solo end: ") + cudaGetErrorString(e));
+        L.finishing = true;
     }
     return SG_OK;
 }
 
-// Blocks until the oldest queued wave of a busy lane has finished.
+// Blocks until the oldest queued wave of a busy lane has finished, or a
+// finishing lane's end.
 sg_status wait_solo(sg_server* S) {
     for (sg_server::Lane& L : S->lanes) {
-        if (L.id < 0 || L.done >= L.next) continue;
+        if (L.id < 0) continue;
+        if (L.finishing) {
+            const cudaError_t e = cudaEventSynchronize(L.end);
+            if (e != cudaSuccess) return fail(SG_ERR_CUDA, std::string("solo wave: ") + cudaGetErrorString(e));
+            return SG_OK;
+        }
+        if (L.done >= L.next) continue;
         const cudaError_t e = cudaEventSynchronize(L.wave_done[L.done % 2]);
         if (e != cudaSuccess) return fail(SG_ERR_CUDA, std::string("solo wave: ") + cudaGetErrorString(e));
         L.done++;
@@ -513,10 +561,10 @@ void serve_loop(sg_server* S) {
             std::unique_lock<std::mutex> lk(S->mu);
             if (!inflight && !lanes_busy(S))
                 S->cv_work.wait(lk, [&] {
-                    return S->stop || !S->pending.empty() || S->admitted > 0 || !S->handoffs.empty();
+                    return S->stop || !S->pending.empty() || S->admitted > 0;
                 });
             if (S->stop) break;
-            admit(S, *S->h_control[j % 2], j);  // hand-offs first: a lane may be reused next
+            admit(S, *S->h_control[j % 2], j);
             start_solo(S);
             launch = S->admitted > 0;
         }

@@ -83,10 +83,10 @@ def test_each_request_matches_single_render_alone_and_mixed(tracers, per_claim):
 
 
 def test_solo_phase_and_handoff_give_the_same_image(tracers):
-    """Large requests render their samples as whole-frame waves in the solo
-    lanes and leave the last one to the pool, while smaller requests arriving
+    """Large requests render every sample as whole-frame waves in the solo
+    lanes, which scale and complete them, while smaller requests arriving
     meanwhile go to the pool. Images equal sg_pt_render's in every case, and
-    with the solo phase turned off."""
+    with the lanes turned off."""
     import time
 
     from sort_b200 import scenes
@@ -97,11 +97,11 @@ def test_solo_phase_and_handoff_give_the_same_image(tracers):
     for solo in (1000, -1):
         srv = server(tracers, path_slots=50_000, pixel_budget=400_000, max_requests=8, samples_per_claim=8,
                      solo_pixels=solo)
-        img, res = srv.wait(srv.submit(*big[:2], *big[2:6], seed=big[6]))  # alone: 47 waves, then the pool
+        img, res = srv.wait(srv.submit(*big[:2], *big[2:6], seed=big[6]))  # alone: 48 waves in a lane
         assert res["status"] == 0, loop_error(srv)
         assert np.array_equal(img.view(np.uint32), refs[0].view(np.uint32))
         waves = srv.stats()["solo_waves"]
-        assert waves == (big[4] - 1 if solo > 0 else 0)
+        assert waves == (big[4] if solo > 0 else 0)
         t_big = srv.submit(*big[:2], *big[2:6], seed=big[6])
         time.sleep(0.02)  # arrivals during the big request's waves
         tickets = [srv.submit(*r[:2], *r[2:6], seed=r[6]) for r in small]
@@ -109,7 +109,7 @@ def test_solo_phase_and_handoff_give_the_same_image(tracers):
             img, res = srv.wait(t)
             assert res["status"] == 0 and np.array_equal(img.view(np.uint32), ref.view(np.uint32))
         lanes_take = [r for r in [big] + small if solo > 0 and r[2] * r[3] >= solo and r[4] >= 2]
-        assert 0 <= srv.stats()["solo_waves"] - waves <= sum(r[4] - 1 for r in lanes_take)
+        assert srv.stats()["solo_waves"] - waves == sum(r[4] for r in lanes_take)
         srv.close()
 
 
