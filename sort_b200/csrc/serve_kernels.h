@@ -2,8 +2,7 @@
 // bounce steps (serve.cu).
 //
 // Work is a ring of pixel samples: entry = (request, pixel, sample). Admission
-// appends the first sample to render (0, or the sample after the waves a
-// request rendered alone) of every pixel of a request; free path slots claim entries
+// appends the admission's first sample to render of every pixel of a request; free path slots claim entries
 // from the ring's head. A path that ends adds its radiance to its pixel; its
 // slot then renders the pixel's next sample itself, up to samples_per_claim
 // samples per claim, and after that appends the pixel's next sample at the
@@ -46,7 +45,7 @@ struct SrvAdmit {
     int32_t request;  // request-table index
     int32_t pixels;
     int64_t first;    // offset among this replay's admitted pixels
-    int32_t sample0;  // first sample to render (earlier ones are in the image already)
+    int32_t sample0;  // first sample to render (earlier ones are in the image already; 0 today)
     int32_t pad;
 };
 

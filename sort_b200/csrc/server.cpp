@@ -1,22 +1,24 @@
 // sg_server (include/sortgpu.h): the host side of the render server.
 //
-// One loop thread per server owns the GPU work: it admits queued requests
-// (FIFO) while a request-table slot and a contiguous image range of the pixel
-// budget are free, stages the admissions, replays the captured bounce-step
-// graph, and reads the per-request completion flags of the previous replay
-// while the next one runs (two replays in flight). A completed request's
-// image is copied to its host buffer on a second stream, then its slot and
-// image range are released and its waiters are woken.
+// One loop thread per server owns the GPU work: it admits the queued
+// requests the solo lanes do not take (in queue order) while a request-table
+// slot and a contiguous image range of the pixel budget are free, stages the
+// admissions, replays the captured bounce-step graph, and reads the
+// per-request completion flags of the previous replay while the next one
+// runs (two replays in flight). A completed request's image is copied to its
+// host buffer on a second stream, then its slot and image range are released
+// and its waiters are woken.
 //
-// Solo phase: a large request at the head of the queue (one at a time) is
-// rendered the way sg_pt_render renders a frame, one wave per sample
-// (pt_wave, on its own buffers), with two waves queued ahead on a second
-// stream, so that the pool keeps serving the other requests meanwhile. When all but its last sample are queued (or it is
-// cancelled) its remaining samples enter the pool like an admission that
-// starts at that sample. A large request in the pool finishes with its
-// slowest pixel (each pixel's samples run one after another in one slot); the
-// waves have no such tail. Each pixel's samples are still added in sample
-// order, so the image does not depend on where the switch happens.
+// Solo lanes: a multi-sample request of at least solo_pixels pixels waits for
+// one of the lanes (oldest first) and is rendered the way sg_pt_render
+// renders a frame, one wave per sample (pt_wave, on the lane's own buffers),
+// two samples in flight on the lane's streams, while the pool serves the
+// other requests; the lane holding the oldest request uses the high-priority
+// streams. After its last wave the lane scales the image and the request
+// completes like a pool request. In the pool a pixel's samples run one after
+// another in one slot, so a request there finishes with its slowest pixel's
+// chain; the waves have no such tail. Each pixel's samples are added in sample
+// order either way, so the image is sg_pt_render's.
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -338,8 +340,8 @@ void start_solo(sg_server* S) {
         if (!reserve(S, id)) return;
         S->pending.erase(it);
         Ticket& t = S->tickets[id];
-        // Not in any replay until the hand-off: a completion flag read back for
-        // its table slot before then belongs to the slot's previous request.
+        // Never in a replay: a completion flag read back for its table slot
+        // belongs to the slot's previous request.
         t.replay = INT64_MAX;
         cudaEventRecord(L.ready, S->stream);
         for (auto& pair : L.stream)
