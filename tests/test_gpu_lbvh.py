@@ -6,9 +6,13 @@ same triangles: every ray's closest distance equals the one through SORT's
 tree (the host builder's) bit for bit, the primitive is the same unless two
 triangles are hit at exactly that distance, and the any-hit answer is the
 same. Two exceptions come from the box arithmetic, not from a fault of either
-tree. Near-ties: when two triangles are hit within 1e-6 (relative) of each
-other, a box entry distance that rounds above the first hit found culls the
-other, so each tree may keep a different one. And a ray that
+tree. Near-ties: when two triangles are hit within rounding of each other, a
+box entry distance that rounds above the first hit found culls the other, so
+each tree may keep a different one. Rounding here is 1e-6 of the distance, or
+a few float32 ulps of the vertices' offsets from the ray origin (the
+watertight test works on those offsets, so its distance carries their
+rounding; it dominates when the origin lies close to large triangles). And a
+ray that
 SORT's slab test (with its 1e-5 clamp of direction components,
 simd/simd_ray_utils.h:61-64, and simd/simd_bbox.h:47-109) sends past a
 triangle's own box by rounding reaches that triangle only through a larger
@@ -61,6 +65,16 @@ def _own_box_missed(tri, prim, rays, i):
     return not tmin <= tmax
 
 
+def _t_slack(tri, prim, rays, i):
+    """Rounding of the watertight distance from ray i to triangle prim: 8 float32
+    ulps of the largest vertex offset from the origin, in units of the ray's
+    largest direction component."""
+    v = np.asarray(tri[prim], np.float64).reshape(3, 3)
+    o = rays[0:3, i].astype(np.float64)
+    d = rays[3:6, i].astype(np.float64)
+    return 8.0 * 2.0 ** -24 * float(np.abs(v - o).max()) / float(np.abs(d).max())
+
+
 def _same_hits(tri, ref, lb, rays, check_ties=True):
     from oracle.oracle import Port
     r = np.ascontiguousarray(rays)
@@ -70,7 +84,8 @@ def _same_hits(tri, ref, lb, rays, check_ties=True):
     ta, tb = ha.t.cpu().numpy(), hb.t.cpu().numpy()
     moved = np.nonzero(ta.view(np.int32) != tb.view(np.int32))[0]
     for i in moved:  # a near-tie, or the nearer hit's own box is missed by the slab test
-        near_tie = pa[i] >= 0 and pb[i] >= 0 and abs(float(ta[i]) - float(tb[i])) <= 1e-6 * float(min(ta[i], tb[i]))
+        near_tie = pa[i] >= 0 and pb[i] >= 0 and abs(float(ta[i]) - float(tb[i])) <= max(
+            1e-6 * float(min(ta[i], tb[i])), _t_slack(tri, int(pa[i]), r, int(i)) + _t_slack(tri, int(pb[i]), r, int(i)))
         p = pa[i] if ta[i] < tb[i] else pb[i]
         assert near_tie or (p >= 0 and _own_box_missed(tri, int(p), r, int(i))), \
             f"ray {i}: {pa[i]}@{ta[i]} vs {pb[i]}@{tb[i]}"
