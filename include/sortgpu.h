@@ -105,7 +105,8 @@ typedef struct {
  * topology, leaf order, boxes). SG_BUILDER_LBVH builds a wide BVH in Morton
  * order entirely on the device, for fast scene admission: not SORT's tree (the
  * same hits and distances except near-ties, where two triangles are hit within
- * 1e-6 of each other and a rounded box entry distance decides which one is
+ * rounding of each other (1e-6 of the distance, more when the ray starts close
+ * to large triangles) and a rounded box entry distance decides which one is
  * kept, and rays whose slab test misses the hit triangle's own box by
  * rounding, so that finding it depends on the leaf boxes), FP32 nodes only,
  * max_depth ignored. SG_BUILDER_PLOC builds a wide BVH

@@ -3,8 +3,9 @@
 // The fast builder for scenes that must be admitted quickly. Its tree is not
 // SORT's (build_tree / build_tree_gpu build that one): hits and distances equal
 // SORT's, because the box and triangle tests are the same, except near-ties
-// (two triangles hit within 1e-6 of each other: a rounded box entry distance
-// decides which one a traversal keeps), and where SORT's slab test
+// (two triangles hit within rounding of each other, 1e-6 of the distance or
+// more when the ray starts close to large triangles: a rounded box entry
+// distance decides which one a traversal keeps), and where SORT's slab test
 // (with its 1e-5 clamp of direction components) misses a hit triangle's own box
 // by rounding: such a triangle is found only through a larger leaf box, which
 // depends on the tree.
